@@ -1,0 +1,125 @@
+"""ctypes bindings to libbcmg.so (the product's C ABI, include/bcmg.h).
+
+The library is loaded from this package's lib/ folder.  There is no Python or
+CPU fallback: if the shared object is missing the import fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(_HERE, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libbcmg.so")
+
+i32 = C.c_int32
+i32p = C.POINTER(C.c_int32)
+f64p = C.POINTER(C.c_double)
+vp = C.c_void_p
+
+
+class Csr(C.Structure):
+    """bcmg_csr (include/bcmg.h)."""
+
+    _fields_ = [("n", i32), ("m", i32), ("nnz", i32), ("row", i32p), ("col", i32p),
+                ("val", f64p)]
+
+
+class Params(C.Structure):
+    """bcmg_params: same field order as the reference's struct params
+    (src/AMG/AMG.cu:20-37)."""
+
+    _fields_ = [("solver_type", C.c_int), ("max_hrc", C.c_int), ("conv_ratio", C.c_double),
+                ("matchtype", C.c_int), ("aggrsweeps", C.c_int), ("aggrtype", C.c_int),
+                ("max_levels", C.c_int), ("cycle_type", C.c_int), ("coarse_solver", C.c_int),
+                ("relax_type", C.c_int), ("prerelax_sweeps", C.c_int),
+                ("postrelax_sweeps", C.c_int), ("itnlim", C.c_int), ("rtol", C.c_double),
+                ("relaxnumber_coarse", C.c_int)]
+
+
+class Ext(C.Structure):
+    """bcmg_ext: extensions beyond the reference's settings."""
+
+    _fields_ = [("precision", C.c_int), ("coarse_storage", C.c_int),
+                ("replace_every", C.c_int), ("use_graphs", C.c_int), ("device", C.c_int),
+                ("verbose", C.c_int), ("max_device_seconds", C.c_double)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iters", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
+                ("rel_residual", C.c_double), ("true_rel_residual", C.c_double),
+                ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("num_hrc", C.c_int),
+                ("estimated_ratio", C.c_double)]
+
+
+# name -> (restype, argtypes); every symbol include/bcmg.h declares.
+SIGNATURES = {
+    "bcmg_last_error": (C.c_char_p, []),
+    "bcmg_status_string": (C.c_char_p, [C.c_int]),
+    "bcmg_version": (C.c_char_p, []),
+    "bcmg_read_matrix": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(Csr)]),
+    "bcmg_write_matrix_mm": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
+    "bcmg_csr_free": (None, [C.POINTER(Csr)]),
+    "bcmg_csr_check": (C.c_int, [C.POINTER(Csr)]),
+    "bcmg_params_default": (None, [C.POINTER(Params)]),
+    "bcmg_params_from_file": (C.c_int, [C.c_char_p, C.POINTER(Params)]),
+    "bcmg_params_check": (C.c_int, [C.POINTER(Params)]),
+    "bcmg_ext_default": (None, [C.POINTER(Ext)]),
+    "bcmg_setup": (C.c_int, [C.POINTER(Csr), C.POINTER(Params), C.POINTER(Ext),
+                             C.POINTER(vp)]),
+    "bcmg_setup_device": (C.c_int, [i32, i32, vp, vp, vp, C.POINTER(Params),
+                                    C.POINTER(Ext), C.POINTER(vp)]),
+    "bcmg_solve": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(SolveInfo)]),
+    "bcmg_solve_legacy": (C.c_int, [C.POINTER(Csr), C.POINTER(Params), C.POINTER(Ext), vp,
+                                    vp, C.POINTER(SolveInfo)]),
+    "bcmg_destroy": (C.c_int, [vp]),
+    "bcmg_set_stream": (C.c_int, [vp, vp]),
+    "bcmg_precond_apply": (C.c_int, [vp, vp, vp]),
+    "bcmg_hierarchy_count": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "bcmg_hierarchy_info": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double)]),
+    "bcmg_level_info": (C.c_int, [vp, C.c_int, C.c_int, i32p, i32p, i32p]),
+    "bcmg_level_copy": (C.c_int, [vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "bcmg_k_pair_aggregate": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i32p, vp, vp,
+                                        vp, vp]),
+    "bcmg_k_galerkin": (C.c_int, [i32, i32, vp, vp, vp, i32, vp, vp, vp, i32p, vp, vp,
+                                  vp]),
+    "bcmg_k_relax": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, C.c_int, vp]),
+    "bcmg_k_spmv": (C.c_int, [i32, i32, vp, vp, vp, C.c_double, vp, C.c_double, vp, vp]),
+    "bcmg_gen_poisson": (C.c_int, [C.c_int, i32, i32, i32, C.POINTER(Csr)]),
+    "bcmg_gen_fv2d": (C.c_int, [i32, i32, C.c_uint64, C.c_double, C.POINTER(Csr)]),
+    "bcmg_gen_rgg": (C.c_int, [i32, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                               C.c_double, C.POINTER(Csr)]),
+    "bcmg_gen_vector": (C.c_int, [C.c_int, C.c_uint64, i32, vp]),
+}
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA library first "
+            "(python -c 'import __graft_entry__ as g; g.build()' or make -C "
+            "bootcmatchg_b200/csrc)")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+class BcmgError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        name = lib.bcmg_status_string(status).decode()
+        msg = (lib.bcmg_last_error() or b"").decode()
+        super().__init__(f"{where}: {name}: {msg}")
+
+
+def check(status: int, where: str) -> None:
+    if status != 0:
+        raise BcmgError(status, where)

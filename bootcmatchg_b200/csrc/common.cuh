@@ -1,0 +1,107 @@
+// CUDA-side helpers shared by the library's .cu files: error checking that
+// turns CUDA failures into bcmg_status, stream-ordered device buffers, launch
+// geometry and small warp utilities.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "host_util.h"
+
+#define BCMG_CUDA(expr)                                                        \
+  do {                                                                         \
+    cudaError_t _e = (expr);                                                   \
+    if (_e != cudaSuccess)                                                     \
+      return ::bcmg::set_error(BCMG_ERR_CUDA, "%s:%d %s: %s", __FILE__,        \
+                               __LINE__, #expr, cudaGetErrorString(_e));       \
+  } while (0)
+
+#define BCMG_LAUNCH_CHECK() BCMG_CUDA(cudaGetLastError())
+
+namespace bcmg {
+
+constexpr int kWarp = 32;
+// 148 SMs on B200; grids of fixed-size reductions are multiples of this.
+constexpr int kNumSM = 148;
+constexpr uint64_t kNoOffer = ~0ull;
+
+inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// Lanes per row for row-group kernels, from the average row length.
+inline int group_for(int64_t nnz, int64_t n) {
+  const int64_t avg = n > 0 ? nnz / n : 1;
+  if (avg <= 4) return 4;
+  if (avg <= 8) return 8;
+  if (avg <= 16) return 16;
+  return 32;
+}
+
+// Stream-ordered device allocation from the device's default memory pool.
+template <typename T>
+bcmg_status dev_alloc(T **p, int64_t count, cudaStream_t s) {
+  *p = nullptr;
+  if (count <= 0) return BCMG_OK;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(p),
+                                  sizeof(T) * static_cast<size_t>(count), s);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_error(e == cudaErrorMemoryAllocation ? BCMG_ERR_ALLOC : BCMG_ERR_CUDA,
+                     "device allocation of %lld bytes failed: %s",
+                     static_cast<long long>(sizeof(T) * count), cudaGetErrorString(e));
+  }
+  return BCMG_OK;
+}
+
+template <typename T>
+void dev_free(T *&p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+  p = nullptr;
+}
+
+// Owning device array freed on the stream it was allocated on.
+template <typename T>
+struct DevBuf {
+  T *ptr = nullptr;
+  int64_t count = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream) {
+    o.ptr = nullptr;
+    o.count = 0;
+  }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) {
+      reset();
+      ptr = o.ptr;
+      count = o.count;
+      stream = o.stream;
+      o.ptr = nullptr;
+      o.count = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  bcmg_status alloc(int64_t n, cudaStream_t s) {
+    reset();
+    stream = s;
+    count = n;
+    return dev_alloc(&ptr, n, s);
+  }
+  void reset() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    count = 0;
+  }
+  T *get() const { return ptr; }
+  T *release() {
+    T *p = ptr;
+    ptr = nullptr;
+    count = 0;
+    return p;
+  }
+};
+
+}  // namespace bcmg

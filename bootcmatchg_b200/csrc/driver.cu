@@ -1,0 +1,777 @@
+// Host orchestration of the solve path: bootstrap setup (hierarchy build),
+// the V/H/W cycle, the composite preconditioner and flexible CG, plus the
+// C ABI entry points that own a bcmg_handle.
+//
+// Control flow follows the reference step by step (citations inline); the
+// arithmetic runs in the kernels of k_setup.cu / k_solve.cu.
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "handle.h"
+
+namespace bcmg {
+
+void DevLevel::release(cudaStream_t s) {
+  if (own_A) {
+    dev_free(row, s);
+    dev_free(col, s);
+    dev_free(val, s);
+  }
+  row = col = nullptr;
+  val = nullptr;
+  dev_free(D, s);
+  dev_free(M, s);
+  dev_free(w, s);
+  dev_free(agg, s);
+  dev_free(rptr, s);
+  dev_free(ridx, s);
+  dev_free(p, s);
+}
+
+namespace {
+
+constexpr int kFtcoarseInc = 100;     // FTCOARSE_INC, matchingAggregation.cu:12
+constexpr double kCoarseRatio = 1.2;  // COARSERATIO_THRSLD, matchingAggregation.cu:13
+constexpr int kBootSolverIt = 15;     // solver_it, AMG.cu:407
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+bcmg_status read_scalar(const double *dev, double *host, cudaStream_t s) {
+  BCMG_CUDA(cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+// ||x||_A = sqrt(x' A x) (CSRm::vectorANorm, src/matrix/CSR.cu:360-368).
+bcmg_status anorm(bcmg_handle *h, const double *x, double *out) {
+  BCMG_TRY(spmv(h->A0.view(), 1.0, x, 0.0, h->tmp, h->stream));
+  BCMG_TRY(dot_dev(h->A0.n, h->tmp, x, h->scal + kAlpha, h->partials, h->stream));
+  double v = 0;
+  BCMG_TRY(read_scalar(h->scal + kAlpha, &v, h->stream));
+  *out = std::sqrt(v);
+  return BCMG_OK;
+}
+
+bcmg_status norm2(bcmg_handle *h, const double *x, double *out) {
+  BCMG_TRY(dot_dev(h->A0.n, x, x, h->scal + kAlpha, h->partials, h->stream));
+  double v = 0;
+  BCMG_TRY(read_scalar(h->scal + kAlpha, &v, h->stream));
+  *out = std::sqrt(v);
+  return BCMG_OK;
+}
+
+// Builds the coarse matrix of one level from `fine` with aggrsweeps pairwise
+// sweeps (matchingAggregation, src/AMG/matchingAggregation.cu:211-295).  On
+// return fine.agg/p/nc/rptr/ridx describe the composed prolongator, *w_out
+// holds the coarse smooth vector (newly allocated) and `coarse` the Galerkin
+// matrix.  fine.w is the sweep-0 smooth vector and is left untouched.
+bcmg_status matching_aggregation(bcmg_handle *h, DevLevel &fine, double **w_out,
+                                 int *ftcoarse, DevLevel &coarse) {
+  cudaStream_t s = h->stream;
+  CsrView cur = fine.view();
+  const double *w_in = fine.w;
+  double *cur_w = fine.w;
+  DevLevel inter;  // intermediate coarse matrix between sweeps
+  bool have_inter = false;
+  DevBuf<int32_t> agg_acc;
+  DevBuf<double> p_acc;
+  int32_t nc_acc = 0;
+  for (int sweep = 0; sweep < h->prm.aggrsweeps; ++sweep) {
+    DevBuf<int32_t> agg_i, rptr_i, ridx_i, crow;
+    DevBuf<double> p_i, wi;
+    int32_t nci = 0;
+    BCMG_TRY(agg_i.alloc(cur.n, s));
+    BCMG_TRY(p_i.alloc(cur.n, s));
+    BCMG_TRY(pair_aggregate(cur, cur_w, agg_i.get(), p_i.get(), &nci, nullptr, nullptr,
+                            nullptr, s));
+    BCMG_TRY(rptr_i.alloc(nci + 1, s));
+    BCMG_TRY(ridx_i.alloc(cur.n, s));
+    BCMG_TRY(transpose_agg(cur.n, agg_i.get(), nci, rptr_i.get(), ridx_i.get(), s));
+    // Galerkin product (matchingAggregation.cu:239-244).
+    int32_t cnnz = 0;
+    BCMG_TRY(crow.alloc(nci + 1, s));
+    BCMG_TRY(galerkin_count(cur, agg_i.get(), p_i.get(), nci, rptr_i.get(), ridx_i.get(),
+                            crow.get(), &cnnz, s));
+    DevBuf<int32_t> ccol;
+    DevBuf<double> cval;
+    BCMG_TRY(ccol.alloc(cnnz, s));
+    BCMG_TRY(cval.alloc(cnnz, s));
+    BCMG_TRY(galerkin_fill(cur, agg_i.get(), p_i.get(), nci, rptr_i.get(), ridx_i.get(),
+                           crow.get(), ccol.get(), cval.get(), s));
+    // w_i = R_i w_{i-1} (matchingAggregation.cu:253).
+    BCMG_TRY(wi.alloc(nci, s));
+    BCMG_TRY(restrict_exact(nci, rptr_i.get(), ridx_i.get(), p_i.get(), cur_w, wi.get(), s));
+    const double size_precoarse = cur.n;
+    const double size_coarse = nci;
+    const double coarse_ratio = size_precoarse / size_coarse;
+    if (sweep == 0) {
+      agg_acc = std::move(agg_i);
+      p_acc = std::move(p_i);
+    } else {
+      // P = P P_i (matchingAggregation.cu:264).
+      BCMG_TRY(compose_p(fine.n, agg_acc.get(), p_acc.get(), agg_i.get(), p_i.get(), s));
+    }
+    nc_acc = nci;
+    if (have_inter) inter.release(s);
+    DevLevel next;
+    next.n = nci;
+    next.nnz = cnnz;
+    next.row = crow.release();
+    next.col = ccol.release();
+    next.val = cval.release();
+    if (cur_w != w_in) dev_free(cur_w, s);
+    cur_w = wi.release();
+    inter = next;
+    have_inter = true;
+    if (coarse_ratio <= kCoarseRatio) *ftcoarse = kFtcoarseInc;
+    cur = inter.view();
+    if (size_coarse <= static_cast<double>(*ftcoarse * h->maxcoarsesize)) break;
+  }
+  // The sweep input w (the level's smooth vector) is kept by the fine level.
+  fine.agg = agg_acc.release();
+  fine.p = p_acc.release();
+  fine.nc = nc_acc;
+  BCMG_TRY(dev_alloc(&fine.rptr, nc_acc + 1, s));
+  BCMG_TRY(dev_alloc(&fine.ridx, fine.n, s));
+  BCMG_TRY(transpose_agg(fine.n, fine.agg, nc_acc, fine.rptr, fine.ridx, s));
+  coarse = inter;
+  *w_out = cur_w;
+  return BCMG_OK;
+}
+
+// adaptiveCoarsening (src/AMG/matchingAggregation.cu:298-423).
+bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy &H) {
+  cudaStream_t s = h->stream;
+  const int maxlevels = h->prm.max_levels;
+  DevLevel l0;
+  l0.n = h->A0.n;
+  l0.nnz = h->A0.nnz;
+  l0.row = h->A0.row;
+  l0.col = h->A0.col;
+  l0.val = h->A0.val;
+  l0.own_A = false;
+  BCMG_TRY(dev_alloc(&l0.D, l0.n, s));
+  BCMG_TRY(dev_alloc(&l0.M, l0.n, s));
+  BCMG_TRY(dev_alloc(&l0.w, l0.n, s));
+  BCMG_TRY(copy(l0.w, w_in, l0.n, s));
+  BCMG_TRY(level_prep(l0.view(), l0.D, l0.M, s));
+  H.lv.push_back(l0);
+  double normw = 0;
+  BCMG_TRY(anorm(h, w_in, &normw));
+  int ftcoarse = 1;
+  double avcoarseratio = 0.0;
+  int level = 0;
+  if (normw > DBL_EPSILON) {
+    for (level = 1; level < maxlevels;) {
+      DevLevel &fine = H.lv[level - 1];
+      double *w = nullptr;
+      DevLevel coarse;
+      BCMG_TRY(matching_aggregation(h, fine, &w, &ftcoarse, coarse));
+      coarse.w = w;
+      BCMG_TRY(dev_alloc(&coarse.D, coarse.n, s));
+      BCMG_TRY(dev_alloc(&coarse.M, coarse.n, s));
+      BCMG_TRY(level_prep(coarse.view(), coarse.D, coarse.M, s));
+      const double size_coarse = coarse.n;
+      const double coarse_ratio = fine.n / size_coarse;
+      avcoarseratio += coarse_ratio;
+      H.lv.push_back(coarse);
+      ++level;
+      if (size_coarse <= static_cast<double>(ftcoarse * h->maxcoarsesize)) break;
+    }
+  } else {
+    // The reference asserts here (finalize_level with 0 levels): keep one
+    // level, i.e. a smoother-only preconditioner.
+    level = 1;
+  }
+  const double nnz0 = H.lv[0].nnz;
+  double c = 0, cw = 0;
+  for (size_t i = 0; i < H.lv.size(); ++i) {
+    c += H.lv[i].nnz;
+    cw += std::pow(2.0, static_cast<double>(i)) * H.lv[i].nnz;
+  }
+  H.op_cmplx = c / nnz0;
+  H.op_wcmplx = cw / nnz0;
+  H.avg_cratio = level > 1 ? avcoarseratio / (level - 1) : 0.0;
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+bcmg_status size_buffers(bcmg_handle *h) {
+  cudaStream_t s = h->stream;
+  size_t L = 0;
+  for (auto &H : h->H) L = std::max(L, H.lv.size());
+  const size_t old = h->buf_n.size();
+  h->rhs.resize(L, nullptr);
+  h->x.resize(L, nullptr);
+  h->xt.resize(L, nullptr);
+  h->res.resize(L, nullptr);
+  h->buf_n.resize(L, 0);
+  for (size_t l = 0; l < L; ++l) {
+    int32_t nmax = 0;
+    for (auto &H : h->H)
+      if (l < H.lv.size()) nmax = std::max(nmax, H.lv[l].n);
+    if (l < old && nmax <= h->buf_n[l]) continue;
+    if (l > 0) {
+      dev_free(h->rhs[l], s);
+      dev_free(h->x[l], s);
+      BCMG_TRY(dev_alloc(&h->rhs[l], nmax, s));
+      BCMG_TRY(dev_alloc(&h->x[l], nmax, s));
+    }
+    dev_free(h->xt[l], s);
+    dev_free(h->res[l], s);
+    BCMG_TRY(dev_alloc(&h->xt[l], nmax, s));
+    BCMG_TRY(dev_alloc(&h->res[l], nmax, s));
+    h->buf_n[l] = nmax;
+  }
+  return BCMG_OK;
+}
+
+// GAMG_cycle (src/SOLVER/GAMG_cycle.cu:25-140); l is 1-based as there.
+// zero[l-1] says the current iterate of level l-1 is identically zero and
+// has not been materialised: the first sweep then reduces to f ./ d.
+bcmg_status cycle(bcmg_handle *h, int k, int l, std::vector<char> &zero) {
+  DevHierarchy &H = h->H[k];
+  const int L = static_cast<int>(H.lv.size());
+  const bcmg_params &p = h->prm;
+  cudaStream_t s = h->stream;
+  DevLevel &lv = H.lv[l - 1];
+  double *res = nullptr;
+  if (l == L) {
+    const double *d = p.coarse_solver == 0 ? lv.D : lv.M;
+    BCMG_TRY(relax(lv.view(), d, h->rhs[l - 1], h->x[l - 1], h->xt[l - 1],
+                   p.relaxnumber_coarse, zero[l - 1] != 0, &res, s));
+    zero[l - 1] = 0;
+    return BCMG_OK;
+  }
+  const double *d = p.relax_type == 0 ? lv.D : lv.M;
+  BCMG_TRY(relax(lv.view(), d, h->rhs[l - 1], h->x[l - 1], h->xt[l - 1], p.prerelax_sweeps,
+                 zero[l - 1] != 0, &res, s));
+  zero[l - 1] = 0;
+  BCMG_TRY(residual(lv.view(), h->rhs[l - 1], h->x[l - 1], h->res[l - 1], s));
+  BCMG_TRY(restrict_vec(lv.nc, lv.rptr, lv.ridx, lv.p, h->res[l - 1], h->rhs[l], s));
+  zero[l] = 1;
+  for (int i = 1; i <= h->grid_sweeps[l - 1]; ++i) {
+    BCMG_TRY(cycle(h, k, l + 1, zero));
+    if (l == L - 1) break;
+  }
+  BCMG_TRY(prolong_add(lv.n, lv.agg, lv.p, h->x[l], h->x[l - 1], s));
+  BCMG_TRY(relax(lv.view(), d, h->rhs[l - 1], h->x[l - 1], h->xt[l - 1], p.postrelax_sweeps,
+                 false, &res, s));
+  return BCMG_OK;
+}
+
+bcmg_status run_cycle(bcmg_handle *h, int k, const double *rhs, double *x, bool x_zero) {
+  h->rhs[0] = const_cast<double *>(rhs);
+  h->x[0] = x;
+  std::vector<char> zero(h->rhs.size(), 0);
+  zero[0] = x_zero ? 1 : 0;
+  bcmg_status st = cycle(h, k, 1, zero);
+  h->rhs[0] = nullptr;
+  h->x[0] = nullptr;
+  return st;
+}
+
+// preconditionApply (src/SOLVER/FCG.cu:112-187).  Level 0 of the cycle works
+// directly on the caller's vectors, so the reference's copies into the level
+// buffers are not needed.
+bcmg_status precond_apply(bcmg_handle *h, const double *rhs, double *x, bool x_zero) {
+  const int nh = static_cast<int>(h->H.size());
+  const int32_t n = h->A0.n;
+  cudaStream_t s = h->stream;
+  if (h->prm.solver_type == 0) {
+    for (int k = 0; k < nh; ++k) BCMG_TRY(run_cycle(h, k, rhs, x, x_zero && k == 0));
+  } else if (h->prm.solver_type == 1) {
+    for (int k = 0; k < nh; ++k) BCMG_TRY(run_cycle(h, k, rhs, x, x_zero && k == 0));
+    for (int k = nh - 1; k >= 0; --k) BCMG_TRY(run_cycle(h, k, rhs, x, false));
+  } else {
+    BCMG_TRY(fill(h->xadd, n, 0.0, s));
+    for (int k = 0; k < nh; ++k) {
+      if (x_zero) {
+        BCMG_TRY(run_cycle(h, k, rhs, h->xk, true));
+      } else {
+        BCMG_TRY(copy(h->xk, x, n, s));
+        BCMG_TRY(run_cycle(h, k, rhs, h->xk, false));
+      }
+      BCMG_TRY(axpy(n, 1.0, h->xk, h->xadd, s));
+    }
+    BCMG_TRY(scale(n, 1.0 / static_cast<double>(nh), h->xadd, s));
+    BCMG_TRY(copy(x, h->xadd, n, s));
+  }
+  return BCMG_OK;
+}
+
+// Bootstrap::innerIterations (src/BOOT/bootstrap.cu:5-44).
+bcmg_status inner_iterations(bcmg_handle *h, double *w) {
+  const int32_t n = h->A0.n;
+  cudaStream_t s = h->stream;
+  double *x = h->xs, *rhs = h->b;
+  BCMG_TRY(fill(x, n, 1.0, s));
+  BCMG_TRY(fill(rhs, n, 0.0, s));
+  double normold = 0, normnew = 0, conv = 1.0;
+  BCMG_TRY(anorm(h, x, &normold));
+  for (int i = 1; i <= kBootSolverIt; ++i) {
+    BCMG_TRY(precond_apply(h, rhs, x, false));
+    BCMG_TRY(anorm(h, x, &normnew));
+    conv = normnew / normold;
+    normold = normnew;
+  }
+  BCMG_TRY(copy(w, x, n, s));
+  BCMG_TRY(scale(n, 1.0 / normnew, w, s));
+  h->estimated_ratio = conv;
+  return BCMG_OK;
+}
+
+bcmg_status alloc_work(bcmg_handle *h) {
+  const int32_t n = h->A0.n;
+  cudaStream_t s = h->stream;
+  for (double **p : {&h->r, &h->v, &h->w, &h->d, &h->q, &h->b, &h->xs, &h->xadd, &h->xk,
+                     &h->tmp})
+    BCMG_TRY(dev_alloc(p, n, s));
+  BCMG_TRY(dev_alloc(&h->partials, 4 * kRedBlocks, s));
+  BCMG_TRY(dev_alloc(&h->scal, kNumScal, s));
+  BCMG_CUDA(cudaMemsetAsync(h->scal, 0, sizeof(double) * kNumScal, s));
+  return BCMG_OK;
+}
+
+// Bootstrap::bootstrap (src/BOOT/bootstrap.cu:46-90).  After the first
+// hierarchy the inner iterations are skipped (bootstrap.cu:68-75), so with
+// max_hrc >= 2 the second hierarchy comes from the same w = 1.
+bcmg_status bootstrap(bcmg_handle *h) {
+  const int32_t n = h->A0.n;
+  cudaStream_t s = h->stream;
+  double *w = nullptr;
+  BCMG_TRY(dev_alloc(&w, n, s));
+  BCMG_TRY(fill(w, n, 1.0, s));  // BootBuildData::initByParams, AMG.cu:442-443
+  h->estimated_ratio = 1.0;
+  int num_hrc = 0;
+  bcmg_status st = BCMG_OK;
+  while (h->estimated_ratio > h->prm.conv_ratio && num_hrc < h->prm.max_hrc) {
+    h->H.emplace_back();
+    st = adaptive_coarsening(h, w, h->H.back());
+    if (st != BCMG_OK) break;
+    ++num_hrc;
+    st = size_buffers(h);
+    if (st != BCMG_OK) break;
+    if (num_hrc > 1) {
+      st = inner_iterations(h, w);
+      if (st != BCMG_OK) break;
+    }
+  }
+  dev_free(w, s);
+  return st;
+}
+
+void destroy_handle(bcmg_handle *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  cudaStream_t s = h->stream;
+  for (auto &H : h->H) H.release(s);
+  h->A0.own_A = true;
+  h->A0.release(s);
+  for (size_t l = 0; l < h->xt.size(); ++l) {
+    if (l > 0) {
+      dev_free(h->rhs[l], s);
+      dev_free(h->x[l], s);
+    }
+    dev_free(h->xt[l], s);
+    dev_free(h->res[l], s);
+  }
+  for (double **p : {&h->r, &h->v, &h->w, &h->d, &h->q, &h->b, &h->xs, &h->xadd, &h->xk,
+                     &h->tmp, &h->partials, &h->scal})
+    dev_free(*p, s);
+  cudaStreamSynchronize(s);
+  if (h->own_stream) cudaStreamDestroy(s);
+  delete h;
+}
+
+bcmg_status setup_common(bcmg_handle *h) {
+  const auto t0 = Clock::now();
+  const int32_t n = h->A0.n;
+  // BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311).
+  h->maxcoarsesize = static_cast<int32_t>(40 * std::pow(static_cast<double>(n), 1. / 3.));
+  // ApplyData::setGridSweeps (src/AMG/AMG.cu:371-394).
+  const int ml = std::max(0, h->prm.max_levels - 1);
+  h->grid_sweeps.assign(std::max(ml, 1), 1);
+  if (h->prm.cycle_type == 1) {
+    for (int i = 0; i < ml; ++i)
+      if (i % 2 == 0) h->grid_sweeps[i] = 2;
+  } else if (h->prm.cycle_type == 2) {
+    for (int i = 0; i < ml - 1; ++i) h->grid_sweeps[i] = 2;
+  }
+  BCMG_TRY(alloc_work(h));
+  BCMG_TRY(bootstrap(h));
+  BCMG_CUDA(cudaStreamSynchronize(h->stream));
+  h->setup_ms = ms_since(t0);
+  return BCMG_OK;
+}
+
+bcmg_status new_handle(const bcmg_params *p, const bcmg_ext *ext, bcmg_handle **out) {
+  if (!p || !out) return set_error(BCMG_ERR_PARAM, "null argument");
+  *out = nullptr;
+  BCMG_TRY(bcmg_params_check(p));
+  auto h = std::make_unique<bcmg_handle>();
+  h->prm = *p;
+  if (ext)
+    h->ext = *ext;
+  else
+    bcmg_ext_default(&h->ext);
+  if (h->ext.precision != BCMG_PREC_FP64 && h->ext.precision != BCMG_PREC_MIXED)
+    return set_error(BCMG_ERR_PARAM, "unknown precision mode %d", h->ext.precision);
+  h->device = h->ext.device;
+  BCMG_CUDA(cudaSetDevice(h->device));
+  BCMG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  h->own_stream = true;
+  *out = h.release();
+  return BCMG_OK;
+}
+
+// FCG (flexibileConjugateGradients_v3, src/SOLVER/FCG.cu:433-585) on device
+// vectors h->b (rhs) and h->xs (initial guess in, solution out).
+bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
+  const int32_t n = h->A0.n;
+  cudaStream_t s = h->stream;
+  const CsrView A = h->A0.view();
+  double *x = h->xs, *b = h->b, *r = h->r, *v = h->v, *w = h->w, *d = h->d, *q = h->q;
+  // r = b - A x0; delta0 = ||r||; ||b||   (FCG.cu:446-457)
+  BCMG_TRY(copy(r, b, n, s));
+  BCMG_TRY(spmv(A, -1.0, x, 1.0, r, s));
+  double delta0 = 0, bnorm = 0;
+  BCMG_TRY(norm2(h, r, &delta0));
+  BCMG_TRY(norm2(h, b, &bnorm));
+  info->iters = 0;
+  info->residual = delta0;
+  info->rel_residual = delta0 > 0 ? 1.0 : 0.0;
+  info->converged = 0;
+  if (delta0 <= DBL_EPSILON * bnorm) {
+    // The reference exits the process here (FCG.cu:459-462).
+    info->converged = 1;
+    info->rel_residual = 0.0;
+    return BCMG_OK;
+  }
+  BCMG_CUDA(cudaMemsetAsync(h->scal, 0, sizeof(double) * kNumScal, s));
+  // First step (FCG.cu:464-495).
+  BCMG_TRY(precond_apply(h, r, v, true));
+  BCMG_TRY(fcg_spmv_dots(A, v, w, r, nullptr, h->partials, h->scal, s));
+  BCMG_TRY(fcg_scalars(h->partials, h->scal, true, s));
+  BCMG_TRY(fcg_update(n, true, v, nullptr, w, nullptr, x, r, h->partials, h->scal, s));
+  BCMG_TRY(copy(d, v, n, s));
+  BCMG_TRY(copy(q, w, n, s));
+  double l2 = 0;
+  int iter = 0;
+  const double target = h->prm.rtol * delta0;
+  double hs[kNumScal];
+  bcmg_status st = BCMG_OK;
+  do {
+    const bool even = (iter % 2) == 0;
+    double *z = even ? v : d, *az = even ? w : q;
+    const double *zp = even ? d : v, *azp = even ? q : w;
+    BCMG_TRY(precond_apply(h, r, z, true));
+    BCMG_TRY(fcg_spmv_dots(A, z, az, r, azp, h->partials, h->scal, s));
+    BCMG_TRY(fcg_scalars(h->partials, h->scal, false, s));
+    BCMG_TRY(fcg_update(n, false, z, zp, az, azp, x, r, h->partials, h->scal, s));
+    BCMG_CUDA(cudaMemcpyAsync(hs, h->scal, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    BCMG_CUDA(cudaStreamSynchronize(s));
+    l2 = hs[kNorm];
+    ++iter;
+    if (hs[kIndef] != 0.0) {
+      st = set_error(BCMG_ERR_INDEFINITE,
+                     "FCG met non-positive curvature at iteration %d (A not SPD?)", iter);
+      break;
+    }
+    if (h->ext.verbose > 1)
+      printf("bootpcg iteration: %d  residual: %e relative residual: %e\n", iter - 1, l2,
+             l2 / delta0);
+  } while (l2 > target && iter < h->prm.itnlim);
+  info->iters = iter + 1;  // FCG.cu:569
+  info->residual = l2;
+  info->rel_residual = l2 / delta0;
+  info->converged = l2 <= target ? 1 : 0;
+  // True residual in FP64: ||b - A x|| / ||b - A x0||.
+  if (st == BCMG_OK) {
+    BCMG_TRY(copy(h->tmp, b, n, s));
+    BCMG_TRY(spmv(A, -1.0, x, 1.0, h->tmp, s));
+    double tr = 0;
+    BCMG_TRY(norm2(h, h->tmp, &tr));
+    info->true_rel_residual = tr / delta0;
+  }
+  return st;
+}
+
+}  // namespace
+}  // namespace bcmg
+
+using namespace bcmg;
+
+extern "C" {
+
+bcmg_status bcmg_setup(const bcmg_csr *A, const bcmg_params *p, const bcmg_ext *ext,
+                       bcmg_handle **out) {
+  clear_error();
+  if (!A || !out) return set_error(BCMG_ERR_PARAM, "null argument");
+  *out = nullptr;
+  BCMG_TRY(bcmg_csr_check(A));
+  bcmg_handle *h = nullptr;
+  BCMG_TRY(new_handle(p, ext, &h));
+  std::unique_ptr<bcmg_handle, void (*)(bcmg_handle *)> guard(h, destroy_handle);
+  DevLevel &a = h->A0;
+  a.n = A->n;
+  a.nnz = A->nnz;
+  BCMG_TRY(dev_alloc(&a.row, a.n + 1, h->stream));
+  BCMG_TRY(dev_alloc(&a.col, a.nnz, h->stream));
+  BCMG_TRY(dev_alloc(&a.val, a.nnz, h->stream));
+  BCMG_CUDA(cudaMemcpyAsync(a.row, A->row, sizeof(int32_t) * (a.n + 1),
+                            cudaMemcpyHostToDevice, h->stream));
+  BCMG_CUDA(cudaMemcpyAsync(a.col, A->col, sizeof(int32_t) * a.nnz, cudaMemcpyHostToDevice,
+                            h->stream));
+  BCMG_CUDA(cudaMemcpyAsync(a.val, A->val, sizeof(double) * a.nnz, cudaMemcpyHostToDevice,
+                            h->stream));
+  BCMG_TRY(setup_common(h));
+  *out = guard.release();
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_setup_device(int32_t n, int32_t nnz, const int32_t *d_row,
+                              const int32_t *d_col, const double *d_val,
+                              const bcmg_params *p, const bcmg_ext *ext, bcmg_handle **out) {
+  clear_error();
+  if (!d_row || !d_col || !d_val || !out || n <= 0 || nnz < n)
+    return set_error(BCMG_ERR_PARAM, "bad device CSR arguments");
+  *out = nullptr;
+  bcmg_handle *h = nullptr;
+  BCMG_TRY(new_handle(p, ext, &h));
+  std::unique_ptr<bcmg_handle, void (*)(bcmg_handle *)> guard(h, destroy_handle);
+  DevLevel &a = h->A0;
+  a.n = n;
+  a.nnz = nnz;
+  BCMG_TRY(dev_alloc(&a.row, n + 1, h->stream));
+  BCMG_TRY(dev_alloc(&a.col, nnz, h->stream));
+  BCMG_TRY(dev_alloc(&a.val, nnz, h->stream));
+  BCMG_CUDA(cudaMemcpyAsync(a.row, d_row, sizeof(int32_t) * (n + 1),
+                            cudaMemcpyDeviceToDevice, h->stream));
+  BCMG_CUDA(cudaMemcpyAsync(a.col, d_col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice,
+                            h->stream));
+  BCMG_CUDA(cudaMemcpyAsync(a.val, d_val, sizeof(double) * nnz, cudaMemcpyDeviceToDevice,
+                            h->stream));
+  BCMG_TRY(setup_common(h));
+  *out = guard.release();
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_solve(bcmg_handle *h, const double *b, double *x, int on_device,
+                       bcmg_solve_info *info) {
+  clear_error();
+  if (!h || !b || !x) return set_error(BCMG_ERR_PARAM, "null argument");
+  bcmg_solve_info local;
+  if (!info) info = &local;
+  std::memset(info, 0, sizeof(*info));
+  BCMG_CUDA(cudaSetDevice(h->device));
+  const auto t0 = Clock::now();
+  const int32_t n = h->A0.n;
+  const cudaMemcpyKind in = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  BCMG_CUDA(cudaMemcpyAsync(h->b, b, sizeof(double) * n, in, h->stream));
+  BCMG_CUDA(cudaMemcpyAsync(h->xs, x, sizeof(double) * n, in, h->stream));
+  bcmg_status st = fcg(h, info);
+  const cudaMemcpyKind outk = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  BCMG_CUDA(cudaMemcpyAsync(x, h->xs, sizeof(double) * n, outk, h->stream));
+  BCMG_CUDA(cudaStreamSynchronize(h->stream));
+  info->solve_ms = ms_since(t0);
+  info->setup_ms = h->setup_ms;
+  info->num_hrc = static_cast<int>(h->H.size());
+  info->estimated_ratio = h->estimated_ratio;
+  return st;
+}
+
+bcmg_status bcmg_solve_legacy(const bcmg_csr *A, const bcmg_params *p, const bcmg_ext *ext,
+                              const double *b, double *x, bcmg_solve_info *info) {
+  if (!A || !b || !x) return set_error(BCMG_ERR_PARAM, "null argument");
+  bcmg_handle *h = nullptr;
+  BCMG_TRY(bcmg_setup(A, p, ext, &h));
+  for (int32_t i = 0; i < A->n; ++i) x[i] = 0.0;  // Sol = 0, solver.cu:222-223
+  bcmg_status st = bcmg_solve(h, b, x, 0, info);
+  bcmg_destroy(h);
+  return st;
+}
+
+bcmg_status bcmg_destroy(bcmg_handle *h) {
+  destroy_handle(h);
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_set_stream(bcmg_handle *h, void *stream) {
+  if (!h) return set_error(BCMG_ERR_PARAM, "null handle");
+  BCMG_CUDA(cudaSetDevice(h->device));
+  BCMG_CUDA(cudaStreamSynchronize(h->stream));
+  if (h->own_stream) BCMG_CUDA(cudaStreamDestroy(h->stream));
+  h->stream = static_cast<cudaStream_t>(stream);
+  h->own_stream = false;
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_precond_apply(bcmg_handle *h, const double *d_r, double *d_z) {
+  if (!h || !d_r || !d_z) return set_error(BCMG_ERR_PARAM, "null argument");
+  BCMG_CUDA(cudaSetDevice(h->device));
+  BCMG_TRY(precond_apply(h, d_r, d_z, false));
+  BCMG_CUDA(cudaStreamSynchronize(h->stream));
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_hierarchy_count(const bcmg_handle *h, int *num_hrc, double *est) {
+  if (!h) return set_error(BCMG_ERR_PARAM, "null handle");
+  if (num_hrc) *num_hrc = static_cast<int>(h->H.size());
+  if (est) *est = h->estimated_ratio;
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_hierarchy_info(const bcmg_handle *h, int hrc, int *num_levels,
+                                double *op_cmplx, double *op_wcmplx, double *avg_cratio) {
+  if (!h || hrc < 0 || hrc >= static_cast<int>(h->H.size()))
+    return set_error(BCMG_ERR_PARAM, "bad hierarchy index");
+  const DevHierarchy &H = h->H[hrc];
+  if (num_levels) *num_levels = static_cast<int>(H.lv.size());
+  if (op_cmplx) *op_cmplx = H.op_cmplx;
+  if (op_wcmplx) *op_wcmplx = H.op_wcmplx;
+  if (avg_cratio) *avg_cratio = H.avg_cratio;
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_level_info(const bcmg_handle *h, int hrc, int level, int32_t *n,
+                            int32_t *nnz, int32_t *n_coarse) {
+  if (!h || hrc < 0 || hrc >= static_cast<int>(h->H.size()))
+    return set_error(BCMG_ERR_PARAM, "bad hierarchy index");
+  const DevHierarchy &H = h->H[hrc];
+  if (level < 0 || level >= static_cast<int>(H.lv.size()))
+    return set_error(BCMG_ERR_PARAM, "bad level index");
+  const DevLevel &l = H.lv[level];
+  if (n) *n = l.n;
+  if (nnz) *nnz = l.nnz;
+  if (n_coarse) *n_coarse = l.nc;
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_level_copy(const bcmg_handle *h, int hrc, int level, int32_t *row,
+                            int32_t *col, double *val, double *D, double *M, int32_t *agg,
+                            double *p, double *w) {
+  if (!h || hrc < 0 || hrc >= static_cast<int>(h->H.size()))
+    return set_error(BCMG_ERR_PARAM, "bad hierarchy index");
+  const DevHierarchy &H = h->H[hrc];
+  if (level < 0 || level >= static_cast<int>(H.lv.size()))
+    return set_error(BCMG_ERR_PARAM, "bad level index");
+  BCMG_CUDA(cudaSetDevice(h->device));
+  const DevLevel &l = H.lv[level];
+  cudaStream_t s = h->stream;
+  auto get = [&](void *dst, const void *src, size_t bytes) -> bcmg_status {
+    if (dst && src && bytes)
+      BCMG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    return BCMG_OK;
+  };
+  BCMG_TRY(get(row, l.row, sizeof(int32_t) * (l.n + 1)));
+  BCMG_TRY(get(col, l.col, sizeof(int32_t) * l.nnz));
+  BCMG_TRY(get(val, l.val, sizeof(double) * l.nnz));
+  BCMG_TRY(get(D, l.D, sizeof(double) * l.n));
+  BCMG_TRY(get(M, l.M, sizeof(double) * l.n));
+  BCMG_TRY(get(w, l.w, sizeof(double) * l.n));
+  if (l.agg) BCMG_TRY(get(agg, l.agg, sizeof(int32_t) * l.n));
+  if (l.p) BCMG_TRY(get(p, l.p, sizeof(double) * l.n));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+// ---- single-step entry points ------------------------------------------
+bcmg_status bcmg_k_pair_aggregate(int32_t n, int32_t nnz, const int32_t *d_row,
+                                  const int32_t *d_col, const double *d_val,
+                                  const double *d_w, int32_t *d_agg, double *d_p,
+                                  int32_t *n_coarse, double *d_W, int32_t *d_suitor,
+                                  int32_t *d_match, void *stream) {
+  clear_error();
+  if (n <= 0 || !d_row || !d_col || !d_val || !d_w || !d_agg || !d_p || !n_coarse)
+    return set_error(BCMG_ERR_PARAM, "bad arguments");
+  CsrView A;
+  A.n = n;
+  A.nnz = nnz;
+  A.row = d_row;
+  A.col = d_col;
+  A.val = d_val;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BCMG_TRY(pair_aggregate(A, d_w, d_agg, d_p, n_coarse, d_W, d_suitor, d_match, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_k_galerkin(int32_t n, int32_t nnz, const int32_t *d_row,
+                            const int32_t *d_col, const double *d_val, int32_t n_coarse,
+                            const int32_t *d_agg, const double *d_p, int32_t *d_crow,
+                            int32_t *c_nnz, int32_t *d_ccol, double *d_cval, void *stream) {
+  clear_error();
+  if (n <= 0 || n_coarse <= 0 || !d_row || !d_col || !d_val || !d_agg || !d_p || !d_crow)
+    return set_error(BCMG_ERR_PARAM, "bad arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CsrView A;
+  A.n = n;
+  A.nnz = nnz;
+  A.row = d_row;
+  A.col = d_col;
+  A.val = d_val;
+  DevBuf<int32_t> rptr, ridx;
+  BCMG_TRY(rptr.alloc(n_coarse + 1, s));
+  BCMG_TRY(ridx.alloc(n, s));
+  BCMG_TRY(transpose_agg(n, d_agg, n_coarse, rptr.get(), ridx.get(), s));
+  if (!d_ccol || !d_cval) {
+    int32_t cnnz = 0;
+    BCMG_TRY(galerkin_count(A, d_agg, d_p, n_coarse, rptr.get(), ridx.get(), d_crow, &cnnz,
+                            s));
+    if (c_nnz) *c_nnz = cnnz;
+  } else {
+    BCMG_TRY(galerkin_fill(A, d_agg, d_p, n_coarse, rptr.get(), ridx.get(), d_crow, d_ccol,
+                           d_cval, s));
+  }
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_k_relax(int32_t n, int32_t nnz, const int32_t *d_row, const int32_t *d_col,
+                         const double *d_val, const double *d_d, const double *d_f,
+                         double *d_u, int k, void *stream) {
+  clear_error();
+  if (n <= 0 || !d_row || !d_col || !d_val || !d_d || !d_f || !d_u || k < 0)
+    return set_error(BCMG_ERR_PARAM, "bad arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CsrView A;
+  A.n = n;
+  A.nnz = nnz;
+  A.row = d_row;
+  A.col = d_col;
+  A.val = d_val;
+  DevBuf<double> tmp;
+  BCMG_TRY(tmp.alloc(n, s));
+  double *res = nullptr;
+  BCMG_TRY(relax(A, d_d, d_f, d_u, tmp.get(), k, false, &res, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_k_spmv(int32_t n, int32_t nnz, const int32_t *d_row, const int32_t *d_col,
+                        const double *d_val, double alpha, const double *d_x, double beta,
+                        double *d_y, void *stream) {
+  clear_error();
+  if (n <= 0 || !d_row || !d_col || !d_val || !d_x || !d_y)
+    return set_error(BCMG_ERR_PARAM, "bad arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CsrView A;
+  A.n = n;
+  A.nnz = nnz;
+  A.row = d_row;
+  A.col = d_col;
+  A.val = d_val;
+  BCMG_TRY(spmv(A, alpha, d_x, beta, d_y, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// Internal definition of bcmg_handle and the device hierarchy.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "bcmg.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace bcmg {
+
+// One level of a hierarchy on the device.  P (to the next level) has one
+// entry per fine row: column agg[i], value p[i]; R = P^T is stored as the
+// aggregates' member lists in ascending order (rptr, ridx).
+struct DevLevel {
+  int32_t n = 0, nnz = 0;
+  int32_t *row = nullptr, *col = nullptr;
+  double *val = nullptr;
+  bool own_A = true;
+  double *D = nullptr, *M = nullptr, *w = nullptr;
+  int32_t nc = 0;
+  int32_t *agg = nullptr, *rptr = nullptr, *ridx = nullptr;
+  double *p = nullptr;
+  CsrView view() const {
+    CsrView v;
+    v.n = n;
+    v.nnz = nnz;
+    v.row = row;
+    v.col = col;
+    v.val = val;
+    return v;
+  }
+  void release(cudaStream_t s);
+};
+
+struct DevHierarchy {
+  std::vector<DevLevel> lv;
+  double op_cmplx = 0, op_wcmplx = 0, avg_cratio = 0;
+  void release(cudaStream_t s) {
+    for (auto &l : lv) l.release(s);
+    lv.clear();
+  }
+};
+
+}  // namespace bcmg
+
+struct bcmg_handle {
+  bcmg_params prm{};
+  bcmg_ext ext{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bcmg::DevLevel A0;  // the input matrix; level 0 of every hierarchy points here
+  std::vector<bcmg::DevHierarchy> H;
+  double estimated_ratio = 1.0;
+  int32_t maxcoarsesize = 0;
+  std::vector<int> grid_sweeps;
+  // Cycle work vectors per level (index 0 is bound to the caller's vectors
+  // during an application, except xt/res which are owned).
+  std::vector<double *> rhs, x, xt, res;
+  std::vector<int32_t> buf_n;
+  // FCG vectors and device scalars.
+  double *r = nullptr, *v = nullptr, *w = nullptr, *d = nullptr, *q = nullptr;
+  double *b = nullptr, *xs = nullptr, *xadd = nullptr, *xk = nullptr, *tmp = nullptr;
+  double *partials = nullptr, *scal = nullptr;
+  double setup_ms = 0.0;
+};

