@@ -42,7 +42,8 @@ class Ext(C.Structure):
 
     _fields_ = [("precision", C.c_int), ("coarse_storage", C.c_int),
                 ("replace_every", C.c_int), ("use_graphs", C.c_int), ("device", C.c_int),
-                ("verbose", C.c_int), ("max_device_seconds", C.c_double)]
+                ("verbose", C.c_int), ("max_device_seconds", C.c_double),
+                ("stream", C.c_void_p)]
 
 
 class SolveInfo(C.Structure):
@@ -57,6 +58,7 @@ SIGNATURES = {
     "bcmg_last_error": (C.c_char_p, []),
     "bcmg_status_string": (C.c_char_p, [C.c_int]),
     "bcmg_version": (C.c_char_p, []),
+    "bcmg_kernel_launches": (C.c_ulonglong, []),
     "bcmg_read_matrix": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(Csr)]),
     "bcmg_write_matrix_mm": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
     "bcmg_csr_free": (None, [C.POINTER(Csr)]),

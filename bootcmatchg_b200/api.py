@@ -142,11 +142,13 @@ class Extensions:
     device: int = 0
     verbose: int = 0
     max_device_seconds: float = 60.0
+    stream: int = 0  # cudaStream_t as an integer (0: the handle makes its own)
 
     def to_c(self) -> Ext:
         e = Ext()
         for f, _ in Ext._fields_:
-            setattr(e, f, getattr(self, f))
+            v = getattr(self, f)
+            setattr(e, f, C.c_void_p(v) if f == "stream" else v)
         return e
 
 

@@ -4,7 +4,10 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <cstdint>
+#include <utility>
 
 #include "host_util.h"
 
@@ -24,6 +27,18 @@ constexpr int kWarp = 32;
 // 148 SMs on B200; grids of fixed-size reductions are multiples of this.
 constexpr int kNumSM = 148;
 constexpr uint64_t kNoOffer = ~0ull;
+
+// Kernel launches issued by this library (bcmg_kernel_launches()).
+extern std::atomic<unsigned long long> g_kernel_launches;
+
+// Every kernel of the library is launched through here so launches are
+// counted.
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t s, Args &&...args) {
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+}
 
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 

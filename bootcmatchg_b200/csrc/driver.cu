@@ -15,6 +15,8 @@
 
 namespace bcmg {
 
+std::atomic<unsigned long long> g_kernel_launches{0};
+
 void DevLevel::release(cudaStream_t s) {
   if (own_A) {
     dev_free(row, s);
@@ -30,6 +32,11 @@ void DevLevel::release(cudaStream_t s) {
   dev_free(rptr, s);
   dev_free(ridx, s);
   dev_free(p, s);
+  if (own_lo) dev_free(val_lo, s);
+  val_lo = nullptr;
+  dev_free(D32, s);
+  dev_free(M32, s);
+  dev_free(p32, s);
 }
 
 namespace {
@@ -203,111 +210,183 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
   return BCMG_OK;
 }
 
-bcmg_status size_buffers(bcmg_handle *h) {
+template <typename XT>
+bcmg_status size_buffers_t(bcmg_handle *h, CycleBufs<XT> &B) {
   cudaStream_t s = h->stream;
   size_t L = 0;
   for (auto &H : h->H) L = std::max(L, H.lv.size());
-  const size_t old = h->buf_n.size();
-  h->rhs.resize(L, nullptr);
-  h->x.resize(L, nullptr);
-  h->xt.resize(L, nullptr);
-  h->res.resize(L, nullptr);
-  h->buf_n.resize(L, 0);
+  const size_t old = B.n.size();
+  B.rhs.resize(L, nullptr);
+  B.x.resize(L, nullptr);
+  B.xt.resize(L, nullptr);
+  B.res.resize(L, nullptr);
+  B.n.resize(L, 0);
   for (size_t l = 0; l < L; ++l) {
     int32_t nmax = 0;
     for (auto &H : h->H)
       if (l < H.lv.size()) nmax = std::max(nmax, H.lv[l].n);
-    if (l < old && nmax <= h->buf_n[l]) continue;
+    if (l < old && nmax <= B.n[l]) continue;
     if (l > 0) {
-      dev_free(h->rhs[l], s);
-      dev_free(h->x[l], s);
-      BCMG_TRY(dev_alloc(&h->rhs[l], nmax, s));
-      BCMG_TRY(dev_alloc(&h->x[l], nmax, s));
+      dev_free(B.rhs[l], s);
+      dev_free(B.x[l], s);
+      BCMG_TRY(dev_alloc(&B.rhs[l], nmax, s));
+      BCMG_TRY(dev_alloc(&B.x[l], nmax, s));
     }
-    dev_free(h->xt[l], s);
-    dev_free(h->res[l], s);
-    BCMG_TRY(dev_alloc(&h->xt[l], nmax, s));
-    BCMG_TRY(dev_alloc(&h->res[l], nmax, s));
-    h->buf_n[l] = nmax;
+    dev_free(B.xt[l], s);
+    dev_free(B.res[l], s);
+    BCMG_TRY(dev_alloc(&B.xt[l], nmax, s));
+    BCMG_TRY(dev_alloc(&B.res[l], nmax, s));
+    B.n[l] = nmax;
+  }
+  const int32_t n = h->A0.n;
+  if (!B.xk) {
+    BCMG_TRY(dev_alloc(&B.xk, n, s));
+    BCMG_TRY(dev_alloc(&B.xadd, n, s));
+    BCMG_TRY(dev_alloc(&B.in0, n, s));
+    BCMG_TRY(dev_alloc(&B.out0, n, s));
   }
   return BCMG_OK;
 }
 
+template <typename XT>
+void free_buffers_t(CycleBufs<XT> &B, cudaStream_t s) {
+  for (size_t l = 0; l < B.xt.size(); ++l) {
+    if (l > 0) {
+      dev_free(B.rhs[l], s);
+      dev_free(B.x[l], s);
+    }
+    dev_free(B.xt[l], s);
+    dev_free(B.res[l], s);
+  }
+  dev_free(B.xk, s);
+  dev_free(B.xadd, s);
+  dev_free(B.in0, s);
+  dev_free(B.out0, s);
+}
+
+// The level data a cycle of vector type XT reads.
+template <typename XT>
+struct Lv;
+template <>
+struct Lv<double> {
+  static MatView mat(const DevLevel &l) { return mat_f64(l.view()); }
+  static const double *D(const DevLevel &l) { return l.D; }
+  static const double *M(const DevLevel &l) { return l.M; }
+  static const double *p(const DevLevel &l) { return l.p; }
+};
+template <>
+struct Lv<float> {
+  static MatView mat(const DevLevel &l) {
+    MatView m;
+    m.n = l.n;
+    m.nnz = l.nnz;
+    m.row = l.row;
+    m.col = l.col;
+    m.val = l.val_lo;
+    m.vtype = l.vtype_lo;
+    return m;
+  }
+  static const float *D(const DevLevel &l) { return l.D32; }
+  static const float *M(const DevLevel &l) { return l.M32; }
+  static const float *p(const DevLevel &l) { return l.p32; }
+};
+
 // GAMG_cycle (src/SOLVER/GAMG_cycle.cu:25-140); l is 1-based as there.
 // zero[l-1] says the current iterate of level l-1 is identically zero and
 // has not been materialised: the first sweep then reduces to f ./ d.
-bcmg_status cycle(bcmg_handle *h, int k, int l, std::vector<char> &zero) {
+template <typename XT>
+bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<char> &zero) {
   DevHierarchy &H = h->H[k];
   const int L = static_cast<int>(H.lv.size());
   const bcmg_params &p = h->prm;
   cudaStream_t s = h->stream;
   DevLevel &lv = H.lv[l - 1];
-  double *res = nullptr;
+  const MatView A = Lv<XT>::mat(lv);
   if (l == L) {
-    const double *d = p.coarse_solver == 0 ? lv.D : lv.M;
-    BCMG_TRY(relax(lv.view(), d, h->rhs[l - 1], h->x[l - 1], h->xt[l - 1],
-                   p.relaxnumber_coarse, zero[l - 1] != 0, &res, s));
+    const XT *d = p.coarse_solver == 0 ? Lv<XT>::D(lv) : Lv<XT>::M(lv);
+    BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.relaxnumber_coarse,
+                         zero[l - 1] != 0, s));
     zero[l - 1] = 0;
     return BCMG_OK;
   }
-  const double *d = p.relax_type == 0 ? lv.D : lv.M;
-  BCMG_TRY(relax(lv.view(), d, h->rhs[l - 1], h->x[l - 1], h->xt[l - 1], p.prerelax_sweeps,
-                 zero[l - 1] != 0, &res, s));
+  const XT *d = p.relax_type == 0 ? Lv<XT>::D(lv) : Lv<XT>::M(lv);
+  BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.prerelax_sweeps,
+                       zero[l - 1] != 0, s));
   zero[l - 1] = 0;
-  BCMG_TRY(residual(lv.view(), h->rhs[l - 1], h->x[l - 1], h->res[l - 1], s));
-  BCMG_TRY(restrict_vec(lv.nc, lv.rptr, lv.ridx, lv.p, h->res[l - 1], h->rhs[l], s));
+  BCMG_TRY(residual_t<XT>(A, B.rhs[l - 1], B.x[l - 1], B.res[l - 1], s));
+  BCMG_TRY(restrict_t<XT>(lv.nc, lv.rptr, lv.ridx, Lv<XT>::p(lv), B.res[l - 1], B.rhs[l], s));
   zero[l] = 1;
   for (int i = 1; i <= h->grid_sweeps[l - 1]; ++i) {
-    BCMG_TRY(cycle(h, k, l + 1, zero));
+    BCMG_TRY(cycle_t<XT>(h, B, k, l + 1, zero));
     if (l == L - 1) break;
   }
-  BCMG_TRY(prolong_add(lv.n, lv.agg, lv.p, h->x[l], h->x[l - 1], s));
-  BCMG_TRY(relax(lv.view(), d, h->rhs[l - 1], h->x[l - 1], h->xt[l - 1], p.postrelax_sweeps,
-                 false, &res, s));
+  BCMG_TRY(prolong_t<XT>(lv.n, lv.agg, Lv<XT>::p(lv), B.x[l], B.x[l - 1], s));
+  BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.postrelax_sweeps, false,
+                       s));
   return BCMG_OK;
 }
 
-bcmg_status run_cycle(bcmg_handle *h, int k, const double *rhs, double *x, bool x_zero) {
-  h->rhs[0] = const_cast<double *>(rhs);
-  h->x[0] = x;
-  std::vector<char> zero(h->rhs.size(), 0);
+template <typename XT>
+bcmg_status run_cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, const XT *rhs, XT *x,
+                        bool x_zero) {
+  B.rhs[0] = const_cast<XT *>(rhs);
+  B.x[0] = x;
+  std::vector<char> zero(B.rhs.size(), 0);
   zero[0] = x_zero ? 1 : 0;
-  bcmg_status st = cycle(h, k, 1, zero);
-  h->rhs[0] = nullptr;
-  h->x[0] = nullptr;
+  bcmg_status st = cycle_t<XT>(h, B, k, 1, zero);
+  B.rhs[0] = nullptr;
+  B.x[0] = nullptr;
   return st;
 }
 
 // preconditionApply (src/SOLVER/FCG.cu:112-187).  Level 0 of the cycle works
 // directly on the caller's vectors, so the reference's copies into the level
 // buffers are not needed.
-bcmg_status precond_apply(bcmg_handle *h, const double *rhs, double *x, bool x_zero) {
+template <typename XT>
+bcmg_status precond_apply_t(bcmg_handle *h, CycleBufs<XT> &B, const XT *rhs, XT *x,
+                            bool x_zero) {
   const int nh = static_cast<int>(h->H.size());
   const int32_t n = h->A0.n;
   cudaStream_t s = h->stream;
   if (h->prm.solver_type == 0) {
-    for (int k = 0; k < nh; ++k) BCMG_TRY(run_cycle(h, k, rhs, x, x_zero && k == 0));
+    for (int k = 0; k < nh; ++k) BCMG_TRY(run_cycle_t<XT>(h, B, k, rhs, x, x_zero && k == 0));
   } else if (h->prm.solver_type == 1) {
-    for (int k = 0; k < nh; ++k) BCMG_TRY(run_cycle(h, k, rhs, x, x_zero && k == 0));
-    for (int k = nh - 1; k >= 0; --k) BCMG_TRY(run_cycle(h, k, rhs, x, false));
+    for (int k = 0; k < nh; ++k) BCMG_TRY(run_cycle_t<XT>(h, B, k, rhs, x, x_zero && k == 0));
+    for (int k = nh - 1; k >= 0; --k) BCMG_TRY(run_cycle_t<XT>(h, B, k, rhs, x, false));
   } else {
-    BCMG_TRY(fill(h->xadd, n, 0.0, s));
+    BCMG_TRY(fill_t<XT>(B.xadd, n, XT(0), s));
     for (int k = 0; k < nh; ++k) {
       if (x_zero) {
-        BCMG_TRY(run_cycle(h, k, rhs, h->xk, true));
+        BCMG_TRY(run_cycle_t<XT>(h, B, k, rhs, B.xk, true));
       } else {
-        BCMG_TRY(copy(h->xk, x, n, s));
-        BCMG_TRY(run_cycle(h, k, rhs, h->xk, false));
+        BCMG_TRY(copy_t<XT>(B.xk, x, n, s));
+        BCMG_TRY(run_cycle_t<XT>(h, B, k, rhs, B.xk, false));
       }
-      BCMG_TRY(axpy(n, 1.0, h->xk, h->xadd, s));
+      BCMG_TRY(axpy_t<XT>(n, XT(1), B.xk, B.xadd, s));
     }
-    BCMG_TRY(scale(n, 1.0 / static_cast<double>(nh), h->xadd, s));
-    BCMG_TRY(copy(x, h->xadd, n, s));
+    BCMG_TRY(scale_t<XT>(n, XT(1) / static_cast<XT>(nh), B.xadd, s));
+    BCMG_TRY(copy_t<XT>(x, B.xadd, n, s));
   }
   return BCMG_OK;
 }
 
-// Bootstrap::innerIterations (src/BOOT/bootstrap.cu:5-44).
+// z = B r on FP64 vectors.  use_mixed selects the FP32 cycle: r is rounded
+// to FP32, the cycle runs in FP32 and its result is widened into z.
+bcmg_status precond_apply(bcmg_handle *h, const double *rhs, double *x, bool x_zero,
+                          bool use_mixed) {
+  if (!use_mixed) return precond_apply_t<double>(h, h->c64, rhs, x, x_zero);
+  const int32_t n = h->A0.n;
+  cudaStream_t s = h->stream;
+  CycleBufs<float> &B = h->c32;
+  BCMG_TRY(convert_d2f(n, rhs, B.in0, s));
+  if (!x_zero) BCMG_TRY(convert_d2f(n, x, B.out0, s));
+  BCMG_TRY(precond_apply_t<float>(h, B, B.in0, B.out0, x_zero));
+  BCMG_TRY(convert_f2d(n, B.out0, x, s));
+  return BCMG_OK;
+}
+
+// Bootstrap::innerIterations (src/BOOT/bootstrap.cu:5-44).  Always FP64 so
+// the bootstrapped hierarchies do not depend on the solve precision.
 bcmg_status inner_iterations(bcmg_handle *h, double *w) {
   const int32_t n = h->A0.n;
   cudaStream_t s = h->stream;
@@ -317,7 +396,7 @@ bcmg_status inner_iterations(bcmg_handle *h, double *w) {
   double normold = 0, normnew = 0, conv = 1.0;
   BCMG_TRY(anorm(h, x, &normold));
   for (int i = 1; i <= kBootSolverIt; ++i) {
-    BCMG_TRY(precond_apply(h, rhs, x, false));
+    BCMG_TRY(precond_apply(h, rhs, x, false, false));
     BCMG_TRY(anorm(h, x, &normnew));
     conv = normnew / normold;
     normold = normnew;
@@ -328,14 +407,58 @@ bcmg_status inner_iterations(bcmg_handle *h, double *w) {
   return BCMG_OK;
 }
 
+// Low-precision copies of every level for the mixed cycle: level 0 in FP32,
+// coarser levels in FP32 / BF16 / FP16 (ext.coarse_storage); D, M and P in
+// FP32.
+bcmg_status prepare_mixed(bcmg_handle *h) {
+  cudaStream_t s = h->stream;
+  DevLevel &a = h->A0;
+  if (!a.val_lo) {
+    BCMG_TRY(dev_alloc(reinterpret_cast<float **>(&a.val_lo), a.nnz, s));
+    a.vtype_lo = kValF32;
+    BCMG_TRY(convert_values(a.nnz, a.val, a.val_lo, kValF32, s));
+  }
+  const int coarse_type = h->ext.coarse_storage == BCMG_STORE_BF16   ? kValBF16
+                          : h->ext.coarse_storage == BCMG_STORE_FP16 ? kValF16
+                                                                     : kValF32;
+  for (auto &H : h->H) {
+    for (size_t l = 0; l < H.lv.size(); ++l) {
+      DevLevel &lv = H.lv[l];
+      if (l == 0) {
+        lv.val_lo = a.val_lo;
+        lv.vtype_lo = kValF32;
+        lv.own_lo = false;
+      } else {
+        const size_t bytes = coarse_type == kValF32 ? 4 : 2;
+        BCMG_TRY(dev_alloc(reinterpret_cast<unsigned char **>(&lv.val_lo),
+                           static_cast<int64_t>(bytes) * lv.nnz, s));
+        lv.vtype_lo = coarse_type;
+        lv.own_lo = true;
+        BCMG_TRY(convert_values(lv.nnz, lv.val, lv.val_lo, coarse_type, s));
+      }
+      BCMG_TRY(dev_alloc(&lv.D32, lv.n, s));
+      BCMG_TRY(dev_alloc(&lv.M32, lv.n, s));
+      BCMG_TRY(convert_d2f(lv.n, lv.D, lv.D32, s));
+      BCMG_TRY(convert_d2f(lv.n, lv.M, lv.M32, s));
+      if (lv.p) {
+        BCMG_TRY(dev_alloc(&lv.p32, lv.n, s));
+        BCMG_TRY(convert_d2f(lv.n, lv.p, lv.p32, s));
+      }
+    }
+  }
+  BCMG_TRY(size_buffers_t<float>(h, h->c32));
+  return BCMG_OK;
+}
+
 bcmg_status alloc_work(bcmg_handle *h) {
   const int32_t n = h->A0.n;
   cudaStream_t s = h->stream;
-  for (double **p : {&h->r, &h->v, &h->w, &h->d, &h->q, &h->b, &h->xs, &h->xadd, &h->xk,
-                     &h->tmp})
+  for (double **p : {&h->r, &h->v, &h->w, &h->d, &h->q, &h->b, &h->xs, &h->tmp})
     BCMG_TRY(dev_alloc(p, n, s));
   BCMG_TRY(dev_alloc(&h->partials, 4 * kRedBlocks, s));
   BCMG_TRY(dev_alloc(&h->scal, kNumScal, s));
+  BCMG_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->host_scal),
+                           sizeof(double) * kNumScal));
   BCMG_CUDA(cudaMemsetAsync(h->scal, 0, sizeof(double) * kNumScal, s));
   return BCMG_OK;
 }
@@ -357,7 +480,7 @@ bcmg_status bootstrap(bcmg_handle *h) {
     st = adaptive_coarsening(h, w, h->H.back());
     if (st != BCMG_OK) break;
     ++num_hrc;
-    st = size_buffers(h);
+    st = size_buffers_t<double>(h, h->c64);
     if (st != BCMG_OK) break;
     if (num_hrc > 1) {
       st = inner_iterations(h, w);
@@ -372,19 +495,15 @@ void destroy_handle(bcmg_handle *h) {
   if (!h) return;
   cudaSetDevice(h->device);
   cudaStream_t s = h->stream;
+  if (h->fcg_exec) cudaGraphExecDestroy(h->fcg_exec);
+  if (h->host_scal) cudaFreeHost(h->host_scal);
   for (auto &H : h->H) H.release(s);
   h->A0.own_A = true;
   h->A0.release(s);
-  for (size_t l = 0; l < h->xt.size(); ++l) {
-    if (l > 0) {
-      dev_free(h->rhs[l], s);
-      dev_free(h->x[l], s);
-    }
-    dev_free(h->xt[l], s);
-    dev_free(h->res[l], s);
-  }
-  for (double **p : {&h->r, &h->v, &h->w, &h->d, &h->q, &h->b, &h->xs, &h->xadd, &h->xk,
-                     &h->tmp, &h->partials, &h->scal})
+  free_buffers_t<double>(h->c64, s);
+  free_buffers_t<float>(h->c32, s);
+  for (double **p : {&h->r, &h->v, &h->w, &h->d, &h->q, &h->b, &h->xs, &h->tmp,
+                     &h->partials, &h->scal})
     dev_free(*p, s);
   cudaStreamSynchronize(s);
   if (h->own_stream) cudaStreamDestroy(s);
@@ -407,6 +526,8 @@ bcmg_status setup_common(bcmg_handle *h) {
   }
   BCMG_TRY(alloc_work(h));
   BCMG_TRY(bootstrap(h));
+  h->mixed = h->ext.precision == BCMG_PREC_MIXED;
+  if (h->mixed) BCMG_TRY(prepare_mixed(h));
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
   h->setup_ms = ms_since(t0);
   return BCMG_OK;
@@ -426,9 +547,81 @@ bcmg_status new_handle(const bcmg_params *p, const bcmg_ext *ext, bcmg_handle **
     return set_error(BCMG_ERR_PARAM, "unknown precision mode %d", h->ext.precision);
   h->device = h->ext.device;
   BCMG_CUDA(cudaSetDevice(h->device));
-  BCMG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  h->own_stream = true;
+  if (h->ext.stream) {
+    h->stream = static_cast<cudaStream_t>(h->ext.stream);
+    h->own_stream = false;
+  } else {
+    BCMG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
   *out = h.release();
+  return BCMG_OK;
+}
+
+// One FCG iteration (the body of the do-while, src/SOLVER/FCG.cu:497-565)
+// on fixed buffers: z = v, Az = w, previous direction d, Ad = q.
+bcmg_status fcg_iteration(bcmg_handle *h, cudaGraphConditionalHandle cond, bool use_cond) {
+  cudaStream_t s = h->stream;
+  const CsrView A = h->A0.view();
+  BCMG_TRY(precond_apply(h, h->r, h->v, true, h->mixed));
+  BCMG_TRY(fcg_spmv_dots(A, h->v, h->w, h->r, h->q, h->partials, h->scal, s));
+  BCMG_TRY(fcg_scalars(h->partials, h->scal, false, s));
+  BCMG_TRY(fcg_update(A.n, false, h->v, h->d, h->w, h->q, h->xs, h->r, h->partials, h->scal,
+                      s));
+  if (h->ext.replace_every > 0)
+    BCMG_TRY(fcg_replace(A, h->b, h->xs, h->r, h->partials, h->scal, h->ext.replace_every, s));
+  BCMG_TRY(fcg_continue(h->scal, cond, use_cond, s));
+  return BCMG_OK;
+}
+
+// Captures the FCG loop once per handle: a graph whose WHILE node repeats one
+// iteration until the device-side condition (k_fcg_continue) turns false,
+// so a whole solve needs no host round trip per iteration.
+bcmg_status build_fcg_graph(bcmg_handle *h) {
+  cudaGraph_t g = nullptr;
+  BCMG_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle cond;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_error(BCMG_ERR_CUDA, "conditional handle: %s", cudaGetErrorString(e));
+  }
+  // cudaGraphNodeParams has no default constructor (it holds a union); use
+  // zeroed storage as the CUDA samples do with their C-style initializers.
+  alignas(cudaGraphNodeParams) unsigned char np_storage[sizeof(cudaGraphNodeParams)];
+  std::memset(np_storage, 0, sizeof(np_storage));
+  cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_storage);
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_error(BCMG_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
+  }
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_error(BCMG_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+  }
+  bcmg_status st = fcg_iteration(h, cond, true);
+  e = cudaStreamEndCapture(h->stream, &body);
+  if (st != BCMG_OK || e != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return st != BCMG_OK ? st
+                         : set_error(BCMG_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+  }
+  e = cudaGraphInstantiate(&h->fcg_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->fcg_exec = nullptr;
+    return set_error(BCMG_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+  }
   return BCMG_OK;
 }
 
@@ -455,53 +648,57 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
     info->rel_residual = 0.0;
     return BCMG_OK;
   }
-  BCMG_CUDA(cudaMemsetAsync(h->scal, 0, sizeof(double) * kNumScal, s));
-  // First step (FCG.cu:464-495).
-  BCMG_TRY(precond_apply(h, r, v, true));
+  const double target = h->prm.rtol * delta0;
+  double init[kNumScal] = {0};
+  init[kTarget] = target;
+  init[kItnlim] = h->prm.itnlim;
+  init[kDelta0] = delta0;
+  init[kBnorm] = bnorm;
+  BCMG_CUDA(cudaMemcpyAsync(h->scal, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  // First step (FCG.cu:464-495): v = B r; w = A v; x += theta v; r -= theta w;
+  // d = v; q = w.
+  BCMG_TRY(precond_apply(h, r, v, true, h->mixed));
   BCMG_TRY(fcg_spmv_dots(A, v, w, r, nullptr, h->partials, h->scal, s));
   BCMG_TRY(fcg_scalars(h->partials, h->scal, true, s));
-  BCMG_TRY(fcg_update(n, true, v, nullptr, w, nullptr, x, r, h->partials, h->scal, s));
-  BCMG_TRY(copy(d, v, n, s));
-  BCMG_TRY(copy(q, w, n, s));
-  double l2 = 0;
-  int iter = 0;
-  const double target = h->prm.rtol * delta0;
-  double hs[kNumScal];
-  bcmg_status st = BCMG_OK;
-  do {
-    const bool even = (iter % 2) == 0;
-    double *z = even ? v : d, *az = even ? w : q;
-    const double *zp = even ? d : v, *azp = even ? q : w;
-    BCMG_TRY(precond_apply(h, r, z, true));
-    BCMG_TRY(fcg_spmv_dots(A, z, az, r, azp, h->partials, h->scal, s));
-    BCMG_TRY(fcg_scalars(h->partials, h->scal, false, s));
-    BCMG_TRY(fcg_update(n, false, z, zp, az, azp, x, r, h->partials, h->scal, s));
-    BCMG_CUDA(cudaMemcpyAsync(hs, h->scal, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  BCMG_TRY(fcg_update(n, true, v, d, w, q, x, r, h->partials, h->scal, s));
+  double *hs = h->host_scal;
+  const bool graphs = h->ext.use_graphs && h->ext.verbose < 2 && h->stream != nullptr;
+  if (graphs && !h->fcg_exec && build_fcg_graph(h) != BCMG_OK) {
+    clear_error();
+    h->fcg_exec = nullptr;
+  }
+  if (graphs && h->fcg_exec) {
+    BCMG_CUDA(cudaGraphLaunch(h->fcg_exec, s));
+    BCMG_CUDA(cudaMemcpyAsync(hs, h->scal, sizeof(double) * kNumScal, cudaMemcpyDeviceToHost,
+                              s));
     BCMG_CUDA(cudaStreamSynchronize(s));
-    l2 = hs[kNorm];
-    ++iter;
-    if (hs[kIndef] != 0.0) {
-      st = set_error(BCMG_ERR_INDEFINITE,
-                     "FCG met non-positive curvature at iteration %d (A not SPD?)", iter);
-      break;
-    }
-    if (h->ext.verbose > 1)
-      printf("bootpcg iteration: %d  residual: %e relative residual: %e\n", iter - 1, l2,
-             l2 / delta0);
-  } while (l2 > target && iter < h->prm.itnlim);
+  } else {
+    do {
+      BCMG_TRY(fcg_iteration(h, 0, false));
+      BCMG_CUDA(cudaMemcpyAsync(hs, h->scal, sizeof(double) * kNumScal,
+                                cudaMemcpyDeviceToHost, s));
+      BCMG_CUDA(cudaStreamSynchronize(s));
+      if (h->ext.verbose > 1)
+        printf("bootpcg iteration: %d  residual: %e relative residual: %e\n",
+               static_cast<int>(hs[kIter]) - 1, hs[kNorm], hs[kNorm] / delta0);
+    } while (hs[kNorm] > target && hs[kIter] < h->prm.itnlim && hs[kIndef] == 0.0);
+  }
+  const double l2 = hs[kNorm];
+  const int iter = static_cast<int>(hs[kIter]);
   info->iters = iter + 1;  // FCG.cu:569
   info->residual = l2;
   info->rel_residual = l2 / delta0;
   info->converged = l2 <= target ? 1 : 0;
+  if (hs[kIndef] != 0.0)
+    return set_error(BCMG_ERR_INDEFINITE,
+                     "FCG met non-positive curvature at iteration %d (A not SPD?)", iter);
   // True residual in FP64: ||b - A x|| / ||b - A x0||.
-  if (st == BCMG_OK) {
-    BCMG_TRY(copy(h->tmp, b, n, s));
-    BCMG_TRY(spmv(A, -1.0, x, 1.0, h->tmp, s));
-    double tr = 0;
-    BCMG_TRY(norm2(h, h->tmp, &tr));
-    info->true_rel_residual = tr / delta0;
-  }
-  return st;
+  BCMG_TRY(copy(h->tmp, b, n, s));
+  BCMG_TRY(spmv(A, -1.0, x, 1.0, h->tmp, s));
+  double tr = 0;
+  BCMG_TRY(norm2(h, h->tmp, &tr));
+  info->true_rel_residual = tr / delta0;
+  return BCMG_OK;
 }
 
 }  // namespace
@@ -599,6 +796,10 @@ bcmg_status bcmg_solve_legacy(const bcmg_csr *A, const bcmg_params *p, const bcm
   return st;
 }
 
+unsigned long long bcmg_kernel_launches(void) {
+  return g_kernel_launches.load(std::memory_order_relaxed);
+}
+
 bcmg_status bcmg_destroy(bcmg_handle *h) {
   destroy_handle(h);
   return BCMG_OK;
@@ -617,7 +818,7 @@ bcmg_status bcmg_set_stream(bcmg_handle *h, void *stream) {
 bcmg_status bcmg_precond_apply(bcmg_handle *h, const double *d_r, double *d_z) {
   if (!h || !d_r || !d_z) return set_error(BCMG_ERR_PARAM, "null argument");
   BCMG_CUDA(cudaSetDevice(h->device));
-  BCMG_TRY(precond_apply(h, d_r, d_z, false));
+  BCMG_TRY(precond_apply(h, d_r, d_z, false, h->mixed));
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
   return BCMG_OK;
 }
@@ -750,8 +951,7 @@ bcmg_status bcmg_k_relax(int32_t n, int32_t nnz, const int32_t *d_row, const int
   A.val = d_val;
   DevBuf<double> tmp;
   BCMG_TRY(tmp.alloc(n, s));
-  double *res = nullptr;
-  BCMG_TRY(relax(A, d_d, d_f, d_u, tmp.get(), k, false, &res, s));
+  BCMG_TRY(relax_t<double>(mat_f64(A), d_d, d_f, d_u, tmp.get(), k, false, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
   return BCMG_OK;
 }

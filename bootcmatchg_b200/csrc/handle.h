@@ -13,7 +13,8 @@ namespace bcmg {
 
 // One level of a hierarchy on the device.  P (to the next level) has one
 // entry per fine row: column agg[i], value p[i]; R = P^T is stored as the
-// aggregates' member lists in ascending order (rptr, ridx).
+// aggregates' member lists in ascending order (rptr, ridx).  The mixed
+// precision cycle reads the low-precision copies (val_lo, D32, M32, p32).
 struct DevLevel {
   int32_t n = 0, nnz = 0;
   int32_t *row = nullptr, *col = nullptr;
@@ -23,6 +24,10 @@ struct DevLevel {
   int32_t nc = 0;
   int32_t *agg = nullptr, *rptr = nullptr, *ridx = nullptr;
   double *p = nullptr;
+  void *val_lo = nullptr;
+  int vtype_lo = kValF32;
+  bool own_lo = true;
+  float *D32 = nullptr, *M32 = nullptr, *p32 = nullptr;
   CsrView view() const {
     CsrView v;
     v.n = n;
@@ -44,6 +49,16 @@ struct DevHierarchy {
   }
 };
 
+// Cycle work vectors of one precision, per level, sized by the largest
+// hierarchy.  rhs[0]/x[0] are bound to the caller's vectors during an
+// application; in0/out0 hold the FP32 images of the FP64 FCG vectors.
+template <typename XT>
+struct CycleBufs {
+  std::vector<XT *> rhs, x, xt, res;
+  std::vector<int32_t> n;
+  XT *xk = nullptr, *xadd = nullptr, *in0 = nullptr, *out0 = nullptr;
+};
+
 }  // namespace bcmg
 
 struct bcmg_handle {
@@ -57,13 +72,14 @@ struct bcmg_handle {
   double estimated_ratio = 1.0;
   int32_t maxcoarsesize = 0;
   std::vector<int> grid_sweeps;
-  // Cycle work vectors per level (index 0 is bound to the caller's vectors
-  // during an application, except xt/res which are owned).
-  std::vector<double *> rhs, x, xt, res;
-  std::vector<int32_t> buf_n;
+  bool mixed = false;  // solve with the FP32 cycle
+  bcmg::CycleBufs<double> c64;
+  bcmg::CycleBufs<float> c32;
   // FCG vectors and device scalars.
   double *r = nullptr, *v = nullptr, *w = nullptr, *d = nullptr, *q = nullptr;
-  double *b = nullptr, *xs = nullptr, *xadd = nullptr, *xk = nullptr, *tmp = nullptr;
+  double *b = nullptr, *xs = nullptr, *tmp = nullptr;
   double *partials = nullptr, *scal = nullptr;
+  double *host_scal = nullptr;          // pinned mirror of scal
+  cudaGraphExec_t fcg_exec = nullptr;   // captured FCG loop (WHILE node)
   double setup_ms = 0.0;
 };

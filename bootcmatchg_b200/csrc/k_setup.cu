@@ -569,8 +569,8 @@ bcmg_status launch_weights(const CsrView &A, const double *w, const double *C,
                            unsigned long long *min_bits, double *W, cudaStream_t s) {
   const int threads = 256;
   const int blocks = ceil_div(static_cast<int64_t>(A.n) * G, threads);
-  k_ah_min<G><<<blocks, threads, 0, s>>>(A.n, A.row, A.col, A.val, w, C, min_bits);
-  k_make_W<G><<<blocks, threads, 0, s>>>(A.n, A.row, A.col, A.val, w, C, min_bits, W);
+  launch(k_ah_min<G>, blocks, threads, 0, s, A.n, A.row, A.col, A.val, w, C, min_bits);
+  launch(k_make_W<G>, blocks, threads, 0, s, A.n, A.row, A.col, A.val, w, C, min_bits, W);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -580,7 +580,7 @@ void launch_suitor(const CsrView &A, const double *W, unsigned long long *offer,
                    int64_t limit, int *err, cudaStream_t s) {
   const int threads = 256;
   const int blocks = ceil_div(static_cast<int64_t>(A.n) * G, threads);
-  k_suitor<G><<<blocks, threads, 0, s>>>(A.n, A.row, A.col, W, offer, limit, err);
+  launch(k_suitor<G>, blocks, threads, 0, s, A.n, A.row, A.col, W, offer, limit, err);
 }
 
 }  // namespace
@@ -588,7 +588,7 @@ void launch_suitor(const CsrView &A, const double *W, unsigned long long *offer,
 // ---------------------------------------------------------------------------
 bcmg_status level_prep(const CsrView &A, double *D, double *M, cudaStream_t s) {
   if (A.n <= 0) return BCMG_OK;
-  k_level_prep<<<ceil_div(A.n, 256), 256, 0, s>>>(A.n, A.row, A.col, A.val, D, M);
+  launch(k_level_prep, ceil_div(A.n, 256), 256, 0, s, A.n, A.row, A.col, A.val, D, M);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -628,7 +628,7 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   BCMG_TRY(err.alloc(1, s));
 
   // Weights.
-  k_make_C<<<nb, T, 0, s>>>(n, A.row, A.col, A.val, w, C.get());
+  launch(k_make_C, nb, T, 0, s, n, A.row, A.col, A.val, w, C.get());
   const unsigned long long dbl_max_bits = 0x7FEFFFFFFFFFFFFFull;
   BCMG_CUDA(cudaMemcpyAsync(minb.get(), &dbl_max_bits, sizeof(dbl_max_bits),
                             cudaMemcpyHostToDevice, s));
@@ -652,21 +652,21 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
     default: launch_suitor<32>(A, W, offer.get(), limit, err.get(), s); break;
   }
   BCMG_LAUNCH_CHECK();
-  k_offer_to_suitor<<<nb, T, 0, s>>>(n, offer.get(), sv.get());
+  launch(k_offer_to_suitor, nb, T, 0, s, n, offer.get(), sv.get());
 
   // unsymFix.
-  k_sym_pairs<<<nb, T, 0, s>>>(n, sv.get(), mv.get());
+  launch(k_sym_pairs, nb, T, 0, s, n, sv.get(), mv.get());
   BCMG_CUDA(cudaMemsetAsync(tgt.get(), 0, sizeof(int32_t) * n, s));
-  k_unsym_targets<<<nb, T, 0, s>>>(n, sv.get(), mv.get(), tgt.get());
+  launch(k_unsym_targets, nb, T, 0, s, n, sv.get(), mv.get(), tgt.get());
   BCMG_CUDA(cudaMemcpyAsync(m2.get(), mv.get(), sizeof(int32_t) * n,
                             cudaMemcpyDeviceToDevice, s));
-  k_unsym_pairs<<<nb, T, 0, s>>>(n, sv.get(), mv.get(), tgt.get(), m2.get());
+  launch(k_unsym_pairs, nb, T, 0, s, n, sv.get(), mv.get(), tgt.get(), m2.get());
 
   // Aggregation and canonical numbering.
-  k_agg_flags<<<nb, T, 0, s>>>(n, m2.get(), w, master.get(), p);
+  launch(k_agg_flags, nb, T, 0, s, n, m2.get(), w, master.get(), p);
   BCMG_LAUNCH_CHECK();
   BCMG_TRY(exclusive_scan(master.get(), rank.get(), n, total.get(), tmp.get(), s));
-  k_agg_assign<<<nb, T, 0, s>>>(n, m2.get(), master.get(), rank.get(), agg);
+  launch(k_agg_assign, nb, T, 0, s, n, m2.get(), master.get(), rank.get(), agg);
   BCMG_LAUNCH_CHECK();
   if (s_out)
     BCMG_CUDA(cudaMemcpyAsync(s_out, sv.get(), sizeof(int32_t) * n,
@@ -698,11 +698,11 @@ bcmg_status transpose_agg(int32_t n, const int32_t *agg, int32_t nc, int32_t *rp
   BCMG_CUDA(cudaMemsetAsync(rptr, 0, sizeof(int32_t) * (nc + 1), s));
   BCMG_CUDA(cudaMemsetAsync(cursor.get(), 0, sizeof(int32_t) * nc, s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
-  k_count_agg<<<ceil_div(n, 256), 256, 0, s>>>(n, agg, nc, rptr, err.get());
+  launch(k_count_agg, ceil_div(n, 256), 256, 0, s, n, agg, nc, rptr, err.get());
   BCMG_LAUNCH_CHECK();
   BCMG_TRY(exclusive_scan(rptr, rptr, nc, rptr + nc, tmp.get(), s));
-  k_fill_agg<<<ceil_div(n, 256), 256, 0, s>>>(n, agg, nc, rptr, cursor.get(), ridx);
-  k_sort_segments<<<ceil_div(nc, 256), 256, 0, s>>>(nc, rptr, ridx);
+  launch(k_fill_agg, ceil_div(n, 256), 256, 0, s, n, agg, nc, rptr, cursor.get(), ridx);
+  launch(k_sort_segments, ceil_div(nc, 256), 256, 0, s, nc, rptr, ridx);
   BCMG_LAUNCH_CHECK();
   int h_err = 0;
   BCMG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -741,17 +741,17 @@ bcmg_status galerkin_pass(bool fill, const CsrView &A, const int32_t *agg,
   // The count pass queues the long rows; the fill pass recomputes the queue
   // the same way by running the count kernel's gather check again.
   if (!fill) {
-    k_gal_warp<false><<<blocks, kGalWarpsPerBlock * 32, smem_warp, s>>>(
+    launch(k_gal_warp<false>, blocks, kGalWarpsPerBlock * 32, smem_warp, s, 
         nc, A.row, A.col, A.val, agg, p, rptr, ridx, crow, nullptr, nullptr,
         long_rows.get(), n_long.get(), err.get());
   } else {
     // Re-detect long rows without touching crow: count into a scratch array.
     DevBuf<int32_t> scratch;
     BCMG_TRY(scratch.alloc(nc, s));
-    k_gal_warp<false><<<blocks, kGalWarpsPerBlock * 32, smem_warp, s>>>(
+    launch(k_gal_warp<false>, blocks, kGalWarpsPerBlock * 32, smem_warp, s, 
         nc, A.row, A.col, A.val, agg, p, rptr, ridx, scratch.get(), nullptr, nullptr,
         long_rows.get(), n_long.get(), err.get());
-    k_gal_warp<true><<<blocks, kGalWarpsPerBlock * 32, smem_warp, s>>>(
+    launch(k_gal_warp<true>, blocks, kGalWarpsPerBlock * 32, smem_warp, s, 
         nc, A.row, A.col, A.val, agg, p, rptr, ridx, crow, ccol, cval, long_rows.get(),
         n_long.get(), err.get());
   }
@@ -761,11 +761,11 @@ bcmg_status galerkin_pass(bool fill, const CsrView &A, const int32_t *agg,
   BCMG_CUDA(cudaStreamSynchronize(s));
   if (h_long > 0) {
     if (!fill)
-      k_gal_long<false><<<h_long, kGalLongThreads, smem_long, s>>>(
+      launch(k_gal_long<false>, h_long, kGalLongThreads, smem_long, s, 
           long_rows.get(), A.row, A.col, A.val, agg, p, rptr, ridx, crow, nullptr,
           nullptr, err.get());
     else
-      k_gal_long<true><<<h_long, kGalLongThreads, smem_long, s>>>(
+      launch(k_gal_long<true>, h_long, kGalLongThreads, smem_long, s, 
           long_rows.get(), A.row, A.col, A.val, agg, p, rptr, ridx, crow, ccol, cval,
           err.get());
     BCMG_LAUNCH_CHECK();
@@ -805,7 +805,7 @@ bcmg_status galerkin_fill(const CsrView &A, const int32_t *agg, const double *p,
 bcmg_status restrict_exact(int32_t nc, const int32_t *rptr, const int32_t *ridx,
                            const double *p, const double *x, double *y, cudaStream_t s) {
   if (nc <= 0) return BCMG_OK;
-  k_restrict_exact<<<ceil_div(nc, 256), 256, 0, s>>>(nc, rptr, ridx, p, x, y);
+  launch(k_restrict_exact, ceil_div(nc, 256), 256, 0, s, nc, rptr, ridx, p, x, y);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -813,7 +813,7 @@ bcmg_status restrict_exact(int32_t nc, const int32_t *rptr, const int32_t *ridx,
 bcmg_status compose_p(int32_t n, int32_t *agg, double *p, const int32_t *agg2,
                       const double *p2, cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
-  k_compose<<<ceil_div(n, 256), 256, 0, s>>>(n, agg, p, agg2, p2);
+  launch(k_compose, ceil_div(n, 256), 256, 0, s, n, agg, p, agg2, p2);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }

@@ -1,5 +1,4 @@
-// Solve-phase kernels in FP64: Jacobi / l1-Jacobi sweeps, SpMV, residual,
-// restriction, prolongation and the fused FCG reductions.  All reductions
+// FCG kernels in FP64: SpMV, dot products and the fused FCG reductions.  All reductions
 // are deterministic: fixed grids, fixed thread-to-row mapping and a
 // fixed-order final reduction replace the reference's FP64 atomics
 // (_triple_innerproduct, src/SOLVER/FCG.cu:6-63) and cuBLAS calls
@@ -36,29 +35,6 @@ __device__ __forceinline__ double row_dot(const int32_t *__restrict__ row,
   return group_sum<G>(t);
 }
 
-// One sweep u_out = ((-(A u) + f) ./ d) + u  (_jacobi_it<0,MW>,
-// src/AMG/relaxation.cu:176-209).
-template <int G>
-__global__ void __launch_bounds__(kThreads)
-    k_relax(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
-            const double *__restrict__ val, const double *__restrict__ d,
-            const double *__restrict__ f, const double *__restrict__ u,
-            double *__restrict__ u_out) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  int32_t i = static_cast<int32_t>(t / G);
-  const int lane = threadIdx.x % G;
-  if (i >= n) i = -1;
-  const double T = row_dot<G>(row, col, val, u, i, lane);
-  if (i >= 0 && lane == 0) u_out[i] = ((-T + f[i]) / d[i]) + u[i];
-}
-
-// First sweep from u = 0: ((-0 + f) ./ d) + 0 = f ./ d.
-__global__ void k_relax_zero(int32_t n, const double *__restrict__ d,
-                             const double *__restrict__ f, double *__restrict__ u_out) {
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) u_out[i] = f[i] / d[i];
-}
-
 template <int G>
 __global__ void __launch_bounds__(kThreads)
     k_spmv(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
@@ -70,59 +46,6 @@ __global__ void __launch_bounds__(kThreads)
   if (i >= n) i = -1;
   const double T = row_dot<G>(row, col, val, x, i, lane);
   if (i >= 0 && lane == 0) y[i] = (beta == 0.0) ? alpha * T : fma(alpha, T, beta * y[i]);
-}
-
-template <int G>
-__global__ void __launch_bounds__(kThreads)
-    k_residual(int32_t n, const int32_t *__restrict__ row,
-               const int32_t *__restrict__ col, const double *__restrict__ val,
-               const double *__restrict__ f, const double *__restrict__ u,
-               double *__restrict__ res) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  int32_t i = static_cast<int32_t>(t / G);
-  const int lane = threadIdx.x % G;
-  if (i >= n) i = -1;
-  const double T = row_dot<G>(row, col, val, u, i, lane);
-  if (i >= 0 && lane == 0) res[i] = f[i] - T;
-}
-
-__global__ void k_restrict(int32_t nc, const int32_t *__restrict__ rptr,
-                           const int32_t *__restrict__ ridx, const double *__restrict__ p,
-                           const double *__restrict__ x, double *__restrict__ y) {
-  const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= nc) return;
-  double s = 0.0;
-  for (int32_t k = rptr[I]; k < rptr[I + 1]; ++k) {
-    const int32_t i = ridx[k];
-    s = fma(p[i], x[i], s);
-  }
-  y[I] = s;
-}
-
-__global__ void k_prolong(int32_t n, const int32_t *__restrict__ agg,
-                          const double *__restrict__ p, const double *__restrict__ xc,
-                          double *__restrict__ xf) {
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) xf[i] = fma(p[i], xc[agg[i]], xf[i]);
-}
-
-__global__ void k_fill(double *x, int64_t n, double v) {
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    x[i] = v;
-}
-
-__global__ void k_axpy(int64_t n, double a, const double *__restrict__ x,
-                       double *__restrict__ y) {
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    y[i] = fma(a, x[i], y[i]);
-}
-
-__global__ void k_scale(int64_t n, double a, double *x) {
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    x[i] = x[i] * a;
 }
 
 // Block sum of NV doubles per thread into partials[blockIdx.x * 4 + k].
@@ -229,14 +152,16 @@ __global__ void k_fcg_scalars(const double *partials, double *scal, int first) {
   }
 }
 
-// first:  x += theta v; r -= theta w                        (FCG.cu:481-484)
-// loop:   z = -theta zp + z; x += theta2 z;                 (_double_merged_axpy,
-//         az = -theta azp + az; r -= theta2 az               FCG.cu:88-98,536-556)
-// plus the partial sums of r.r for ||r||.
+// first:  x += theta z; r -= theta az; zp = z; azp = az     (FCG.cu:481-495)
+// loop:   zp = -theta zp + z; x += theta2 zp;               (_double_merged_axpy,
+//         azp = -theta azp + az; r -= theta2 azp             FCG.cu:88-98,536-556)
+// plus the partial sums of r.r for ||r||.  The new direction overwrites the
+// previous one in (zp, azp), so every iteration uses the same buffers (the
+// reference alternates (v,w) and (d,q) instead, FCG.cu:499-556).
 __global__ void __launch_bounds__(kThreads)
-    k_fcg_update(int64_t n, int first, double *__restrict__ z,
-                 const double *__restrict__ zp, double *__restrict__ az,
-                 const double *__restrict__ azp, double *__restrict__ x,
+    k_fcg_update(int64_t n, int first, const double *__restrict__ z,
+                 double *__restrict__ zp, const double *__restrict__ az,
+                 double *__restrict__ azp, double *__restrict__ x,
                  double *__restrict__ r, const double *__restrict__ scal,
                  double *partials) {
   double acc[1] = {0.0};
@@ -248,9 +173,9 @@ __global__ void __launch_bounds__(kThreads)
     if (!first) {
       zi = fma(-theta, zp[i], zi);
       ai = fma(-theta, azp[i], ai);
-      z[i] = zi;
-      az[i] = ai;
     }
+    zp[i] = zi;
+    azp[i] = ai;
     x[i] = fma(theta2, zi, x[i]);
     const double ri = fma(-theta2, ai, r[i]);
     r[i] = ri;
@@ -264,8 +189,58 @@ __global__ void k_norm_final(const double *partials, double *scal) {
   if (threadIdx.x == 0) scal[kNorm] = sqrt(s);
 }
 
-template <template <int> class K>
-struct Dispatch;
+// End of one FCG iteration: count it and decide whether the do-while of
+// FCG.cu:497-565 continues (||r|| > rtol delta0 and iter < itnlim and no
+// breakdown).  Inside a graph the decision drives the WHILE node.
+__global__ void k_fcg_continue(double *scal, cudaGraphConditionalHandle cond, int use_cond) {
+  const double iter = scal[kIter] + 1.0;
+  scal[kIter] = iter;
+  const bool go = scal[kNorm] > scal[kTarget] && iter < scal[kItnlim] && scal[kIndef] == 0.0;
+  if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
+}
+
+
+// Residual replacement (mixed precision): after iteration i the recursive
+// residual is replaced by the true one r = b - A x in FP64 when i is a
+// multiple of `every` or when the recursive norm has reached the target, so
+// convergence is always decided on the true residual.
+__global__ void k_replace_flag(double *scal, int every) {
+  const int i = static_cast<int>(scal[kIter]) + 1;
+  const bool due = (every > 0 && i % every == 0) || scal[kNorm] <= scal[kTarget];
+  scal[kReplace] = due ? 1.0 : 0.0;
+}
+
+template <int G>
+__global__ void __launch_bounds__(kThreads)
+    k_true_residual(int32_t n, const int32_t *__restrict__ row,
+                    const int32_t *__restrict__ col, const double *__restrict__ val,
+                    const double *__restrict__ b, const double *__restrict__ x,
+                    double *__restrict__ r, const double *__restrict__ scal,
+                    double *partials) {
+  if (scal[kReplace] == 0.0) return;
+  double acc[1] = {0.0};
+  const int lane = threadIdx.x % G;
+  const int64_t groups = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
+  const int64_t g0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G;
+  const int64_t rounds = (n + groups - 1) / groups;
+  for (int64_t rd = 0; rd < rounds; ++rd) {
+    const int64_t gi = g0 + rd * groups;
+    const int32_t i = gi < n ? static_cast<int32_t>(gi) : -1;
+    const double T = row_dot<G>(row, col, val, x, i, lane);
+    if (i >= 0 && lane == 0) {
+      const double ri = b[i] - T;
+      r[i] = ri;
+      acc[0] = fma(ri, ri, acc[0]);
+    }
+  }
+  block_partials<1>(acc, partials);
+}
+
+__global__ void k_norm_final_if(const double *partials, double *scal) {
+  if (scal[kReplace] == 0.0) return;
+  const double s = reduce_partials(partials, 0);
+  if (threadIdx.x == 0) scal[kNorm] = sqrt(s);
+}
 
 inline int grid_for(int64_t work) {
   const int64_t b = (work + kThreads - 1) / kThreads;
@@ -274,47 +249,6 @@ inline int grid_for(int64_t work) {
 
 }  // namespace
 
-bcmg_status relax(const CsrView &A, const double *d, const double *f, double *u,
-                  double *u_tmp, int k, bool zero_start, double **result, cudaStream_t s) {
-  *result = u;
-  const int32_t n = A.n;
-  if (n <= 0) return BCMG_OK;
-  if (k <= 0) {
-    if (zero_start) BCMG_TRY(fill(u, n, 0.0, s));
-    return BCMG_OK;
-  }
-  const int G = group_for(A.nnz, n);
-  const int blocks = grid_for(static_cast<int64_t>(n) * G);
-  auto sweep = [&](const double *src, double *dst) {
-    switch (G) {
-      case 4: k_relax<4><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, d, f, src, dst); break;
-      case 8: k_relax<8><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, d, f, src, dst); break;
-      case 16: k_relax<16><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, d, f, src, dst); break;
-      default: k_relax<32><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, d, f, src, dst); break;
-    }
-  };
-  // Arrange the ping-pong so the final iterate lands in u.
-  double *cur;
-  int left = k;
-  if (zero_start) {
-    cur = (k % 2 == 1) ? u : u_tmp;
-    k_relax_zero<<<ceil_div(n, kThreads), kThreads, 0, s>>>(n, d, f, cur);
-    --left;
-  } else if (k % 2 == 1) {
-    BCMG_CUDA(cudaMemcpyAsync(u_tmp, u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    cur = u_tmp;
-  } else {
-    cur = u;
-  }
-  for (; left > 0; --left) {
-    double *dst = (cur == u) ? u_tmp : u;
-    sweep(cur, dst);
-    cur = dst;
-  }
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
-}
-
 bcmg_status spmv(const CsrView &A, double alpha, const double *x, double beta, double *y,
                  cudaStream_t s) {
   const int32_t n = A.n;
@@ -322,81 +256,19 @@ bcmg_status spmv(const CsrView &A, double alpha, const double *x, double beta, d
   const int G = group_for(A.nnz, n);
   const int blocks = grid_for(static_cast<int64_t>(n) * G);
   switch (G) {
-    case 4: k_spmv<4><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, alpha, x, beta, y); break;
-    case 8: k_spmv<8><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, alpha, x, beta, y); break;
-    case 16: k_spmv<16><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, alpha, x, beta, y); break;
-    default: k_spmv<32><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, alpha, x, beta, y); break;
+    case 4: launch(k_spmv<4>, blocks, kThreads, 0, s, n, A.row, A.col, A.val, alpha, x, beta, y); break;
+    case 8: launch(k_spmv<8>, blocks, kThreads, 0, s, n, A.row, A.col, A.val, alpha, x, beta, y); break;
+    case 16: launch(k_spmv<16>, blocks, kThreads, 0, s, n, A.row, A.col, A.val, alpha, x, beta, y); break;
+    default: launch(k_spmv<32>, blocks, kThreads, 0, s, n, A.row, A.col, A.val, alpha, x, beta, y); break;
   }
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
-}
-
-bcmg_status residual(const CsrView &A, const double *f, const double *u, double *res,
-                     cudaStream_t s) {
-  const int32_t n = A.n;
-  if (n <= 0) return BCMG_OK;
-  const int G = group_for(A.nnz, n);
-  const int blocks = grid_for(static_cast<int64_t>(n) * G);
-  switch (G) {
-    case 4: k_residual<4><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, f, u, res); break;
-    case 8: k_residual<8><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, f, u, res); break;
-    case 16: k_residual<16><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, f, u, res); break;
-    default: k_residual<32><<<blocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, f, u, res); break;
-  }
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
-}
-
-bcmg_status restrict_vec(int32_t nc, const int32_t *rptr, const int32_t *ridx,
-                         const double *p, const double *x, double *y, cudaStream_t s) {
-  if (nc <= 0) return BCMG_OK;
-  k_restrict<<<ceil_div(nc, kThreads), kThreads, 0, s>>>(nc, rptr, ridx, p, x, y);
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
-}
-
-bcmg_status prolong_add(int32_t n, const int32_t *agg, const double *p, const double *xc,
-                        double *xf, cudaStream_t s) {
-  if (n <= 0) return BCMG_OK;
-  k_prolong<<<ceil_div(n, kThreads), kThreads, 0, s>>>(n, agg, p, xc, xf);
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
-}
-
-bcmg_status fill(double *x, int64_t n, double v, cudaStream_t s) {
-  if (n <= 0) return BCMG_OK;
-  const int blocks = static_cast<int>(std::min<int64_t>(grid_for(n), 8 * kNumSM));
-  k_fill<<<blocks, kThreads, 0, s>>>(x, n, v);
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
-}
-
-bcmg_status copy(double *dst, const double *src, int64_t n, cudaStream_t s) {
-  if (n <= 0 || dst == src) return BCMG_OK;
-  BCMG_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  return BCMG_OK;
-}
-
-bcmg_status axpy(int64_t n, double alpha, const double *x, double *y, cudaStream_t s) {
-  if (n <= 0) return BCMG_OK;
-  const int blocks = static_cast<int>(std::min<int64_t>(grid_for(n), 8 * kNumSM));
-  k_axpy<<<blocks, kThreads, 0, s>>>(n, alpha, x, y);
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
-}
-
-bcmg_status scale(int64_t n, double alpha, double *x, cudaStream_t s) {
-  if (n <= 0) return BCMG_OK;
-  const int blocks = static_cast<int>(std::min<int64_t>(grid_for(n), 8 * kNumSM));
-  k_scale<<<blocks, kThreads, 0, s>>>(n, alpha, x);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
 bcmg_status dot_dev(int64_t n, const double *a, const double *b, double *out,
                     double *partials, cudaStream_t s) {
-  k_dot_partials<<<kRedBlocks, kThreads, 0, s>>>(n, a, b, partials);
-  k_dot_final<<<1, kThreads, 0, s>>>(partials, out);
+  launch(k_dot_partials, kRedBlocks, kThreads, 0, s, n, a, b, partials);
+  launch(k_dot_final, 1, kThreads, 0, s, partials, out);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -408,27 +280,49 @@ bcmg_status fcg_spmv_dots(const CsrView &A, const double *v, double *w, const do
   const int32_t n = A.n;
   const int G = group_for(A.nnz, n);
   switch (G) {
-    case 4: k_fcg_spmv_dots<4><<<kRedBlocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, v, w, r, q, partials); break;
-    case 8: k_fcg_spmv_dots<8><<<kRedBlocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, v, w, r, q, partials); break;
-    case 16: k_fcg_spmv_dots<16><<<kRedBlocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, v, w, r, q, partials); break;
-    default: k_fcg_spmv_dots<32><<<kRedBlocks, kThreads, 0, s>>>(n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    case 4: launch(k_fcg_spmv_dots<4>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    case 8: launch(k_fcg_spmv_dots<8>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    case 16: launch(k_fcg_spmv_dots<16>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    default: launch(k_fcg_spmv_dots<32>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
   }
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
 bcmg_status fcg_scalars(double *partials, double *scal, bool first, cudaStream_t s) {
-  k_fcg_scalars<<<1, kThreads, 0, s>>>(partials, scal, first ? 1 : 0);
+  launch(k_fcg_scalars, 1, kThreads, 0, s, partials, scal, first ? 1 : 0);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
-bcmg_status fcg_update(int64_t n, bool first, double *z, const double *zp, double *az,
-                       const double *azp, double *x, double *r, double *partials,
-                       double *scal, cudaStream_t s) {
-  k_fcg_update<<<kRedBlocks, kThreads, 0, s>>>(n, first ? 1 : 0, z, zp, az, azp, x, r,
+bcmg_status fcg_continue(double *scal, cudaGraphConditionalHandle cond, bool use_cond,
+                         cudaStream_t s) {
+  launch(k_fcg_continue, 1, 1, 0, s, scal, cond, use_cond ? 1 : 0);
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
+bcmg_status fcg_update(int64_t n, bool first, const double *z, double *zp,
+                       const double *az, double *azp, double *x, double *r,
+                       double *partials, double *scal, cudaStream_t s) {
+  launch(k_fcg_update, kRedBlocks, kThreads, 0, s, n, first ? 1 : 0, z, zp, az, azp, x, r,
                                                scal, partials);
-  k_norm_final<<<1, kThreads, 0, s>>>(partials, scal);
+  launch(k_norm_final, 1, kThreads, 0, s, partials, scal);
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
+bcmg_status fcg_replace(const CsrView &A, const double *b, const double *x, double *r,
+                        double *partials, double *scal, int every, cudaStream_t s) {
+  launch(k_replace_flag, 1, 1, 0, s, scal, every);
+  const int G = group_for(A.nnz, A.n);
+  switch (G) {
+    case 4: launch(k_true_residual<4>, kRedBlocks, kThreads, 0, s, A.n, A.row, A.col, A.val, b, x, r, scal, partials); break;
+    case 8: launch(k_true_residual<8>, kRedBlocks, kThreads, 0, s, A.n, A.row, A.col, A.val, b, x, r, scal, partials); break;
+    case 16: launch(k_true_residual<16>, kRedBlocks, kThreads, 0, s, A.n, A.row, A.col, A.val, b, x, r, scal, partials); break;
+    default: launch(k_true_residual<32>, kRedBlocks, kThreads, 0, s, A.n, A.row, A.col, A.val, b, x, r, scal, partials); break;
+  }
+  launch(k_norm_final_if, 1, kThreads, 0, s, partials, scal);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }

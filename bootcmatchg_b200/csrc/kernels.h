@@ -37,30 +37,71 @@ bcmg_status restrict_exact(int32_t nc, const int32_t *rptr, const int32_t *ridx,
 bcmg_status compose_p(int32_t n, int32_t *agg, double *p, const int32_t *agg2,
                       const double *p2, cudaStream_t s);
 
-// ---- solve (k_solve.cu) ----------------------------------------------------
-// k sweeps of u <- ((-(A u) + f) ./ d) + u; u_tmp is a ping-pong buffer.
-// If zero_start, u is taken as 0 on entry (first sweep is f ./ d).  Returns
-// in *result whichever of u / u_tmp holds the final iterate.
-bcmg_status relax(const CsrView &A, const double *d, const double *f, double *u,
-                  double *u_tmp, int k, bool zero_start, double **result,
-                  cudaStream_t s);
-// y = alpha A x + beta y
+// ---- cycle (k_cycle.cu) ----------------------------------------------------
+// Value storage of a level matrix used by the cycle.
+enum ValType { kValF64 = 0, kValF32 = 1, kValBF16 = 2, kValF16 = 3 };
+
+struct MatView {
+  int32_t n = 0, nnz = 0;
+  const int32_t *row = nullptr, *col = nullptr;
+  const void *val = nullptr;
+  int vtype = kValF64;
+};
+
+// k sweeps of u <- ((-(A u) + f) ./ d) + u, result in u; u_tmp is the
+// ping-pong buffer.  zero_start: u is taken as 0 (first sweep is f ./ d).
+// XT = double needs FP64 values; XT = float takes FP32 / BF16 / FP16 values.
+template <typename XT>
+bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp, int k,
+                    bool zero_start, cudaStream_t s);
+template <typename XT>  // res = f - A u
+bcmg_status residual_t(const MatView &A, const XT *f, const XT *u, XT *res, cudaStream_t s);
+template <typename XT>  // y[I] = sum_{i in I} p_i x_i
+bcmg_status restrict_t(int32_t nc, const int32_t *rptr, const int32_t *ridx, const XT *p,
+                       const XT *x, XT *y, cudaStream_t s);
+template <typename XT>  // xf[i] += p_i xc[agg_i]
+bcmg_status prolong_t(int32_t n, const int32_t *agg, const XT *p, const XT *xc, XT *xf,
+                      cudaStream_t s);
+template <typename XT>
+bcmg_status fill_t(XT *x, int64_t n, XT v, cudaStream_t s);
+template <typename XT>  // y = a x + y
+bcmg_status axpy_t(int64_t n, XT a, const XT *x, XT *y, cudaStream_t s);
+template <typename XT>
+bcmg_status scale_t(int64_t n, XT a, XT *x, cudaStream_t s);
+template <typename XT>
+bcmg_status copy_t(XT *dst, const XT *src, int64_t n, cudaStream_t s);
+bcmg_status convert_d2f(int64_t n, const double *in, float *out, cudaStream_t s);
+bcmg_status convert_f2d(int64_t n, const float *in, double *out, cudaStream_t s);
+// FP64 values to FP32 / BF16 / FP16 storage (vtype).
+bcmg_status convert_values(int64_t n, const double *in, void *out, int vtype, cudaStream_t s);
+
+inline MatView mat_f64(const CsrView &A) {
+  MatView m;
+  m.n = A.n;
+  m.nnz = A.nnz;
+  m.row = A.row;
+  m.col = A.col;
+  m.val = A.val;
+  m.vtype = kValF64;
+  return m;
+}
+inline bcmg_status fill(double *x, int64_t n, double v, cudaStream_t s) {
+  return fill_t<double>(x, n, v, s);
+}
+inline bcmg_status copy(double *dst, const double *src, int64_t n, cudaStream_t s) {
+  return copy_t<double>(dst, src, n, s);
+}
+inline bcmg_status axpy(int64_t n, double a, const double *x, double *y, cudaStream_t s) {
+  return axpy_t<double>(n, a, x, y, s);
+}
+inline bcmg_status scale(int64_t n, double a, double *x, cudaStream_t s) {
+  return scale_t<double>(n, a, x, s);
+}
+
+// ---- FCG (k_solve.cu) ------------------------------------------------------
+// y = alpha A x + beta y (FP64)
 bcmg_status spmv(const CsrView &A, double alpha, const double *x, double beta,
                  double *y, cudaStream_t s);
-// res = f - A u
-bcmg_status residual(const CsrView &A, const double *f, const double *u, double *res,
-                     cudaStream_t s);
-// y[I] = sum_{i in I} p_i x_i
-bcmg_status restrict_vec(int32_t nc, const int32_t *rptr, const int32_t *ridx,
-                         const double *p, const double *x, double *y, cudaStream_t s);
-// xf[i] += p_i xc[agg_i]
-bcmg_status prolong_add(int32_t n, const int32_t *agg, const double *p,
-                        const double *xc, double *xf, cudaStream_t s);
-bcmg_status fill(double *x, int64_t n, double v, cudaStream_t s);
-bcmg_status copy(double *dst, const double *src, int64_t n, cudaStream_t s);
-// y = alpha x + y
-bcmg_status axpy(int64_t n, double alpha, const double *x, double *y, cudaStream_t s);
-bcmg_status scale(int64_t n, double alpha, double *x, cudaStream_t s);
 
 // Deterministic FP64 reductions into device scalars.
 constexpr int kRedBlocks = 4 * 148;
@@ -75,7 +116,7 @@ bcmg_status dot_dev(int64_t n, const double *a, const double *b, double *out,
 // FCG device scalars.
 enum FcgScal {
   kAlpha = 0, kBeta, kGamma, kDelta, kTheta, kTheta2, kNorm, kDelta0,
-  kBnorm, kIndef, kNumScal
+  kBnorm, kIndef, kIter, kTarget, kItnlim, kReplace, kNumScal
 };
 // w = A v fused with alpha = r.v, beta = w.v, gamma = q.v (q may be null).
 bcmg_status fcg_spmv_dots(const CsrView &A, const double *v, double *w,
@@ -83,11 +124,19 @@ bcmg_status fcg_spmv_dots(const CsrView &A, const double *v, double *w,
                           double *scal, cudaStream_t s);
 // first==true: delta = beta, theta = alpha / delta; else FCG v3 recurrences.
 bcmg_status fcg_scalars(double *partials, double *scal, bool first, cudaStream_t s);
-// first step: x += theta v; r -= theta w; norm.
-// loop step:  z = -theta zp + z; x += theta2 z; az = -theta azp + az;
-//             r -= theta2 az; norm.
-bcmg_status fcg_update(int64_t n, bool first, double *z, const double *zp,
-                       double *az, const double *azp, double *x, double *r,
+// first step: x += theta z; r -= theta az; zp = z; azp = az; norm.
+// loop step:  zp = -theta zp + z; x += theta2 zp; azp = -theta azp + az;
+//             r -= theta2 azp; norm.
+bcmg_status fcg_update(int64_t n, bool first, const double *z, double *zp,
+                       const double *az, double *azp, double *x, double *r,
                        double *partials, double *scal, cudaStream_t s);
+// Residual replacement: if iteration kIter+1 is a multiple of `every` or the
+// recursive norm reached the target, r = b - A x and ||r|| recomputed (FP64).
+bcmg_status fcg_replace(const CsrView &A, const double *b, const double *x, double *r,
+                        double *partials, double *scal, int every, cudaStream_t s);
+// Counts the iteration and evaluates the loop condition (into the graph's
+// WHILE condition when use_cond).
+bcmg_status fcg_continue(double *scal, cudaGraphConditionalHandle cond, bool use_cond,
+                         cudaStream_t s);
 
 }  // namespace bcmg

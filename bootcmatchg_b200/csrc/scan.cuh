@@ -106,9 +106,9 @@ inline bcmg_status exclusive_scan(const int32_t *in, int32_t *out, int64_t n,
     return BCMG_OK;
   }
   const int nt = ceil_div(n, kTile);
-  tile_sums<<<nt, kBlock, 0, s>>>(in, n, tmp);
-  scan_tiles<<<1, kBlock, 0, s>>>(tmp, nt, total_dev);
-  scan_apply<<<nt, kBlock, 0, s>>>(in, n, tmp, out);
+  launch(tile_sums, nt, kBlock, 0, s, in, n, tmp);
+  launch(scan_tiles, 1, kBlock, 0, s, tmp, nt, total_dev);
+  launch(scan_apply, nt, kBlock, 0, s, in, n, tmp, out);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }

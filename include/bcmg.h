@@ -92,6 +92,8 @@ typedef struct bcmg_ext {
   int    device;          /* CUDA device ordinal                               */
   int    verbose;         /* 0 quiet, 1 #META lines, 2 per-iteration residual  */
   double max_device_seconds; /* bound on any single device loop (matching)     */
+  void  *stream;          /* cudaStream_t to run on from setup on (NULL: the
+                             handle creates its own); the caller keeps it alive */
 } bcmg_ext;
 
 /* Per-solve report.  residual is the recursive ||r||_2 that FCG returns
@@ -115,6 +117,8 @@ typedef struct bcmg_handle bcmg_handle;
 const char *bcmg_last_error(void);            /* thread-local message          */
 const char *bcmg_status_string(int status);
 const char *bcmg_version(void);
+/* Number of CUDA kernels this library has launched in this process. */
+unsigned long long bcmg_kernel_launches(void);
 
 /* ---- matrix input (replaces readMatrixFromFile, src/matrix/matrixIO.cu:4) --
  * m_type 0: Matrix Market coordinate real/integer, general or symmetric
@@ -128,8 +132,8 @@ bcmg_status bcmg_read_matrix(const char *path, int m_type, bcmg_csr *out);
 /* Matrix Market writer (CSRMatrixPrintMM, src/matrix/matrixIO.cu:292-335). */
 bcmg_status bcmg_write_matrix_mm(const char *path, const bcmg_csr *A);
 void        bcmg_csr_free(bcmg_csr *A);
-/* Validates and canonicalises a caller CSR in place (sorted columns, no
- * duplicates, diagonal present, finite values). */
+/* Validates a caller CSR: square, in-range strictly increasing columns,
+ * a diagonal entry in every row, finite values. */
 bcmg_status bcmg_csr_check(const bcmg_csr *A);
 
 /* ---- settings (replaces AMG::Params::initFromFile, src/AMG/AMG.cu:480-526) */

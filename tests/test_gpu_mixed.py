@@ -1,0 +1,76 @@
+"""GPU tests of the mixed-precision cycle and the graph-captured FCG loop.
+
+Mixed precision: FP32 cycle (level 0 FP32, coarse levels FP32/BF16/FP16),
+FP64 FCG with residual replacement.  Tolerance: the true FP64 relative
+residual at most 1.05 rtol (rtol 1e-8) and the solution within 1e-6 relative
+of the FP64 oracle's.  The hierarchy itself is built in FP64 and must stay
+bit-identical to the oracle's in every precision mode.
+"""
+import numpy as np
+import pytest
+
+import bootcmatchg_b200 as bc
+from helpers import c1_params
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("storage", [bc.STORE_FP32, bc.STORE_BF16, bc.STORE_FP16])
+@pytest.mark.parametrize("case", ["poisson27_24", "fv2d_96"])
+def test_mixed_solve_meets_fp64_tolerance(case, storage):
+    A = bc.poisson(27, 24, 24, 24) if case == "poisson27_24" else bc.fv2d(96, 96, seed=2)
+    p = c1_params()
+    b = bc.vector(1, 1, A.n)
+    ext = bc.Extensions(precision=bc.PREC_MIXED, coarse_storage=storage, replace_every=10)
+    with bc.Handle(A, p, ext) as h:
+        x, info = h.solve(b)
+        lv = h.level(0, 1)
+    o = orc.OracleHandle(A, p)
+    olv = o.level(0, 1)
+    assert np.array_equal(lv.A.val, olv["val"])  # setup stays FP64 and exact
+    xo, oi, _ = o.solve(b)
+    assert info.converged
+    r = b - A.to_scipy() @ x
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05 * p.rtol
+    assert info.true_rel_residual <= 1.05 * p.rtol
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
+    assert info.iters <= oi["iters"] + 6
+
+
+def test_mixed_bootstrap_composite():
+    A = bc.fv2d(80, 80, seed=2)
+    p = c1_params()
+    p.max_hrc, p.conv_ratio, p.solver_type = 3, 0.1, 1
+    b = bc.vector(2, 2, A.n)
+    ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=5)
+    with bc.Handle(A, p, ext) as h, bc.Handle(A, p) as h64:
+        assert h.num_hierarchies() == h64.num_hierarchies()
+        x, info = h.solve(b)
+        x64, info64 = h64.solve(b)
+    assert info.converged and info.true_rel_residual <= 1.05 * p.rtol
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-6
+
+
+@pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
+def test_graph_loop_equals_host_loop(prec):
+    A = bc.poisson(7, 20, 20, 20)
+    p = c1_params()
+    b = bc.vector(1, 4, A.n)
+    e1 = bc.Extensions(precision=prec, use_graphs=1, replace_every=7 if prec else 0)
+    e0 = bc.Extensions(precision=prec, use_graphs=0, replace_every=7 if prec else 0)
+    with bc.Handle(A, p, e1) as h1, bc.Handle(A, p, e0) as h0:
+        x1, i1 = h1.solve(b)
+        x0, i0 = h0.solve(b)
+        x1b, i1b = h1.solve(b)  # second solve reuses the captured graph
+    assert i1.iters == i0.iters == i1b.iters
+    assert np.array_equal(x1, x0) and np.array_equal(x1, x1b)
+
+
+def test_itnlim_respected():
+    A = bc.poisson(7, 16, 16, 16)
+    p = c1_params()
+    p.itnlim, p.rtol = 3, 1e-14
+    with bc.Handle(A, p) as h:
+        x, info = h.solve(np.ones(A.n))
+    assert info.iters == 4 and not info.converged  # num_iter = iter + 1
