@@ -43,7 +43,7 @@ class Ext(C.Structure):
     _fields_ = [("precision", C.c_int), ("coarse_storage", C.c_int),
                 ("replace_every", C.c_int), ("use_graphs", C.c_int), ("device", C.c_int),
                 ("verbose", C.c_int), ("max_device_seconds", C.c_double),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("sliced", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -83,6 +83,9 @@ SIGNATURES = {
                                       C.POINTER(C.c_double)]),
     "bcmg_level_info": (C.c_int, [vp, C.c_int, C.c_int, i32p, i32p, i32p]),
     "bcmg_level_copy": (C.c_int, [vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "bcmg_level_relax": (C.c_int, [vp, C.c_int, C.c_int, vp, vp, C.c_int]),
+    "bcmg_level_format": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64), i32p, i32p]),
     "bcmg_k_pair_aggregate": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i32p, vp, vp,
                                         vp, vp]),
     "bcmg_k_galerkin": (C.c_int, [i32, i32, vp, vp, vp, i32, vp, vp, vp, i32p, vp, vp,

@@ -143,6 +143,7 @@ class Extensions:
     verbose: int = 0
     max_device_seconds: float = 60.0
     stream: int = 0  # cudaStream_t as an integer (0: the handle makes its own)
+    sliced: int = 1  # solve on the sliced copies of the levels
 
     def to_c(self) -> Ext:
         e = Ext()

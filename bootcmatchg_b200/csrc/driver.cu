@@ -37,6 +37,9 @@ void DevLevel::release(cudaStream_t s) {
   dev_free(D32, s);
   dev_free(M32, s);
   dev_free(p32, s);
+  own64.release(s);
+  ownlo.release(s);
+  s64 = slo = nullptr;
 }
 
 namespace {
@@ -269,7 +272,14 @@ template <typename XT>
 struct Lv;
 template <>
 struct Lv<double> {
-  static MatView mat(const DevLevel &l) { return mat_f64(l.view()); }
+  static MatView mat(const DevLevel &l) {
+    MatView m = mat_f64(l.view());
+    if (l.s64 && l.s64->nslices) {
+      m.has_sl = true;
+      m.sl = l.s64->view();
+    }
+    return m;
+  }
   static const double *D(const DevLevel &l) { return l.D; }
   static const double *M(const DevLevel &l) { return l.M; }
   static const double *p(const DevLevel &l) { return l.p; }
@@ -284,6 +294,10 @@ struct Lv<float> {
     m.col = l.col;
     m.val = l.val_lo;
     m.vtype = l.vtype_lo;
+    if (l.slo && l.slo->nslices) {
+      m.has_sl = true;
+      m.sl = l.slo->view();
+    }
     return m;
   }
   static const float *D(const DevLevel &l) { return l.D32; }
@@ -450,6 +464,34 @@ bcmg_status prepare_mixed(bcmg_handle *h) {
   return BCMG_OK;
 }
 
+// Sliced copies for the solve phase: the FP64 cycle reads s64 on every level,
+// the mixed cycle slo; level 0 always has an FP64 copy for the FCG SpMV.
+// Level 0 is shared by all hierarchies, so its copies live in h->A0.
+bcmg_status prepare_solve_formats(bcmg_handle *h) {
+  cudaStream_t s = h->stream;
+  DevLevel &a = h->A0;
+  if (!a.own64.nslices) BCMG_TRY(sliced_build(a.view(), kValF64, &a.own64, s));
+  if (h->mixed && !a.ownlo.nslices) BCMG_TRY(sliced_build(a.view(), kValF32, &a.ownlo, s));
+  for (auto &H : h->H) {
+    for (size_t l = 0; l < H.lv.size(); ++l) {
+      DevLevel &lv = H.lv[l];
+      if (l == 0) {
+        lv.s64 = &a.own64;
+        lv.slo = h->mixed ? &a.ownlo : nullptr;
+        continue;
+      }
+      if (h->mixed) {
+        if (!lv.ownlo.nslices) BCMG_TRY(sliced_build(lv.view(), lv.vtype_lo, &lv.ownlo, s));
+        lv.slo = &lv.ownlo;
+      } else {
+        if (!lv.own64.nslices) BCMG_TRY(sliced_build(lv.view(), kValF64, &lv.own64, s));
+        lv.s64 = &lv.own64;
+      }
+    }
+  }
+  return BCMG_OK;
+}
+
 bcmg_status alloc_work(bcmg_handle *h) {
   const int32_t n = h->A0.n;
   cudaStream_t s = h->stream;
@@ -528,6 +570,7 @@ bcmg_status setup_common(bcmg_handle *h) {
   BCMG_TRY(bootstrap(h));
   h->mixed = h->ext.precision == BCMG_PREC_MIXED;
   if (h->mixed) BCMG_TRY(prepare_mixed(h));
+  if (h->ext.sliced) BCMG_TRY(prepare_solve_formats(h));
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
   h->setup_ms = ms_since(t0);
   return BCMG_OK;
@@ -558,13 +601,21 @@ bcmg_status new_handle(const bcmg_params *p, const bcmg_ext *ext, bcmg_handle **
   return BCMG_OK;
 }
 
+// w = A v with the fused dots, on the sliced FP64 copy of A when present.
+bcmg_status spmv_dots(bcmg_handle *h, const double *v, double *w, const double *r,
+                      const double *q) {
+  if (h->A0.own64.nslices)
+    return sliced_fcg_spmv_dots(h->A0.own64.view(), v, w, r, q, h->partials, h->stream);
+  return fcg_spmv_dots(h->A0.view(), v, w, r, q, h->partials, h->scal, h->stream);
+}
+
 // One FCG iteration (the body of the do-while, src/SOLVER/FCG.cu:497-565)
 // on fixed buffers: z = v, Az = w, previous direction d, Ad = q.
 bcmg_status fcg_iteration(bcmg_handle *h, cudaGraphConditionalHandle cond, bool use_cond) {
   cudaStream_t s = h->stream;
   const CsrView A = h->A0.view();
   BCMG_TRY(precond_apply(h, h->r, h->v, true, h->mixed));
-  BCMG_TRY(fcg_spmv_dots(A, h->v, h->w, h->r, h->q, h->partials, h->scal, s));
+  BCMG_TRY(spmv_dots(h, h->v, h->w, h->r, h->q));
   BCMG_TRY(fcg_scalars(h->partials, h->scal, false, s));
   BCMG_TRY(fcg_update(A.n, false, h->v, h->d, h->w, h->q, h->xs, h->r, h->partials, h->scal,
                       s));
@@ -658,7 +709,7 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
   // First step (FCG.cu:464-495): v = B r; w = A v; x += theta v; r -= theta w;
   // d = v; q = w.
   BCMG_TRY(precond_apply(h, r, v, true, h->mixed));
-  BCMG_TRY(fcg_spmv_dots(A, v, w, r, nullptr, h->partials, h->scal, s));
+  BCMG_TRY(spmv_dots(h, v, w, r, nullptr));
   BCMG_TRY(fcg_scalars(h->partials, h->scal, true, s));
   BCMG_TRY(fcg_update(n, true, v, d, w, q, x, r, h->partials, h->scal, s));
   double *hs = h->host_scal;
@@ -881,6 +932,62 @@ bcmg_status bcmg_level_copy(const bcmg_handle *h, int hrc, int level, int32_t *r
   if (l.agg) BCMG_TRY(get(agg, l.agg, sizeof(int32_t) * l.n));
   if (l.p) BCMG_TRY(get(p, l.p, sizeof(double) * l.n));
   BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_level_relax(bcmg_handle *h, int hrc, int level, const void *d_f, void *d_u,
+                             int k) {
+  clear_error();
+  if (!h || hrc < 0 || hrc >= static_cast<int>(h->H.size()) || !d_f || !d_u || k < 0)
+    return set_error(BCMG_ERR_PARAM, "bad arguments");
+  DevHierarchy &H = h->H[hrc];
+  if (level < 0 || level >= static_cast<int>(H.lv.size()))
+    return set_error(BCMG_ERR_PARAM, "bad level index");
+  BCMG_CUDA(cudaSetDevice(h->device));
+  const DevLevel &lv = H.lv[level];
+  const bool coarsest = level == static_cast<int>(H.lv.size()) - 1;
+  const int type = coarsest ? h->prm.coarse_solver : h->prm.relax_type;
+  if (h->mixed) {
+    const float *dd = type == 0 ? Lv<float>::D(lv) : Lv<float>::M(lv);
+    BCMG_TRY(relax_t<float>(Lv<float>::mat(lv), dd, static_cast<const float *>(d_f),
+                            static_cast<float *>(d_u), h->c32.xt[level], k, false, h->stream));
+  } else {
+    const double *dd = type == 0 ? Lv<double>::D(lv) : Lv<double>::M(lv);
+    BCMG_TRY(relax_t<double>(Lv<double>::mat(lv), dd, static_cast<const double *>(d_f),
+                             static_cast<double *>(d_u), h->c64.xt[level], k, false,
+                             h->stream));
+  }
+  BCMG_CUDA(cudaStreamSynchronize(h->stream));
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_level_format(const bcmg_handle *h, int hrc, int level, int64_t *slots,
+                              int64_t *column_slots, int32_t *slices, int32_t *value_bytes) {
+  if (!h || hrc < 0 || hrc >= static_cast<int>(h->H.size()))
+    return set_error(BCMG_ERR_PARAM, "bad hierarchy index");
+  const DevHierarchy &H = h->H[hrc];
+  if (level < 0 || level >= static_cast<int>(H.lv.size()))
+    return set_error(BCMG_ERR_PARAM, "bad level index");
+  const DevLevel &lv = H.lv[level];
+  const SlicedMat *S = h->mixed ? lv.slo : lv.s64;
+  if (slots) *slots = S ? S->slots : 0;
+  if (slices) *slices = S ? S->nslices : 0;
+  if (value_bytes)
+    *value_bytes = !S ? 0 : (S->vtype == kValF64 ? 8 : (S->vtype == kValF32 ? 4 : 2));
+  if (column_slots) {
+    *column_slots = 0;
+    if (S && S->nslices) {
+      std::vector<int32_t> kind(S->nslices), width(S->nslices);
+      BCMG_CUDA(cudaSetDevice(h->device));
+      BCMG_CUDA(cudaMemcpyAsync(kind.data(), S->kind, sizeof(int32_t) * S->nslices,
+                                cudaMemcpyDeviceToHost, h->stream));
+      BCMG_CUDA(cudaMemcpyAsync(width.data(), S->width, sizeof(int32_t) * S->nslices,
+                                cudaMemcpyDeviceToHost, h->stream));
+      BCMG_CUDA(cudaStreamSynchronize(h->stream));
+      for (int32_t i = 0; i < S->nslices; ++i)
+        if (!kind[i]) *column_slots += width[i];
+    }
+  }
   return BCMG_OK;
 }
 

@@ -28,6 +28,10 @@ struct DevLevel {
   int vtype_lo = kValF32;
   bool own_lo = true;
   float *D32 = nullptr, *M32 = nullptr, *p32 = nullptr;
+  // Sliced solve-phase copies (own64/ownlo owned here; s64/slo may point to
+  // the handle's level-0 copies).
+  SlicedMat own64, ownlo;
+  const SlicedMat *s64 = nullptr, *slo = nullptr;
   CsrView view() const {
     CsrView v;
     v.n = n;

@@ -461,6 +461,8 @@ void bcmg_ext_default(bcmg_ext *e) {
   e->device = 0;
   e->verbose = 0;
   e->max_device_seconds = 60.0;
+  e->stream = nullptr;
+  e->sliced = 1;
 }
 
 }  // extern "C"

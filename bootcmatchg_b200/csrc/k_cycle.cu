@@ -174,6 +174,7 @@ void launch_residual(int G, int blocks, cudaStream_t s, const MatView &A, const 
 // FP32 / BF16 / FP16 values.
 template <typename XT>
 bcmg_status check_types(const MatView &A) {
+  if (A.has_sl) return BCMG_OK;  // the sliced launchers check their own types
   const bool ok = std::is_same<XT, double>::value ? A.vtype == kValF64 : A.vtype != kValF64;
   if (!ok) return set_error(BCMG_ERR_INTERNAL, "value/vector type mismatch (%d)", A.vtype);
   return BCMG_OK;
@@ -244,7 +245,10 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
   }
   for (; left > 0; --left) {
     XT *dst = (cur == u) ? u_tmp : u;
-    relax_sweep<XT>(G, blocks, s, A, d, f, cur, dst);
+    if (A.has_sl)
+      BCMG_TRY(sliced_relax_sweep<XT>(A.sl, d, f, cur, dst, s));
+    else
+      relax_sweep<XT>(G, blocks, s, A, d, f, cur, dst);
     cur = dst;
   }
   BCMG_LAUNCH_CHECK();
@@ -255,6 +259,7 @@ template <typename XT>
 bcmg_status residual_t(const MatView &A, const XT *f, const XT *u, XT *res, cudaStream_t s) {
   if (A.n <= 0) return BCMG_OK;
   BCMG_TRY(check_types<XT>(A));
+  if (A.has_sl) return sliced_residual<XT>(A.sl, f, u, res, s);
   const int G = group_for(A.nnz, A.n);
   residual_pass<XT>(G, grid_for(static_cast<int64_t>(A.n) * G), s, A, f, u, res);
   BCMG_LAUNCH_CHECK();

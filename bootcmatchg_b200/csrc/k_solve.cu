@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "reduce.cuh"
 
 namespace bcmg {
 namespace {
@@ -46,41 +47,6 @@ __global__ void __launch_bounds__(kThreads)
   if (i >= n) i = -1;
   const double T = row_dot<G>(row, col, val, x, i, lane);
   if (i >= 0 && lane == 0) y[i] = (beta == 0.0) ? alpha * T : fma(alpha, T, beta * y[i]);
-}
-
-// Block sum of NV doubles per thread into partials[blockIdx.x * 4 + k].
-template <int NV>
-__device__ __forceinline__ void block_partials(double (&v)[NV], double *partials) {
-  __shared__ double sh[kThreads / 32][4];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < NV; ++k) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    if (lane == 0) sh[wid][k] = v[k];
-  }
-  __syncthreads();
-  if (threadIdx.x < NV) {
-    double s = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) s += sh[w][threadIdx.x];
-    partials[blockIdx.x * 4 + threadIdx.x] = s;
-  }
-}
-
-// Fixed-order sum of the partials of NV quantities by one block.
-__device__ __forceinline__ double reduce_partials(const double *partials, int k) {
-  __shared__ double sh[kThreads];
-  double s = 0.0;
-  for (int b = threadIdx.x; b < kRedBlocks; b += blockDim.x) s += partials[b * 4 + k];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-    __syncthreads();
-  }
-  const double r = sh[0];
-  __syncthreads();
-  return r;
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -145,10 +111,22 @@ __global__ void k_fcg_scalars(const double *partials, double *scal, int first) {
     const double delta = scal[kDelta];
     const double theta = gamma / delta;
     const double nd = beta - (gamma * gamma) / delta;
-    scal[kTheta] = theta;
-    scal[kDelta] = nd;
-    scal[kTheta2] = alpha / nd;
-    if (!(nd > 0.0)) scal[kIndef] = 1.0;
+    if (nd > 0.0) {
+      scal[kTheta] = theta;
+      scal[kDelta] = nd;
+      scal[kTheta2] = alpha / nd;
+    } else if (alpha == 0.0 && gamma == 0.0) {
+      // r = 0 exactly (so z = B r = 0): the previous step was exact.  The
+      // reference's do-while still runs this iteration and divides 0 by 0
+      // (FCG.cu:531-534); here the update becomes a no-op instead.
+      scal[kTheta] = 0.0;
+      scal[kTheta2] = 0.0;
+    } else {
+      scal[kTheta] = theta;
+      scal[kDelta] = nd;
+      scal[kTheta2] = alpha / nd;
+      scal[kIndef] = 1.0;
+    }
   }
 }
 

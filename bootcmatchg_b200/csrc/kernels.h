@@ -41,11 +41,47 @@ bcmg_status compose_p(int32_t n, int32_t *agg, double *p, const int32_t *agg2,
 // Value storage of a level matrix used by the cycle.
 enum ValType { kValF64 = 0, kValF32 = 1, kValBF16 = 2, kValF16 = 3 };
 
+// Sliced solve-phase format (k_sliced.cu): 32-row slices, slot-major values;
+// kind[s] = 1: shared column offsets soff[sptr[s] + k]; 0: explicit columns
+// scol[32 sptr[s] + 32 k + lane].
+struct SlicedView {
+  int32_t n = 0, nslices = 0;
+  const int32_t *sptr = nullptr, *width = nullptr, *kind = nullptr;
+  const int32_t *scol = nullptr, *soff = nullptr;
+  const void *val = nullptr;
+  int vtype = kValF64;
+};
+
+struct SlicedMat {
+  int32_t n = 0, nslices = 0, slots = 0;
+  int32_t *sptr = nullptr, *width = nullptr, *kind = nullptr, *scol = nullptr,
+          *soff = nullptr;
+  void *val = nullptr;
+  int vtype = kValF64;
+  void release(cudaStream_t s);
+  SlicedView view() const;
+};
+
+// Builds the sliced copy of a CSR matrix with values converted to vtype.
+bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s);
+template <typename XT>  // u_out = ((-(A u) + f) ./ d) + u
+bcmg_status sliced_relax_sweep(const SlicedView &S, const XT *d, const XT *f, const XT *u,
+                               XT *u_out, cudaStream_t s);
+template <typename XT>  // res = f - A u
+bcmg_status sliced_residual(const SlicedView &S, const XT *f, const XT *u, XT *res,
+                            cudaStream_t s);
+// FCG SpMV w = A v fused with alpha = r.v, beta = w.v, gamma = q.v (FP64 values).
+bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w,
+                                 const double *r, const double *q, double *partials,
+                                 cudaStream_t s);
+
 struct MatView {
   int32_t n = 0, nnz = 0;
   const int32_t *row = nullptr, *col = nullptr;
   const void *val = nullptr;
   int vtype = kValF64;
+  bool has_sl = false;  // use the sliced copy for sweeps and residuals
+  SlicedView sl;
 };
 
 // k sweeps of u <- ((-(A u) + f) ./ d) + u, result in u; u_tmp is the

@@ -7,6 +7,7 @@
 #include "common.cuh"
 
 namespace bcmg {
+namespace {  // kernels get internal linkage in every file that includes this
 namespace scan_detail {
 
 constexpr int kBlock = 256;
@@ -95,6 +96,7 @@ __global__ void scan_apply(const int32_t *__restrict__ in, int64_t n,
 }
 
 }  // namespace scan_detail
+}  // namespace
 
 // out[i] = sum_{k<i} in[i]; *total_dev (device, may be null) = sum of all.
 // `in` and `out` may alias.  tmp must hold ceil(n / 2048) ints.

@@ -94,6 +94,7 @@ typedef struct bcmg_ext {
   double max_device_seconds; /* bound on any single device loop (matching)     */
   void  *stream;          /* cudaStream_t to run on from setup on (NULL: the
                              handle creates its own); the caller keeps it alive */
+  int    sliced;          /* solve on the sliced copies of the levels (default 1) */
 } bcmg_ext;
 
 /* Per-solve report.  residual is the recursive ||r||_2 that FCG returns
@@ -189,6 +190,20 @@ bcmg_status bcmg_level_info(const bcmg_handle *h, int hrc, int level,
 bcmg_status bcmg_level_copy(const bcmg_handle *h, int hrc, int level,
                             int32_t *row, int32_t *col, double *val, double *D,
                             double *M, int32_t *agg, double *p, double *w);
+
+/* k smoother sweeps of one level exactly as the solve-phase cycle runs them
+ * (relax_type's diagonal, the level's solve format and precision).  f and u
+ * are device vectors of the level's size: FP64 for BCMG_PREC_FP64 handles,
+ * FP32 for BCMG_PREC_MIXED handles.  Used to time the dominant kernel. */
+bcmg_status bcmg_level_relax(bcmg_handle *h, int hrc, int level, const void *d_f,
+                             void *d_u, int k);
+/* Storage of one level's solve-phase copy: value slots (32 values each),
+ * slots of slices with explicit columns (the rest share column offsets and
+ * store no indices), slices, bytes per value (0: the level is solved from
+ * CSR). */
+bcmg_status bcmg_level_format(const bcmg_handle *h, int hrc, int level,
+                              int64_t *slots, int64_t *column_slots,
+                              int32_t *slices, int32_t *value_bytes);
 
 /* ---- single-step entry points on device pointers --------------------------
  * Used by the parity tests; stream may be NULL (legacy default stream).

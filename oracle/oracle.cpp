@@ -679,10 +679,23 @@ int fcg(orc_handle &h, const double *b, double *x, int itnlim, bcmg_solve_info *
     alpha = dot(r.data(), z.data(), n);
     beta = dot(az.data(), z.data(), n);
     gamma = dot(azp.data(), z.data(), n);
-    theta = gamma / delta;
-    delta = beta - (gamma * gamma) / delta;
-    if (!(delta > 0.0)) status = BCMG_ERR_INDEFINITE;
-    const double theta2 = alpha / delta;
+    double theta2;
+    const double nd = beta - (gamma * gamma) / delta;
+    if (nd > 0.0) {
+      theta = gamma / delta;
+      delta = nd;
+      theta2 = alpha / delta;
+    } else if (alpha == 0.0 && gamma == 0.0) {
+      // Exact previous step (r = 0, z = 0): the reference divides 0 by 0
+      // here (FCG.cu:531-534); treat the iteration as a no-op.
+      theta = 0.0;
+      theta2 = 0.0;
+    } else {
+      theta = gamma / delta;
+      delta = nd;
+      theta2 = alpha / delta;
+      status = BCMG_ERR_INDEFINITE;
+    }
 #pragma omp parallel for schedule(static)
     for (int32_t i = 0; i < n; ++i) {
       const double zi = -theta * zp[i] + z[i];
@@ -725,6 +738,22 @@ int orc_setup(const bcmg_csr *A, const bcmg_params *p, orc_handle **out) {
       static_cast<int32_t>(40 * std::pow(static_cast<double>(A->n), 1. / 3.));
   h->grid_sweeps = grid_sweeps(p->cycle_type, p->max_levels);
   bootstrap(*h);
+  *out = h.release();
+  return BCMG_OK;
+}
+
+int orc_setup_from_w(const bcmg_csr *A, const bcmg_params *p, const double *w,
+                     orc_handle **out) {
+  if (!A || !p || !w || !out) return BCMG_ERR_PARAM;
+  auto h = std::make_unique<orc_handle>();
+  h->prm = *p;
+  h->A0 = std::make_shared<Csr>(from_bcmg(A));
+  h->maxcoarsesize =
+      static_cast<int32_t>(40 * std::pow(static_cast<double>(A->n), 1. / 3.));
+  h->grid_sweeps = grid_sweeps(p->cycle_type, p->max_levels);
+  Vec wv(w, w + A->n);
+  h->H.push_back(adaptive_coarsening(*h, wv));
+  size_buffers(*h);
   *out = h.release();
   return BCMG_OK;
 }

@@ -37,6 +37,10 @@ void orc_set_threads(int nthreads);
 int orc_get_threads(void);
 
 int orc_setup(const bcmg_csr *A, const bcmg_params *p, orc_handle **out);
+/* One hierarchy (adaptiveCoarsening) from a given smooth vector w, without
+ * the bootstrap loop: checks a bootstrapped hierarchy from identical inputs. */
+int orc_setup_from_w(const bcmg_csr *A, const bcmg_params *p, const double *w,
+                     orc_handle **out);
 int orc_solve(orc_handle *h, const double *b, double *x, bcmg_solve_info *info);
 int orc_precond_apply(orc_handle *h, const double *r, double *z);
 void orc_destroy(orc_handle *h);

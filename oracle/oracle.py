@@ -47,6 +47,7 @@ _SIG = {
     "orc_set_threads": (None, [C.c_int]),
     "orc_get_threads": (C.c_int, []),
     "orc_setup": (C.c_int, [C.POINTER(_Csr), C.POINTER(_Params), C.POINTER(vp)]),
+    "orc_setup_from_w": (C.c_int, [C.POINTER(_Csr), C.POINTER(_Params), vp, C.POINTER(vp)]),
     "orc_solve": (C.c_int, [vp, vp, vp, C.POINTER(_Info)]),
     "orc_fcg_sample": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(C.c_double)]),
     "orc_precond_apply": (C.c_int, [vp, vp, vp]),
@@ -110,11 +111,17 @@ def _params(p):
 class OracleHandle:
     """FP64 host setup + solve of the same method (parity oracle)."""
 
-    def __init__(self, A, params):
+    def __init__(self, A, params, w=None):
+        """Bootstrap setup; with w, a single hierarchy coarsened from w."""
         self._h = C.c_void_p()
         self._A = A
         c, p = _csr(A), _params(params)
-        _check(olib.orc_setup(C.byref(c), C.byref(p), C.byref(self._h)), "setup")
+        if w is None:
+            _check(olib.orc_setup(C.byref(c), C.byref(p), C.byref(self._h)), "setup")
+        else:
+            self._w = np.ascontiguousarray(w, dtype=np.float64)
+            _check(olib.orc_setup_from_w(C.byref(c), C.byref(p), _ptr(self._w),
+                                         C.byref(self._h)), "setup_from_w")
         self.n = A.n
 
     def close(self):

@@ -74,3 +74,40 @@ def test_itnlim_respected():
     with bc.Handle(A, p) as h:
         x, info = h.solve(np.ones(A.n))
     assert info.iters == 4 and not info.converged  # num_iter = iter + 1
+
+
+@pytest.mark.parametrize("case", ["poisson27_20", "rgg_20000"])
+def test_sliced_level_relax_matches_oracle(case):
+    """Sweeps on the sliced copies (offset slices on the stencil level 0,
+    explicit-column slices on coarse / irregular levels) against the oracle's
+    CSR sweep, FP64."""
+    import ctypes as C
+    import torch
+    from bootcmatchg_b200._lib import check, lib
+    A = bc.poisson(27, 20, 20, 20) if case == "poisson27_20" else bc.rgg(20000, seed=3)
+    p = c1_params()
+    with bc.Handle(A, p) as h:
+        L = h.hierarchy_info()["num_levels"]
+        for level in range(min(3, L)):
+            lv = h.level(0, level)
+            f, u0 = bc.vector(1, level + 1, lv.n), bc.vector(2, level + 2, lv.n)
+            ft = torch.from_numpy(f).cuda()
+            ut = torch.from_numpy(u0).cuda()
+            check(lib.bcmg_level_relax(h.ptr, 0, level, C.c_void_p(ft.data_ptr()),
+                                       C.c_void_p(ut.data_ptr()), 3), "level_relax")
+            d = lv.M if (level < L - 1 or p.coarse_solver == 4) else lv.D
+            ref = orc.relax(lv.A, d, f, u0, 3)
+            np.testing.assert_allclose(ut.cpu().numpy(), ref, rtol=1e-12,
+                                       atol=1e-12 * np.abs(ref).max())
+
+
+def test_sliced_and_csr_solves_agree():
+    A = bc.rgg(30000, seed=2)
+    p = c1_params()
+    b = bc.vector(1, 8, A.n)
+    with bc.Handle(A, p, bc.Extensions(sliced=1)) as h1, \
+            bc.Handle(A, p, bc.Extensions(sliced=0)) as h0:
+        x1, i1 = h1.solve(b)
+        x0, i0 = h0.solve(b)
+    assert abs(i1.iters - i0.iters) <= 1
+    assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) < 1e-7

@@ -146,11 +146,12 @@ def test_relax_and_spmv_parity():
                                atol=1e-12)
 
 
-def compare_hierarchies(h, o, hrc=0):
-    gi, oi = h.hierarchy_info(hrc), o.hierarchy_info(hrc)
+def compare_hierarchies(h, o, hrc=0, ohrc=None):
+    ohrc = hrc if ohrc is None else ohrc
+    gi, oi = h.hierarchy_info(hrc), o.hierarchy_info(ohrc)
     assert gi["num_levels"] == oi["num_levels"], (gi, oi)
     for l in range(gi["num_levels"]):
-        g, r = h.level(hrc, l), o.level(hrc, l)
+        g, r = h.level(hrc, l), o.level(ohrc, l)
         assert (g.n, g.nnz, g.n_coarse) == (r["n"], r["nnz"], r["n_coarse"]), l
         for name, a, b in (("row", g.A.row, r["row"]), ("col", g.A.col, r["col"]),
                            ("val", g.A.val, r["val"]), ("D", g.D, r["D"]), ("M", g.M, r["M"]),
@@ -202,8 +203,16 @@ def test_bootstrap_composites_cycles(solver_type, cycle_type):
         onh, oest = o.num_hierarchies()
         assert nh == onh == 3
         assert abs(est - oest) <= 1e-9 * abs(oest)
-        for k in range(nh):
-            compare_hierarchies(h, o, k)
+        # Hierarchies 1 and 2 come from w = 1: bit-exact.  Hierarchy 3 comes
+        # from the w of 15 composite cycles, whose sums round differently on
+        # the GPU: w within 1e-10, and the hierarchy bit-exact when the oracle
+        # coarsens from the GPU's w.
+        compare_hierarchies(h, o, 0)
+        compare_hierarchies(h, o, 1)
+        gw = h.level(2, 0).w
+        np.testing.assert_allclose(gw, o.level(2, 0)["w"], rtol=1e-10,
+                                   atol=1e-12 * np.abs(gw).max())
+        compare_hierarchies(h, orc.OracleHandle(A, p, w=gw), 2, 0)
         # one preconditioner application from a nonzero guess
         r0, z0 = bc.vector(1, 5, A.n), bc.vector(1, 6, A.n)
         rt, zt = dev(r0), dev(z0)
