@@ -11,11 +11,19 @@
 #include <cstring>
 #include <memory>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "handle.h"
 
 namespace bcmg {
 
 std::atomic<unsigned long long> g_kernel_launches{0};
+
+// NVTX range for the lifetime of a scope (profilers filter on these names).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 void DevLevel::release(cudaStream_t s) {
   if (own_A) {
@@ -553,6 +561,7 @@ void destroy_handle(bcmg_handle *h) {
 }
 
 bcmg_status setup_common(bcmg_handle *h) {
+  NvtxRange range("bcmg_setup");
   const auto t0 = Clock::now();
   const int32_t n = h->A0.n;
   // BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311).
@@ -820,6 +829,7 @@ bcmg_status bcmg_solve(bcmg_handle *h, const double *b, double *x, int on_device
   if (!info) info = &local;
   std::memset(info, 0, sizeof(*info));
   BCMG_CUDA(cudaSetDevice(h->device));
+  NvtxRange range("bcmg_solve");
   const auto t0 = Clock::now();
   const int32_t n = h->A0.n;
   const cudaMemcpyKind in = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -944,6 +954,7 @@ bcmg_status bcmg_level_relax(bcmg_handle *h, int hrc, int level, const void *d_f
   if (level < 0 || level >= static_cast<int>(H.lv.size()))
     return set_error(BCMG_ERR_PARAM, "bad level index");
   BCMG_CUDA(cudaSetDevice(h->device));
+  NvtxRange range("bcmg_level_relax");
   const DevLevel &lv = H.lv[level];
   const bool coarsest = level == static_cast<int>(H.lv.size()) - 1;
   const int type = coarsest ? h->prm.coarse_solver : h->prm.relax_type;
