@@ -91,6 +91,7 @@ SIGNATURES = {
     "bcmg_k_galerkin": (C.c_int, [i32, i32, vp, vp, vp, i32, vp, vp, vp, i32p, vp, vp,
                                   vp]),
     "bcmg_k_relax": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, C.c_int, vp]),
+    "bcmg_k_relax_noalloc": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, C.c_int, vp]),
     "bcmg_k_spmv": (C.c_int, [i32, i32, vp, vp, vp, C.c_double, vp, C.c_double, vp, vp]),
     "bcmg_gen_poisson": (C.c_int, [C.c_int, i32, i32, i32, C.POINTER(Csr)]),
     "bcmg_gen_fv2d": (C.c_int, [i32, i32, C.c_uint64, C.c_double, C.POINTER(Csr)]),

@@ -239,6 +239,18 @@ bcmg_status bcmg_k_relax(int32_t n, int32_t nnz, const int32_t *d_row,
                          const int32_t *d_col, const double *d_val,
                          const double *d_d, const double *d_f, double *d_u,
                          int k, void *stream);
+/* bcmg_k_relax without any device allocation; no counterpart in the
+ * reference.  For callers that may not allocate device memory at the point
+ * of the call (another framework's allocator owns the device, a plugin with
+ * a fixed footprint, a latency-critical loop).  Its ping-pong vector is a
+ * process-lifetime device buffer of 1,048,576 doubles (8 MiB on every GPU
+ * that loads the library): n above that is rejected with BCMG_ERR_PARAM.
+ * The first call on a device looks the buffer up and should come before any
+ * stream capture; calls that overlap on the GPU share the buffer and race. */
+bcmg_status bcmg_k_relax_noalloc(int32_t n, int32_t nnz, const int32_t *d_row,
+                                 const int32_t *d_col, const double *d_val,
+                                 const double *d_d, const double *d_f, double *d_u,
+                                 int k, void *stream);
 /* y = alpha A x + beta y (CSRVector_product_adaptive_miniwarp,
  * src/matrix/CSR.cu:926-960). */
 bcmg_status bcmg_k_spmv(int32_t n, int32_t nnz, const int32_t *d_row,
