@@ -6,6 +6,9 @@ teardown -- plus the copy of x back to the host, i.e. the same work as the
 e2e number of bench.py.  Every workload runs in a child process so the
 reference's stdout (#META lines) can be parsed.  Prints one JSON line per
 workload.  Usage (GPU box): python oracle/ref/time_ref_solve.py [workload ...]
+On a B200 the stock solve() stopped with an illegal memory access
+(src/matrix/CSR.cu:140) on both default workloads, so it is not run again;
+the script is kept as the record of that attempt.
 TEST INFRASTRUCTURE ONLY.
 """
 from __future__ import annotations
