@@ -42,6 +42,7 @@ if ROOT not in sys.path:
 import numpy as np  # noqa: E402
 
 METRIC = "solves/s to rtol 1e-8, mixed vs FP64 AMG-FCG"
+BATCH_RHS = 32
 
 
 def log(*a):
@@ -79,6 +80,13 @@ def make_workload(bc, name):
         A = bc.poisson(7, 96, 96, 96)
         b = bc.vector(1, 3, A.n)
         desc = "3-D 7-point Poisson 96^3, b ~ N(0,1) seed 3"
+    elif name == "poisson7_96_x32":
+        A = bc.poisson(7, 96, 96, 96)
+        # 32 right-hand sides: one N(0,1) stream from seed 3, column-major.
+        b = np.asfortranarray(bc.vector(1, 3, A.n * BATCH_RHS).reshape(A.n, BATCH_RHS,
+                                                                       order="F"))
+        desc = ("3-D 7-point Poisson 96^3 with 32 simultaneous right-hand sides "
+                "~ N(0,1) seed 3 (column-major), one shared hierarchy")
     else:
         raise SystemExit(f"unknown workload {name}")
     return A, b, p, desc
@@ -162,6 +170,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def aggregate_over_ranks(ms_local, steps, units_per_step, world, dist=None, device=None):
+    """Whole-job throughput of N replicas: the slowest rank's device time
+    (MAX over ranks) and all ranks' units divided by it."""
+    ms = ms_local
+    if world > 1:
+        import torch
+        t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, world * steps * units_per_step / (ms / 1e3)
+
+
 # ---------------------------------------------------------------------------
 def run_cpu_baseline(bc, orc, A, b, p, iters_hint, threads):
     """Oracle on a bounded sample: full setup + 3 FCG iterations, scaled to a
@@ -178,7 +198,8 @@ def run_cpu_baseline(bc, orc, A, b, p, iters_hint, threads):
     per_solve = setup_s + iters_hint * it_s
     return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": threads, "kind": "port",
             "sample": (f"oracle setup ({setup_s:.2f} s) + {k} FCG iterations "
-                       f"({it_s:.3f} s each), scaled to {iters_hint} iterations")}
+                       f"({it_s:.3f} s each), scaled to {iters_hint} iterations"),
+            "setup_s": setup_s, "iter_s": it_s}
 
 
 def run_reference(args):
@@ -191,6 +212,12 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
     A, b, p, desc = make_workload(bc, args.workload)
+    nrhs = 1
+    if b.ndim == 2:
+        # Multi-right-hand-side workload: one setup shared by all columns;
+        # column 0's iteration count stands for every column.
+        nrhs = b.shape[1]
+        b = np.ascontiguousarray(b[:, 0])
     t0 = time.perf_counter()
     h = orc.OracleHandle(A, p)
     setup_s = time.perf_counter() - t0
@@ -202,10 +229,12 @@ def run_reference(args):
     # itnlim=1 = first FCG step + one loop pass = 2 preconditioned iterations.
     samples = [h.fcg_sample(b, 1) / 2 for _ in range(args.steps)]
     it_s = statistics.median(samples)
-    per_solve = setup_s + iters * it_s
+    per_solve = (setup_s + nrhs * iters * it_s) / nrhs
     value = 1.0 / per_solve
     sample = (f"setup {setup_s:.2f} s once + {iters} iterations x median of {args.steps} "
               f"two-iteration samples ({it_s:.3f} s per iteration)")
+    if nrhs > 1:
+        sample += f"; one setup shared by {nrhs} right-hand sides"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": it_s * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -285,13 +314,8 @@ def run_ours(args):
     barrier()
     launches = lib.bcmg_kernel_launches() - l0
     clocks = sampler.stop(local)
-    ms = t_start.elapsed_time(t_end)
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * args.steps / (ms_max / 1e3)
+    ms_max, value = aggregate_over_ranks(t_start.elapsed_time(t_end), args.steps, 1, world,
+                                         dist, dev)
     info = infos[-1]
     xs = x.cpu().numpy()
     res = b_h - A.to_scipy() @ xs
@@ -327,12 +351,8 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
-    e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e2e_value = world * e2e_steps / (e_ms / 1e3)
+    e_ms, e2e_value = aggregate_over_ranks(e0.elapsed_time(e1), e2e_steps, 1, world, dist,
+                                           dev)
     h2d = (A.n + 1) * 4 + A.nnz * 12 + A.n * 8 * 2
     d2h = A.n * 8
 
@@ -425,6 +445,373 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args):
+    """Multi-right-hand-side workload: one step = setup of the shared
+    hierarchy + bcmg_solve_batch of all 32 columns + teardown; value counts
+    every column as one solve."""
+    import torch
+    import torch.distributed as dist
+
+    import bootcmatchg_b200 as bc
+    from bootcmatchg_b200._lib import check, lib, Csr, SolveInfo
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    A, B_h, p, desc = make_workload(bc, args.workload)
+    nrhs = B_h.shape[1]
+    prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
+    stream = torch.cuda.Stream(device=dev)
+    ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0, device=local,
+                        stream=stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        row = torch.from_numpy(A.row).to(dev)
+        col = torch.from_numpy(A.col).to(dev)
+        val = torch.from_numpy(A.val).to(dev)
+        # Column-major n x nrhs on the device: row j of a (nrhs, n) tensor is
+        # column j.
+        Bd = torch.from_numpy(np.ascontiguousarray(B_h.T)).to(dev)
+        Xd = torch.zeros_like(Bd)
+    stream.synchronize()
+
+    def step():
+        h = bc.Handle.from_device(A.n, A.nnz, row.data_ptr(), col.data_ptr(), val.data_ptr(),
+                                  p, ext)
+        with torch.cuda.stream(stream):
+            Xd.zero_()
+        infos = h.solve_batch_device(nrhs, Bd.data_ptr(), A.n, Xd.data_ptr(), A.n)
+        h.close()
+        return infos
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        infos = step()
+    if not all(i.converged for i in infos):
+        raise SystemExit("warm-up batch did not converge")
+    sampler = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(
+        os.path.join(ROOT, "gpurun_out")) else ".", f"clocks_rank{rank}.csv"))
+    barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    l0 = lib.bcmg_kernel_launches()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    all_infos = [step() for _ in range(args.steps)]
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    launches = lib.bcmg_kernel_launches() - l0
+    clocks = sampler.stop(local)
+    ms_max, value = aggregate_over_ranks(t0.elapsed_time(t1), args.steps, nrhs, world, dist,
+                                         dev)
+    infos = all_infos[-1]
+    X = Xd.cpu().numpy().T
+    As = A.to_scipy()
+    true_rel = max(float(np.linalg.norm(B_h[:, j] - As @ X[:, j]) / np.linalg.norm(B_h[:, j]))
+                   for j in range(nrhs))
+
+    # Solve-only rate (hierarchy kept) and the one-column-at-a-time rate on
+    # the same handle, for the batching gain.
+    h = bc.Handle.from_device(A.n, A.nnz, row.data_ptr(), col.data_ptr(), val.data_ptr(), p, ext)
+    h.solve_batch_device(nrhs, Bd.data_ptr(), A.n, Xd.data_ptr(), A.n)
+    torch.cuda.synchronize(dev)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    with torch.cuda.stream(stream):
+        Xd.zero_()
+    h.solve_batch_device(nrhs, Bd.data_ptr(), A.n, Xd.data_ptr(), A.n)
+    s1.record(stream)
+    torch.cuda.synchronize(dev)
+    batch_solve_ms = s0.elapsed_time(s1)
+    with torch.cuda.stream(stream):
+        xs = torch.zeros(A.n, dtype=torch.float64, device=dev)
+    stream.synchronize()
+    single = []
+    for j in range(min(nrhs, 8)):
+        with torch.cuda.stream(stream):
+            xs.zero_()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        si = h.solve_device(Bd[j].data_ptr(), xs.data_ptr())
+        g1.record(stream)
+        torch.cuda.synchronize(dev)
+        single.append((g0.elapsed_time(g1), si.iters))
+    cfg = [h.batch_config(nrhs, 0, l) for l in range(h.hierarchy_info(0)["num_levels"])]
+    # Roofline: the level-0 batched smoother sweep on 32 interleaved columns.
+    W = cfg[0]["width"]
+    xdt, xbytes = (torch.float32, 4) if prec == bc.PREC_MIXED else (torch.float64, 8)
+    vbytes = 4 if prec == bc.PREC_MIXED else 8
+    with torch.cuda.stream(stream):
+        f = torch.from_numpy(B_h[:, :W].copy()).to(dev).to(xdt).contiguous()
+        u = torch.zeros_like(f)
+    stream.synchronize()
+    sweeps = 20
+    check(lib.bcmg_level_relax_batch(h.ptr, 0, 0, W, C.c_void_p(f.data_ptr()),
+                                     C.c_void_p(u.data_ptr()), 2), "relax_batch warmup")
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    check(lib.bcmg_level_relax_batch(h.ptr, 0, 0, W, C.c_void_p(f.data_ptr()),
+                                     C.c_void_p(u.data_ptr()), sweeps), "relax_batch")
+    r1.record(stream)
+    torch.cuda.synchronize(dev)
+    h.close()
+    sweep_s = r0.elapsed_time(r1) / 1e3 / sweeps
+    # values + columns + row pointers + d, then f and u read and u' written
+    # for W columns (u gathered once).
+    sweep_bytes = A.nnz * (vbytes + 4) + (A.n + 1) * 4 + A.n * xbytes + 3 * A.n * W * xbytes
+    achieved = sweep_bytes / sweep_s / 1e9
+    peak, peak_kind = measured_peaks()
+
+    # e2e: host CSR + host right-hand sides through the C ABI.
+    pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+    h_row, h_col, h_val = pin(A.row), pin(A.col), pin(A.val)
+    h_B = pin(np.ascontiguousarray(B_h.T))
+    h_X = torch.zeros((nrhs, A.n), dtype=torch.float64).pin_memory()
+    c = Csr()
+    c.n, c.m, c.nnz = A.n, A.n, A.nnz
+    c.row = C.cast(h_row.data_ptr(), C.POINTER(C.c_int32))
+    c.col = C.cast(h_col.data_ptr(), C.POINTER(C.c_int32))
+    c.val = C.cast(h_val.data_ptr(), C.POINTER(C.c_double))
+    pc, ec = p.to_c(), ext.to_c()
+
+    def e2e_step():
+        hh = C.c_void_p()
+        check(lib.bcmg_setup(C.byref(c), C.byref(pc), C.byref(ec), C.byref(hh)), "setup")
+        h_X.zero_()
+        infos_c = (SolveInfo * nrhs)()
+        check(lib.bcmg_solve_batch(hh, nrhs, C.c_void_p(h_B.data_ptr()), A.n,
+                                   C.c_void_p(h_X.data_ptr()), A.n, 0, infos_c), "solve_batch")
+        lib.bcmg_destroy(hh)
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e_ms, e2e_value = aggregate_over_ranks(e0.elapsed_time(e1), e2e_steps, nrhs, world, dist,
+                                           dev)
+    h2d = (A.n + 1) * 4 + A.nnz * 12 + 2 * A.n * nrhs * 8
+    d2h = A.n * nrhs * 8
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        try:
+            one = run_cpu_baseline(bc, orc, A, B_h[:, 0].copy(), p, infos[0].iters,
+                                   os.cpu_count() or 1)
+            # setup once for all columns, then every column's iterations
+            per_batch = one["setup_s"] + sum(i.iters for i in infos) * one["iter_s"]
+            cpu = {"value": nrhs / per_batch, "unit": "solves/s", "cores": one["cores"],
+                   "kind": "port",
+                   "sample": one["sample"] + f"; one setup shared by {nrhs} columns"}
+        except Exception as exc:
+            cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {exc}"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    single_ms = statistics.median(t for t, _ in single)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if prec == bc.PREC_MIXED else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "precision": args.precision,
+                   "params": params_dict(p), "n": A.n, "nnz": A.nnz, "nrhs": nrhs,
+                   "parallelism": f"replicas{world}",
+                   "l2": "interleaved 32-column blocks (%.0f MB each in FP32) exceed "
+                         "the 126 MB L2; no flush" % (A.n * nrhs * 4 / 1e6),
+                   "step": "setup (shared hierarchy) + batched FCG of all columns + "
+                           "teardown"},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "k_bt_rowop (level-0 batched l1-Jacobi sweep, %d columns)" % W,
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": committed_traffic("k_bt_rowop",
+                                                  f"{args.workload}:{args.precision}"),
+                     "algorithmic_bytes": sweep_bytes, "launch_ms": sweep_s * 1e3},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "detail": {"iters": [i.iters for i in infos], "setup_ms": infos[0].setup_ms,
+                   "batch_solve_ms": batch_solve_ms,
+                   "solve_only_solves_per_s": nrhs / (batch_solve_ms / 1e3),
+                   "single_rhs_solve_ms_median": single_ms,
+                   "single_rhs_solves_per_s": 1e3 / single_ms,
+                   "single_rhs_iters": [it for _, it in single],
+                   "max_true_rel_residual": true_rel, "shapes": cfg,
+                   "e2e_steps": e2e_steps},
+    }
+    print(json.dumps(line), flush=True)
+    log(f"[bench] {args.workload} {args.precision}: {value:.1f} solves/s "
+        f"({ms_max / args.steps:.1f} ms per {nrhs}-column step), solve-only "
+        f"{nrhs / (batch_solve_ms / 1e3):.1f} solves/s vs one-at-a-time "
+        f"{1e3 / single_ms:.1f}; sweep {achieved:.0f} GB/s ({achieved / peak:.2f})")
+    return 0
+
+
+def serve_requests(bc, count, seed):
+    """The serving stream: per request a matrix spec and a right-hand-side
+    seed.  New matrices are 7-point or 27-point 3-D Poisson grids with side
+    log-uniform in [16, 160] or random geometric graph Laplacians (unit
+    cube, mean degree 12, weights U[0.5, 2], shift 1e-3) with n log-uniform
+    in [1e4, 2e6]; 30% of requests reuse a previously seen matrix (one of the
+    64 most recent) with a new N(0,1) right-hand side."""
+    rng = np.random.default_rng(seed)
+    reqs, seen = [], []
+    for k in range(count):
+        if seen and rng.random() < 0.3:
+            key = seen[int(rng.integers(0, len(seen)))]
+        else:
+            kind = int(rng.integers(0, 3))
+            if kind < 2:
+                side = int(np.exp(rng.uniform(np.log(16), np.log(160))))
+                spec = ("poisson", 7 if kind == 0 else 27, side)
+            else:
+                n = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+                spec = ("rgg", n, int(rng.integers(1, 1 << 30)))
+            key = (len(reqs) + 1, spec)
+            seen.append(key)
+            seen = seen[-64:]
+        reqs.append((key, 7919 * (k + 1)))
+    return reqs
+
+
+def make_matrix(bc, spec):
+    if spec[0] == "poisson":
+        return bc.poisson(spec[1], spec[2], spec[2], spec[2])
+    return bc.rgg(spec[1], seed=spec[2])
+
+
+def run_serve(args):
+    """Serving stream: requests with Poisson arrivals at args.rate per second
+    go to a bcmg_server (continuous batching, hierarchy cache, admission under
+    a 150 GB footprint cap).  value = completed solves / (last completion -
+    first submission); latency = submission -> solution on the host."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import bootcmatchg_b200 as bc
+    from bootcmatchg_b200._lib import lib
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0  # replicas of the stream add nothing: one GPU per server
+    p = c1_settings(bc)
+    prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
+    ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
+    reqs = serve_requests(bc, args.requests, 11)
+    rng = np.random.default_rng(12)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, len(reqs)))
+    # Host matrices are generated ahead of their arrival by a thread pool and
+    # kept while a later request may reuse them.
+    pool = ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4))
+    futures = {}
+    last_use = {}
+    for i, (key, _) in enumerate(reqs):
+        last_use[key] = i
+    ahead = 0  # requests whose matrices are being generated
+
+    def prefetch(upto):
+        nonlocal ahead
+        while ahead < min(upto, len(reqs)):
+            key = reqs[ahead][0]
+            if key not in futures:
+                futures[key] = pool.submit(make_matrix, bc, key[1])
+            ahead += 1
+    srv = bc.Server(p, ext, slots=args.slots, mem_cap_gb=150.0, cache_cap_gb=60.0,
+                    max_batch=32)
+    l0 = lib.bcmg_kernel_launches()
+    results = [None] * len(reqs)
+    lag = []
+    lock = threading.Lock()
+
+    def waiter(i, t, A):
+        x, r = srv.wait(t)
+        with lock:
+            results[i] = r
+        del A
+
+    threads = []
+    t0 = time.perf_counter()
+    prefetch(48)
+    for i, (key, rseed) in enumerate(reqs):
+        prefetch(i + 48)
+        A = futures[key].result()
+        b = bc.vector(1, rseed, A.n)
+        now = time.perf_counter() - t0
+        if arrivals[i] > now:
+            time.sleep(arrivals[i] - now)
+        lag.append(max(0.0, (time.perf_counter() - t0) - arrivals[i]))
+        t = srv.submit(A, b, key=hash(key) & 0x7FFFFFFFFFFFFFFF)
+        th = threading.Thread(target=waiter, args=(i, t, A))
+        th.start()
+        threads.append(th)
+        if last_use[key] == i:
+            # The host copy is no longer needed once no later request uses it
+            # (the server reads A only while setting it up, which the waiter
+            # thread's reference keeps alive until the request is done).
+            futures[key] = None
+    for th in threads:
+        th.join()
+    t_end = time.perf_counter()
+    st = srv.stats()
+    srv.close()
+    pool.shutdown()
+    launches = lib.bcmg_kernel_launches() - l0
+    lat = np.array([r.latency_ms for r in results])
+    qms = np.array([r.queue_ms for r in results])
+    conv = sum(r.solve.converged for r in results)
+    wall = t_end - t0
+    value = len(reqs) / wall
+    line = {
+        "metric": "solves/s to rtol 1e-8 and p50/p99 latency, served stream", "value": value,
+        "unit": "solves/s", "n_gpus": 1, "steps": len(reqs), "warmup": 0,
+        "ms_per_step": 1e3 * wall / len(reqs), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if prec else "f64", "data": "synthetic",
+        "config": {"workload": "serve_stream", "requests": len(reqs), "rate_per_s": args.rate,
+                   "slots": args.slots, "mem_cap_gb": 150, "cache_cap_gb": 60,
+                   "max_batch": 32, "precision": args.precision,
+                   "description": serve_requests.__doc__.split("\n\n")[0].replace("\n", " ")},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                       "p99": float(np.percentile(lat, 99)), "mean": float(lat.mean()),
+                       "max": float(lat.max())},
+        "queue_ms": {"p50": float(np.percentile(qms, 50)), "p99": float(np.percentile(qms, 99))},
+        "e2e": {"value": value, "unit": "solves/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "gpu_launches": int(launches),
+        "detail": {"converged": int(conv), "server": st,
+                   "arrival_lag_ms_p99": 1e3 * float(np.percentile(lag, 99)),
+                   "groups": int(sum(1 for r in results if r.group > 1)),
+                   "cache_hits": int(sum(r.cache_hit for r in results))},
+    }
+    print(json.dumps(line), flush=True)
+    log(f"[bench] serve_stream rate {args.rate}/s: {value:.1f} solves/s, latency p50 "
+        f"{line['latency_ms']['p50']:.1f} ms p99 {line['latency_ms']['p99']:.1f} ms, "
+        f"{conv}/{len(reqs)} converged, setups {st['setups']}, hits {st['cache_hits']}, "
+        f"batches {st['batches']}")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -432,7 +819,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="poisson27_128",
-                    choices=["poisson27_128", "poisson7_32", "fv2d_2048", "poisson7_96"])
+                    choices=["poisson27_128", "poisson7_32", "fv2d_2048", "poisson7_96",
+                             "poisson7_96_x32", "serve_stream"])
+    ap.add_argument("--requests", type=int, default=300, help="serve_stream: requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve_stream: arrivals per s")
+    ap.add_argument("--slots", type=int, default=4, help="serve_stream: solves in flight")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -441,6 +832,10 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serve_stream":
+        return run_serve(args)
+    if args.workload.endswith("_x32"):
+        return run_batch(args)
     return run_ours(args)
 
 

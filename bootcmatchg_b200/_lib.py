@@ -43,7 +43,7 @@ class Ext(C.Structure):
     _fields_ = [("precision", C.c_int), ("coarse_storage", C.c_int),
                 ("replace_every", C.c_int), ("use_graphs", C.c_int), ("device", C.c_int),
                 ("verbose", C.c_int), ("max_device_seconds", C.c_double),
-                ("stream", C.c_void_p), ("sliced", C.c_int)]
+                ("stream", C.c_void_p), ("sliced", C.c_int), ("autotune", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -51,6 +51,24 @@ class SolveInfo(C.Structure):
                 ("rel_residual", C.c_double), ("true_rel_residual", C.c_double),
                 ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("num_hrc", C.c_int),
                 ("estimated_ratio", C.c_double)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("slots", C.c_int), ("mem_cap_gb", C.c_double),
+                ("cache_cap_gb", C.c_double), ("max_batch", C.c_int), ("params", Params),
+                ("ext", Ext)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("solve", SolveInfo), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
+                ("group", C.c_int), ("cache_hit", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "failed", "setups",
+                                          "cache_hits", "batches", "evictions",
+                                          "peak_resident_bytes", "resident_bytes")] + \
+               [("cached_hierarchies", C.c_int), ("queued", C.c_int), ("running", C.c_int)]
 
 
 # name -> (restype, argtypes); every symbol include/bcmg.h declares.
@@ -77,6 +95,20 @@ SIGNATURES = {
     "bcmg_destroy": (C.c_int, [vp]),
     "bcmg_set_stream": (C.c_int, [vp, vp]),
     "bcmg_precond_apply": (C.c_int, [vp, vp, vp]),
+    "bcmg_solve_batch": (C.c_int, [vp, i32, vp, C.c_int64, vp, C.c_int64, C.c_int,
+                                   C.POINTER(SolveInfo)]),
+    "bcmg_precond_apply_batch": (C.c_int, [vp, i32, vp, C.c_int64, vp, C.c_int64]),
+    "bcmg_level_relax_batch": (C.c_int, [vp, C.c_int, C.c_int, i32, vp, vp, C.c_int]),
+    "bcmg_device_bytes": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+    "bcmg_server_opts_default": (None, [C.POINTER(ServerOpts)]),
+    "bcmg_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(vp)]),
+    "bcmg_server_submit": (C.c_int, [vp, C.POINTER(Csr), C.c_uint64, vp, vp,
+                                     C.POINTER(C.c_uint64)]),
+    "bcmg_server_wait": (C.c_int, [vp, C.c_uint64, C.c_double, C.POINTER(RequestInfo)]),
+    "bcmg_server_stats_get": (C.c_int, [vp, C.POINTER(ServerStats)]),
+    "bcmg_server_destroy": (C.c_int, [vp]),
+    "bcmg_batch_config": (C.c_int, [vp, i32, C.c_int, C.c_int, i32p, i32p, i32p,
+                                    C.POINTER(C.c_double)]),
     "bcmg_hierarchy_count": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "bcmg_hierarchy_info": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double),

@@ -16,8 +16,10 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import _lib
 from ._lib import Csr, Ext, Params as _CParams, SolveInfo, check, lib
 
+ERR_PARAM, ERR_ALLOC, ERR_PENDING = 1, 3, 11
 PREC_FP64 = 0
 PREC_MIXED = 1
 STORE_FP32, STORE_BF16, STORE_FP16 = 0, 1, 2
@@ -144,6 +146,7 @@ class Extensions:
     max_device_seconds: float = 60.0
     stream: int = 0  # cudaStream_t as an integer (0: the handle makes its own)
     sliced: int = 1  # solve on the sliced copies of the levels
+    autotune: int = 1  # batched solves: time the row-kernel shapes per level
 
     def to_c(self) -> Ext:
         e = Ext()
@@ -255,6 +258,45 @@ class Handle:
         check(lib.bcmg_precond_apply(self._h, C.c_void_p(r_ptr), C.c_void_p(z_ptr)),
               "bcmg_precond_apply")
 
+    def solve_batch(self, B: np.ndarray, X0: np.ndarray | None = None
+                    ) -> tuple[np.ndarray, list[SolveResult]]:
+        """Solves A X = B for the columns of B (n x nrhs) on the shared
+        hierarchy; returns X and one SolveResult per column."""
+        B = np.asfortranarray(B, dtype=np.float64)
+        if B.ndim != 2 or B.shape[0] != self.n:
+            raise ValueError(f"B must be {self.n} x nrhs")
+        nrhs = B.shape[1]
+        X = (np.zeros((self.n, nrhs), order="F") if X0 is None
+             else np.array(X0, dtype=np.float64, order="F", copy=True))
+        infos = (SolveInfo * nrhs)()
+        st = lib.bcmg_solve_batch(self._h, nrhs, _ptr(B), self.n, _ptr(X), self.n, 0, infos)
+        check(st, "bcmg_solve_batch")
+        return X, [SolveResult.from_c(i) for i in infos]
+
+    def solve_batch_device(self, nrhs: int, b_ptr: int, ldb: int, x_ptr: int, ldx: int
+                           ) -> list[SolveResult]:
+        infos = (SolveInfo * nrhs)()
+        check(lib.bcmg_solve_batch(self._h, nrhs, C.c_void_p(b_ptr), ldb, C.c_void_p(x_ptr),
+                                   ldx, 1, infos), "bcmg_solve_batch")
+        return [SolveResult.from_c(i) for i in infos]
+
+    def precond_apply_batch_device(self, nrhs: int, r_ptr: int, ldr: int, z_ptr: int,
+                                   ldz: int) -> None:
+        check(lib.bcmg_precond_apply_batch(self._h, nrhs, C.c_void_p(r_ptr), ldr,
+                                           C.c_void_p(z_ptr), ldz), "bcmg_precond_apply_batch")
+
+    def batch_config(self, nrhs: int, hrc: int, level: int) -> dict:
+        w, v, t, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        check(lib.bcmg_batch_config(self._h, nrhs, hrc, level, C.byref(w), C.byref(v),
+                                    C.byref(t), C.byref(ms)), "bcmg_batch_config")
+        return {"width": w.value, "cols_per_lane": v.value, "threads": t.value,
+                "tune_ms": ms.value}
+
+    def device_bytes(self) -> int:
+        b = C.c_uint64()
+        check(lib.bcmg_device_bytes(self._h, C.byref(b)), "bcmg_device_bytes")
+        return b.value
+
     def set_stream(self, stream_ptr: int) -> None:
         check(lib.bcmg_set_stream(self._h, C.c_void_p(stream_ptr)), "bcmg_set_stream")
 
@@ -286,6 +328,75 @@ class Handle:
                                   _ptr(D), _ptr(M), None if last else _ptr(agg),
                                   None if last else _ptr(p), _ptr(w)), "level_copy")
         return LevelData(n, nnz, nc, CsrMatrix(n, row, col, val), D, M, w, agg, p)
+
+
+@dataclass
+class RequestResult:
+    solve: SolveResult
+    latency_ms: float
+    queue_ms: float
+    group: int
+    cache_hit: bool
+
+
+class Server:
+    """Solve server (bcmg_server_*): continuous batching of solve requests
+    with a hierarchy cache and memory-capped admission on one GPU."""
+
+    def __init__(self, params: Params, ext: Extensions | None = None, slots: int = 4,
+                 mem_cap_gb: float = 150.0, cache_cap_gb: float = 60.0, max_batch: int = 32,
+                 device: int = 0):
+        o = _lib.ServerOpts()
+        lib.bcmg_server_opts_default(C.byref(o))
+        o.device, o.slots, o.mem_cap_gb = device, slots, mem_cap_gb
+        o.cache_cap_gb, o.max_batch = cache_cap_gb, max_batch
+        o.params = params.to_c()
+        o.ext = (ext or Extensions(device=device)).to_c()
+        self._s = C.c_void_p()
+        check(lib.bcmg_server_create(C.byref(o), C.byref(self._s)), "bcmg_server_create")
+        self._live = {}  # ticket -> objects that must outlive the request
+
+    def submit(self, A: CsrMatrix, b: np.ndarray, key: int = 0) -> int:
+        c = A.as_c()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(A.n)
+        t = C.c_uint64()
+        check(lib.bcmg_server_submit(self._s, C.byref(c), key, _ptr(b), _ptr(x), C.byref(t)),
+              "bcmg_server_submit")
+        self._live[t.value] = (c, A, x)
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = -1.0) -> tuple[np.ndarray, RequestResult]:
+        info = _lib.RequestInfo()
+        st = lib.bcmg_server_wait(self._s, ticket, timeout, C.byref(info))
+        if st == ERR_PENDING:
+            raise TimeoutError(f"request {ticket} pending")
+        _, _, x = self._live.pop(ticket, (None, None, None))
+        check(st, "bcmg_server_wait")
+        return x, RequestResult(SolveResult.from_c(info.solve), info.latency_ms, info.queue_ms,
+                                info.group, bool(info.cache_hit))
+
+    def stats(self) -> dict:
+        s = _lib.ServerStats()
+        check(lib.bcmg_server_stats_get(self._s, C.byref(s)), "bcmg_server_stats_get")
+        return {f: getattr(s, f) for f, _ in _lib.ServerStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_s", None) and self._s.value:
+            lib.bcmg_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def solve(A: CsrMatrix, params: Params, rhs: np.ndarray,

@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <memory>
 
 #include <nvtx3/nvToolsExt.h>
@@ -61,6 +62,43 @@ double ms_since(Clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
 }
 
+// Phase timing report for ext.verbose >= 1: synchronises the stream at each
+// phase boundary and accumulates wall time per phase name (stderr).
+struct PhaseClock {
+  bool on = false;
+  cudaStream_t s = nullptr;
+  Clock::time_point t;
+  std::vector<std::pair<const char *, double>> acc;
+  void start(bool enable, cudaStream_t st) {
+    on = enable;
+    s = st;
+    acc.clear();
+    if (on) {
+      cudaStreamSynchronize(s);
+      t = Clock::now();
+    }
+  }
+  void tick(const char *name) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    const double ms = ms_since(t);
+    t = Clock::now();
+    for (auto &a : acc)
+      if (a.first == name) {
+        a.second += ms;
+        return;
+      }
+    acc.emplace_back(name, ms);
+  }
+  void report(const char *what) {
+    if (!on) return;
+    fprintf(stderr, "[bcmg] %s:", what);
+    for (auto &a : acc) fprintf(stderr, " %s=%.2fms", a.first, a.second);
+    fprintf(stderr, "\n");
+  }
+};
+thread_local PhaseClock g_clock;
+
 bcmg_status read_scalar(const double *dev, double *host, cudaStream_t s) {
   BCMG_CUDA(cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
@@ -69,7 +107,10 @@ bcmg_status read_scalar(const double *dev, double *host, cudaStream_t s) {
 
 // ||x||_A = sqrt(x' A x) (CSRm::vectorANorm, src/matrix/CSR.cu:360-368).
 bcmg_status anorm(bcmg_handle *h, const double *x, double *out) {
-  BCMG_TRY(spmv(h->A0.view(), 1.0, x, 0.0, h->tmp, h->stream));
+  if (h->A0.own64.nslices)
+    BCMG_TRY(sliced_spmv(h->A0.own64.view(), x, h->tmp, h->stream));
+  else
+    BCMG_TRY(spmv(h->A0.view(), 1.0, x, 0.0, h->tmp, h->stream));
   BCMG_TRY(dot_dev(h->A0.n, h->tmp, x, h->scal + kAlpha, h->partials, h->stream));
   double v = 0;
   BCMG_TRY(read_scalar(h->scal + kAlpha, &v, h->stream));
@@ -107,22 +148,28 @@ bcmg_status matching_aggregation(bcmg_handle *h, DevLevel &fine, double **w_out,
     int32_t nci = 0;
     BCMG_TRY(agg_i.alloc(cur.n, s));
     BCMG_TRY(p_i.alloc(cur.n, s));
+    g_clock.tick("other");
     BCMG_TRY(pair_aggregate(cur, cur_w, agg_i.get(), p_i.get(), &nci, nullptr, nullptr,
                             nullptr, s));
+    g_clock.tick("match+aggregate");
     BCMG_TRY(rptr_i.alloc(nci + 1, s));
     BCMG_TRY(ridx_i.alloc(cur.n, s));
     BCMG_TRY(transpose_agg(cur.n, agg_i.get(), nci, rptr_i.get(), ridx_i.get(), s));
     // Galerkin product (matchingAggregation.cu:239-244).
     int32_t cnnz = 0;
     BCMG_TRY(crow.alloc(nci + 1, s));
-    BCMG_TRY(galerkin_count(cur, agg_i.get(), p_i.get(), nci, rptr_i.get(), ridx_i.get(),
-                            crow.get(), &cnnz, s));
+    int32_t *ccol_raw = nullptr;
+    double *cval_raw = nullptr;
+    g_clock.tick("transpose");
+    BCMG_TRY(galerkin(cur, agg_i.get(), p_i.get(), nci, rptr_i.get(), ridx_i.get(), crow.get(),
+                      &ccol_raw, &cval_raw, &cnnz, s));
+    g_clock.tick("galerkin");
     DevBuf<int32_t> ccol;
     DevBuf<double> cval;
-    BCMG_TRY(ccol.alloc(cnnz, s));
-    BCMG_TRY(cval.alloc(cnnz, s));
-    BCMG_TRY(galerkin_fill(cur, agg_i.get(), p_i.get(), nci, rptr_i.get(), ridx_i.get(),
-                           crow.get(), ccol.get(), cval.get(), s));
+    ccol.ptr = ccol_raw;
+    ccol.stream = s;
+    cval.ptr = cval_raw;
+    cval.stream = s;
     // w_i = R_i w_{i-1} (matchingAggregation.cu:253).
     BCMG_TRY(wi.alloc(nci, s));
     BCMG_TRY(restrict_exact(nci, rptr_i.get(), ridx_i.get(), p_i.get(), cur_w, wi.get(), s));
@@ -175,6 +222,7 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
   l0.col = h->A0.col;
   l0.val = h->A0.val;
   l0.own_A = false;
+  if (h->A0.own64.nslices) l0.s64 = &h->A0.own64;
   BCMG_TRY(dev_alloc(&l0.D, l0.n, s));
   BCMG_TRY(dev_alloc(&l0.M, l0.n, s));
   BCMG_TRY(dev_alloc(&l0.w, l0.n, s));
@@ -196,6 +244,10 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
       BCMG_TRY(dev_alloc(&coarse.D, coarse.n, s));
       BCMG_TRY(dev_alloc(&coarse.M, coarse.n, s));
       BCMG_TRY(level_prep(coarse.view(), coarse.D, coarse.M, s));
+      // FP64 sliced copy now if an FP64 cycle will read this level (the FP64
+      // solve, or the bootstrap's inner iterations).
+      if (h->ext.sliced && (h->ext.precision == BCMG_PREC_FP64 || h->prm.max_hrc > 1))
+        BCMG_TRY(sliced_build(coarse.view(), kValF64, &coarse.own64, s));
       const double size_coarse = coarse.n;
       const double coarse_ratio = fine.n / size_coarse;
       avcoarseratio += coarse_ratio;
@@ -278,13 +330,26 @@ void free_buffers_t(CycleBufs<XT> &B, cudaStream_t s) {
 // The level data a cycle of vector type XT reads.
 template <typename XT>
 struct Lv;
+// The sliced copies of a level: level 0 points to the handle's shared copy,
+// other levels own theirs (resolved here, never stored as a self-pointer,
+// since levels live in a growing std::vector).
+inline const SlicedMat *sliced64(const DevLevel &l) {
+  if (l.s64) return l.s64;
+  return l.own64.nslices ? &l.own64 : nullptr;
+}
+inline const SlicedMat *slicedlo(const DevLevel &l) {
+  if (l.slo) return l.slo;
+  return l.ownlo.nslices ? &l.ownlo : nullptr;
+}
+
 template <>
 struct Lv<double> {
   static MatView mat(const DevLevel &l) {
     MatView m = mat_f64(l.view());
-    if (l.s64 && l.s64->nslices) {
+    const SlicedMat *S = sliced64(l);
+    if (S && S->nslices) {
       m.has_sl = true;
-      m.sl = l.s64->view();
+      m.sl = S->view();
     }
     return m;
   }
@@ -302,9 +367,10 @@ struct Lv<float> {
     m.col = l.col;
     m.val = l.val_lo;
     m.vtype = l.vtype_lo;
-    if (l.slo && l.slo->nslices) {
+    const SlicedMat *S = slicedlo(l);
+    if (S && S->nslices) {
       m.has_sl = true;
-      m.sl = l.slo->view();
+      m.sl = S->view();
     }
     return m;
   }
@@ -417,6 +483,7 @@ bcmg_status inner_iterations(bcmg_handle *h, double *w) {
   BCMG_TRY(fill(rhs, n, 0.0, s));
   double normold = 0, normnew = 0, conv = 1.0;
   BCMG_TRY(anorm(h, x, &normold));
+  g_clock.tick("other");
   for (int i = 1; i <= kBootSolverIt; ++i) {
     BCMG_TRY(precond_apply(h, rhs, x, false, false));
     BCMG_TRY(anorm(h, x, &normnew));
@@ -426,6 +493,7 @@ bcmg_status inner_iterations(bcmg_handle *h, double *w) {
   BCMG_TRY(copy(w, x, n, s));
   BCMG_TRY(scale(n, 1.0 / normnew, w, s));
   h->estimated_ratio = conv;
+  g_clock.tick("inner_iterations");
   return BCMG_OK;
 }
 
@@ -490,10 +558,8 @@ bcmg_status prepare_solve_formats(bcmg_handle *h) {
       }
       if (h->mixed) {
         if (!lv.ownlo.nslices) BCMG_TRY(sliced_build(lv.view(), lv.vtype_lo, &lv.ownlo, s));
-        lv.slo = &lv.ownlo;
       } else {
         if (!lv.own64.nslices) BCMG_TRY(sliced_build(lv.view(), kValF64, &lv.own64, s));
-        lv.s64 = &lv.own64;
       }
     }
   }
@@ -507,8 +573,6 @@ bcmg_status alloc_work(bcmg_handle *h) {
     BCMG_TRY(dev_alloc(p, n, s));
   BCMG_TRY(dev_alloc(&h->partials, 4 * kRedBlocks, s));
   BCMG_TRY(dev_alloc(&h->scal, kNumScal, s));
-  BCMG_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->host_scal),
-                           sizeof(double) * kNumScal));
   BCMG_CUDA(cudaMemsetAsync(h->scal, 0, sizeof(double) * kNumScal, s));
   return BCMG_OK;
 }
@@ -546,7 +610,7 @@ void destroy_handle(bcmg_handle *h) {
   cudaSetDevice(h->device);
   cudaStream_t s = h->stream;
   if (h->fcg_exec) cudaGraphExecDestroy(h->fcg_exec);
-  if (h->host_scal) cudaFreeHost(h->host_scal);
+  destroy_batch(h);
   for (auto &H : h->H) H.release(s);
   h->A0.own_A = true;
   h->A0.release(s);
@@ -563,6 +627,7 @@ void destroy_handle(bcmg_handle *h) {
 bcmg_status setup_common(bcmg_handle *h) {
   NvtxRange range("bcmg_setup");
   const auto t0 = Clock::now();
+  g_clock.start(h->ext.verbose >= 1, h->stream);
   const int32_t n = h->A0.n;
   // BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311).
   h->maxcoarsesize = static_cast<int32_t>(40 * std::pow(static_cast<double>(n), 1. / 3.));
@@ -576,12 +641,18 @@ bcmg_status setup_common(bcmg_handle *h) {
     for (int i = 0; i < ml - 1; ++i) h->grid_sweeps[i] = 2;
   }
   BCMG_TRY(alloc_work(h));
+  if (h->ext.sliced) BCMG_TRY(sliced_build(h->A0.view(), kValF64, &h->A0.own64, h->stream));
+  g_clock.tick("alloc");
   BCMG_TRY(bootstrap(h));
+  g_clock.tick("other");
   h->mixed = h->ext.precision == BCMG_PREC_MIXED;
   if (h->mixed) BCMG_TRY(prepare_mixed(h));
+  g_clock.tick("mixed_copies");
   if (h->ext.sliced) BCMG_TRY(prepare_solve_formats(h));
+  g_clock.tick("sliced_copies");
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
   h->setup_ms = ms_since(t0);
+  g_clock.report("setup");
   return BCMG_OK;
 }
 
@@ -599,6 +670,14 @@ bcmg_status new_handle(const bcmg_params *p, const bcmg_ext *ext, bcmg_handle **
     return set_error(BCMG_ERR_PARAM, "unknown precision mode %d", h->ext.precision);
   h->device = h->ext.device;
   BCMG_CUDA(cudaSetDevice(h->device));
+  // Keep freed blocks in the device's default pool (the stream-ordered
+  // allocator every work array comes from) instead of returning them to the
+  // driver at each synchronisation: repeated setups then reuse the mappings.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   if (h->ext.stream) {
     h->stream = static_cast<cudaStream_t>(h->ext.stream);
     h->own_stream = false;
@@ -638,51 +717,9 @@ bcmg_status fcg_iteration(bcmg_handle *h, cudaGraphConditionalHandle cond, bool 
 // iteration until the device-side condition (k_fcg_continue) turns false,
 // so a whole solve needs no host round trip per iteration.
 bcmg_status build_fcg_graph(bcmg_handle *h) {
-  cudaGraph_t g = nullptr;
-  BCMG_CUDA(cudaGraphCreate(&g, 0));
-  cudaGraphConditionalHandle cond;
-  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
-    return set_error(BCMG_ERR_CUDA, "conditional handle: %s", cudaGetErrorString(e));
-  }
-  // cudaGraphNodeParams has no default constructor (it holds a union); use
-  // zeroed storage as the CUDA samples do with their C-style initializers.
-  alignas(cudaGraphNodeParams) unsigned char np_storage[sizeof(cudaGraphNodeParams)];
-  std::memset(np_storage, 0, sizeof(np_storage));
-  cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_storage);
-  np.type = cudaGraphNodeTypeConditional;
-  np.conditional.handle = cond;
-  np.conditional.type = cudaGraphCondTypeWhile;
-  np.conditional.size = 1;
-  cudaGraphNode_t node;
-  e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
-    return set_error(BCMG_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
-  }
-  cudaGraph_t body = np.conditional.phGraph_out[0];
-  e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
-                                    cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
-    return set_error(BCMG_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
-  }
-  bcmg_status st = fcg_iteration(h, cond, true);
-  e = cudaStreamEndCapture(h->stream, &body);
-  if (st != BCMG_OK || e != cudaSuccess) {
-    cudaGetLastError();
-    cudaGraphDestroy(g);
-    return st != BCMG_OK ? st
-                         : set_error(BCMG_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
-  }
-  e = cudaGraphInstantiate(&h->fcg_exec, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) {
-    h->fcg_exec = nullptr;
-    return set_error(BCMG_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
-  }
-  return BCMG_OK;
+  return capture_while_loop(
+      h->stream, [h](cudaGraphConditionalHandle cond) { return fcg_iteration(h, cond, true); },
+      &h->fcg_exec);
 }
 
 // FCG (flexibileConjugateGradients_v3, src/SOLVER/FCG.cu:433-585) on device
@@ -723,10 +760,12 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
   BCMG_TRY(fcg_update(n, true, v, d, w, q, x, r, h->partials, h->scal, s));
   double *hs = h->host_scal;
   const bool graphs = h->ext.use_graphs && h->ext.verbose < 2 && h->stream != nullptr;
+  g_clock.tick("first_step");
   if (graphs && !h->fcg_exec && build_fcg_graph(h) != BCMG_OK) {
     clear_error();
     h->fcg_exec = nullptr;
   }
+  g_clock.tick("graph_build");
   if (graphs && h->fcg_exec) {
     BCMG_CUDA(cudaGraphLaunch(h->fcg_exec, s));
     BCMG_CUDA(cudaMemcpyAsync(hs, h->scal, sizeof(double) * kNumScal, cudaMemcpyDeviceToHost,
@@ -743,6 +782,7 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
                static_cast<int>(hs[kIter]) - 1, hs[kNorm], hs[kNorm] / delta0);
     } while (hs[kNorm] > target && hs[kIter] < h->prm.itnlim && hs[kIndef] == 0.0);
   }
+  g_clock.tick("fcg_loop");
   const double l2 = hs[kNorm];
   const int iter = static_cast<int>(hs[kIter]);
   info->iters = iter + 1;  // FCG.cu:569
@@ -762,6 +802,103 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
 }
 
 }  // namespace
+
+// Device bytes a level holds (pointer fields that are set; shared arrays are
+// counted by their owner).
+size_t level_bytes(const DevLevel &l) {
+  const size_t n = static_cast<size_t>(l.n), nnz = static_cast<size_t>(l.nnz);
+  size_t b = 0;
+  if (l.own_A && l.row) b += 4 * (n + 1) + 12 * nnz;
+  for (const double *v : {l.D, l.M, l.w, l.p})
+    if (v) b += 8 * n;
+  if (l.agg) b += 4 * n;
+  if (l.rptr) b += 4 * (static_cast<size_t>(l.nc) + 1);
+  if (l.ridx) b += 4 * n;
+  if (l.own_lo && l.val_lo) b += (l.vtype_lo == kValF32 ? 4 : 2) * nnz;
+  for (const float *v : {l.D32, l.M32, l.p32})
+    if (v) b += 4 * n;
+  return b + l.own64.bytes() + l.ownlo.bytes();
+}
+
+template <typename XT>
+size_t cycle_bytes(const CycleBufs<XT> &B, size_t n0, size_t width) {
+  size_t b = 0;
+  for (size_t l = 0; l < B.n.size(); ++l) {
+    const size_t per = static_cast<size_t>(B.n[l]) * width * sizeof(XT);
+    b += per * ((B.xt[l] ? 1 : 0) + (B.res[l] ? 1 : 0));
+    if (l > 0) b += per * ((B.rhs[l] ? 1 : 0) + (B.x[l] ? 1 : 0));
+  }
+  const XT *top[] = {B.xk, B.xadd, B.in0, B.out0};
+  for (const XT *v : top)
+    if (v) b += n0 * width * sizeof(XT);
+  return b;
+}
+template size_t cycle_bytes<double>(const CycleBufs<double> &, size_t, size_t);
+template size_t cycle_bytes<float>(const CycleBufs<float> &, size_t, size_t);
+
+size_t handle_bytes(const bcmg_handle *h) {
+  const size_t n = static_cast<size_t>(h->A0.n);
+  size_t b = 4 * (n + 1) + 12 * static_cast<size_t>(h->A0.nnz);
+  if (h->A0.val_lo) b += 4 * static_cast<size_t>(h->A0.nnz);
+  b += h->A0.own64.bytes() + h->A0.ownlo.bytes();
+  for (const auto &H : h->H)
+    for (const auto &l : H.lv) b += level_bytes(l);
+  b += cycle_bytes(h->c64, n, 1) + cycle_bytes(h->c32, n, 1);
+  b += 8 * 8 * n + 8 * (4 * static_cast<size_t>(kRedBlocks) + kNumScal);
+  return b + batch_bytes(h);
+}
+
+bcmg_status capture_while_loop(cudaStream_t stream,
+                               const std::function<bcmg_status(cudaGraphConditionalHandle)> &body_fn,
+                               cudaGraphExec_t *out) {
+  *out = nullptr;
+  cudaGraph_t g = nullptr;
+  BCMG_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle cond;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_error(BCMG_ERR_CUDA, "conditional handle: %s", cudaGetErrorString(e));
+  }
+  // cudaGraphNodeParams has no default constructor (it holds a union); use
+  // zeroed storage as the CUDA samples do with their C-style initializers.
+  alignas(cudaGraphNodeParams) unsigned char np_storage[sizeof(cudaGraphNodeParams)];
+  std::memset(np_storage, 0, sizeof(np_storage));
+  cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_storage);
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_error(BCMG_ERR_CUDA, "conditional node: %s", cudaGetErrorString(e));
+  }
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return set_error(BCMG_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+  }
+  bcmg_status st = body_fn(cond);
+  e = cudaStreamEndCapture(stream, &body);
+  if (st != BCMG_OK || e != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return st != BCMG_OK ? st
+                         : set_error(BCMG_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+  }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return set_error(BCMG_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+  }
+  return BCMG_OK;
+}
+
 }  // namespace bcmg
 
 using namespace bcmg;
@@ -831,6 +968,7 @@ bcmg_status bcmg_solve(bcmg_handle *h, const double *b, double *x, int on_device
   BCMG_CUDA(cudaSetDevice(h->device));
   NvtxRange range("bcmg_solve");
   const auto t0 = Clock::now();
+  g_clock.start(h->ext.verbose >= 1, h->stream);
   const int32_t n = h->A0.n;
   const cudaMemcpyKind in = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   BCMG_CUDA(cudaMemcpyAsync(h->b, b, sizeof(double) * n, in, h->stream));
@@ -840,6 +978,8 @@ bcmg_status bcmg_solve(bcmg_handle *h, const double *b, double *x, int on_device
   BCMG_CUDA(cudaMemcpyAsync(x, h->xs, sizeof(double) * n, outk, h->stream));
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
   info->solve_ms = ms_since(t0);
+  g_clock.tick("finish");
+  g_clock.report("solve");
   info->setup_ms = h->setup_ms;
   info->num_hrc = static_cast<int>(h->H.size());
   info->estimated_ratio = h->estimated_ratio;
@@ -859,6 +999,12 @@ bcmg_status bcmg_solve_legacy(const bcmg_csr *A, const bcmg_params *p, const bcm
 
 unsigned long long bcmg_kernel_launches(void) {
   return g_kernel_launches.load(std::memory_order_relaxed);
+}
+
+bcmg_status bcmg_device_bytes(const bcmg_handle *h, uint64_t *bytes) {
+  if (!h || !bytes) return set_error(BCMG_ERR_PARAM, "null argument");
+  *bytes = handle_bytes(h);
+  return BCMG_OK;
 }
 
 bcmg_status bcmg_destroy(bcmg_handle *h) {
@@ -980,7 +1126,7 @@ bcmg_status bcmg_level_format(const bcmg_handle *h, int hrc, int level, int64_t 
   if (level < 0 || level >= static_cast<int>(H.lv.size()))
     return set_error(BCMG_ERR_PARAM, "bad level index");
   const DevLevel &lv = H.lv[level];
-  const SlicedMat *S = h->mixed ? lv.slo : lv.s64;
+  const SlicedMat *S = h->mixed ? slicedlo(lv) : sliced64(lv);
   if (slots) *slots = S ? S->slots : 0;
   if (slices) *slices = S ? S->nslices : 0;
   if (value_bytes)
@@ -1041,15 +1187,18 @@ bcmg_status bcmg_k_galerkin(int32_t n, int32_t nnz, const int32_t *d_row,
   BCMG_TRY(rptr.alloc(n_coarse + 1, s));
   BCMG_TRY(ridx.alloc(n, s));
   BCMG_TRY(transpose_agg(n, d_agg, n_coarse, rptr.get(), ridx.get(), s));
-  if (!d_ccol || !d_cval) {
-    int32_t cnnz = 0;
-    BCMG_TRY(galerkin_count(A, d_agg, d_p, n_coarse, rptr.get(), ridx.get(), d_crow, &cnnz,
-                            s));
-    if (c_nnz) *c_nnz = cnnz;
-  } else {
-    BCMG_TRY(galerkin_fill(A, d_agg, d_p, n_coarse, rptr.get(), ridx.get(), d_crow, d_ccol,
-                           d_cval, s));
+  int32_t *ccol = nullptr;
+  double *cval = nullptr;
+  int32_t cnnz = 0;
+  BCMG_TRY(galerkin(A, d_agg, d_p, n_coarse, rptr.get(), ridx.get(), d_crow, &ccol, &cval,
+                    &cnnz, s));
+  if (c_nnz) *c_nnz = cnnz;
+  if (d_ccol && d_cval && cnnz > 0) {
+    BCMG_CUDA(cudaMemcpyAsync(d_ccol, ccol, sizeof(int32_t) * cnnz, cudaMemcpyDeviceToDevice, s));
+    BCMG_CUDA(cudaMemcpyAsync(d_cval, cval, sizeof(double) * cnnz, cudaMemcpyDeviceToDevice, s));
   }
+  dev_free(ccol, s);
+  dev_free(cval, s);
   BCMG_CUDA(cudaStreamSynchronize(s));
   return BCMG_OK;
 }

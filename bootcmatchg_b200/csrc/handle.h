@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <vector>
 
 #include "bcmg.h"
@@ -63,6 +64,23 @@ struct CycleBufs {
   XT *xk = nullptr, *xadd = nullptr, *in0 = nullptr, *out0 = nullptr;
 };
 
+// Multi-right-hand-side solve state (batch.cu), created by the first batched
+// solve of a handle.
+struct BatchState;
+void destroy_batch(bcmg_handle *h);
+size_t batch_bytes(const bcmg_handle *h);  // device bytes of the batch state
+
+// Device bytes held by a handle (hierarchies, solve copies, work vectors).
+size_t handle_bytes(const bcmg_handle *h);
+template <typename XT>
+size_t cycle_bytes(const CycleBufs<XT> &B, size_t n0, size_t width);
+
+// Captures body(cond) into the body of a WHILE node (initial condition 1) and
+// instantiates the graph.
+bcmg_status capture_while_loop(cudaStream_t stream,
+                               const std::function<bcmg_status(cudaGraphConditionalHandle)> &body,
+                               cudaGraphExec_t *out);
+
 }  // namespace bcmg
 
 struct bcmg_handle {
@@ -83,7 +101,8 @@ struct bcmg_handle {
   double *r = nullptr, *v = nullptr, *w = nullptr, *d = nullptr, *q = nullptr;
   double *b = nullptr, *xs = nullptr, *tmp = nullptr;
   double *partials = nullptr, *scal = nullptr;
-  double *host_scal = nullptr;          // pinned mirror of scal
+  double host_scal[bcmg::kNumScal] = {};  // host mirror of scal
   cudaGraphExec_t fcg_exec = nullptr;   // captured FCG loop (WHILE node)
+  bcmg::BatchState *batch = nullptr;    // multi-right-hand-side solves
   double setup_ms = 0.0;
 };

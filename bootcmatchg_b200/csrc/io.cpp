@@ -287,6 +287,7 @@ const char *bcmg_status_string(int status) {
     case BCMG_ERR_INVALID_MATRIX: return "BCMG_ERR_INVALID_MATRIX";
     case BCMG_ERR_UNSUPPORTED: return "BCMG_ERR_UNSUPPORTED";
     case BCMG_ERR_INTERNAL: return "BCMG_ERR_INTERNAL";
+    case BCMG_ERR_PENDING: return "BCMG_ERR_PENDING";
     default: return "BCMG_ERR_UNKNOWN";
   }
 }
@@ -463,6 +464,7 @@ void bcmg_ext_default(bcmg_ext *e) {
   e->max_device_seconds = 60.0;
   e->stream = nullptr;
   e->sliced = 1;
+  e->autotune = 1;
 }
 
 }  // extern "C"

@@ -71,18 +71,21 @@ __device__ __forceinline__ unsigned group_mask() {
 }
 
 // min |AH| over off-diagonal entries (find_Max_Min with AbsMin,
-// src/AMG/matching.cu:319-329,401-431).  Non-negative doubles order like
-// their bit patterns, so the global min is an integer atomicMin.
+// src/AMG/matching.cu:319-329,401-431).  Grid-stride over rows, block
+// reduction, one atomicMin per block: non-negative doubles order like their
+// bit patterns, so the global min is an integer atomicMin (exact, order-free).
 template <int G>
-__global__ void k_ah_min(int32_t n, const int32_t *__restrict__ row,
-                         const int32_t *__restrict__ col,
-                         const double *__restrict__ val, const double *__restrict__ w,
-                         const double *__restrict__ C, unsigned long long *min_bits) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int32_t i = static_cast<int32_t>(t / G);
+__global__ void __launch_bounds__(256)
+    k_ah_min(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+             const double *__restrict__ val, const double *__restrict__ w,
+             const double *__restrict__ C, unsigned long long *min_bits) {
+  __shared__ double wmin[8];
   const int lane = threadIdx.x % G;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
   double m = DBL_MAX;
-  if (i < n) {
+  for (int64_t gi = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G; gi < n;
+       gi += stride) {
+    const int32_t i = static_cast<int32_t>(gi);
     const double ci = C[i], wi = w[i];
     for (int32_t j = row[i] + lane; j < row[i + 1]; j += G) {
       const int32_t c = col[j];
@@ -93,8 +96,13 @@ __global__ void k_ah_min(int32_t n, const int32_t *__restrict__ row,
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m < DBL_MAX)
-    atomicMin(min_bits, static_cast<unsigned long long>(__double_as_longlong(m)));
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < static_cast<int>(blockDim.x >> 5); ++k) m = fmin(m, wmin[k]);
+    if (m < DBL_MAX)
+      atomicMin(min_bits, static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
 }
 
 // W_ij = log(|AH_ij| / (0.999 mu)) (_make_w with MAXIMUM_PRODUCT_MATRIX_OP 1,
@@ -119,82 +127,233 @@ __global__ void k_make_W(int32_t n, const int32_t *__restrict__ row,
   }
 }
 
-// Suitor matching (kernel_for_matching, src/AMG/suitor.cu:242-392).  A group
-// of G lanes works one proposer at a time: it finds the neighbour y of
-// largest (W_xy, y) whose current offer it beats (find_Candidate,
-// suitor.cu:118-214), then installs its offer with a 64-bit CAS.  An offer is
-// (edge index << 32 | proposer): the edge index recovers the immutable weight,
-// so no lock is needed (the reference spins on per-vertex locks,
-// suitor.cu:19-38,69-110).  A displaced proposer is taken over by the
-// displacing group (set_suitor, suitor.cu:89-93).  Offers only increase under
-// the strict order (weight, proposer id), so the final state is the unique
-// proposer-optimal one whatever the interleaving.  Each group is bounded by
-// `limit` iterations; on overrun it raises *err and returns.
-template <int G>
-__global__ void k_suitor(int32_t n, const int32_t *__restrict__ row,
-                         const int32_t *__restrict__ col, const double *__restrict__ W,
-                         unsigned long long *offer, int64_t limit, int *err) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int32_t gid = static_cast<int32_t>(t / G);
-  const int lane = threadIdx.x % G;
-  if (gid >= n) return;
-  const unsigned mask = group_mask<G>();
-  volatile unsigned long long *voffer = offer;
-  int32_t cur = gid;
-  for (int64_t it = 0;; ++it) {
-    if (it >= limit) {
-      if (lane == 0) atomicExch(err, 1);
-      return;
+// Suitor matching (kernel_for_matching, src/AMG/suitor.cu:242-392).
+//
+// Preferences are static: proposer x ranks its neighbours y by (W_xy, y)
+// descending (find_Candidate, suitor.cu:118-214, ties to the higher id), so
+// each row is first sorted into that order (k_sort_prefs).  A proposer offers
+// to the first neighbour in its sorted row whose current offer it beats; a
+// receiver keeps the best offer under (weight, proposer id) (suitor.cu:158).
+// Offers only increase, so a neighbour a proposer once could not beat (or was
+// displaced from) stays unbeatable: each proposer resumes its scan where it
+// stopped (next[]), and all proposals together read each row about once.
+// An offer is one 64-bit word (sorted position << 32 | proposer); the
+// position recovers the immutable weight, so a CAS replaces the reference's
+// per-vertex spin locks (suitor.cu:19-38,69-110).  A displaced proposer is
+// taken over by the displacing thread (set_suitor, suitor.cu:89-93).  The
+// final state is the proposer-optimal (Gale-Shapley) one, independent of the
+// interleaving.  next[] is written without synchronisation: any value a
+// thread can observe is a valid resume point (it never skips a neighbour
+// that could still be beaten), so a stale read only costs a rescan.
+
+// Position-ordered preference: a before b.
+__device__ __forceinline__ bool pref_before(double wa, int32_t ya, double wb, int32_t yb) {
+  return wa > wb || (wa == wb && ya > yb);
+}
+
+constexpr int kSortCap = 1024;        // entries per warp (shared memory sort)
+constexpr int kSortCapLong = 4096;    // entries per block
+constexpr int kSortWarps = 4;
+
+// Sorts rows of W (over A's pattern) into preference order: sW, scol.
+// Unusable entries (diagonal, W <= 0, NaN) sort last as -1.
+__global__ void __launch_bounds__(kSortWarps * 32)
+    k_sort_prefs(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+                 const double *__restrict__ W, double *sW, int32_t *scol, int32_t *long_rows,
+                 int32_t *n_long) {
+  __shared__ double shw[kSortWarps][kSortCap];
+  __shared__ int32_t shy[kSortWarps][kSortCap];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int32_t i = blockIdx.x * kSortWarps + wid;
+  if (i >= n) return;
+  const int32_t b = row[i], T = row[i + 1] - b;
+  auto usable = [&](int32_t j, double wv) { return col[j] != i && wv > 0.0; };
+  if (T <= 32) {
+    // Register bitonic sort across the warp.
+    double wv = -1.0;
+    int32_t yv = -1;
+    if (lane < T) {
+      const double x = W[b + lane];
+      yv = col[b + lane];
+      wv = usable(b + lane, x) ? x : -1.0;
     }
-    double bw = 0.0;
-    int32_t by = -1, be = -1;
-    unsigned long long bo = kNoOffer;
-    const int32_t jb = row[cur], je = row[cur + 1];
-    for (int32_t k = jb + lane; k < je; k += G) {
-      const int32_t y = col[k];
-      const double we = W[k];
-      if (y == cur || !(we > 0.0)) continue;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        const double pw = __shfl_xor_sync(0xffffffffu, wv, j);
+        const int32_t py = __shfl_xor_sync(0xffffffffu, yv, j);
+        const bool lower = (lane & j) == 0;
+        const bool asc = (lane & k) == 0;
+        const bool pb = pref_before(pw, py, wv, yv);  // partner ranks first
+        const bool take = (lower == asc) ? pb : !pb;
+        if (take) {
+          wv = pw;
+          yv = py;
+        }
+      }
+    }
+    if (lane < T) {
+      sW[b + lane] = wv;
+      scol[b + lane] = yv;
+    }
+    return;
+  }
+  if (T > kSortCap) {
+    if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
+    return;
+  }
+  int P2 = 64;
+  while (P2 < T) P2 <<= 1;
+  double *ws = shw[wid];
+  int32_t *ys = shy[wid];
+  for (int t = lane; t < P2; t += 32) {
+    if (t < T) {
+      const double x = W[b + t];
+      ws[t] = usable(b + t, x) ? x : -1.0;
+      ys[t] = col[b + t];
+    } else {
+      ws[t] = -1.0;
+      ys[t] = -1;
+    }
+  }
+  __syncwarp();
+  for (int k = 2; k <= P2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = lane; t < P2 / 2; t += 32) {
+        const int i0 = 2 * j * (t / j) + (t % j), i1 = i0 + j;
+        const bool asc = (i0 & k) == 0;
+        const bool swap = asc ? pref_before(ws[i1], ys[i1], ws[i0], ys[i0])
+                              : pref_before(ws[i0], ys[i0], ws[i1], ys[i1]);
+        if (swap) {
+          const double tw = ws[i0];
+          ws[i0] = ws[i1];
+          ws[i1] = tw;
+          const int32_t ty = ys[i0];
+          ys[i0] = ys[i1];
+          ys[i1] = ty;
+        }
+      }
+      __syncwarp();
+    }
+  for (int t = lane; t < T; t += 32) {
+    sW[b + t] = ws[t];
+    scol[b + t] = ys[t];
+  }
+}
+
+// Same sort for the rows queued as longer than kSortCap: each block takes
+// queue entries blockIdx.x, blockIdx.x + gridDim.x, ...
+__global__ void __launch_bounds__(256)
+    k_sort_prefs_long(const int32_t *__restrict__ long_rows, const int32_t *__restrict__ n_long,
+                      const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+                      const double *__restrict__ W, double *sW, int32_t *scol, int *err) {
+  extern __shared__ __align__(16) unsigned char sort_dyn[];
+  double *ws = reinterpret_cast<double *>(sort_dyn);
+  int32_t *ys = reinterpret_cast<int32_t *>(sort_dyn + sizeof(double) * kSortCapLong);
+  for (int32_t q = blockIdx.x; q < *n_long; q += gridDim.x) {
+  const int32_t i = long_rows[q];
+  const int32_t b = row[i], T = row[i + 1] - b;
+  if (T > kSortCapLong) {
+    if (threadIdx.x == 0) atomicExch(err, 2);
+    return;
+  }
+  int P2 = 64;
+  while (P2 < T) P2 <<= 1;
+  for (int t = threadIdx.x; t < P2; t += blockDim.x) {
+    if (t < T) {
+      const double x = W[b + t];
+      ws[t] = (col[b + t] != i && x > 0.0) ? x : -1.0;
+      ys[t] = col[b + t];
+    } else {
+      ws[t] = -1.0;
+      ys[t] = -1;
+    }
+  }
+  __syncthreads();
+  for (int k = 2; k <= P2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < P2 / 2; t += blockDim.x) {
+        const int i0 = 2 * j * (t / j) + (t % j), i1 = i0 + j;
+        const bool asc = (i0 & k) == 0;
+        const bool swap = asc ? pref_before(ws[i1], ys[i1], ws[i0], ys[i0])
+                              : pref_before(ws[i0], ys[i0], ws[i1], ys[i1]);
+        if (swap) {
+          const double tw = ws[i0];
+          ws[i0] = ws[i1];
+          ws[i1] = tw;
+          const int32_t ty = ys[i0];
+          ys[i0] = ys[i1];
+          ys[i1] = ty;
+        }
+      }
+      __syncthreads();
+    }
+  for (int t = threadIdx.x; t < T; t += blockDim.x) {
+    sW[b + t] = ws[t];
+    scol[b + t] = ys[t];
+  }
+  __syncthreads();
+  }
+}
+
+// One thread per initial proposer; `limit` bounds the steps of a thread
+// (advances, successful and failed CASes); on overrun *err is raised.
+__global__ void __launch_bounds__(256)
+    k_suitor(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ scol,
+             const double *__restrict__ sW, int32_t *next, unsigned long long *offer,
+             int64_t limit, int *err) {
+  const int32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n) return;
+  volatile unsigned long long *voffer = offer;
+  volatile int32_t *vnext = next;
+  int32_t cur = gid;
+  int64_t steps = 0;
+  while (true) {
+    int32_t k = vnext[cur];
+    const int32_t e = row[cur + 1];
+    unsigned long long won = kNoOffer;
+    bool found = false;
+    while (k < e) {
+      if (++steps > limit) {
+        atomicExch(err, 1);
+        return;
+      }
+      const double wk = sW[k];
+      if (!(wk > 0.0)) {
+        k = e;
+        break;
+      }
+      const int32_t y = scol[k];
       const unsigned long long o = voffer[y];
       double cw = 0.0;
       int32_t cid = -1;
       if (o != kNoOffer) {
-        cw = W[static_cast<int32_t>(o >> 32)];
+        cw = sW[static_cast<int32_t>(o >> 32)];
         cid = static_cast<int32_t>(o & 0xffffffffull);
       }
-      if (!(we > cw || (we == cw && cur > cid))) continue;
-      if (by < 0 || we > bw || (we == bw && y > by)) {
-        bw = we;
-        by = y;
-        be = k;
-        bo = o;
+      if (wk > cw || (wk == cw && cur > cid)) {
+        const unsigned long long mine =
+            (static_cast<unsigned long long>(static_cast<uint32_t>(k)) << 32) |
+            static_cast<uint32_t>(cur);
+        if (atomicCAS(offer + y, o, mine) == o) {
+          won = o;
+          found = true;
+          break;
+        }
+        continue;  // the offer changed: test the same neighbour again
       }
+      ++k;
     }
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) {
-      const double w2 = __shfl_xor_sync(mask, bw, o, G);
-      const int32_t y2 = __shfl_xor_sync(mask, by, o, G);
-      const int32_t e2 = __shfl_xor_sync(mask, be, o, G);
-      const unsigned long long o2 = __shfl_xor_sync(mask, bo, o, G);
-      const bool better = y2 >= 0 && (by < 0 || w2 > bw || (w2 == bw && y2 > by));
-      if (better) {
-        bw = w2;
-        by = y2;
-        be = e2;
-        bo = o2;
-      }
-    }
-    if (by < 0) return;
-    unsigned long long old = 0;
-    if (lane == 0)
-      old = atomicCAS(offer + by, bo,
-                      (static_cast<unsigned long long>(static_cast<uint32_t>(be)) << 32) |
-                          static_cast<uint32_t>(cur));
-    old = __shfl_sync(mask, old, 0, G);
-    if (old == bo) {
-      if (bo == kNoOffer) return;
-      cur = static_cast<int32_t>(bo & 0xffffffffull);
-    }
+    vnext[cur] = found ? k + 1 : e;
+    if (!found || won == kNoOffer) return;
+    cur = static_cast<int32_t>(won & 0xffffffffull);  // the displaced proposer
   }
+}
+
+__global__ void k_init_next(int32_t n, const int32_t *__restrict__ row, int32_t *next) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) next[i] = row[i];
 }
 
 __global__ void k_offer_to_suitor(int32_t n, const unsigned long long *__restrict__ offer,
@@ -448,17 +607,54 @@ __device__ bool gal_run_sum(const GalSmem &sm, int k, int T, int32_t *J, double 
   return true;
 }
 
-// Warp-team Galerkin: FILL=false counts distinct coarse columns into cnt[I];
-// FILL=true writes row I.  Rows over kGalCap terms are queued for the block
-// kernel (count pass) or skipped (fill pass).
-template <bool FILL>
+// Term count of each coarse row: the summed lengths of its members' rows.
+__global__ void k_gal_terms(int32_t nc, const int32_t *__restrict__ row,
+                            const int32_t *__restrict__ rptr,
+                            const int32_t *__restrict__ ridx, int32_t *tcount) {
+  const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nc) return;
+  int32_t t = 0;
+  for (int32_t k = rptr[I]; k < rptr[I + 1]; ++k) {
+    const int32_t i = ridx[k];
+    t += row[i + 1] - row[i];
+  }
+  tcount[I] = t;
+}
+
+// Writes the runs of a sorted coarse row: (J, sum) at tJ/tV[base + rank] and
+// the number of runs in runs[I].  Run by one warp.
+__device__ void gal_emit(const GalSmem &sm, int T, int32_t I, int64_t base, int32_t *tJ,
+                         double *tV, int32_t *runs, int *err, int lane) {
+  int carry = 0;
+  for (int b0 = 0; b0 < T; b0 += 32) {
+    const int k = b0 + lane;
+    const bool h = k < T && gal_head(sm, k);
+    const unsigned hm = __ballot_sync(0xffffffffu, h);
+    if (h) {
+      int32_t J;
+      double sum;
+      if (gal_run_sum(sm, k, T, &J, &sum)) {
+        const int64_t pos = base + carry + __popc(hm & ((1u << lane) - 1u));
+        tJ[pos] = J;
+        tV[pos] = sum;
+      } else {
+        atomicExch(err, 2);
+      }
+    }
+    carry += __popc(hm);
+  }
+  if (lane == 0) runs[I] = carry;
+}
+
+// Sort-and-reduce pass, one warp per coarse row; rows over kGalCap terms
+// are queued for k_gal_rows_long.
 __global__ void __launch_bounds__(kGalWarpsPerBlock * 32)
-    k_gal_warp(int32_t nc, const int32_t *__restrict__ row,
-               const int32_t *__restrict__ col, const double *__restrict__ val,
-               const int32_t *__restrict__ agg, const double *__restrict__ p,
-               const int32_t *__restrict__ rptr, const int32_t *__restrict__ ridx,
-               int32_t *cnt_or_crow, int32_t *ccol, double *cval, int32_t *long_rows,
-               int32_t *n_long, int *err) {
+    k_gal_rows(int32_t nc, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+               const double *__restrict__ val, const int32_t *__restrict__ agg,
+               const double *__restrict__ p, const int32_t *__restrict__ rptr,
+               const int32_t *__restrict__ ridx, const int32_t *__restrict__ tpos,
+               int32_t *tJ, double *tV, int32_t *runs, int32_t *long_rows, int32_t *n_long,
+               int *err) {
   extern __shared__ __align__(16) unsigned char gal_dyn[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t I = blockIdx.x * kGalWarpsPerBlock + wid;
@@ -467,73 +663,48 @@ __global__ void __launch_bounds__(kGalWarpsPerBlock * 32)
                         kGalCap);
   const int T = gal_gather<32>(I, row, col, val, agg, p, rptr, ridx, sm, kGalCap, lane);
   if (T < 0) {
-    if (!FILL && lane == 0) {
-      long_rows[atomicAdd(n_long, 1)] = I;
-      cnt_or_crow[I] = 0;
-    }
+    if (lane == 0) long_rows[atomicAdd(n_long, 1)] = I;
     return;
   }
-  int carry = 0;
-  const int32_t out0 = FILL ? cnt_or_crow[I] : 0;
-  for (int base = 0; base < T; base += 32) {
-    const int k = base + lane;
-    const bool h = k < T && gal_head(sm, k);
-    const unsigned hm = __ballot_sync(0xffffffffu, h);
-    if (FILL && h) {
-      int32_t J;
-      double s;
-      if (gal_run_sum(sm, k, T, &J, &s)) {
-        const int32_t pos = out0 + carry + __popc(hm & ((1u << lane) - 1u));
-        ccol[pos] = J;
-        cval[pos] = s;
-      } else {
-        atomicExch(err, 2);
-      }
-    }
-    carry += __popc(hm);
-  }
-  if (!FILL && lane == 0) cnt_or_crow[I] = carry;
+  gal_emit(sm, T, I, tpos[I], tJ, tV, runs, err, lane);
 }
 
-// Block-team Galerkin for the queued long rows (one block per row).
-template <bool FILL>
+// The queued long rows, one block per row (grid-stride over the queue).
 __global__ void __launch_bounds__(kGalLongThreads)
-    k_gal_long(const int32_t *__restrict__ long_rows, const int32_t *__restrict__ row,
-               const int32_t *__restrict__ col, const double *__restrict__ val,
-               const int32_t *__restrict__ agg, const double *__restrict__ p,
-               const int32_t *__restrict__ rptr, const int32_t *__restrict__ ridx,
-               int32_t *cnt_or_crow, int32_t *ccol, double *cval, int *err) {
+    k_gal_rows_long(const int32_t *__restrict__ long_rows, const int32_t *__restrict__ n_long,
+                    const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+                    const double *__restrict__ val, const int32_t *__restrict__ agg,
+                    const double *__restrict__ p, const int32_t *__restrict__ rptr,
+                    const int32_t *__restrict__ ridx, const int32_t *__restrict__ tpos,
+                    int32_t *tJ, double *tV, int32_t *runs, int *err) {
   extern __shared__ __align__(16) unsigned char gal_dyn[];
-  const int32_t I = long_rows[blockIdx.x];
   GalSmem sm = gal_smem(gal_dyn, kGalCapLong);
-  const int T = gal_gather<kGalLongThreads>(I, row, col, val, agg, p, rptr, ridx, sm,
-                                            kGalCapLong, threadIdx.x);
-  if (T < 0) {
-    if (threadIdx.x == 0) atomicExch(err, 3);
-    return;
-  }
-  if (threadIdx.x >= 32) return;
-  const int lane = threadIdx.x;
-  int carry = 0;
-  const int32_t out0 = FILL ? cnt_or_crow[I] : 0;
-  for (int base = 0; base < T; base += 32) {
-    const int k = base + lane;
-    const bool h = k < T && gal_head(sm, k);
-    const unsigned hm = __ballot_sync(0xffffffffu, h);
-    if (FILL && h) {
-      int32_t J;
-      double s;
-      if (gal_run_sum(sm, k, T, &J, &s)) {
-        const int32_t pos = out0 + carry + __popc(hm & ((1u << lane) - 1u));
-        ccol[pos] = J;
-        cval[pos] = s;
-      } else {
-        atomicExch(err, 2);
-      }
+  for (int32_t q = blockIdx.x; q < *n_long; q += gridDim.x) {
+    const int32_t I = long_rows[q];
+    const int T = gal_gather<kGalLongThreads>(I, row, col, val, agg, p, rptr, ridx, sm,
+                                              kGalCapLong, threadIdx.x);
+    if (T < 0) {
+      if (threadIdx.x == 0) atomicExch(err, 3);
+      return;
     }
-    carry += __popc(hm);
+    if (threadIdx.x < 32) gal_emit(sm, T, I, tpos[I], tJ, tV, runs, err, threadIdx.x);
+    __syncthreads();
   }
-  if (!FILL && lane == 0) cnt_or_crow[I] = carry;
+}
+
+// Moves each row's runs from its term-sized slot to its final CSR position.
+__global__ void k_gal_compact(int32_t nc, const int32_t *__restrict__ tpos,
+                              const int32_t *__restrict__ crow,
+                              const int32_t *__restrict__ tJ, const double *__restrict__ tV,
+                              int32_t *ccol, double *cval) {
+  const int lane = threadIdx.x & 31;
+  const int32_t I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (I >= nc) return;
+  const int32_t src = tpos[I], dst = crow[I], len = crow[I + 1] - crow[I];
+  for (int32_t k = lane; k < len; k += 32) {
+    ccol[dst + k] = tJ[src + k];
+    cval[dst + k] = tV[src + k];
+  }
 }
 
 // y[I] = sum over members i of I (ascending) of p_i x_i, from the first term.
@@ -569,18 +740,11 @@ bcmg_status launch_weights(const CsrView &A, const double *w, const double *C,
                            unsigned long long *min_bits, double *W, cudaStream_t s) {
   const int threads = 256;
   const int blocks = ceil_div(static_cast<int64_t>(A.n) * G, threads);
-  launch(k_ah_min<G>, blocks, threads, 0, s, A.n, A.row, A.col, A.val, w, C, min_bits);
+  launch(k_ah_min<G>, std::min(blocks, 8 * kNumSM), threads, 0, s, A.n, A.row, A.col, A.val, w,
+         C, min_bits);
   launch(k_make_W<G>, blocks, threads, 0, s, A.n, A.row, A.col, A.val, w, C, min_bits, W);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
-}
-
-template <int G>
-void launch_suitor(const CsrView &A, const double *W, unsigned long long *offer,
-                   int64_t limit, int *err, cudaStream_t s) {
-  const int threads = 256;
-  const int blocks = ceil_div(static_cast<int64_t>(A.n) * G, threads);
-  launch(k_suitor<G>, blocks, threads, 0, s, A.n, A.row, A.col, W, offer, limit, err);
 }
 
 }  // namespace
@@ -640,17 +804,32 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
     default: BCMG_TRY(launch_weights<32>(A, w, C.get(), minb.get(), W, s)); break;
   }
 
-  // Suitor matching; every group is bounded by the total number of
-  // successful offers (<= nnz) plus failed CASes (each caused by a success).
-  BCMG_CUDA(cudaMemsetAsync(offer.get(), 0xff, sizeof(unsigned long long) * n, s));
+  // Preference-sorted rows, then the suitor proposals.
+  DevBuf<double> sW;
+  DevBuf<int32_t> scol, next, long_rows, n_long;
+  BCMG_TRY(sW.alloc(A.nnz, s));
+  BCMG_TRY(scol.alloc(A.nnz, s));
+  BCMG_TRY(next.alloc(n, s));
+  BCMG_TRY(long_rows.alloc(n, s));
+  BCMG_TRY(n_long.alloc(1, s));
+  BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
-  const int64_t limit = 2 * static_cast<int64_t>(A.nnz) + 64;
-  switch (G) {
-    case 4: launch_suitor<4>(A, W, offer.get(), limit, err.get(), s); break;
-    case 8: launch_suitor<8>(A, W, offer.get(), limit, err.get(), s); break;
-    case 16: launch_suitor<16>(A, W, offer.get(), limit, err.get(), s); break;
-    default: launch_suitor<32>(A, W, offer.get(), limit, err.get(), s); break;
+  launch(k_sort_prefs, ceil_div(n, kSortWarps), kSortWarps * 32, 0, s, n, A.row, A.col, W,
+         sW.get(), scol.get(), long_rows.get(), n_long.get());
+  {
+    const size_t smem = (sizeof(double) + sizeof(int32_t)) * kSortCapLong;
+    BCMG_CUDA(cudaFuncSetAttribute(k_sort_prefs_long,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    launch(k_sort_prefs_long, std::min(n, kNumSM), 256, smem, s, long_rows.get(),
+           n_long.get(), A.row, A.col, W, sW.get(), scol.get(), err.get());
+    BCMG_LAUNCH_CHECK();
   }
+  BCMG_CUDA(cudaMemsetAsync(offer.get(), 0xff, sizeof(unsigned long long) * n, s));
+  launch(k_init_next, nb, T, 0, s, n, A.row, next.get());
+  const int64_t limit = 8 * static_cast<int64_t>(A.nnz) + 1024;
+  launch(k_suitor, nb, T, 0, s, n, A.row, scol.get(), sW.get(), next.get(), offer.get(), limit,
+         err.get());
   BCMG_LAUNCH_CHECK();
   launch(k_offer_to_suitor, nb, T, 0, s, n, offer.get(), sv.get());
 
@@ -679,6 +858,8 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   BCMG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaMemcpyAsync(&h_nc, total.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
+  if (h_err == 2)
+    return set_error(BCMG_ERR_UNSUPPORTED, "a row has more than %d entries", kSortCapLong);
   if (h_err)
     return set_error(BCMG_ERR_DEVICE_TIMEOUT,
                      "suitor matching exceeded its iteration bound (n=%d, nnz=%d)", n,
@@ -712,94 +893,63 @@ bcmg_status transpose_agg(int32_t n, const int32_t *agg, int32_t nc, int32_t *rp
   return BCMG_OK;
 }
 
-namespace {
-
-bcmg_status galerkin_pass(bool fill, const CsrView &A, const int32_t *agg,
-                          const double *p, int32_t nc, const int32_t *rptr,
-                          const int32_t *ridx, int32_t *crow, int32_t *cnnz,
-                          int32_t *ccol, double *cval, cudaStream_t s) {
-  if (nc <= 0) {
-    if (cnnz) *cnnz = 0;
-    return BCMG_OK;
-  }
-  DevBuf<int32_t> long_rows, n_long, tmp;
+// Galerkin product (matchingAggregation.cu:239-244): A_c in CSR, ccol/cval
+// allocated here on stream s.
+bcmg_status galerkin(const CsrView &A, const int32_t *agg, const double *p, int32_t nc,
+                     const int32_t *rptr, const int32_t *ridx, int32_t *crow,
+                     int32_t **ccol_out, double **cval_out, int32_t *cnnz, cudaStream_t s) {
+  *ccol_out = nullptr;
+  *cval_out = nullptr;
+  *cnnz = 0;
+  if (nc <= 0) return BCMG_OK;
+  DevBuf<int32_t> tpos, tJ, long_rows, n_long, tmp;
+  DevBuf<double> tV;
   DevBuf<int> err;
+  BCMG_TRY(tpos.alloc(nc + 1, s));
+  BCMG_TRY(tJ.alloc(std::max<int32_t>(A.nnz, 1), s));
+  BCMG_TRY(tV.alloc(std::max<int32_t>(A.nnz, 1), s));
   BCMG_TRY(long_rows.alloc(nc, s));
   BCMG_TRY(n_long.alloc(1, s));
   BCMG_TRY(err.alloc(1, s));
+  BCMG_TRY(tmp.alloc(scan_tmp_size(nc), s));
   BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
+  launch(k_gal_terms, ceil_div(nc, 256), 256, 0, s, nc, A.row, rptr, ridx, tpos.get());
+  BCMG_TRY(exclusive_scan(tpos.get(), tpos.get(), nc, tpos.get() + nc, tmp.get(), s));
   const size_t smem_warp = static_cast<size_t>(kGalWarpsPerBlock) * kGalCap * kGalBytesPerTerm;
   const size_t smem_long = static_cast<size_t>(kGalCapLong) * kGalBytesPerTerm;
-  BCMG_CUDA(cudaFuncSetAttribute(k_gal_long<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+  BCMG_CUDA(cudaFuncSetAttribute(k_gal_rows_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem_long)));
-  BCMG_CUDA(cudaFuncSetAttribute(k_gal_long<true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem_long)));
-  const int blocks = ceil_div(nc, kGalWarpsPerBlock);
-  // The count pass queues the long rows; the fill pass recomputes the queue
-  // the same way by running the count kernel's gather check again.
-  if (!fill) {
-    launch(k_gal_warp<false>, blocks, kGalWarpsPerBlock * 32, smem_warp, s, 
-        nc, A.row, A.col, A.val, agg, p, rptr, ridx, crow, nullptr, nullptr,
-        long_rows.get(), n_long.get(), err.get());
-  } else {
-    // Re-detect long rows without touching crow: count into a scratch array.
-    DevBuf<int32_t> scratch;
-    BCMG_TRY(scratch.alloc(nc, s));
-    launch(k_gal_warp<false>, blocks, kGalWarpsPerBlock * 32, smem_warp, s, 
-        nc, A.row, A.col, A.val, agg, p, rptr, ridx, scratch.get(), nullptr, nullptr,
-        long_rows.get(), n_long.get(), err.get());
-    launch(k_gal_warp<true>, blocks, kGalWarpsPerBlock * 32, smem_warp, s, 
-        nc, A.row, A.col, A.val, agg, p, rptr, ridx, crow, ccol, cval, long_rows.get(),
-        n_long.get(), err.get());
-  }
+  launch(k_gal_rows, ceil_div(nc, kGalWarpsPerBlock), kGalWarpsPerBlock * 32, smem_warp, s, nc,
+         A.row, A.col, A.val, agg, p, rptr, ridx, tpos.get(), tJ.get(), tV.get(), crow,
+         long_rows.get(), n_long.get(), err.get());
+  launch(k_gal_rows_long, std::min(nc, kNumSM), kGalLongThreads, smem_long, s, long_rows.get(),
+         n_long.get(), A.row, A.col, A.val, agg, p, rptr, ridx, tpos.get(), tJ.get(), tV.get(),
+         crow, err.get());
   BCMG_LAUNCH_CHECK();
-  int32_t h_long = 0;
-  BCMG_CUDA(cudaMemcpyAsync(&h_long, n_long.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  BCMG_CUDA(cudaStreamSynchronize(s));
-  if (h_long > 0) {
-    if (!fill)
-      launch(k_gal_long<false>, h_long, kGalLongThreads, smem_long, s, 
-          long_rows.get(), A.row, A.col, A.val, agg, p, rptr, ridx, crow, nullptr,
-          nullptr, err.get());
-    else
-      launch(k_gal_long<true>, h_long, kGalLongThreads, smem_long, s, 
-          long_rows.get(), A.row, A.col, A.val, agg, p, rptr, ridx, crow, ccol, cval,
-          err.get());
-    BCMG_LAUNCH_CHECK();
-  }
-  if (!fill) {
-    BCMG_TRY(tmp.alloc(scan_tmp_size(nc), s));
-    BCMG_TRY(exclusive_scan(crow, crow, nc, crow + nc, tmp.get(), s));
-    BCMG_CUDA(cudaMemcpyAsync(cnnz, crow + nc, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  }
+  // crow holds the run counts: scan them into row pointers.
+  BCMG_TRY(exclusive_scan(crow, crow, nc, crow + nc, tmp.get(), s));
   int h_err = 0;
+  int32_t h_nnz = 0;
   BCMG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaMemcpyAsync(&h_nnz, crow + nc, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
   if (h_err == 3)
     return set_error(BCMG_ERR_UNSUPPORTED,
                      "a coarse row has more than %d Galerkin terms", kGalCapLong);
   if (h_err)
     return set_error(BCMG_ERR_INTERNAL, "Galerkin run longer than %d terms", kGalMaxRun);
+  DevBuf<int32_t> ccol;
+  DevBuf<double> cval;
+  BCMG_TRY(ccol.alloc(std::max<int32_t>(h_nnz, 1), s));
+  BCMG_TRY(cval.alloc(std::max<int32_t>(h_nnz, 1), s));
+  launch(k_gal_compact, ceil_div(static_cast<int64_t>(nc) * 32, 256), 256, 0, s, nc, tpos.get(),
+         crow, tJ.get(), tV.get(), ccol.get(), cval.get());
+  BCMG_LAUNCH_CHECK();
+  *cnnz = h_nnz;
+  *ccol_out = ccol.release();
+  *cval_out = cval.release();
   return BCMG_OK;
-}
-
-}  // namespace
-
-bcmg_status galerkin_count(const CsrView &A, const int32_t *agg, const double *p,
-                           int32_t nc, const int32_t *rptr, const int32_t *ridx,
-                           int32_t *crow, int32_t *cnnz, cudaStream_t s) {
-  return galerkin_pass(false, A, agg, p, nc, rptr, ridx, crow, cnnz, nullptr, nullptr, s);
-}
-
-bcmg_status galerkin_fill(const CsrView &A, const int32_t *agg, const double *p,
-                          int32_t nc, const int32_t *rptr, const int32_t *ridx,
-                          const int32_t *crow, int32_t *ccol, double *cval,
-                          cudaStream_t s) {
-  return galerkin_pass(true, A, agg, p, nc, rptr, ridx, const_cast<int32_t *>(crow),
-                       nullptr, ccol, cval, s);
 }
 
 bcmg_status restrict_exact(int32_t nc, const int32_t *rptr, const int32_t *ridx,

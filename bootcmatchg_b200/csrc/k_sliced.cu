@@ -13,7 +13,9 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <climits>
+#include <vector>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -127,51 +129,58 @@ __global__ void k_slice_fill(int32_t n, int32_t nslices, const int32_t *__restri
   }
 }
 
-// Row sum of one slice row: t = sum_k val[k] * x[col_k].
+// Row sum of one slice row: t = sum_k val[k] * x[col_k].  Slots are taken
+// eight at a time with all eight value loads issued before the gathers and
+// the FMAs, so each thread keeps eight independent loads in flight (the
+// sweep is bound by memory latency, not by issue).
+constexpr int kBatch = 8;
+
+template <typename VT, typename XT, bool OFFSETS>
+__device__ __forceinline__ XT sliced_dot_kind(const SlicedView &S, const VT *__restrict__ v,
+                                              const XT *__restrict__ x, int32_t sp, int W,
+                                              int32_t r) {
+  XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
+  const int32_t *off = S.soff + sp;
+  const int32_t *cidx =
+      OFFSETS ? nullptr : S.scol + static_cast<int64_t>(sp) * 32 + (threadIdx.x & 31);
+  const int32_t hi = S.n - 1;
+#define BCMG_SLICED_COLUMN(k_)                                                       \
+  (OFFSETS ? min(max(r + __ldg(off + (k_)), 0), hi) : cidx[static_cast<int64_t>(k_) * 32])
+  int k = 0;
+  for (; k + kBatch <= W; k += kBatch) {
+    VT a[kBatch];
+    int32_t c[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      a[u] = v[static_cast<int64_t>(k + u) * 32];
+      c[u] = BCMG_SLICED_COLUMN(k + u);
+    }
+    XT xv[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) xv[u] = __ldg(x + c[u]);
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) t[u & 3] = fma(static_cast<XT>(widen(a[u])), xv[u], t[u & 3]);
+  }
+  for (; k < W; ++k)
+    t[k & 3] = fma(static_cast<XT>(widen(v[static_cast<int64_t>(k) * 32])),
+                   __ldg(x + BCMG_SLICED_COLUMN(k)), t[k & 3]);
+#undef BCMG_SLICED_COLUMN
+  return (t[0] + t[1]) + (t[2] + t[3]);
+}
+
 template <typename VT, typename XT>
 __device__ __forceinline__ XT sliced_dot(const SlicedView &S, const VT *__restrict__ val,
                                          const XT *__restrict__ x, int32_t s, int32_t r,
                                          int lane) {
-  const int64_t base = static_cast<int64_t>(S.sptr[s]) * 32;
+  const int32_t sp = S.sptr[s];
   const int W = S.width[s];
-  XT t0 = XT(0), t1 = XT(0);
-  const VT *v = val + base + lane;
-  if (S.kind[s]) {
-    const int32_t *off = S.soff + S.sptr[s];
-    const int32_t hi = S.n - 1;
-    int k = 0;
-    for (; k + 1 < W; k += 2) {
-      const int32_t c0 = min(max(r + __ldg(off + k), 0), hi);
-      const int32_t c1 = min(max(r + __ldg(off + k + 1), 0), hi);
-      const XT a0 = static_cast<XT>(widen(v[static_cast<int64_t>(k) * 32]));
-      const XT a1 = static_cast<XT>(widen(v[static_cast<int64_t>(k + 1) * 32]));
-      t0 = fma(a0, __ldg(x + c0), t0);
-      t1 = fma(a1, __ldg(x + c1), t1);
-    }
-    if (k < W) {
-      const int32_t c0 = min(max(r + __ldg(off + k), 0), hi);
-      t0 = fma(static_cast<XT>(widen(v[static_cast<int64_t>(k) * 32])), __ldg(x + c0), t0);
-    }
-  } else {
-    const int32_t *c = S.scol + base + lane;
-    int k = 0;
-    for (; k + 1 < W; k += 2) {
-      const int32_t c0 = c[static_cast<int64_t>(k) * 32];
-      const int32_t c1 = c[static_cast<int64_t>(k + 1) * 32];
-      const XT a0 = static_cast<XT>(widen(v[static_cast<int64_t>(k) * 32]));
-      const XT a1 = static_cast<XT>(widen(v[static_cast<int64_t>(k + 1) * 32]));
-      t0 = fma(a0, __ldg(x + c0), t0);
-      t1 = fma(a1, __ldg(x + c1), t1);
-    }
-    if (k < W)
-      t0 = fma(static_cast<XT>(widen(v[static_cast<int64_t>(k) * 32])),
-               __ldg(x + c[static_cast<int64_t>(k) * 32]), t0);
-  }
-  return t0 + t1;
+  const VT *v = val + static_cast<int64_t>(sp) * 32 + lane;
+  if (S.kind[s]) return sliced_dot_kind<VT, XT, true>(S, v, x, sp, W, r);
+  return sliced_dot_kind<VT, XT, false>(S, v, x, sp, W, r);
 }
 
 template <typename VT, typename XT>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
     k_sl_relax(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ d,
                const XT *__restrict__ f, const XT *__restrict__ u, XT *__restrict__ u_out) {
   const int lane = threadIdx.x & 31;
@@ -183,7 +192,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 }
 
 template <typename VT, typename XT>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
     k_sl_residual(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ f,
                   const XT *__restrict__ u, XT *__restrict__ res) {
   const int lane = threadIdx.x & 31;
@@ -196,7 +205,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 
 // FCG SpMV on the sliced FP64 copy with the three dot products fused; fixed
 // grid (kRedBlocks) and slice-to-block mapping keep the partials deterministic.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
     k_sl_fcg_spmv_dots(SlicedView S, const double *__restrict__ v, double *__restrict__ w,
                        const double *__restrict__ r, const double *__restrict__ q,
                        double *partials) {
@@ -218,6 +227,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
   block_partials<3>(acc, partials);
 }
 
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
+    k_sl_spmv(SlicedView S, const double *__restrict__ val, const double *__restrict__ x,
+              double *__restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  if (s >= S.nslices) return;
+  const int32_t r = s * 32 + lane;
+  const double T = sliced_dot<double, double>(S, val, x, s, r, lane);
+  if (r < S.n) y[r] = T;
+}
+
 template <typename VT, typename XT>
 void sl_relax_launch(const SlicedView &S, const XT *d, const XT *f, const XT *src, XT *dst,
                      cudaStream_t st) {
@@ -234,6 +254,14 @@ void sl_residual_launch(const SlicedView &S, const XT *f, const XT *u, XT *res,
 
 }  // namespace
 
+size_t SlicedMat::bytes() const {
+  if (!nslices) return 0;
+  const size_t vbytes = vtype == kValF64 ? 8 : (vtype == kValF32 ? 4 : 2);
+  const size_t sl = static_cast<size_t>(slots) * 32;
+  return vbytes * sl + 16 + (has_columns ? 4 * sl : 0) + 4 * (static_cast<size_t>(slots) + 1) +
+         4 * (3 * static_cast<size_t>(nslices) + 1);
+}
+
 void SlicedMat::release(cudaStream_t s) {
   dev_free(sptr, s);
   dev_free(width, s);
@@ -243,6 +271,7 @@ void SlicedMat::release(cudaStream_t s) {
   if (val) cudaFreeAsync(val, s);
   val = nullptr;
   nslices = 0;
+  has_columns = false;
 }
 
 SlicedView SlicedMat::view() const {
@@ -277,12 +306,18 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
   BCMG_TRY(tmp.alloc(scan_tmp_size(ns), s));
   BCMG_TRY(exclusive_scan(out->width, out->sptr, ns, out->sptr + ns, tmp.get(), s));
   int32_t slots = 0;
+  std::vector<int32_t> kinds(ns);
   BCMG_CUDA(cudaMemcpyAsync(&slots, out->sptr + ns, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaMemcpyAsync(kinds.data(), out->kind, sizeof(int32_t) * ns,
+                            cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
   out->slots = slots;
   const size_t vbytes = vtype == kValF64 ? 8 : (vtype == kValF32 ? 4 : 2);
   BCMG_CUDA(cudaMallocAsync(&out->val, vbytes * static_cast<size_t>(slots) * 32 + 16, s));
-  BCMG_TRY(dev_alloc(&out->scol, static_cast<int64_t>(slots) * 32, s));
+  // Explicit columns are only read in column slices; a matrix made of offset
+  // slices alone (a stencil) stores none.
+  out->has_columns = std::any_of(kinds.begin(), kinds.end(), [](int32_t k) { return k == 0; });
+  if (out->has_columns) BCMG_TRY(dev_alloc(&out->scol, static_cast<int64_t>(slots) * 32, s));
   BCMG_TRY(dev_alloc(&out->soff, slots + 1, s));
   switch (vtype) {
     case kValF64:
@@ -359,6 +394,14 @@ bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w
                                  cudaStream_t s) {
   if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "FCG SpMV needs FP64 values");
   launch(k_sl_fcg_spmv_dots, kRedBlocks, kWarpsPerBlock * 32, 0, s, S, v, w, r, q, partials);
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
+bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStream_t s) {
+  if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced SpMV needs FP64 values");
+  launch(k_sl_spmv, ceil_div(S.nslices, kWarpsPerBlock), kWarpsPerBlock * 32, 0, s, S,
+         static_cast<const double *>(S.val), x, y);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cstddef>
 #include <cstdint>
 
 #include "bcmg.h"
@@ -24,13 +25,11 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg,
                            int32_t *s_out, int32_t *m_out, cudaStream_t s);
 bcmg_status transpose_agg(int32_t n, const int32_t *agg, int32_t nc,
                           int32_t *rptr, int32_t *ridx, cudaStream_t s);
-bcmg_status galerkin_count(const CsrView &A, const int32_t *agg, const double *p,
-                           int32_t nc, const int32_t *rptr, const int32_t *ridx,
-                           int32_t *crow, int32_t *cnnz, cudaStream_t s);
-bcmg_status galerkin_fill(const CsrView &A, const int32_t *agg, const double *p,
-                          int32_t nc, const int32_t *rptr, const int32_t *ridx,
-                          const int32_t *crow, int32_t *ccol, double *cval,
-                          cudaStream_t s);
+// A_c = P^T A P into crow (nc+1, caller-allocated) and *ccol/*cval
+// (allocated on stream s, *cnnz entries).
+bcmg_status galerkin(const CsrView &A, const int32_t *agg, const double *p, int32_t nc,
+                     const int32_t *rptr, const int32_t *ridx, int32_t *crow,
+                     int32_t **ccol, double **cval, int32_t *cnnz, cudaStream_t s);
 bcmg_status restrict_exact(int32_t nc, const int32_t *rptr, const int32_t *ridx,
                            const double *p, const double *x, double *y,
                            cudaStream_t s);
@@ -58,7 +57,9 @@ struct SlicedMat {
           *soff = nullptr;
   void *val = nullptr;
   int vtype = kValF64;
+  bool has_columns = false;  // scol allocated (some slice is a column slice)
   void release(cudaStream_t s);
+  size_t bytes() const;  // device bytes held
   SlicedView view() const;
 };
 
@@ -70,6 +71,8 @@ bcmg_status sliced_relax_sweep(const SlicedView &S, const XT *d, const XT *f, co
 template <typename XT>  // res = f - A u
 bcmg_status sliced_residual(const SlicedView &S, const XT *f, const XT *u, XT *res,
                             cudaStream_t s);
+// y = A x on a sliced FP64 copy.
+bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStream_t s);
 // FCG SpMV w = A v fused with alpha = r.v, beta = w.v, gamma = q.v (FP64 values).
 bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w,
                                  const double *r, const double *q, double *partials,

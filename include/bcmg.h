@@ -39,7 +39,8 @@ typedef enum bcmg_status {
   BCMG_ERR_DEVICE_TIMEOUT = 7,  /* a bounded device loop ran out of iterations    */
   BCMG_ERR_INVALID_MATRIX = 8,  /* not square, missing diagonal, bad index, NaN   */
   BCMG_ERR_UNSUPPORTED = 9,     /* option the path does not implement             */
-  BCMG_ERR_INTERNAL = 10
+  BCMG_ERR_INTERNAL = 10,
+  BCMG_ERR_PENDING = 11         /* bcmg_server_wait: the request is not done yet  */
 } bcmg_status;
 
 /* Host CSR matrix: 0-based, int32 row pointers and column indices, FP64
@@ -95,6 +96,9 @@ typedef struct bcmg_ext {
   void  *stream;          /* cudaStream_t to run on from setup on (NULL: the
                              handle creates its own); the caller keeps it alive */
   int    sliced;          /* solve on the sliced copies of the levels (default 1) */
+  int    autotune;        /* batched solves: time the row-kernel shapes of every
+                             level once per batch width (default 1); 0 uses a
+                             fixed rule.  Results are identical either way.   */
 } bcmg_ext;
 
 /* Per-solve report.  residual is the recursive ||r||_2 that FCG returns
@@ -167,7 +171,92 @@ bcmg_status bcmg_solve(bcmg_handle *h, const double *b, double *x,
 bcmg_status bcmg_solve_legacy(const bcmg_csr *A, const bcmg_params *p,
                               const bcmg_ext *ext, const double *b, double *x,
                               bcmg_solve_info *info);
+/* ---- multiple right-hand sides (no counterpart in the reference, which
+ * solves one right-hand side per solve() call) ------------------------------
+ * Solves A X = B for nrhs right-hand sides sharing the handle's hierarchy.
+ * B and X are column-major n x nrhs with leading dimensions ldb, ldx >= n, on
+ * the host or (on_device) the handle's device; X holds the initial guesses on
+ * entry and the solutions on return.  Up to 32 columns run together: one
+ * cycle per FCG iteration serves all of them and every column keeps its own
+ * FCG scalars, iteration count and stopping test, exactly as bcmg_solve would
+ * for that column alone.  infos: nrhs entries (or NULL); solve_ms is the time
+ * of the group of up to 32 columns the entry belongs to.  Returns
+ * BCMG_ERR_INDEFINITE if any column broke down (the others are still solved
+ * and reported). */
+bcmg_status bcmg_solve_batch(bcmg_handle *h, int32_t nrhs, const double *B, int64_t ldb,
+                             double *X, int64_t ldx, int on_device, bcmg_solve_info *infos);
+/* Z = M R for nrhs device columns (column-major, leading dimensions >= n):
+ * the batched preconditioner of bcmg_solve_batch, from Z = 0. */
+bcmg_status bcmg_precond_apply_batch(bcmg_handle *h, int32_t nrhs, const double *d_R,
+                                     int64_t ldr, double *d_Z, int64_t ldz);
+/* k batched smoother sweeps on level `level` of hierarchy `hrc` for `width`
+ * interleaved columns (width a power of two <= 32; element (i, c) at
+ * u[i * width + c]), in the cycle's precision (FP32 for BCMG_PREC_MIXED,
+ * else FP64), exactly as the batched cycle runs them.  f and u must be
+ * 16-byte aligned. */
+bcmg_status bcmg_level_relax_batch(bcmg_handle *h, int hrc, int level, int32_t width,
+                                   const void *d_f, void *d_u, int k);
+/* The row-kernel shape a batch of nrhs columns uses on level `level` of
+ * hierarchy `hrc` (hrc < 0: the FCG SpMV on the input matrix): batch width,
+ * columns per lane and threads per block, plus the time the batch state took
+ * to build and tune (ms). */
+bcmg_status bcmg_batch_config(bcmg_handle *h, int32_t nrhs, int hrc, int level,
+                              int32_t *width, int32_t *cols_per_lane, int32_t *block_threads,
+                              double *tune_ms);
+
+/* Device memory the handle holds, in bytes (hierarchies, their solve-phase
+ * copies, cycle and Krylov work vectors, batch state). */
+bcmg_status bcmg_device_bytes(const bcmg_handle *h, uint64_t *bytes);
 bcmg_status bcmg_destroy(bcmg_handle *h);
+
+/* ---- solve server (no counterpart in the reference) ------------------------
+ * Continuous batching of solve requests on one GPU: `slots` worker threads
+ * with their own CUDA streams run requests from a FIFO queue.  A request
+ * starts when a slot is free and the estimated device footprint of all
+ * resident hierarchies and work blocks plus its own stays under mem_cap_gb
+ * (idle cached hierarchies are evicted least-recently-used to make room).
+ * Finished hierarchies stay cached by matrix key up to cache_cap_gb, and
+ * queued requests on the same key (up to max_batch) run together as one
+ * bcmg_solve_batch on the shared hierarchy. */
+typedef struct bcmg_server bcmg_server;
+typedef struct bcmg_server_opts {
+  int         device;
+  int         slots;          /* requests in flight (default 4)               */
+  double      mem_cap_gb;     /* admission cap on device footprint (150)      */
+  double      cache_cap_gb;   /* budget of cached idle hierarchies (60)       */
+  int         max_batch;      /* same-key requests solved together (<= 32)    */
+  bcmg_params params;         /* settings of every request                    */
+  bcmg_ext    ext;            /* precision etc.; stream and device are set
+                                 by the server                                */
+} bcmg_server_opts;
+typedef struct bcmg_request_info {
+  bcmg_solve_info solve;
+  double latency_ms;          /* submit -> result written                     */
+  double queue_ms;            /* submit -> start on a slot                    */
+  int    group;               /* requests solved together with it (1 alone)   */
+  int    cache_hit;           /* hierarchy came from the cache                */
+} bcmg_request_info;
+typedef struct bcmg_server_stats {
+  uint64_t submitted, completed, failed, setups, cache_hits, batches, evictions;
+  uint64_t peak_resident_bytes, resident_bytes;
+  int      cached_hierarchies, queued, running;
+} bcmg_server_stats;
+void bcmg_server_opts_default(bcmg_server_opts *o);
+bcmg_status bcmg_server_create(const bcmg_server_opts *opt, bcmg_server **out);
+/* Queues one solve A x = b from x0 = 0.  key identifies the matrix (0: a
+ * hash of A's arrays).  A's arrays are read only if the key needs a setup and
+ * must stay valid until the request is done; b is copied; x (n doubles) is
+ * written when the request finishes. */
+bcmg_status bcmg_server_submit(bcmg_server *s, const bcmg_csr *A, uint64_t key,
+                               const double *b, double *x, uint64_t *ticket);
+/* Waits up to timeout_s seconds (< 0: forever) for a request; returns its
+ * status (BCMG_ERR_PENDING if it is not done) and releases the ticket once
+ * done. */
+bcmg_status bcmg_server_wait(bcmg_server *s, uint64_t ticket, double timeout_s,
+                             bcmg_request_info *info);
+bcmg_status bcmg_server_stats_get(bcmg_server *s, bcmg_server_stats *out);
+/* Finishes every queued request, then frees the cache and the streams. */
+bcmg_status bcmg_server_destroy(bcmg_server *s);
 /* Binds the handle to a CUDA stream (cudaStream_t passed as void*). */
 bcmg_status bcmg_set_stream(bcmg_handle *h, void *stream);
 /* z = B r for the composite preconditioner (preconditionApply,
