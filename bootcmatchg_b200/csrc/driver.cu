@@ -651,6 +651,7 @@ bcmg_status setup_common(bcmg_handle *h) {
   if (h->ext.sliced) BCMG_TRY(prepare_solve_formats(h));
   g_clock.tick("sliced_copies");
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
+  BCMG_TRY(sliced_wait_status(h->stream));
   h->setup_ms = ms_since(t0);
   g_clock.report("setup");
   return BCMG_OK;
@@ -783,6 +784,7 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
     } while (hs[kNorm] > target && hs[kIter] < h->prm.itnlim && hs[kIndef] == 0.0);
   }
   g_clock.tick("fcg_loop");
+  BCMG_TRY(sliced_wait_status(s));
   const double l2 = hs[kNorm];
   const int iter = static_cast<int>(hs[kIter]);
   info->iters = iter + 1;  // FCG.cu:569
@@ -1115,7 +1117,7 @@ bcmg_status bcmg_level_relax(bcmg_handle *h, int hrc, int level, const void *d_f
                              h->stream));
   }
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
-  return BCMG_OK;
+  return sliced_wait_status(h->stream);
 }
 
 bcmg_status bcmg_level_format(const bcmg_handle *h, int hrc, int level, int64_t *slots,
@@ -1134,15 +1136,13 @@ bcmg_status bcmg_level_format(const bcmg_handle *h, int hrc, int level, int64_t 
   if (column_slots) {
     *column_slots = 0;
     if (S && S->nslices) {
-      std::vector<int32_t> kind(S->nslices), width(S->nslices);
+      std::vector<int4> meta(S->nslices);
       BCMG_CUDA(cudaSetDevice(h->device));
-      BCMG_CUDA(cudaMemcpyAsync(kind.data(), S->kind, sizeof(int32_t) * S->nslices,
-                                cudaMemcpyDeviceToHost, h->stream));
-      BCMG_CUDA(cudaMemcpyAsync(width.data(), S->width, sizeof(int32_t) * S->nslices,
+      BCMG_CUDA(cudaMemcpyAsync(meta.data(), S->meta, sizeof(int4) * S->nslices,
                                 cudaMemcpyDeviceToHost, h->stream));
       BCMG_CUDA(cudaStreamSynchronize(h->stream));
       for (int32_t i = 0; i < S->nslices; ++i)
-        if (!kind[i]) *column_slots += width[i];
+        if (!meta[i].z) *column_slots += meta[i].y;
     }
   }
   return BCMG_OK;

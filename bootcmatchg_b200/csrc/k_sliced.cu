@@ -1,20 +1,39 @@
 // Sliced matrix format for the solve phase and its kernels.
 //
 // Rows are cut into slices of 32 (one warp, one thread per row).  A slice
-// stores W slots of 32 values in slot-major order, so every value load of a
-// warp is one contiguous 32-element segment.  Two slot kinds:
+// stores W slots of 32 values in slot-major order, so every slot of a slice
+// is one contiguous 32-element segment and a slice is one contiguous block.
+// Two slot kinds:
 //   offset slice: the slice's rows share a set of W column offsets
 //                 (col - row), e.g. a stencil; column indices are implicit
-//                 (row + offset) and only W offsets are stored per slice;
+//                 (row + offset) and W offsets are stored per slice.  Runs of
+//                 consecutive slices with identical offset lists read one
+//                 copy (the run head's), which stays cache-resident;
 //   column slice: W = longest row; explicit int32 columns per slot (SELL-32).
 // Missing entries are stored as 0 (with an in-range column), which adds exact
-// zeros to the row sums.  Built on the device from the level's CSR after
-// setup; CSR stays the setup / introspection format.
+// zeros to the row sums.  Values, columns and offsets are padded by kSlotPad
+// slots so a batch of loads may run past a slice's last slot without a bounds
+// test (those products are discarded).  Built on the device from the level's
+// CSR after setup; CSR stays the setup / introspection format.
+//
+// Row passes (smoother sweep, residual, SpMV, FCG SpMV + dots) run as one
+// warp-specialised pipeline per CTA: a producer warp streams each chunk of
+// kPipeWarps consecutive slices (values, explicit columns, slice metadata and
+// the row vectors the epilogue reads) into shared memory with bulk async
+// copies (cp.async.bulk, the TMA engine) under full/empty mbarriers, while the
+// kPipeWarps consumer warps compute the previous chunks.  A consumer warp
+// issues all gathers of a batch of slots before its first FMA, so each warp
+// keeps a full row's gathers in flight.  Every wait is bounded; a wait that
+// runs out sets a device error word (sliced_wait_status) and the kernel
+// returns without touching the stage.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include <algorithm>
 #include <climits>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -25,8 +44,17 @@
 namespace bcmg {
 namespace {
 
-constexpr int kWarpsPerBlock = 8;
+constexpr int kWarpsPerBlock = 8;    // build kernels: one warp per slice
 constexpr int kMaxOffsetSlots = 64;  // wider unions fall back to column slices
+constexpr int kPipeWarps = 8;        // consumer warps per CTA = slices per chunk
+constexpr int kPipeStages = 2;
+constexpr int kPipeThreads = (kPipeWarps + 1) * 32;
+constexpr int kSlotPad = 32;                       // >= the largest slot batch
+constexpr size_t kMaxStageBytes = 108 * 1024;      // two stages fit in 227 KB
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
+
+// Set by a pipeline wait that ran out (a bulk copy that never landed).
+__device__ int g_sliced_wait_error;
 
 __device__ __forceinline__ double widen(double v) { return v; }
 __device__ __forceinline__ float widen(float v) { return v; }
@@ -45,6 +73,8 @@ __device__ __forceinline__ __nv_bfloat16 narrow<__nv_bfloat16>(double v) {
 }
 template <>
 __device__ __forceinline__ __half narrow<__half>(double v) { return __double2half(v); }
+
+// ---- format build -----------------------------------------------------------
 
 // Pass 1: per slice, the longest row and the size of the union of column
 // offsets (merging the 32 sorted rows); chooses the slice kind and width.
@@ -81,6 +111,23 @@ __global__ void k_slice_shape(int32_t n, int32_t nslices, const int32_t *__restr
     kind[s] = offsets ? 1 : 0;
     width[s] = offsets ? distinct : maxlen;
   }
+}
+
+// Format statistics from the scanned slot pointers: stats[0] = the most slots
+// in one chunk of kPipeWarps slices, stats[1] = 1 if any slice is a column
+// slice.
+__global__ void k_slice_stats(int32_t nslices, const int32_t *__restrict__ sptr,
+                              const int32_t *__restrict__ kind, int32_t *stats) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t s0 = c * kPipeWarps;
+  if (s0 >= nslices) return;
+  const int32_t s1 = min(s0 + kPipeWarps, nslices);
+  atomicMax(stats, sptr[s1] - sptr[s0]);
+  for (int32_t s = s0; s < s1; ++s)
+    if (!kind[s]) {
+      atomicOr(stats + 1, 1);
+      break;
+    }
 }
 
 // Pass 2: fill values (and columns or offsets).
@@ -124,148 +171,495 @@ __global__ void k_slice_fill(int32_t n, int32_t nslices, const int32_t *__restri
       const int32_t j = b + k;
       const bool have = j < e;
       sval[base + static_cast<int64_t>(k) * 32 + lane] = narrow<VT>(have ? val[j] : 0.0);
-      scol[base + static_cast<int64_t>(k) * 32 + lane] = have ? col[j] : rr;
+      if (scol) scol[base + static_cast<int64_t>(k) * 32 + lane] = have ? col[j] : rr;
     }
   }
 }
 
-// Row sum of one slice row: t = sum_k val[k] * x[col_k].  Slots are taken
-// eight at a time with all eight value loads issued before the gathers and
-// the FMAs, so each thread keeps eight independent loads in flight (the
-// sweep is bound by memory latency, not by issue).
-constexpr int kBatch = 8;
-
-template <typename VT, typename XT, bool OFFSETS>
-__device__ __forceinline__ XT sliced_dot_kind(const SlicedView &S, const VT *__restrict__ v,
-                                              const XT *__restrict__ x, int32_t sp, int W,
-                                              int32_t r) {
-  XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
-  const int32_t *off = S.soff + sp;
-  const int32_t *cidx =
-      OFFSETS ? nullptr : S.scol + static_cast<int64_t>(sp) * 32 + (threadIdx.x & 31);
-  const int32_t hi = S.n - 1;
-#define BCMG_SLICED_COLUMN(k_)                                                       \
-  (OFFSETS ? min(max(r + __ldg(off + (k_)), 0), hi) : cidx[static_cast<int64_t>(k_) * 32])
-  int k = 0;
-  for (; k + kBatch <= W; k += kBatch) {
-    VT a[kBatch];
-    int32_t c[kBatch];
-#pragma unroll
-    for (int u = 0; u < kBatch; ++u) {
-      a[u] = v[static_cast<int64_t>(k + u) * 32];
-      c[u] = BCMG_SLICED_COLUMN(k + u);
-    }
-    XT xv[kBatch];
-#pragma unroll
-    for (int u = 0; u < kBatch; ++u) xv[u] = __ldg(x + c[u]);
-#pragma unroll
-    for (int u = 0; u < kBatch; ++u) t[u & 3] = fma(static_cast<XT>(widen(a[u])), xv[u], t[u & 3]);
+// flag[s] = 1 when slice s starts a new run: it is a column slice, or its
+// offset list differs from slice s-1's.
+__global__ void k_slice_runs(int32_t nslices, const int32_t *__restrict__ sptr,
+                             const int32_t *__restrict__ width,
+                             const int32_t *__restrict__ kind,
+                             const int32_t *__restrict__ soff, int32_t *flag) {
+  const int lane = threadIdx.x & 31;
+  const int32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  if (s >= nslices) return;
+  bool same = s > 0 && kind[s] && kind[s - 1] && width[s] == width[s - 1];
+  if (same) {
+    const int32_t *a = soff + sptr[s], *b = soff + sptr[s - 1];
+    bool eq = true;
+    for (int k = lane; k < width[s]; k += 32) eq = eq && a[k] == b[k];
+    same = __all_sync(0xffffffffu, eq);
   }
-  for (; k < W; ++k)
-    t[k & 3] = fma(static_cast<XT>(widen(v[static_cast<int64_t>(k) * 32])),
-                   __ldg(x + BCMG_SLICED_COLUMN(k)), t[k & 3]);
-#undef BCMG_SLICED_COLUMN
+  if (lane == 0) flag[s] = same ? 0 : 1;
+}
+
+__global__ void k_slice_heads(int32_t nslices, const int32_t *__restrict__ flag,
+                              const int32_t *__restrict__ rid, int32_t *head) {
+  const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nslices && flag[s]) head[rid[s]] = s;
+}
+
+__global__ void k_slice_meta(int32_t nslices, const int32_t *__restrict__ sptr,
+                             const int32_t *__restrict__ width,
+                             const int32_t *__restrict__ kind,
+                             const int32_t *__restrict__ flag,
+                             const int32_t *__restrict__ rid,
+                             const int32_t *__restrict__ head, int4 *meta) {
+  const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslices) return;
+  const int32_t h = head[rid[s] + flag[s] - 1];
+  meta[s] = make_int4(sptr[s], width[s], kind[s], sptr[h]);
+}
+
+// ---- pipeline primitives (mbarrier + bulk async copy) ---------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+      "selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase with the given parity; false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+  if (mbar_test(b, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_test(b, parity))
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  return true;
+}
+// Global -> shared bulk copy (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Gathers issued as volatile loads so a batch is in flight before its first
+// use (the index is computed outside, the address inside).
+__device__ __forceinline__ float gather(const float *x, int32_t i) {
+  float v;
+  asm volatile(
+      "{ .reg .s64 a; mul.wide.s32 a, %2, 4; add.s64 a, %1, a; ld.global.nc.f32 %0, [a]; }"
+      : "=f"(v)
+      : "l"(x), "r"(i));
+  return v;
+}
+__device__ __forceinline__ double gather(const double *x, int32_t i) {
+  double v;
+  asm volatile(
+      "{ .reg .s64 a; mul.wide.s32 a, %2, 8; add.s64 a, %1, a; ld.global.nc.f64 %0, [a]; }"
+      : "=d"(v)
+      : "l"(x), "r"(i));
+  return v;
+}
+
+// Row sum t = sum_k val[k] * x[col_k] of one slice row, slots in batches of
+// KB.  v: the slice's values at this lane (shared or global memory); cidx: the
+// slice's explicit columns at this lane (column slices), else off: the
+// slice's offsets (offset slices).  Loads past slot W-1 stay inside the
+// padding and their products are dropped.  The four partial sums by slot
+// index mod 4 fix the summation order.
+template <typename VT, typename XT, int KB>
+__device__ __forceinline__ XT slice_row_sum(const VT *v, const int32_t *cidx,
+                                            const int32_t *off, int W, int32_t r, int32_t hi,
+                                            const XT *__restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
+  for (int k = 0; k < W; k += KB) {
+    XT xv[KB];
+    if (cidx) {
+#pragma unroll
+      for (int q = 0; q < KB; ++q) xv[q] = gather(x, min(max(cidx[(k + q) * 32], 0), hi));
+    } else {
+      const int32_t offl = __ldg(off + k + lane);
+#pragma unroll
+      for (int q = 0; q < KB; ++q)
+        xv[q] = gather(x, min(max(r + __shfl_sync(0xffffffffu, offl, q), 0), hi));
+    }
+#pragma unroll
+    for (int q = 0; q < KB; ++q)
+      if (k + q < W)
+        t[q & 3] = fma(static_cast<XT>(widen(v[(k + q) * 32])), xv[q], t[q & 3]);
+  }
   return (t[0] + t[1]) + (t[2] + t[3]);
 }
 
-template <typename VT, typename XT>
-__device__ __forceinline__ XT sliced_dot(const SlicedView &S, const VT *__restrict__ val,
-                                         const XT *__restrict__ x, int32_t s, int32_t r,
-                                         int lane) {
-  const int32_t sp = S.sptr[s];
-  const int W = S.width[s];
-  const VT *v = val + static_cast<int64_t>(sp) * 32 + lane;
-  if (S.kind[s]) return sliced_dot_kind<VT, XT, true>(S, v, x, sp, W, r);
-  return sliced_dot_kind<VT, XT, false>(S, v, x, sp, W, r);
-}
+// ---- epilogues ---------------------------------------------------------------
+// NV row vectors are staged per chunk (rows()[i] in global memory); apply()
+// consumes the row sum T of row r with those NV values.
 
-template <typename VT, typename XT>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
-    k_sl_relax(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ d,
-               const XT *__restrict__ f, const XT *__restrict__ u, XT *__restrict__ u_out) {
-  const int lane = threadIdx.x & 31;
-  const int32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-  if (s >= S.nslices) return;
-  const int32_t r = s * 32 + lane;
-  const XT T = sliced_dot<VT, XT>(S, val, u, s, r, lane);
-  if (r < S.n) u_out[r] = ((-T + f[r]) / d[r]) + u[r];
-}
+template <typename XT>
+struct EpiRelax {  // out = ((-T + f) / d) + u
+  static constexpr int NV = 3;
+  const XT *f, *d, *u;
+  XT *out;
+  __device__ const XT *row_vec(int i) const { return i == 0 ? f : (i == 1 ? d : u); }
+  __device__ void apply(int32_t r, XT T, const XT *rv) { out[r] = ((-T + rv[0]) / rv[1]) + rv[2]; }
+  __device__ void finish(int, int) {}
+};
 
-template <typename VT, typename XT>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
-    k_sl_residual(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ f,
-                  const XT *__restrict__ u, XT *__restrict__ res) {
-  const int lane = threadIdx.x & 31;
-  const int32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-  if (s >= S.nslices) return;
-  const int32_t r = s * 32 + lane;
-  const XT T = sliced_dot<VT, XT>(S, val, u, s, r, lane);
-  if (r < S.n) res[r] = f[r] - T;
-}
+template <typename XT>
+struct EpiResidual {  // out = f - T
+  static constexpr int NV = 1;
+  const XT *f;
+  XT *out;
+  __device__ const XT *row_vec(int) const { return f; }
+  __device__ void apply(int32_t r, XT T, const XT *rv) { out[r] = rv[0] - T; }
+  __device__ void finish(int, int) {}
+};
 
-// FCG SpMV on the sliced FP64 copy with the three dot products fused; fixed
-// grid (kRedBlocks) and slice-to-block mapping keep the partials deterministic.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
-    k_sl_fcg_spmv_dots(SlicedView S, const double *__restrict__ v, double *__restrict__ w,
-                       const double *__restrict__ r, const double *__restrict__ q,
-                       double *partials) {
-  double acc[3] = {0.0, 0.0, 0.0};
-  const int lane = threadIdx.x & 31;
-  const double *val = static_cast<const double *>(S.val);
-  for (int32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); s < S.nslices;
-       s += gridDim.x * kWarpsPerBlock) {
-    const int32_t row = s * 32 + lane;
-    const double T = sliced_dot<double, double>(S, val, v, s, row, lane);
-    if (row < S.n) {
-      w[row] = T;
-      const double vi = v[row];
-      acc[0] = fma(r[row], vi, acc[0]);
-      acc[1] = fma(T, vi, acc[1]);
-      if (q) acc[2] = fma(q[row], vi, acc[2]);
+struct EpiSpmv {  // out = T
+  static constexpr int NV = 0;
+  double *out;
+  __device__ const double *row_vec(int) const { return nullptr; }
+  __device__ void apply(int32_t r, double T, const double *) { out[r] = T; }
+  __device__ void finish(int, int) {}
+};
+
+// FCG: w = T with alpha = r.v, beta = w.v, gamma = q.v (v is the gathered
+// vector); per-CTA partial sums in warp order, written to partials[4 b + k].
+struct EpiFcgDots {
+  static constexpr int NV = 3;
+  const double *v, *r, *q;  // q == nullptr: no gamma
+  double *w, *partials;
+  double acc[3];
+  __device__ const double *row_vec(int i) const { return i == 0 ? v : (i == 1 ? r : (q ? q : v)); }
+  __device__ void apply(int32_t row, double T, const double *rv) {
+    w[row] = T;
+    acc[0] = fma(rv[1], rv[0], acc[0]);
+    acc[1] = fma(T, rv[0], acc[1]);
+    if (q) acc[2] = fma(rv[2], rv[0], acc[2]);
+  }
+  __device__ void finish(int wid, int lane) {
+    __shared__ double red[kPipeWarps][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double a = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+      if (lane == 0) red[wid][k] = a;
+    }
+    // consumer warps only (the producer warp has left)
+    asm volatile("bar.sync 1, %0;" ::"n"(kPipeWarps * 32) : "memory");
+    if (wid == 0 && lane < 3) {
+      double s = 0.0;
+      for (int w2 = 0; w2 < kPipeWarps; ++w2) s += red[w2][lane];
+      partials[blockIdx.x * 4 + lane] = s;
+      for (int b = blockIdx.x + gridDim.x; b < kRedBlocks; b += gridDim.x)
+        partials[b * 4 + lane] = 0.0;
     }
   }
-  block_partials<3>(acc, partials);
+};
+
+// Shared-memory layout of one stage, identical on host and device.
+struct StageLayout {
+  uint32_t vals, cols, meta, rows, bytes;
+  __host__ __device__ StageLayout(int cap_slots, int vbytes, int xbytes, bool cols_staged,
+                                  int nv) {
+    const uint32_t slots = static_cast<uint32_t>(cap_slots + kSlotPad);
+    vals = 0;
+    cols = vals + slots * 32u * vbytes;
+    meta = cols + (cols_staged ? slots * 32u * 4u : 0u);
+    rows = meta + kPipeWarps * 16u;
+    bytes = rows + static_cast<uint32_t>(nv) * kPipeWarps * 32u * xbytes;
+    bytes = (bytes + 127u) & ~127u;
+  }
+};
+
+struct __align__(16) StageCtl {
+  int32_t slot0, staged, rows_staged, pad;
+};
+
+template <typename VT, typename XT, typename Epi, int KB>
+__global__ void __launch_bounds__(kPipeThreads)
+    k_sl_pipe(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ x, Epi epi,
+              int cap_slots, int cols_staged) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[kPipeStages], empty[kPipeStages];
+  __shared__ StageCtl ctl[kPipeStages];
+  constexpr int NVS = Epi::NV > 0 ? Epi::NV : 1;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int32_t nchunks = (S.nslices + kPipeWarps - 1) / kPipeWarps;
+  const StageLayout L(cap_slots, sizeof(VT), sizeof(XT), cols_staged != 0, Epi::NV);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kPipeStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], kPipeWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (wid == kPipeWarps) {  // producer
+    if (lane != 0) return;
+    uint32_t armed = 0;  // stages whose last phase carries a copy
+    // Row vectors are staged only from 16-byte aligned bases.
+    bool rows_aligned = Epi::NV > 0;
+    for (int i = 0; i < Epi::NV; ++i)
+      rows_aligned = rows_aligned && (reinterpret_cast<uintptr_t>(epi.row_vec(i)) & 15u) == 0;
+    int32_t c = blockIdx.x;
+    int32_t p0 = c < nchunks ? __ldg(S.sptr + c * kPipeWarps) : 0;
+    int32_t p1 = c < nchunks ? __ldg(S.sptr + min((c + 1) * kPipeWarps, S.nslices)) : 0;
+    int j = 0;
+    for (; c < nchunks; ++j, c += gridDim.x) {
+      const int32_t cn = c + gridDim.x;  // next chunk's bounds, loaded ahead
+      const int32_t q0 = cn < nchunks ? __ldg(S.sptr + cn * kPipeWarps) : 0;
+      const int32_t q1 = cn < nchunks ? __ldg(S.sptr + min((cn + 1) * kPipeWarps, S.nslices)) : 0;
+      const int st = j % kPipeStages;
+      if (j >= kPipeStages &&
+          !mbar_wait(&empty[st], static_cast<uint32_t>(((j / kPipeStages) - 1) & 1))) {
+        atomicExch(&g_sliced_wait_error, 1);
+        break;
+      }
+      const int32_t s0 = c * kPipeWarps, s1 = min(s0 + kPipeWarps, S.nslices);
+      const int32_t r0 = s0 * 32, r1 = min(s1 * 32, S.n);
+      const uint32_t rbytes = static_cast<uint32_t>(r1 - r0) * sizeof(XT);
+      const bool rows_ok = rows_aligned && (rbytes % 16u) == 0;
+      const bool fits = p1 - p0 <= cap_slots;
+      ctl[st].slot0 = p0;
+      ctl[st].staged = fits;
+      ctl[st].rows_staged = rows_ok;
+      unsigned char *base = smem + static_cast<size_t>(st) * L.bytes;
+      if (fits) {
+        const uint32_t nsl = static_cast<uint32_t>(p1 - p0) * 32u;
+        const uint32_t vb = nsl * sizeof(VT);
+        const uint32_t cb = cols_staged ? nsl * 4u : 0u;
+        const uint32_t mb = static_cast<uint32_t>(s1 - s0) * 16u;
+        mbar_arrive_tx(&full[st], vb + cb + mb + (rows_ok ? Epi::NV * rbytes : 0u));
+        if (vb) bulk_load(base + L.vals, val + static_cast<int64_t>(p0) * 32, vb, &full[st]);
+        if (cb) bulk_load(base + L.cols, S.scol + static_cast<int64_t>(p0) * 32, cb, &full[st]);
+        bulk_load(base + L.meta, S.meta + s0, mb, &full[st]);
+        if (rows_ok)
+          for (int i = 0; i < Epi::NV; ++i)
+            bulk_load(base + L.rows + i * kPipeWarps * 32 * sizeof(XT), epi.row_vec(i) + r0,
+                      rbytes, &full[st]);
+        armed |= 1u << st;
+      } else {
+        armed &= ~(1u << st);
+        mbar_arrive(&full[st]);
+      }
+      p0 = q0;
+      p1 = q1;
+    }
+    // Copies still in flight complete before the producer leaves.
+    for (int k = 0; k < kPipeStages && k < j; ++k) {
+      const int jj = j - 1 - k;
+      const int st = jj % kPipeStages;
+      if ((armed >> st) & 1u) {
+        if (!mbar_wait(&full[st], static_cast<uint32_t>((jj / kPipeStages) & 1)))
+          atomicExch(&g_sliced_wait_error, 1);
+      }
+    }
+    return;
+  }
+
+  // consumers
+  const int32_t hi = S.n - 1;
+  int32_t c = blockIdx.x;
+  for (int j = 0; c < nchunks; ++j, c += gridDim.x) {
+    const int st = j % kPipeStages;
+    if (!mbar_wait(&full[st], static_cast<uint32_t>((j / kPipeStages) & 1))) {
+      atomicExch(&g_sliced_wait_error, 1);
+      break;
+    }
+    const StageCtl cl = ctl[st];
+    const unsigned char *base = smem + static_cast<size_t>(st) * L.bytes;
+    const int32_t s = c * kPipeWarps + wid;
+    if (s < S.nslices) {
+      const int32_t r = s * 32 + lane;
+      const int4 m = cl.staged ? reinterpret_cast<const int4 *>(base + L.meta)[wid]
+                               : __ldg(S.meta + s);
+      XT rv[NVS];
+#pragma unroll
+      for (int i = 0; i < NVS; ++i) rv[i] = XT(0);
+      if (r < S.n) {
+        if (cl.staged && cl.rows_staged) {
+          const XT *rs = reinterpret_cast<const XT *>(base + L.rows) + wid * 32 + lane;
+#pragma unroll
+          for (int i = 0; i < Epi::NV; ++i) rv[i] = rs[i * kPipeWarps * 32];
+        } else {
+#pragma unroll
+          for (int i = 0; i < Epi::NV; ++i) rv[i] = epi.row_vec(i)[r];
+        }
+      }
+      XT T;
+      if (cl.staged) {
+        const int64_t rel = static_cast<int64_t>(m.x - cl.slot0) * 32 + lane;
+        const VT *v = reinterpret_cast<const VT *>(base + L.vals) + rel;
+        const int32_t *ci =
+            m.z ? nullptr
+                : (cols_staged ? reinterpret_cast<const int32_t *>(base + L.cols) + rel
+                               : S.scol + static_cast<int64_t>(m.x) * 32 + lane);
+        T = slice_row_sum<VT, XT, KB>(v, ci, S.soff + m.w, m.y, r, hi, x);
+      } else {
+        const int64_t at = static_cast<int64_t>(m.x) * 32 + lane;
+        T = slice_row_sum<VT, XT, KB>(val + at, m.z ? nullptr : S.scol + at, S.soff + m.w, m.y,
+                                      r, hi, x);
+      }
+      if (r < S.n) epi.apply(r, T, rv);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[st]);
+  }
+  epi.finish(wid, lane);
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4)
-    k_sl_spmv(SlicedView S, const double *__restrict__ val, const double *__restrict__ x,
-              double *__restrict__ y) {
-  const int lane = threadIdx.x & 31;
-  const int32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-  if (s >= S.nslices) return;
-  const int32_t r = s * 32 + lane;
-  const double T = sliced_dot<double, double>(S, val, x, s, r, lane);
-  if (r < S.n) y[r] = T;
+// ---- launch configuration ----------------------------------------------------
+
+struct PipeCfg {
+  int grid = 0;
+  size_t smem = 0;
+};
+
+// Occupancy-derived persistent grid for one kernel and stage size, cached
+// (the occupancy query and the shared-memory attribute are host calls made
+// once per kernel and size, outside any stream capture: sliced_build warms
+// the cache for the kernels a matrix will use).
+template <typename K>
+bcmg_status pipe_cfg(K kernel, size_t stage_bytes, int32_t nchunks, PipeCfg *out) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, size_t>, int> cache;
+  const size_t smem = kPipeStages * stage_bytes;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(reinterpret_cast<const void *>(kernel), smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      per_sm = it->second;
+    } else {
+      // Always the largest size any matrix may ask for, so a later matrix
+      // never lowers the limit another one relies on.
+      BCMG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kPipeStages * kMaxStageBytes)));
+      BCMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPipeThreads,
+                                                              smem));
+      if (per_sm < 1) return set_error(BCMG_ERR_INTERNAL, "sliced pipeline does not fit an SM");
+      cache[key] = per_sm;
+    }
+  }
+  int dev = 0, sms = kNumSM;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // At most kRedBlocks CTAs: the FCG epilogue writes one partial per CTA.
+  out->grid = static_cast<int>(std::min<int64_t>(
+      std::min<int64_t>(nchunks, static_cast<int64_t>(per_sm) * sms), kRedBlocks));
+  out->smem = smem;
+  return BCMG_OK;
+}
+
+inline int value_bytes(int vtype) {
+  return vtype == kValF64 ? 8 : (vtype == kValF32 ? 4 : 2);
+}
+
+template <typename VT, typename XT, typename Epi>
+bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaStream_t st,
+                        bool warm_only = false) {
+  if (S.nslices <= 0) return BCMG_OK;
+  const int32_t nchunks = ceil_div(S.nslices, kPipeWarps);
+  const StageLayout L(S.cap_slots, sizeof(VT), sizeof(XT), S.cols_staged != 0, Epi::NV);
+  PipeCfg cfg;
+#define BCMG_PIPE_KB(KB_)                                                                   \
+  do {                                                                                      \
+    auto kern = k_sl_pipe<VT, XT, Epi, KB_>;                                                \
+    BCMG_TRY(pipe_cfg(kern, L.bytes, nchunks, &cfg));                                       \
+    if (!warm_only)                                                                         \
+      launch(kern, cfg.grid, kPipeThreads, cfg.smem, st, S, static_cast<const VT *>(S.val), \
+             x, epi, S.cap_slots, S.cols_staged);                                           \
+  } while (0)
+  if (S.batch <= 8) BCMG_PIPE_KB(8);
+  else if (S.batch <= 16) BCMG_PIPE_KB(16);
+  else BCMG_PIPE_KB(28);
+#undef BCMG_PIPE_KB
+  if (!warm_only) BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
 }
 
 template <typename VT, typename XT>
-void sl_relax_launch(const SlicedView &S, const XT *d, const XT *f, const XT *src, XT *dst,
-                     cudaStream_t st) {
-  launch(k_sl_relax<VT, XT>, ceil_div(S.nslices, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st,
-         S, static_cast<const VT *>(S.val), d, f, src, dst);
+bcmg_status relax_as(const SlicedView &S, const XT *d, const XT *f, const XT *u, XT *u_out,
+                     cudaStream_t st, bool warm_only = false) {
+  EpiRelax<XT> e{f, d, u, u_out};
+  return pipe_launch<VT, XT>(S, u, e, st, warm_only);
 }
 
 template <typename VT, typename XT>
-void sl_residual_launch(const SlicedView &S, const XT *f, const XT *u, XT *res,
-                        cudaStream_t st) {
-  launch(k_sl_residual<VT, XT>, ceil_div(S.nslices, kWarpsPerBlock), kWarpsPerBlock * 32, 0,
-         st, S, static_cast<const VT *>(S.val), f, u, res);
+bcmg_status residual_as(const SlicedView &S, const XT *f, const XT *u, XT *res,
+                        cudaStream_t st, bool warm_only = false) {
+  EpiResidual<XT> e{f, res};
+  return pipe_launch<VT, XT>(S, u, e, st, warm_only);
+}
+
+// Fills the occupancy cache for the kernels this matrix will run, so no
+// attribute or occupancy call happens inside a captured solve.
+bcmg_status warm_kernels(const SlicedView &S) {
+  switch (S.vtype) {
+    case kValF64: {
+      BCMG_TRY((relax_as<double, double>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
+      BCMG_TRY((residual_as<double, double>(S, nullptr, nullptr, nullptr, 0, true)));
+      EpiSpmv e1{nullptr};
+      BCMG_TRY((pipe_launch<double, double>(S, static_cast<const double *>(nullptr), e1, 0, true)));
+      EpiFcgDots e2{};
+      BCMG_TRY((pipe_launch<double, double>(S, static_cast<const double *>(nullptr), e2, 0, true)));
+      break;
+    }
+    case kValF32:
+      BCMG_TRY((relax_as<float, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
+      BCMG_TRY((residual_as<float, float>(S, nullptr, nullptr, nullptr, 0, true)));
+      break;
+    case kValBF16:
+      BCMG_TRY((relax_as<__nv_bfloat16, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
+      BCMG_TRY((residual_as<__nv_bfloat16, float>(S, nullptr, nullptr, nullptr, 0, true)));
+      break;
+    default:
+      BCMG_TRY((relax_as<__half, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
+      BCMG_TRY((residual_as<__half, float>(S, nullptr, nullptr, nullptr, 0, true)));
+      break;
+  }
+  return BCMG_OK;
 }
 
 }  // namespace
 
 size_t SlicedMat::bytes() const {
   if (!nslices) return 0;
-  const size_t vbytes = vtype == kValF64 ? 8 : (vtype == kValF32 ? 4 : 2);
-  const size_t sl = static_cast<size_t>(slots) * 32;
-  return vbytes * sl + 16 + (has_columns ? 4 * sl : 0) + 4 * (static_cast<size_t>(slots) + 1) +
-         4 * (3 * static_cast<size_t>(nslices) + 1);
+  const size_t vb = value_bytes(vtype);
+  const size_t sl = (static_cast<size_t>(slots) + kSlotPad) * 32;
+  return vb * sl + (has_columns ? 4 * sl : 0) + 4 * (static_cast<size_t>(slots) + kSlotPad) +
+         4 * (static_cast<size_t>(nslices) + 1) + 16 * static_cast<size_t>(nslices);
 }
 
 void SlicedMat::release(cudaStream_t s) {
   dev_free(sptr, s);
-  dev_free(width, s);
-  dev_free(kind, s);
+  dev_free(meta, s);
   dev_free(scol, s);
   dev_free(soff, s);
   if (val) cudaFreeAsync(val, s);
@@ -279,12 +673,14 @@ SlicedView SlicedMat::view() const {
   v.n = n;
   v.nslices = nslices;
   v.sptr = sptr;
-  v.width = width;
-  v.kind = kind;
+  v.meta = meta;
   v.scol = scol;
   v.soff = soff;
   v.val = val;
   v.vtype = vtype;
+  v.cap_slots = cap_slots;
+  v.cols_staged = has_columns ? 1 : 0;
+  v.batch = batch;
   return v;
 }
 
@@ -296,52 +692,90 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
   out->n = n;
   out->nslices = ns;
   out->vtype = vtype;
+  DevBuf<int32_t> width, kind, stats, tmp;
   BCMG_TRY(dev_alloc(&out->sptr, ns + 1, s));
-  BCMG_TRY(dev_alloc(&out->width, ns, s));
-  BCMG_TRY(dev_alloc(&out->kind, ns, s));
-  const int blocks = ceil_div(ns, kWarpsPerBlock);
-  launch(k_slice_shape, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row, A.col, out->width,
-         out->kind);
-  DevBuf<int32_t> tmp;
+  BCMG_TRY(dev_alloc(&out->meta, ns, s));
+  BCMG_TRY(width.alloc(ns, s));
+  BCMG_TRY(kind.alloc(ns, s));
+  BCMG_TRY(stats.alloc(3, s));
   BCMG_TRY(tmp.alloc(scan_tmp_size(ns), s));
-  BCMG_TRY(exclusive_scan(out->width, out->sptr, ns, out->sptr + ns, tmp.get(), s));
-  int32_t slots = 0;
-  std::vector<int32_t> kinds(ns);
-  BCMG_CUDA(cudaMemcpyAsync(&slots, out->sptr + ns, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  BCMG_CUDA(cudaMemcpyAsync(kinds.data(), out->kind, sizeof(int32_t) * ns,
+  const int blocks = ceil_div(ns, kWarpsPerBlock);
+  launch(k_slice_shape, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row, A.col, width.get(),
+         kind.get());
+  BCMG_TRY(exclusive_scan(width.get(), out->sptr, ns, out->sptr + ns, tmp.get(), s));
+  BCMG_CUDA(cudaMemsetAsync(stats.get(), 0, 3 * sizeof(int32_t), s));
+  const int32_t nchunks = ceil_div(ns, kPipeWarps);
+  launch(k_slice_stats, ceil_div(nchunks, 256), 256, 0, s, ns, out->sptr, kind.get(),
+         stats.get());
+  BCMG_LAUNCH_CHECK();
+  int32_t h_stats[3] = {0, 0, 0};
+  BCMG_CUDA(cudaMemcpyAsync(h_stats, stats.get(), 2 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            s));
+  BCMG_CUDA(cudaMemcpyAsync(h_stats + 2, out->sptr + ns, sizeof(int32_t),
                             cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
+  const int32_t slots = h_stats[2];
   out->slots = slots;
-  const size_t vbytes = vtype == kValF64 ? 8 : (vtype == kValF32 ? 4 : 2);
-  BCMG_CUDA(cudaMallocAsync(&out->val, vbytes * static_cast<size_t>(slots) * 32 + 16, s));
+  out->has_columns = h_stats[1] != 0;
+  out->batch = static_cast<int32_t>((static_cast<int64_t>(slots) + ns - 1) / ns);
+  const size_t vb = value_bytes(vtype);
+  const int64_t padded = static_cast<int64_t>(slots) + kSlotPad;
+  BCMG_CUDA(cudaMallocAsync(&out->val, vb * static_cast<size_t>(padded) * 32, s));
+  BCMG_CUDA(cudaMemsetAsync(static_cast<char *>(out->val) + vb * static_cast<size_t>(slots) * 32,
+                            0, vb * kSlotPad * 32, s));
   // Explicit columns are only read in column slices; a matrix made of offset
   // slices alone (a stencil) stores none.
-  out->has_columns = std::any_of(kinds.begin(), kinds.end(), [](int32_t k) { return k == 0; });
-  if (out->has_columns) BCMG_TRY(dev_alloc(&out->scol, static_cast<int64_t>(slots) * 32, s));
-  BCMG_TRY(dev_alloc(&out->soff, slots + 1, s));
+  if (out->has_columns) {
+    BCMG_TRY(dev_alloc(&out->scol, padded * 32, s));
+    BCMG_CUDA(cudaMemsetAsync(out->scol, 0, sizeof(int32_t) * padded * 32, s));
+  }
+  BCMG_TRY(dev_alloc(&out->soff, padded, s));
+  BCMG_CUDA(cudaMemsetAsync(out->soff, 0, sizeof(int32_t) * padded, s));
   switch (vtype) {
     case kValF64:
       launch(k_slice_fill<double>, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row, A.col,
-             A.val, out->sptr, out->width, out->kind, static_cast<double *>(out->val),
+             A.val, out->sptr, width.get(), kind.get(), static_cast<double *>(out->val),
              out->scol, out->soff);
       break;
     case kValF32:
       launch(k_slice_fill<float>, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row, A.col,
-             A.val, out->sptr, out->width, out->kind, static_cast<float *>(out->val),
+             A.val, out->sptr, width.get(), kind.get(), static_cast<float *>(out->val),
              out->scol, out->soff);
       break;
     case kValBF16:
       launch(k_slice_fill<__nv_bfloat16>, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row,
-             A.col, A.val, out->sptr, out->width, out->kind,
+             A.col, A.val, out->sptr, width.get(), kind.get(),
              static_cast<__nv_bfloat16 *>(out->val), out->scol, out->soff);
       break;
     default:
       launch(k_slice_fill<__half>, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row, A.col,
-             A.val, out->sptr, out->width, out->kind, static_cast<__half *>(out->val),
+             A.val, out->sptr, width.get(), kind.get(), static_cast<__half *>(out->val),
              out->scol, out->soff);
       break;
   }
   BCMG_LAUNCH_CHECK();
+  // Runs of identical offset lists share the run head's copy.
+  {
+    DevBuf<int32_t> flag, rid, head;
+    BCMG_TRY(flag.alloc(ns, s));
+    BCMG_TRY(rid.alloc(ns + 1, s));
+    BCMG_TRY(head.alloc(ns, s));
+    launch(k_slice_runs, blocks, kWarpsPerBlock * 32, 0, s, ns, out->sptr, width.get(),
+           kind.get(), out->soff, flag.get());
+    BCMG_TRY(exclusive_scan(flag.get(), rid.get(), ns, rid.get() + ns, tmp.get(), s));
+    launch(k_slice_heads, ceil_div(ns, 256), 256, 0, s, ns, flag.get(), rid.get(), head.get());
+    launch(k_slice_meta, ceil_div(ns, 256), 256, 0, s, ns, out->sptr, width.get(), kind.get(),
+           flag.get(), rid.get(), head.get(), out->meta);
+    BCMG_LAUNCH_CHECK();
+  }
+  // Stage capacity: the largest chunk, capped so two stages fit in shared
+  // memory (larger chunks are read from global memory by the consumers).
+  const size_t per_slot = 32 * (vb + (out->has_columns ? 4 : 0));
+  const size_t fixed = kPipeWarps * 16 + 3 * kPipeWarps * 32 * 8 + 128;
+  const int32_t cap_max =
+      static_cast<int32_t>((kMaxStageBytes - fixed) / per_slot) - kSlotPad;
+  out->cap_slots = std::max<int32_t>(1, std::min<int32_t>(h_stats[0], cap_max));
+  BCMG_TRY(warm_kernels(out->view()));
   return BCMG_OK;
 }
 
@@ -350,22 +784,19 @@ bcmg_status sliced_relax_sweep(const SlicedView &S, const XT *d, const XT *f, co
                                XT *u_out, cudaStream_t s) {
   if (std::is_same<XT, double>::value) {
     if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
-    sl_relax_launch<double, double>(S, reinterpret_cast<const double *>(d),
+    return relax_as<double, double>(S, reinterpret_cast<const double *>(d),
                                     reinterpret_cast<const double *>(f),
                                     reinterpret_cast<const double *>(u),
                                     reinterpret_cast<double *>(u_out), s);
-  } else {
-    const float *df = reinterpret_cast<const float *>(d);
-    const float *ff = reinterpret_cast<const float *>(f);
-    const float *uf = reinterpret_cast<const float *>(u);
-    float *of = reinterpret_cast<float *>(u_out);
-    if (S.vtype == kValF32) sl_relax_launch<float, float>(S, df, ff, uf, of, s);
-    else if (S.vtype == kValBF16) sl_relax_launch<__nv_bfloat16, float>(S, df, ff, uf, of, s);
-    else if (S.vtype == kValF16) sl_relax_launch<__half, float>(S, df, ff, uf, of, s);
-    else return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
   }
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
+  const float *df = reinterpret_cast<const float *>(d);
+  const float *ff = reinterpret_cast<const float *>(f);
+  const float *uf = reinterpret_cast<const float *>(u);
+  float *of = reinterpret_cast<float *>(u_out);
+  if (S.vtype == kValF32) return relax_as<float, float>(S, df, ff, uf, of, s);
+  if (S.vtype == kValBF16) return relax_as<__nv_bfloat16, float>(S, df, ff, uf, of, s);
+  if (S.vtype == kValF16) return relax_as<__half, float>(S, df, ff, uf, of, s);
+  return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
 }
 
 template <typename XT>
@@ -373,36 +804,46 @@ bcmg_status sliced_residual(const SlicedView &S, const XT *f, const XT *u, XT *r
                             cudaStream_t s) {
   if (std::is_same<XT, double>::value) {
     if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
-    sl_residual_launch<double, double>(S, reinterpret_cast<const double *>(f),
+    return residual_as<double, double>(S, reinterpret_cast<const double *>(f),
                                        reinterpret_cast<const double *>(u),
                                        reinterpret_cast<double *>(res), s);
-  } else {
-    const float *ff = reinterpret_cast<const float *>(f);
-    const float *uf = reinterpret_cast<const float *>(u);
-    float *rf = reinterpret_cast<float *>(res);
-    if (S.vtype == kValF32) sl_residual_launch<float, float>(S, ff, uf, rf, s);
-    else if (S.vtype == kValBF16) sl_residual_launch<__nv_bfloat16, float>(S, ff, uf, rf, s);
-    else if (S.vtype == kValF16) sl_residual_launch<__half, float>(S, ff, uf, rf, s);
-    else return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
   }
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
+  const float *ff = reinterpret_cast<const float *>(f);
+  const float *uf = reinterpret_cast<const float *>(u);
+  float *rf = reinterpret_cast<float *>(res);
+  if (S.vtype == kValF32) return residual_as<float, float>(S, ff, uf, rf, s);
+  if (S.vtype == kValBF16) return residual_as<__nv_bfloat16, float>(S, ff, uf, rf, s);
+  if (S.vtype == kValF16) return residual_as<__half, float>(S, ff, uf, rf, s);
+  return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
 }
 
 bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w,
                                  const double *r, const double *q, double *partials,
                                  cudaStream_t s) {
   if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "FCG SpMV needs FP64 values");
-  launch(k_sl_fcg_spmv_dots, kRedBlocks, kWarpsPerBlock * 32, 0, s, S, v, w, r, q, partials);
-  BCMG_LAUNCH_CHECK();
-  return BCMG_OK;
+  EpiFcgDots e{v, r, q, w, partials, {0.0, 0.0, 0.0}};
+  return pipe_launch<double, double>(S, v, e, s);
 }
 
 bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStream_t s) {
   if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced SpMV needs FP64 values");
-  launch(k_sl_spmv, ceil_div(S.nslices, kWarpsPerBlock), kWarpsPerBlock * 32, 0, s, S,
-         static_cast<const double *>(S.val), x, y);
-  BCMG_LAUNCH_CHECK();
+  EpiSpmv e{y};
+  return pipe_launch<double, double>(S, x, e, s);
+}
+
+bcmg_status sliced_wait_status(cudaStream_t s) {
+  int flag = 0;
+  BCMG_CUDA(cudaMemcpyFromSymbolAsync(&flag, g_sliced_wait_error, sizeof(int), 0,
+                                      cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  if (flag) {
+    const int zero = 0;
+    BCMG_CUDA(cudaMemcpyToSymbolAsync(g_sliced_wait_error, &zero, sizeof(int), 0,
+                                      cudaMemcpyHostToDevice, s));
+    BCMG_CUDA(cudaStreamSynchronize(s));
+    return set_error(BCMG_ERR_DEVICE_TIMEOUT,
+                     "a sliced row pass gave up waiting for its staged copies");
+  }
   return BCMG_OK;
 }
 

@@ -40,23 +40,30 @@ bcmg_status compose_p(int32_t n, int32_t *agg, double *p, const int32_t *agg2,
 // Value storage of a level matrix used by the cycle.
 enum ValType { kValF64 = 0, kValF32 = 1, kValBF16 = 2, kValF16 = 3 };
 
-// Sliced solve-phase format (k_sliced.cu): 32-row slices, slot-major values;
-// kind[s] = 1: shared column offsets soff[sptr[s] + k]; 0: explicit columns
-// scol[32 sptr[s] + 32 k + lane].
+// Sliced solve-phase format (k_sliced.cu): 32-row slices, slot-major values.
+// meta[s] = {first slot, width W, kind, offset base}: kind 1 = shared column
+// offsets soff[base + k] (base = the first slice of a run of slices with the
+// same offsets); kind 0 = explicit columns scol[32 first + 32 k + lane].
+// Values, columns and offsets are padded past the last slot.
 struct SlicedView {
   int32_t n = 0, nslices = 0;
-  const int32_t *sptr = nullptr, *width = nullptr, *kind = nullptr;
+  const int32_t *sptr = nullptr;  // first slot of each slice (nslices + 1)
+  const int4 *meta = nullptr;
   const int32_t *scol = nullptr, *soff = nullptr;
   const void *val = nullptr;
   int vtype = kValF64;
+  int32_t cap_slots = 0;    // slots one pipeline stage holds
+  int32_t cols_staged = 0;  // explicit columns exist (and are staged)
+  int32_t batch = 0;        // mean slice width (chooses the slot batch size)
 };
 
 struct SlicedMat {
   int32_t n = 0, nslices = 0, slots = 0;
-  int32_t *sptr = nullptr, *width = nullptr, *kind = nullptr, *scol = nullptr,
-          *soff = nullptr;
+  int32_t *sptr = nullptr, *scol = nullptr, *soff = nullptr;
+  int4 *meta = nullptr;
   void *val = nullptr;
   int vtype = kValF64;
+  int32_t cap_slots = 0, batch = 0;
   bool has_columns = false;  // scol allocated (some slice is a column slice)
   void release(cudaStream_t s);
   size_t bytes() const;  // device bytes held
@@ -77,6 +84,9 @@ bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStr
 bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w,
                                  const double *r, const double *q, double *partials,
                                  cudaStream_t s);
+// BCMG_ERR_DEVICE_TIMEOUT (and the flag cleared) if a sliced row pass gave up
+// waiting for its staged copies since the last call; synchronises s.
+bcmg_status sliced_wait_status(cudaStream_t s);
 
 struct MatView {
   int32_t n = 0, nnz = 0;
