@@ -387,14 +387,14 @@ def run_ours(args):
         # metadata, and u (gathered once), f, d read + u' written
         sweep_bytes = (vbytes.value * 32 * slots.value + 4 * 32 * cslots.value +
                        16 * nsl.value + 4 * xbytes * A.n)
-        kname = "k_sl_relax (level-0 l1-Jacobi sweep, sliced)"
+        kname = "k_sl_pipe<EpiRelax> (level-0 l1-Jacobi sweep, sliced, pipelined)"
     else:
         sweep_bytes = 12 * A.nnz + 4 * (A.n + 1) + 36 * A.n
         kname = "k_relax_t (level-0 l1-Jacobi sweep, CSR)"
     csr_equiv = 12 * A.nnz + 4 * (A.n + 1) + 36 * A.n
     achieved = sweep_bytes / sweep_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = committed_traffic("k_sl_relax", f"{args.workload}:{args.precision}")
+    traffic = committed_traffic("k_sl_pipe", f"{args.workload}:{args.precision}")
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:

@@ -98,6 +98,11 @@ struct PhaseClock {
   }
 };
 thread_local PhaseClock g_clock;
+}  // namespace
+
+void phase_tick(const char *name) { g_clock.tick(name); }
+
+namespace {
 
 bcmg_status read_scalar(const double *dev, double *host, cudaStream_t s) {
   BCMG_CUDA(cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -627,6 +632,7 @@ void destroy_handle(bcmg_handle *h) {
 bcmg_status setup_common(bcmg_handle *h) {
   NvtxRange range("bcmg_setup");
   const auto t0 = Clock::now();
+  BCMG_TRY(csr_validate(h->A0.view(), h->stream));
   g_clock.start(h->ext.verbose >= 1, h->stream);
   const int32_t n = h->A0.n;
   // BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311).
@@ -912,7 +918,15 @@ bcmg_status bcmg_setup(const bcmg_csr *A, const bcmg_params *p, const bcmg_ext *
   clear_error();
   if (!A || !out) return set_error(BCMG_ERR_PARAM, "null argument");
   *out = nullptr;
-  BCMG_TRY(bcmg_csr_check(A));
+  // Only the O(1) checks here; the entries are validated on the device after
+  // the upload (csr_validate), which is far faster than a host pass.
+  if (!A->row || (A->nnz > 0 && (!A->col || !A->val)))
+    return set_error(BCMG_ERR_PARAM, "null CSR array");
+  if (A->n <= 0 || A->n != A->m)
+    return set_error(BCMG_ERR_INVALID_MATRIX, "matrix must be square with n > 0 (%d x %d)",
+                     A->n, A->m);
+  if (A->row[0] != 0 || A->row[A->n] != A->nnz)
+    return set_error(BCMG_ERR_INVALID_MATRIX, "row pointer does not span [0, nnz]");
   bcmg_handle *h = nullptr;
   BCMG_TRY(new_handle(p, ext, &h));
   std::unique_ptr<bcmg_handle, void (*)(bcmg_handle *)> guard(h, destroy_handle);

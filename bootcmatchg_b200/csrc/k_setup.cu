@@ -804,6 +804,7 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
     default: BCMG_TRY(launch_weights<32>(A, w, C.get(), minb.get(), W, s)); break;
   }
 
+  phase_tick("weights");
   // Preference-sorted rows, then the suitor proposals.
   DevBuf<double> sW;
   DevBuf<int32_t> scol, next, long_rows, n_long;
@@ -825,6 +826,7 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
            n_long.get(), A.row, A.col, W, sW.get(), scol.get(), err.get());
     BCMG_LAUNCH_CHECK();
   }
+  phase_tick("sort_prefs");
   BCMG_CUDA(cudaMemsetAsync(offer.get(), 0xff, sizeof(unsigned long long) * n, s));
   launch(k_init_next, nb, T, 0, s, n, A.row, next.get());
   const int64_t limit = 8 * static_cast<int64_t>(A.nnz) + 1024;
@@ -832,6 +834,7 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
          err.get());
   BCMG_LAUNCH_CHECK();
   launch(k_offer_to_suitor, nb, T, 0, s, n, offer.get(), sv.get());
+  phase_tick("suitor");
 
   // unsymFix.
   launch(k_sym_pairs, nb, T, 0, s, n, sv.get(), mv.get());
@@ -916,6 +919,7 @@ bcmg_status galerkin(const CsrView &A, const int32_t *agg, const double *p, int3
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
   launch(k_gal_terms, ceil_div(nc, 256), 256, 0, s, nc, A.row, rptr, ridx, tpos.get());
   BCMG_TRY(exclusive_scan(tpos.get(), tpos.get(), nc, tpos.get() + nc, tmp.get(), s));
+  phase_tick("gal_terms");
   const size_t smem_warp = static_cast<size_t>(kGalWarpsPerBlock) * kGalCap * kGalBytesPerTerm;
   const size_t smem_long = static_cast<size_t>(kGalCapLong) * kGalBytesPerTerm;
   BCMG_CUDA(cudaFuncSetAttribute(k_gal_rows_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -927,6 +931,7 @@ bcmg_status galerkin(const CsrView &A, const int32_t *agg, const double *p, int3
          n_long.get(), A.row, A.col, A.val, agg, p, rptr, ridx, tpos.get(), tJ.get(), tV.get(),
          crow, err.get());
   BCMG_LAUNCH_CHECK();
+  phase_tick("gal_rows");
   // crow holds the run counts: scan them into row pointers.
   BCMG_TRY(exclusive_scan(crow, crow, nc, crow + nc, tmp.get(), s));
   int h_err = 0;

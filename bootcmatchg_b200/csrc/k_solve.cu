@@ -225,6 +225,36 @@ inline int grid_for(int64_t work) {
   return static_cast<int>(b < 1 ? 1 : b);
 }
 
+
+// Structural check of a device CSR matrix, one thread per row: row bounds,
+// columns in range and strictly increasing, finite values, a diagonal entry.
+// The smallest offending row wins: err = (row << 8) | code.
+__global__ void k_csr_validate(int32_t n, int32_t nnz, const int32_t *__restrict__ row,
+                               const int32_t *__restrict__ col,
+                               const double *__restrict__ val,
+                               unsigned long long *err) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t b = row[i], e = row[i + 1];
+  int code = 0;
+  if (b < 0 || e < b || e > nnz) {
+    code = kCsrBadRow;
+  } else {
+    bool diag = false;
+    int32_t prev = -1;
+    for (int32_t j = b; j < e && !code; ++j) {
+      const int32_t c = col[j];
+      if (c < 0 || c >= n) code = kCsrBadColumn;
+      else if (c <= prev) code = kCsrUnsorted;
+      else if (!isfinite(val[j])) code = kCsrNonFinite;
+      diag = diag || c == i;
+      prev = c;
+    }
+    if (!code && !diag) code = kCsrNoDiagonal;
+  }
+  if (code) atomicMin(err, (static_cast<unsigned long long>(i) << 8) | code);
+}
+
 }  // namespace
 
 bcmg_status spmv(const CsrView &A, double alpha, const double *x, double beta, double *y,
@@ -303,6 +333,35 @@ bcmg_status fcg_replace(const CsrView &A, const double *b, const double *x, doub
   launch(k_norm_final_if, 1, kThreads, 0, s, partials, scal);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
+}
+
+bcmg_status csr_validate(const CsrView &A, cudaStream_t s) {
+  if (A.n <= 0) return set_error(BCMG_ERR_INVALID_MATRIX, "matrix must have n > 0");
+  DevBuf<unsigned long long> err;
+  BCMG_TRY(err.alloc(1, s));
+  BCMG_CUDA(cudaMemsetAsync(err.get(), 0xff, sizeof(unsigned long long), s));
+  launch(k_csr_validate, ceil_div(A.n, kThreads), kThreads, 0, s, A.n, A.nnz, A.row, A.col,
+         A.val, err.get());
+  BCMG_LAUNCH_CHECK();
+  unsigned long long h = 0;
+  BCMG_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  if (h == ~0ull) return BCMG_OK;
+  const long long r = static_cast<long long>(h >> 8);
+  switch (static_cast<int>(h & 0xff)) {
+    case kCsrBadRow:
+      return set_error(BCMG_ERR_INVALID_MATRIX, "row %lld has a bad row pointer range", r);
+    case kCsrBadColumn:
+      return set_error(BCMG_ERR_INVALID_MATRIX, "row %lld: column out of range", r);
+    case kCsrUnsorted:
+      return set_error(BCMG_ERR_INVALID_MATRIX, "row %lld: columns not strictly increasing",
+                       r);
+    case kCsrNonFinite:
+      return set_error(BCMG_ERR_INVALID_MATRIX, "row %lld: non-finite value", r);
+    default:
+      return set_error(BCMG_ERR_INVALID_MATRIX,
+                       "row %lld has no diagonal entry (the AH builder needs one)", r);
+  }
 }
 
 }  // namespace bcmg

@@ -18,6 +18,10 @@ struct CsrView {
   const double *val = nullptr;
 };
 
+// Phase timing hook (driver.cu): with ext.verbose >= 1 it synchronises the
+// stream and charges the elapsed wall time to `name`; otherwise a no-op.
+void phase_tick(const char *name);
+
 // ---- setup (k_setup.cu; FP64, no FMA contraction) -------------------------
 bcmg_status level_prep(const CsrView &A, double *D, double *M, cudaStream_t s);
 bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg,
@@ -148,6 +152,12 @@ inline bcmg_status scale(int64_t n, double a, double *x, cudaStream_t s) {
 }
 
 // ---- FCG (k_solve.cu) ------------------------------------------------------
+// Structural check of a device CSR matrix (row pointers, columns in range and
+// strictly increasing, finite values, a diagonal in every row); synchronises s
+// and returns BCMG_ERR_INVALID_MATRIX naming the first offending row.
+enum CsrFault { kCsrBadRow = 1, kCsrBadColumn, kCsrUnsorted, kCsrNonFinite, kCsrNoDiagonal };
+bcmg_status csr_validate(const CsrView &A, cudaStream_t s);
+
 // y = alpha A x + beta y (FP64)
 bcmg_status spmv(const CsrView &A, double alpha, const double *x, double beta,
                  double *y, cudaStream_t s);
