@@ -8,6 +8,7 @@
 // reductions whose order could vary are either exact (min, integer sums) or
 // run in a fixed order, so setup is deterministic run to run.
 #include <cfloat>
+#include <climits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -106,26 +107,8 @@ __global__ void __launch_bounds__(256)
 }
 
 // W_ij = log(|AH_ij| / (0.999 mu)) (_make_w with MAXIMUM_PRODUCT_MATRIX_OP 1,
-// src/AMG/matching.cu:387-395), stored over A's pattern with 0 on the
-// diagonal (the matcher ignores weights <= 0).
-template <int G>
-__global__ void k_make_W(int32_t n, const int32_t *__restrict__ row,
-                         const int32_t *__restrict__ col,
-                         const double *__restrict__ val, const double *__restrict__ w,
-                         const double *__restrict__ C,
-                         const unsigned long long *__restrict__ min_bits,
-                         double *__restrict__ W) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int32_t i = static_cast<int32_t>(t / G);
-  const int lane = threadIdx.x % G;
-  if (i >= n) return;
-  const double den = 0.999 * __longlong_as_double(static_cast<long long>(*min_bits));
-  const double ci = C[i], wi = w[i];
-  for (int32_t j = row[i] + lane; j < row[i + 1]; j += G) {
-    const int32_t c = col[j];
-    W[j] = (c == i) ? 0.0 : log(fabs(ah_value(val[j], ci, C[c], wi, w[c])) / den);
-  }
-}
+// src/AMG/matching.cu:387-395) is computed inside the preference sort
+// (match_weight), so W is never stored unless a caller asks for it.
 
 // Suitor matching (kernel_for_matching, src/AMG/suitor.cu:242-392).
 //
@@ -137,9 +120,12 @@ __global__ void k_make_W(int32_t n, const int32_t *__restrict__ row,
 // Offers only increase, so a neighbour a proposer once could not beat (or was
 // displaced from) stays unbeatable: each proposer resumes its scan where it
 // stopped (next[]), and all proposals together read each row about once.
-// An offer is one 64-bit word (sorted position << 32 | proposer); the
-// position recovers the immutable weight, so a CAS replaces the reference's
-// per-vertex spin locks (suitor.cu:19-38,69-110).  A displaced proposer is
+// With symmetric weights (every SPD input: W is bitwise symmetric when A is)
+// an offer is the proposer's position in the receiver's own sorted row and a
+// single atomicMin tests and installs it (k_suitor_sym).  Otherwise an offer
+// is one 64-bit word (sorted position << 32 | proposer); the position
+// recovers the immutable weight, so a CAS replaces the reference's per-vertex
+// spin locks (suitor.cu:19-38,69-110).  A displaced proposer is
 // taken over by the displacing thread (set_suitor, suitor.cu:89-93).  The
 // final state is the proposer-optimal (Gale-Shapley) one, independent of the
 // interleaving.  next[] is written without synchronisation: any value a
@@ -151,160 +137,307 @@ __device__ __forceinline__ bool pref_before(double wa, int32_t ya, double wb, in
   return wa > wb || (wa == wb && ya > yb);
 }
 
-constexpr int kSortCap = 1024;        // entries per warp (shared memory sort)
-constexpr int kSortCapLong = 4096;    // entries per block
+constexpr int kSortCapLong = 4096;  // entries per block (shared memory sort)
 constexpr int kSortWarps = 4;
+constexpr int kSortRegMax = 128;    // longest row sorted in registers (4 per lane)
 
-// Sorts rows of W (over A's pattern) into preference order: sW, scol.
-// Unusable entries (diagonal, W <= 0, NaN) sort last as -1.
+// Within a row the columns are strictly increasing, so comparing original
+// offsets t orders entries exactly as comparing their columns: the sort keys
+// are (W, t) and ties go to the larger t (the higher column id).
+
+// The matching weight of entry e = (i, c) (k_make_W formula); -1 marks an
+// entry the matcher never uses (the diagonal, W <= 0, NaN).  W_out, when
+// given, receives W over A's pattern with 0 on the diagonal.
+__device__ __forceinline__ double match_weight(int32_t i, int32_t e, double ci, double wi,
+                                               const int32_t *__restrict__ col,
+                                               const double *__restrict__ val,
+                                               const double *__restrict__ w,
+                                               const double *__restrict__ C, double den,
+                                               double *W_out) {
+  const int32_t c = col[e];
+  if (c == i) {
+    if (W_out) W_out[e] = 0.0;
+    return -1.0;
+  }
+  const double x = log(fabs(ah_value(val[e], ci, C[c], wi, w[c])) / den);
+  if (W_out) W_out[e] = x;
+  return x > 0.0 ? x : -1.0;
+}
+
+// Writes one sorted entry: scol/sW at sorted position pos, and the inverse
+// permutation inv[b + t] = pos.
+__device__ __forceinline__ void put_sorted(int32_t b, int pos, int t, double wv,
+                                           const int32_t *__restrict__ col, double *sW,
+                                           int32_t *scol, int32_t *inv) {
+  sW[b + pos] = wv;
+  scol[b + pos] = col[b + t];
+  inv[b + t] = pos;
+}
+
+// Bitonic sort of 32*E (weight, offset) pairs held E per lane (position
+// e*32 + lane) into preference order.
+template <int E>
+__device__ __forceinline__ void warp_bitonic(double (&wv)[E], int32_t (&tv)[E], int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int f = e ^ (j >> 5);
+          if (f > e) {
+            const bool asc = ((e * 32 + lane) & k) == 0;
+            const bool pb = pref_before(wv[f], tv[f], wv[e], tv[e]);
+            if (asc ? pb : !pb) {
+              const double tw = wv[e];
+              wv[e] = wv[f];
+              wv[f] = tw;
+              const int32_t tt = tv[e];
+              tv[e] = tv[f];
+              tv[f] = tt;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int p = e * 32 + lane;
+          const double pw = __shfl_xor_sync(0xffffffffu, wv[e], j);
+          const int32_t pt = __shfl_xor_sync(0xffffffffu, tv[e], j);
+          const bool lower = (p & j) == 0;
+          const bool asc = (p & k) == 0;
+          const bool pb = pref_before(pw, pt, wv[e], tv[e]);  // partner ranks first
+          if ((lower == asc) ? pb : !pb) {
+            wv[e] = pw;
+            tv[e] = pt;
+          }
+        }
+      }
+    }
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void sort_row_regs(int32_t i, int32_t b, int T, double ci, double wi,
+                                              const int32_t *__restrict__ col,
+                                              const double *__restrict__ val,
+                                              const double *__restrict__ w,
+                                              const double *__restrict__ C, double den,
+                                              double *W_out, double *sW, int32_t *scol,
+                                              int32_t *inv, int32_t *ucnt, int lane) {
+  double wv[E];
+  int32_t tv[E];
+  int nu = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int t = e * 32 + lane;
+    wv[e] = -1.0;
+    tv[e] = -1;
+    if (t < T) {
+      wv[e] = match_weight(i, b + t, ci, wi, col, val, w, C, den, W_out);
+      tv[e] = t;
+      nu += wv[e] > 0.0 ? 1 : 0;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nu += __shfl_xor_sync(0xffffffffu, nu, o);
+  warp_bitonic<E>(wv, tv, lane);
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int pos = e * 32 + lane;
+    if (pos < T) put_sorted(b, pos, tv[e], wv[e], col, sW, scol, inv);
+  }
+  if (lane == 0) ucnt[i] = nu;
+}
+
+// Computes each row's matching weights and sorts the row into preference
+// order: sW, scol, the inverse permutation inv (original offset -> sorted
+// position) and the number of usable entries per row (ucnt).  One warp per
+// row, in registers; rows longer than kSortRegMax are queued for
+// k_sort_prefs_long.
 __global__ void __launch_bounds__(kSortWarps * 32)
     k_sort_prefs(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
-                 const double *__restrict__ W, double *sW, int32_t *scol, int32_t *long_rows,
+                 const double *__restrict__ val, const double *__restrict__ w,
+                 const double *__restrict__ C,
+                 const unsigned long long *__restrict__ min_bits, double *W_out, double *sW,
+                 int32_t *scol, int32_t *inv, int32_t *ucnt, int32_t *long_rows,
                  int32_t *n_long) {
-  __shared__ double shw[kSortWarps][kSortCap];
-  __shared__ int32_t shy[kSortWarps][kSortCap];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int32_t i = blockIdx.x * kSortWarps + wid;
   if (i >= n) return;
   const int32_t b = row[i], T = row[i + 1] - b;
-  auto usable = [&](int32_t j, double wv) { return col[j] != i && wv > 0.0; };
-  if (T <= 32) {
-    // Register bitonic sort across the warp.
-    double wv = -1.0;
-    int32_t yv = -1;
-    if (lane < T) {
-      const double x = W[b + lane];
-      yv = col[b + lane];
-      wv = usable(b + lane, x) ? x : -1.0;
-    }
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        const double pw = __shfl_xor_sync(0xffffffffu, wv, j);
-        const int32_t py = __shfl_xor_sync(0xffffffffu, yv, j);
-        const bool lower = (lane & j) == 0;
-        const bool asc = (lane & k) == 0;
-        const bool pb = pref_before(pw, py, wv, yv);  // partner ranks first
-        const bool take = (lower == asc) ? pb : !pb;
-        if (take) {
-          wv = pw;
-          yv = py;
-        }
-      }
-    }
-    if (lane < T) {
-      sW[b + lane] = wv;
-      scol[b + lane] = yv;
-    }
-    return;
-  }
-  if (T > kSortCap) {
+  if (T > kSortRegMax) {
     if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
     return;
   }
-  int P2 = 64;
-  while (P2 < T) P2 <<= 1;
-  double *ws = shw[wid];
-  int32_t *ys = shy[wid];
-  for (int t = lane; t < P2; t += 32) {
-    if (t < T) {
-      const double x = W[b + t];
-      ws[t] = usable(b + t, x) ? x : -1.0;
-      ys[t] = col[b + t];
-    } else {
-      ws[t] = -1.0;
-      ys[t] = -1;
-    }
-  }
-  __syncwarp();
-  for (int k = 2; k <= P2; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int t = lane; t < P2 / 2; t += 32) {
-        const int i0 = 2 * j * (t / j) + (t % j), i1 = i0 + j;
-        const bool asc = (i0 & k) == 0;
-        const bool swap = asc ? pref_before(ws[i1], ys[i1], ws[i0], ys[i0])
-                              : pref_before(ws[i0], ys[i0], ws[i1], ys[i1]);
-        if (swap) {
-          const double tw = ws[i0];
-          ws[i0] = ws[i1];
-          ws[i1] = tw;
-          const int32_t ty = ys[i0];
-          ys[i0] = ys[i1];
-          ys[i1] = ty;
-        }
-      }
-      __syncwarp();
-    }
-  for (int t = lane; t < T; t += 32) {
-    sW[b + t] = ws[t];
-    scol[b + t] = ys[t];
-  }
+  const double den = 0.999 * __longlong_as_double(static_cast<long long>(*min_bits));
+  const double ci = C[i], wi = w[i];
+  if (T <= 32)
+    sort_row_regs<1>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+  else if (T <= 64)
+    sort_row_regs<2>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+  else
+    sort_row_regs<4>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
 }
 
-// Same sort for the rows queued as longer than kSortCap: each block takes
-// queue entries blockIdx.x, blockIdx.x + gridDim.x, ...
+// Same for the queued long rows, one block per row in shared memory: each
+// block takes queue entries blockIdx.x, blockIdx.x + gridDim.x, ...
 __global__ void __launch_bounds__(256)
     k_sort_prefs_long(const int32_t *__restrict__ long_rows, const int32_t *__restrict__ n_long,
                       const int32_t *__restrict__ row, const int32_t *__restrict__ col,
-                      const double *__restrict__ W, double *sW, int32_t *scol, int *err) {
+                      const double *__restrict__ val, const double *__restrict__ w,
+                      const double *__restrict__ C,
+                      const unsigned long long *__restrict__ min_bits, double *W_out,
+                      double *sW, int32_t *scol, int32_t *inv, int32_t *ucnt, int *err) {
   extern __shared__ __align__(16) unsigned char sort_dyn[];
+  __shared__ int nu_sh;
   double *ws = reinterpret_cast<double *>(sort_dyn);
-  int32_t *ys = reinterpret_cast<int32_t *>(sort_dyn + sizeof(double) * kSortCapLong);
+  int32_t *ts = reinterpret_cast<int32_t *>(sort_dyn + sizeof(double) * kSortCapLong);
+  const double den = 0.999 * __longlong_as_double(static_cast<long long>(*min_bits));
   for (int32_t q = blockIdx.x; q < *n_long; q += gridDim.x) {
-  const int32_t i = long_rows[q];
-  const int32_t b = row[i], T = row[i + 1] - b;
-  if (T > kSortCapLong) {
-    if (threadIdx.x == 0) atomicExch(err, 2);
-    return;
-  }
-  int P2 = 64;
-  while (P2 < T) P2 <<= 1;
-  for (int t = threadIdx.x; t < P2; t += blockDim.x) {
-    if (t < T) {
-      const double x = W[b + t];
-      ws[t] = (col[b + t] != i && x > 0.0) ? x : -1.0;
-      ys[t] = col[b + t];
-    } else {
-      ws[t] = -1.0;
-      ys[t] = -1;
+    const int32_t i = long_rows[q];
+    const int32_t b = row[i], T = row[i + 1] - b;
+    if (T > kSortCapLong) {
+      if (threadIdx.x == 0) atomicExch(err, 2);
+      return;
     }
-  }
-  __syncthreads();
-  for (int k = 2; k <= P2; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int t = threadIdx.x; t < P2 / 2; t += blockDim.x) {
-        const int i0 = 2 * j * (t / j) + (t % j), i1 = i0 + j;
-        const bool asc = (i0 & k) == 0;
-        const bool swap = asc ? pref_before(ws[i1], ys[i1], ws[i0], ys[i0])
-                              : pref_before(ws[i0], ys[i0], ws[i1], ys[i1]);
-        if (swap) {
-          const double tw = ws[i0];
-          ws[i0] = ws[i1];
-          ws[i1] = tw;
-          const int32_t ty = ys[i0];
-          ys[i0] = ys[i1];
-          ys[i1] = ty;
-        }
+    if (threadIdx.x == 0) nu_sh = 0;
+    __syncthreads();
+    const double ci = C[i], wi = w[i];
+    int P2 = 64;
+    while (P2 < T) P2 <<= 1;
+    int nu = 0;
+    for (int t = threadIdx.x; t < P2; t += blockDim.x) {
+      if (t < T) {
+        ws[t] = match_weight(i, b + t, ci, wi, col, val, w, C, den, W_out);
+        ts[t] = t;
+        nu += ws[t] > 0.0 ? 1 : 0;
+      } else {
+        ws[t] = -1.0;
+        ts[t] = -1;
       }
-      __syncthreads();
     }
-  for (int t = threadIdx.x; t < T; t += blockDim.x) {
-    sW[b + t] = ws[t];
-    scol[b + t] = ys[t];
+    atomicAdd(&nu_sh, nu);
+    __syncthreads();
+    for (int k = 2; k <= P2; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int t = threadIdx.x; t < P2 / 2; t += blockDim.x) {
+          const int i0 = ((t & ~(j - 1)) << 1) | (t & (j - 1)), i1 = i0 + j;  // j = 2^m
+          const bool asc = (i0 & k) == 0;
+          const bool swap = asc ? pref_before(ws[i1], ts[i1], ws[i0], ts[i0])
+                                : pref_before(ws[i0], ts[i0], ws[i1], ts[i1]);
+          if (swap) {
+            const double tw = ws[i0];
+            ws[i0] = ws[i1];
+            ws[i1] = tw;
+            const int32_t tt = ts[i0];
+            ts[i0] = ts[i1];
+            ts[i1] = tt;
+          }
+        }
+        __syncthreads();
+      }
+    for (int t = threadIdx.x; t < T; t += blockDim.x)
+      put_sorted(b, t, ts[t], ws[t], col, sW, scol, inv);
+    if (threadIdx.x == 0) ucnt[i] = nu_sh;
+    __syncthreads();
   }
-  __syncthreads();
+}
+
+// Symmetric weights: receiver y ranks proposers x by (W_xy, x) descending,
+// which for W_xy = W_yx is y's own preference order, so an offer can be the
+// proposer's position in y's sorted row.  key[k] (for sorted entry k of row x
+// pointing to y) = the index of x's entry in y's sorted row (row[y] plus the
+// position; offers at one receiver compare like positions).  Any usable entry whose
+// transposed entry is missing or carries a different weight (bit for bit)
+// sets *nonsym, and the general matcher runs instead.
+template <int G>
+__global__ void k_sym_keys(int32_t n, const int32_t *__restrict__ row,
+                           const int32_t *__restrict__ col, const double *__restrict__ sW,
+                           const int32_t *__restrict__ inv, int32_t *key, int *nonsym) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int32_t y = static_cast<int32_t>(t / G);
+  const int lane = threadIdx.x % G;
+  if (y >= n) return;
+  const int32_t by = row[y], ey = row[y + 1];
+  for (int32_t a = by + lane; a < ey; a += G) {
+    const int32_t x = col[a];
+    const int32_t pa = inv[a];
+    const double wya = sW[by + pa];
+    if (x == y || !(wya > 0.0)) continue;
+    // the entry (x, y): binary search of y in row x (columns increasing)
+    int32_t lo = row[x], hi = row[x + 1] - 1;
+    const int32_t bx = lo;
+    while (lo < hi) {
+      const int32_t mid = (lo + hi) >> 1;
+      if (col[mid] < y) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo > hi || col[lo] != y) {
+      atomicExch(nonsym, 1);
+      continue;
+    }
+    const int32_t pb = inv[lo];
+    if (__double_as_longlong(sW[bx + pb]) != __double_as_longlong(wya)) {
+      atomicExch(nonsym, 1);
+      continue;
+    }
+    key[bx + pb] = by + pa;
+  }
+}
+
+// Suitor with symmetric weights: offer[y] = index of the current suitor's
+// entry in y's sorted row (kNoSuitor if none); a smaller index is a better
+// offer,
+// so one atomicMin both tests and installs an offer.  Same proposal chains
+// and resume points as k_suitor; exits at once when *nonsym is set.
+constexpr int32_t kNoSuitor = INT_MAX;  // above any entry index (nnz < 2^31)
+
+__global__ void __launch_bounds__(256)
+    k_suitor_sym(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ ucnt,
+                 const int32_t *__restrict__ scol, const int32_t *__restrict__ key,
+                 int32_t *next, int32_t *offer, int64_t limit, const int *__restrict__ nonsym,
+                 int *err) {
+  const int32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n || *nonsym) return;
+  volatile int32_t *vnext = next;
+  int32_t cur = gid;
+  int64_t steps = 0;
+  while (true) {
+    int32_t k = vnext[cur];
+    const int32_t e = row[cur] + ucnt[cur];
+    int32_t old = kNoSuitor, y = -1;
+    bool found = false;
+    while (k < e) {
+      if (++steps > limit) {
+        atomicExch(err, 1);
+        return;
+      }
+      y = scol[k];
+      const int32_t mine = key[k];
+      old = atomicMin(offer + y, mine);
+      if (old > mine) {
+        found = true;
+        break;
+      }
+      ++k;
+    }
+    vnext[cur] = found ? k + 1 : e;
+    if (!found || old == kNoSuitor) return;
+    cur = scol[old];  // the displaced proposer
   }
 }
 
 // One thread per initial proposer; `limit` bounds the steps of a thread
-// (advances, successful and failed CASes); on overrun *err is raised.
+// (advances, successful and failed CASes); on overrun *err is raised.  Used
+// when the weights are not symmetric (exits at once otherwise).
 __global__ void __launch_bounds__(256)
     k_suitor(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ scol,
              const double *__restrict__ sW, int32_t *next, unsigned long long *offer,
-             int64_t limit, int *err) {
+             int64_t limit, const int *__restrict__ nonsym, int *err) {
   const int32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= n) return;
+  if (gid >= n || !*nonsym) return;
   volatile unsigned long long *voffer = offer;
   volatile int32_t *vnext = next;
   int32_t cur = gid;
@@ -351,17 +484,31 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-__global__ void k_init_next(int32_t n, const int32_t *__restrict__ row, int32_t *next) {
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) next[i] = row[i];
-}
-
-__global__ void k_offer_to_suitor(int32_t n, const unsigned long long *__restrict__ offer,
-                                  int32_t *s) {
+// Resume points at each row's start; no offers yet.
+__global__ void k_init_match(int32_t n, const int32_t *__restrict__ row, int32_t *next,
+                             unsigned long long *offer, int32_t *offer_sym) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const unsigned long long o = offer[i];
-  s[i] = o == kNoOffer ? -1 : static_cast<int32_t>(o & 0xffffffffull);
+  next[i] = row[i];
+  offer[i] = kNoOffer;
+  offer_sym[i] = kNoSuitor;
+}
+
+// Suitor array from whichever matcher ran.
+__global__ void k_offer_to_suitor(int32_t n, const int32_t *__restrict__ row,
+                                  const int32_t *__restrict__ scol,
+                                  const unsigned long long *__restrict__ offer,
+                                  const int32_t *__restrict__ offer_sym,
+                                  const int *__restrict__ nonsym, int32_t *s) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (*nonsym) {
+    const unsigned long long o = offer[i];
+    s[i] = o == kNoOffer ? -1 : static_cast<int32_t>(o & 0xffffffffull);
+  } else {
+    const int32_t o = offer_sym[i];
+    s[i] = o == kNoSuitor ? -1 : scol[o];
+  }
 }
 
 // unsymFix pass 1 (_setSymPair, src/AMG/unsymMatching.cu:32-50).
@@ -554,7 +701,7 @@ __device__ int gal_gather(int32_t I, const int32_t *__restrict__ row,
   for (int k = 2; k <= P2; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int t = tid; t < P2 / 2; t += TEAM) {
-        const int i0 = 2 * j * (t / j) + (t % j);
+        const int i0 = ((t & ~(j - 1)) << 1) | (t & (j - 1));  // j = 2^m
         const int i1 = i0 + j;
         const bool asc = (i0 & k) == 0;
         const unsigned long long a = sm.key[i0], b = sm.key[i1];
@@ -575,8 +722,50 @@ __device__ __forceinline__ bool gal_head(const GalSmem &sm, int k) {
 
 // Sums the run starting at head position k; returns false if the run is
 // longer than kGalMaxRun.
+// Canonical-order compare-exchange of two run terms (a before b after it).
+__device__ __forceinline__ void gal_cx(int &ia, int32_t &mna, int32_t &mxa, int32_t &ta, int &ib,
+                                       int32_t &mnb, int32_t &mxb, int32_t &tb) {
+  const bool greater = mna > mnb || (mna == mnb && (mxa > mxb || (mxa == mxb && ta > tb)));
+  if (greater) {
+    int t0 = ia; ia = ib; ib = t0;
+    int32_t t1 = mna; mna = mnb; mnb = t1;
+    t1 = mxa; mxa = mxb; mxb = t1;
+    t1 = ta; ta = tb; tb = t1;
+  }
+}
+
 __device__ bool gal_run_sum(const GalSmem &sm, int k, int T, int32_t *J, double *sum) {
   const unsigned long long jj = sm.key[k] >> 32;
+  int len = 1;
+  while (len <= 4 && k + len < T && (sm.key[k + len] >> 32) == jj) ++len;
+  if (len <= 4) {
+    // Runs of at most four terms (pairwise aggregates: |I| |J| <= 4): a
+    // four-input sorting network on (min(i,j), max(i,j), i) in registers;
+    // absent terms carry INT_MAX keys and sort last.
+    int id[4];
+    int32_t mn[4], mx[4], ti[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool ok = q < len;
+      id[q] = ok ? static_cast<int>(sm.key[k + q] & 0xffffffffull) : 0;
+      const int32_t a = ok ? sm.ti[id[q]] : INT_MAX, b = ok ? sm.tj[id[q]] : INT_MAX;
+      ti[q] = a;
+      mn[q] = min(a, b);
+      mx[q] = max(a, b);
+    }
+    gal_cx(id[0], mn[0], mx[0], ti[0], id[1], mn[1], mx[1], ti[1]);
+    gal_cx(id[2], mn[2], mx[2], ti[2], id[3], mn[3], mx[3], ti[3]);
+    gal_cx(id[0], mn[0], mx[0], ti[0], id[2], mn[2], mx[2], ti[2]);
+    gal_cx(id[1], mn[1], mx[1], ti[1], id[3], mn[3], mx[3], ti[3]);
+    gal_cx(id[1], mn[1], mx[1], ti[1], id[2], mn[2], mx[2], ti[2]);
+    double s = sm.tv[id[0]];
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+      if (q < len) s = s + sm.tv[id[q]];
+    *J = static_cast<int32_t>(jj);
+    *sum = s;
+    return true;
+  }
   int idx[kGalMaxRun];
   int r = 0;
   for (int q = k; q < T && (sm.key[q] >> 32) == jj; ++q) {
@@ -736,13 +925,12 @@ __global__ void k_compose(int32_t n, int32_t *agg, double *p,
 }
 
 template <int G>
-bcmg_status launch_weights(const CsrView &A, const double *w, const double *C,
-                           unsigned long long *min_bits, double *W, cudaStream_t s) {
+bcmg_status launch_min(const CsrView &A, const double *w, const double *C,
+                       unsigned long long *min_bits, cudaStream_t s) {
   const int threads = 256;
   const int blocks = ceil_div(static_cast<int64_t>(A.n) * G, threads);
-  launch(k_ah_min<G>, std::min(blocks, 8 * kNumSM), threads, 0, s, A.n, A.row, A.col, A.val, w,
-         C, min_bits);
-  launch(k_make_W<G>, blocks, threads, 0, s, A.n, A.row, A.col, A.val, w, C, min_bits, W);
+  launch(k_ah_min<G>, std::min(blocks, 64 * kNumSM), threads, 0, s, A.n, A.row, A.col, A.val,
+         w, C, min_bits);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -769,16 +957,11 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   }
   const int T = 256;
   const int nb = ceil_div(n, T);
-  DevBuf<double> C, Wb;
+  DevBuf<double> C;
   DevBuf<unsigned long long> offer, minb;
   DevBuf<int32_t> sv, mv, m2, tgt, master, rank, tmp, total;
   DevBuf<int> err;
   BCMG_TRY(C.alloc(n, s));
-  double *W = W_out;
-  if (!W) {
-    BCMG_TRY(Wb.alloc(A.nnz, s));
-    W = Wb.get();
-  }
   BCMG_TRY(offer.alloc(n, s));
   BCMG_TRY(minb.alloc(1, s));
   BCMG_TRY(sv.alloc(n, s));
@@ -798,42 +981,62 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
                             cudaMemcpyHostToDevice, s));
   const int G = group_for(A.nnz, n);
   switch (G) {
-    case 4: BCMG_TRY(launch_weights<4>(A, w, C.get(), minb.get(), W, s)); break;
-    case 8: BCMG_TRY(launch_weights<8>(A, w, C.get(), minb.get(), W, s)); break;
-    case 16: BCMG_TRY(launch_weights<16>(A, w, C.get(), minb.get(), W, s)); break;
-    default: BCMG_TRY(launch_weights<32>(A, w, C.get(), minb.get(), W, s)); break;
+    case 4: BCMG_TRY(launch_min<4>(A, w, C.get(), minb.get(), s)); break;
+    case 8: BCMG_TRY(launch_min<8>(A, w, C.get(), minb.get(), s)); break;
+    case 16: BCMG_TRY(launch_min<16>(A, w, C.get(), minb.get(), s)); break;
+    default: BCMG_TRY(launch_min<32>(A, w, C.get(), minb.get(), s)); break;
   }
 
   phase_tick("weights");
   // Preference-sorted rows, then the suitor proposals.
   DevBuf<double> sW;
-  DevBuf<int32_t> scol, next, long_rows, n_long;
+  DevBuf<int32_t> scol, inv, ucnt, key, offer_sym, next, long_rows, n_long;
+  DevBuf<int> nonsym;
   BCMG_TRY(sW.alloc(A.nnz, s));
   BCMG_TRY(scol.alloc(A.nnz, s));
+  BCMG_TRY(inv.alloc(A.nnz, s));
+  BCMG_TRY(key.alloc(A.nnz, s));
+  BCMG_TRY(ucnt.alloc(n, s));
+  BCMG_TRY(offer_sym.alloc(n, s));
   BCMG_TRY(next.alloc(n, s));
   BCMG_TRY(long_rows.alloc(n, s));
   BCMG_TRY(n_long.alloc(1, s));
+  BCMG_TRY(nonsym.alloc(1, s));
   BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
-  launch(k_sort_prefs, ceil_div(n, kSortWarps), kSortWarps * 32, 0, s, n, A.row, A.col, W,
-         sW.get(), scol.get(), long_rows.get(), n_long.get());
+  BCMG_CUDA(cudaMemsetAsync(nonsym.get(), 0, sizeof(int), s));
+  launch(k_sort_prefs, ceil_div(n, kSortWarps), kSortWarps * 32, 0, s, n, A.row, A.col, A.val,
+         w, C.get(), minb.get(), W_out, sW.get(), scol.get(), inv.get(), ucnt.get(),
+         long_rows.get(), n_long.get());
   {
     const size_t smem = (sizeof(double) + sizeof(int32_t)) * kSortCapLong;
     BCMG_CUDA(cudaFuncSetAttribute(k_sort_prefs_long,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(smem)));
     launch(k_sort_prefs_long, std::min(n, kNumSM), 256, smem, s, long_rows.get(),
-           n_long.get(), A.row, A.col, W, sW.get(), scol.get(), err.get());
+           n_long.get(), A.row, A.col, A.val, w, C.get(), minb.get(), W_out, sW.get(),
+           scol.get(), inv.get(), ucnt.get(), err.get());
     BCMG_LAUNCH_CHECK();
   }
-  phase_tick("sort_prefs");
-  BCMG_CUDA(cudaMemsetAsync(offer.get(), 0xff, sizeof(unsigned long long) * n, s));
-  launch(k_init_next, nb, T, 0, s, n, A.row, next.get());
-  const int64_t limit = 8 * static_cast<int64_t>(A.nnz) + 1024;
-  launch(k_suitor, nb, T, 0, s, n, A.row, scol.get(), sW.get(), next.get(), offer.get(), limit,
-         err.get());
+  switch (G) {
+    case 4: launch(k_sym_keys<4>, ceil_div(static_cast<int64_t>(n) * 4, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
+    case 8: launch(k_sym_keys<8>, ceil_div(static_cast<int64_t>(n) * 8, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
+    case 16: launch(k_sym_keys<16>, ceil_div(static_cast<int64_t>(n) * 16, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
+    default: launch(k_sym_keys<32>, ceil_div(static_cast<int64_t>(n) * 32, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
+  }
   BCMG_LAUNCH_CHECK();
-  launch(k_offer_to_suitor, nb, T, 0, s, n, offer.get(), sv.get());
+  phase_tick("sort_prefs");
+  // Both matchers are launched; the one that does not apply (by *nonsym)
+  // returns at once, so no host round trip decides between them.
+  launch(k_init_match, nb, T, 0, s, n, A.row, next.get(), offer.get(), offer_sym.get());
+  const int64_t limit = 8 * static_cast<int64_t>(A.nnz) + 1024;
+  launch(k_suitor_sym, nb, T, 0, s, n, A.row, ucnt.get(), scol.get(), key.get(), next.get(),
+         offer_sym.get(), limit, nonsym.get(), err.get());
+  launch(k_suitor, nb, T, 0, s, n, A.row, scol.get(), sW.get(), next.get(), offer.get(), limit,
+         nonsym.get(), err.get());
+  BCMG_LAUNCH_CHECK();
+  launch(k_offer_to_suitor, nb, T, 0, s, n, A.row, scol.get(), offer.get(), offer_sym.get(),
+         nonsym.get(), sv.get());
   phase_tick("suitor");
 
   // unsymFix.
