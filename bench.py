@@ -271,8 +271,11 @@ def run_ours(args):
     A, b_h, p, desc = make_workload(bc, args.workload)
     prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
     stream = torch.cuda.Stream(device=dev)
-    ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0, device=local,
-                        stream=stream.cuda_stream)
+    # The anisotropic FV workload stores its coarse levels in BF16 (FP32
+    # accumulation); the others keep FP32 coarse values.
+    storage = bc.STORE_BF16 if args.workload == "fv2d_2048" else bc.STORE_FP32
+    ext = bc.Extensions(precision=prec, coarse_storage=storage, replace_every=10 if prec else 0,
+                        device=local, stream=stream.cuda_stream)
 
     with torch.cuda.stream(stream):
         row = torch.from_numpy(A.row).to(dev)
@@ -320,6 +323,52 @@ def run_ours(args):
     xs = x.cpu().numpy()
     res = b_h - A.to_scipy() @ xs
     true_rel = float(np.linalg.norm(res) / np.linalg.norm(b_h))
+
+    # ---- comparison legs (same process, same inputs, untimed by the driver) ----
+    def timed_ms(fn, reps):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = [fn() for _ in range(reps)]
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps, out
+
+    def cached_ms(ext_):
+        # solves on one hierarchy, setup excluded (the reference's solve_time)
+        hh = bc.Handle.from_device(A.n, A.nnz, row.data_ptr(), col.data_ptr(), val.data_ptr(),
+                                   p, ext_)
+
+        def one():
+            with torch.cuda.stream(stream):
+                x.zero_()
+            return hh.solve_device(b.data_ptr(), x.data_ptr())
+        one()
+        ms, out = timed_ms(one, max(3, args.steps))
+        hh.close()
+        return ms, out[-1].iters
+
+    ext64 = bc.Extensions(precision=bc.PREC_FP64, device=local, stream=stream.cuda_stream)
+    compare = {}
+    if prec == bc.PREC_MIXED:
+        ext_saved = ext
+        ext = ext64
+        step()
+        fp64_ms, fp64_infos = timed_ms(step, args.steps)
+        ext = ext_saved
+        compare["fp64_full_solve"] = {"solves_per_s": 1e3 / fp64_ms, "ms_per_solve": fp64_ms,
+                                      "iters": fp64_infos[-1].iters,
+                                      "setup_ms": fp64_infos[-1].setup_ms}
+        compare["mixed_over_fp64_full_solve"] = fp64_ms / (ms_max / args.steps)
+    mixed_c, mixed_it = cached_ms(ext)
+    compare["cached_hierarchy"] = {"ms_per_solve": mixed_c, "solves_per_s": 1e3 / mixed_c,
+                                   "iters": mixed_it}
+    if prec == bc.PREC_MIXED:
+        fp64_c, fp64_it = cached_ms(ext64)
+        compare["cached_hierarchy"].update({"fp64_ms_per_solve": fp64_c,
+                                            "fp64_solves_per_s": 1e3 / fp64_c,
+                                            "fp64_iters": fp64_it,
+                                            "mixed_over_fp64": fp64_c / mixed_c})
 
     # ---- e2e: reference-shaped C-ABI call with pinned host buffers -----------
     pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
@@ -435,7 +484,7 @@ def run_ours(args):
         "clocks": clocks,
         "detail": {"iters": info.iters, "setup_ms": info.setup_ms, "solve_ms": info.solve_ms,
                    "rel_residual": info.rel_residual, "true_rel_residual": true_rel,
-                   "e2e_steps": e2e_steps},
+                   "e2e_steps": e2e_steps, "compare": compare},
     }
     print(json.dumps(line), flush=True)
     log(f"[bench] {args.workload} {args.precision}: {value:.3f} solves/s "
@@ -824,7 +873,7 @@ def main():
     ap.add_argument("--requests", type=int, default=300, help="serve_stream: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serve_stream: arrivals per s")
     ap.add_argument("--slots", type=int, default=4, help="serve_stream: solves in flight")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
