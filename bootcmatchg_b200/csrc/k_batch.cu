@@ -84,12 +84,13 @@ __device__ __forceinline__ void bt_row_sum(const int32_t *__restrict__ col,
         vk[u] = __shfl_sync(kFull, vj, k0 + u, L);
       }
       Cols<XT, V> xv[kUnroll];
-      // Entry k0 + u of this chunk exists for this row when it lies inside
-      // both the chunk (kn entries) and the row.
+      // All kUnroll gathers are issued unconditionally, so they are in flight
+      // together: an absent entry carries column 0 (a valid row) and its
+      // product is dropped below.  Entry k0 + u exists for this row when it
+      // lies inside both the chunk (kn entries) and the row.
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u)
-        if (k0 + u < kn && base + k0 + u < len)
-          xv[u] = ldc<XT, V>(x + static_cast<int64_t>(ck[u]) * W + cofs);
+        xv[u] = ldc<XT, V>(x + static_cast<int64_t>(ck[u]) * W + cofs);
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u)
         if (k0 + u < kn && base + k0 + u < len) {
@@ -121,15 +122,20 @@ __global__ void __launch_bounds__(256)
     j0 = row[i];
     len = row[i + 1] - j0;
   }
+  // The row's own f, u and d do not depend on the row sum: load them first.
+  const int64_t o = static_cast<int64_t>(i) * W + static_cast<int64_t>(g) * V;
+  const Cols<XT, V> fv = ldc<XT, V>(f + o);
+  Cols<XT, V> uv;
+  XT di = XT(1);
+  if (MODE == kModeRelax) {
+    uv = ldc<XT, V>(u + o);
+    di = d[i];
+  }
   XT acc[V];
   bt_row_sum<V, VT, XT>(col, val, u, W, L, g, j0, len, acc);
   if (!valid) return;
-  const int64_t o = static_cast<int64_t>(i) * W + static_cast<int64_t>(g) * V;
-  const Cols<XT, V> fv = ldc<XT, V>(f + o);
   Cols<XT, V> res;
   if (MODE == kModeRelax) {
-    const XT di = d[i];
-    const Cols<XT, V> uv = ldc<XT, V>(u + o);
 #pragma unroll
     for (int v = 0; v < V; ++v) res.v[v] = ((-acc[v] + fv.v[v]) / di) + uv.v[v];
   } else {
