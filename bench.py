@@ -348,7 +348,10 @@ def run_ours(args):
         hh.close()
         return ms, out[-1].iters
 
-    ext64 = bc.Extensions(precision=bc.PREC_FP64, device=local, stream=stream.cuda_stream)
+    # The comparison denominator is the plain FP64 path: FP64 values, no
+    # exact narrowing of the stored values.
+    ext64 = bc.Extensions(precision=bc.PREC_FP64, device=local, stream=stream.cuda_stream,
+                          narrow_values=0)
     compare = {}
     if prec == bc.PREC_MIXED:
         ext_saved = ext
@@ -369,6 +372,9 @@ def run_ours(args):
                                             "fp64_solves_per_s": 1e3 / fp64_c,
                                             "fp64_iters": fp64_it,
                                             "mixed_over_fp64": fp64_c / mixed_c})
+        ext64n = bc.Extensions(precision=bc.PREC_FP64, device=local, stream=stream.cuda_stream)
+        fp64n_c, _ = cached_ms(ext64n)
+        compare["cached_hierarchy"]["fp64_narrowed_ms_per_solve"] = fp64n_c
 
     # ---- e2e: reference-shaped C-ABI call with pinned host buffers -----------
     pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
@@ -484,7 +490,8 @@ def run_ours(args):
         "clocks": clocks,
         "detail": {"iters": info.iters, "setup_ms": info.setup_ms, "solve_ms": info.solve_ms,
                    "rel_residual": info.rel_residual, "true_rel_residual": true_rel,
-                   "e2e_steps": e2e_steps, "compare": compare},
+                   "e2e_steps": e2e_steps, "compare": compare,
+                   "level0_cycle_value_bytes": vbytes.value},
     }
     print(json.dumps(line), flush=True)
     log(f"[bench] {args.workload} {args.precision}: {value:.3f} solves/s "

@@ -43,7 +43,8 @@ class Ext(C.Structure):
     _fields_ = [("precision", C.c_int), ("coarse_storage", C.c_int),
                 ("replace_every", C.c_int), ("use_graphs", C.c_int), ("device", C.c_int),
                 ("verbose", C.c_int), ("max_device_seconds", C.c_double),
-                ("stream", C.c_void_p), ("sliced", C.c_int), ("autotune", C.c_int)]
+                ("stream", C.c_void_p), ("sliced", C.c_int), ("autotune", C.c_int),
+                ("narrow_values", C.c_int)]
 
 
 class SolveInfo(C.Structure):

@@ -147,6 +147,7 @@ class Extensions:
     stream: int = 0  # cudaStream_t as an integer (0: the handle makes its own)
     sliced: int = 1  # solve on the sliced copies of the levels
     autotune: int = 1  # batched solves: time the row-kernel shapes per level
+    narrow_values: int = 1  # store solve-phase values narrower when exact
 
     def to_c(self) -> Ext:
         e = Ext()

@@ -252,7 +252,7 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
       // FP64 sliced copy now if an FP64 cycle will read this level (the FP64
       // solve, or the bootstrap's inner iterations).
       if (h->ext.sliced && (h->ext.precision == BCMG_PREC_FP64 || h->prm.max_hrc > 1))
-        BCMG_TRY(sliced_build(coarse.view(), kValF64, &coarse.own64, s));
+        BCMG_TRY(sliced_build(coarse.view(), kValF64, &coarse.own64, s, h->ext.narrow_values != 0));
       const double size_coarse = coarse.n;
       const double coarse_ratio = fine.n / size_coarse;
       avcoarseratio += coarse_ratio;
@@ -551,8 +551,8 @@ bcmg_status prepare_mixed(bcmg_handle *h) {
 bcmg_status prepare_solve_formats(bcmg_handle *h) {
   cudaStream_t s = h->stream;
   DevLevel &a = h->A0;
-  if (!a.own64.nslices) BCMG_TRY(sliced_build(a.view(), kValF64, &a.own64, s));
-  if (h->mixed && !a.ownlo.nslices) BCMG_TRY(sliced_build(a.view(), kValF32, &a.ownlo, s));
+  if (!a.own64.nslices) BCMG_TRY(sliced_build(a.view(), kValF64, &a.own64, s, h->ext.narrow_values != 0));
+  if (h->mixed && !a.ownlo.nslices) BCMG_TRY(sliced_build(a.view(), kValF32, &a.ownlo, s, h->ext.narrow_values != 0));
   for (auto &H : h->H) {
     for (size_t l = 0; l < H.lv.size(); ++l) {
       DevLevel &lv = H.lv[l];
@@ -562,9 +562,9 @@ bcmg_status prepare_solve_formats(bcmg_handle *h) {
         continue;
       }
       if (h->mixed) {
-        if (!lv.ownlo.nslices) BCMG_TRY(sliced_build(lv.view(), lv.vtype_lo, &lv.ownlo, s));
+        if (!lv.ownlo.nslices) BCMG_TRY(sliced_build(lv.view(), lv.vtype_lo, &lv.ownlo, s, h->ext.narrow_values != 0));
       } else {
-        if (!lv.own64.nslices) BCMG_TRY(sliced_build(lv.view(), kValF64, &lv.own64, s));
+        if (!lv.own64.nslices) BCMG_TRY(sliced_build(lv.view(), kValF64, &lv.own64, s, h->ext.narrow_values != 0));
       }
     }
   }
@@ -647,7 +647,7 @@ bcmg_status setup_common(bcmg_handle *h) {
     for (int i = 0; i < ml - 1; ++i) h->grid_sweeps[i] = 2;
   }
   BCMG_TRY(alloc_work(h));
-  if (h->ext.sliced) BCMG_TRY(sliced_build(h->A0.view(), kValF64, &h->A0.own64, h->stream));
+  if (h->ext.sliced) BCMG_TRY(sliced_build(h->A0.view(), kValF64, &h->A0.own64, h->stream, h->ext.narrow_values != 0));
   g_clock.tick("alloc");
   BCMG_TRY(bootstrap(h));
   g_clock.tick("other");

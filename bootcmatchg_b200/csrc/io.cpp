@@ -465,6 +465,7 @@ void bcmg_ext_default(bcmg_ext *e) {
   e->stream = nullptr;
   e->sliced = 1;
   e->autotune = 1;
+  e->narrow_values = 1;
 }
 
 }  // extern "C"

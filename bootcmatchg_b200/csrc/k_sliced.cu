@@ -130,6 +130,21 @@ __global__ void k_slice_stats(int32_t nslices, const int32_t *__restrict__ sptr,
     }
 }
 
+// Which narrower types hold every value exactly (bitwise round trip):
+// bit 0 FP32, bit 1 BF16, bit 2 FP16; stats[2] starts at 7 and is and-ed.
+__global__ void k_value_exact(int64_t nnz, const double *__restrict__ val, int32_t *stats) {
+  int ok = 7;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < nnz;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v = val[e];
+    if (static_cast<double>(static_cast<float>(v)) != v) ok &= ~1;
+    if (static_cast<double>(__bfloat162float(__double2bfloat16(v))) != v) ok &= ~2;
+    if (static_cast<double>(__half2float(__double2half(v))) != v) ok &= ~4;
+  }
+  ok = __reduce_and_sync(0xffffffffu, ok);
+  if ((threadIdx.x & 31) == 0 && ok != 7) atomicAnd(stats + 2, ok);
+}
+
 // Pass 2: fill values (and columns or offsets).
 template <typename VT>
 __global__ void k_slice_fill(int32_t n, int32_t nslices, const int32_t *__restrict__ row,
@@ -399,8 +414,15 @@ struct __align__(16) StageCtl {
   int32_t slot0, staged, rows_staged, pad;
 };
 
+// Resident CTAs per SM the register budget is sized for: FP64 vectors keep
+// two CTAs (16 consumer warps), FP32 vectors four (more would spill).
+template <typename XT>
+constexpr int pipe_min_blocks() {
+  return sizeof(XT) == 8 ? 2 : 4;
+}
+
 template <typename VT, typename XT, typename Epi, int KB>
-__global__ void __launch_bounds__(kPipeThreads)
+__global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
     k_sl_pipe(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ x, Epi epi,
               int cap_slots, int cols_staged) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -620,31 +642,39 @@ bcmg_status residual_as(const SlicedView &S, const XT *f, const XT *u, XT *res,
 
 // Fills the occupancy cache for the kernels this matrix will run, so no
 // attribute or occupancy call happens inside a captured solve.
-bcmg_status warm_kernels(const SlicedView &S) {
-  switch (S.vtype) {
-    case kValF64: {
-      BCMG_TRY((relax_as<double, double>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
-      BCMG_TRY((residual_as<double, double>(S, nullptr, nullptr, nullptr, 0, true)));
-      EpiSpmv e1{nullptr};
-      BCMG_TRY((pipe_launch<double, double>(S, static_cast<const double *>(nullptr), e1, 0, true)));
-      EpiFcgDots e2{};
-      BCMG_TRY((pipe_launch<double, double>(S, static_cast<const double *>(nullptr), e2, 0, true)));
-      break;
-    }
-    case kValF32:
-      BCMG_TRY((relax_as<float, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
-      BCMG_TRY((residual_as<float, float>(S, nullptr, nullptr, nullptr, 0, true)));
-      break;
-    case kValBF16:
-      BCMG_TRY((relax_as<__nv_bfloat16, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
-      BCMG_TRY((residual_as<__nv_bfloat16, float>(S, nullptr, nullptr, nullptr, 0, true)));
-      break;
-    default:
-      BCMG_TRY((relax_as<__half, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
-      BCMG_TRY((residual_as<__half, float>(S, nullptr, nullptr, nullptr, 0, true)));
-      break;
-  }
+template <typename VT>
+bcmg_status warm_f64_vectors(const SlicedView &S) {
+  BCMG_TRY((relax_as<VT, double>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
+  BCMG_TRY((residual_as<VT, double>(S, nullptr, nullptr, nullptr, 0, true)));
+  EpiSpmv e1{nullptr};
+  BCMG_TRY((pipe_launch<VT, double>(S, static_cast<const double *>(nullptr), e1, 0, true)));
+  EpiFcgDots e2{};
+  BCMG_TRY((pipe_launch<VT, double>(S, static_cast<const double *>(nullptr), e2, 0, true)));
   return BCMG_OK;
+}
+
+template <typename VT>
+bcmg_status warm_f32_vectors(const SlicedView &S) {
+  BCMG_TRY((relax_as<VT, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
+  BCMG_TRY((residual_as<VT, float>(S, nullptr, nullptr, nullptr, 0, true)));
+  return BCMG_OK;
+}
+
+bcmg_status warm_kernels(const SlicedView &S) {
+  if (S.xtype == kValF64) {
+    switch (S.vtype) {
+      case kValF64: return warm_f64_vectors<double>(S);
+      case kValF32: return warm_f64_vectors<float>(S);
+      case kValBF16: return warm_f64_vectors<__nv_bfloat16>(S);
+      default: return warm_f64_vectors<__half>(S);
+    }
+  }
+  switch (S.vtype) {
+    case kValF32: return warm_f32_vectors<float>(S);
+    case kValBF16: return warm_f32_vectors<__nv_bfloat16>(S);
+    case kValF16: return warm_f32_vectors<__half>(S);
+    default: return set_error(BCMG_ERR_INTERNAL, "FP32-vector copy with FP64 values");
+  }
 }
 
 }  // namespace
@@ -681,40 +711,62 @@ SlicedView SlicedMat::view() const {
   v.cap_slots = cap_slots;
   v.cols_staged = has_columns ? 1 : 0;
   v.batch = batch;
+  v.xtype = xtype;
   return v;
 }
 
-bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s) {
+bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s,
+                         bool narrow) {
   out->release(s);
   const int32_t n = A.n;
   if (n <= 0) return BCMG_OK;
   const int32_t ns = ceil_div(n, 32);
   out->n = n;
   out->nslices = ns;
+  out->xtype = vtype == kValF64 ? kValF64 : kValF32;
   out->vtype = vtype;
   DevBuf<int32_t> width, kind, stats, tmp;
   BCMG_TRY(dev_alloc(&out->sptr, ns + 1, s));
   BCMG_TRY(dev_alloc(&out->meta, ns, s));
   BCMG_TRY(width.alloc(ns, s));
   BCMG_TRY(kind.alloc(ns, s));
-  BCMG_TRY(stats.alloc(3, s));
+  BCMG_TRY(stats.alloc(3, s));  // chunk max, any column slice, exact types
   BCMG_TRY(tmp.alloc(scan_tmp_size(ns), s));
   const int blocks = ceil_div(ns, kWarpsPerBlock);
   launch(k_slice_shape, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row, A.col, width.get(),
          kind.get());
   BCMG_TRY(exclusive_scan(width.get(), out->sptr, ns, out->sptr + ns, tmp.get(), s));
-  BCMG_CUDA(cudaMemsetAsync(stats.get(), 0, 3 * sizeof(int32_t), s));
+  BCMG_CUDA(cudaMemsetAsync(stats.get(), 0, 2 * sizeof(int32_t), s));
+  const bool try_narrow = narrow && (vtype == kValF64 || vtype == kValF32) && A.nnz > 0;
+  {
+    const int32_t all = 7;
+    BCMG_CUDA(cudaMemcpyAsync(stats.get() + 2, &all, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  }
+  if (try_narrow)
+    launch(k_value_exact, std::min<int64_t>(ceil_div(A.nnz, 256), 8 * kNumSM), 256, 0, s,
+           static_cast<int64_t>(A.nnz), A.val, stats.get());
   const int32_t nchunks = ceil_div(ns, kPipeWarps);
   launch(k_slice_stats, ceil_div(nchunks, 256), 256, 0, s, ns, out->sptr, kind.get(),
          stats.get());
   BCMG_LAUNCH_CHECK();
-  int32_t h_stats[3] = {0, 0, 0};
-  BCMG_CUDA(cudaMemcpyAsync(h_stats, stats.get(), 2 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+  int32_t h_stats[4] = {0, 0, 0, 0};
+  BCMG_CUDA(cudaMemcpyAsync(h_stats, stats.get(), 3 * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             s));
-  BCMG_CUDA(cudaMemcpyAsync(h_stats + 2, out->sptr + ns, sizeof(int32_t),
+  BCMG_CUDA(cudaMemcpyAsync(h_stats + 3, out->sptr + ns, sizeof(int32_t),
                             cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
-  const int32_t slots = h_stats[2];
+  const int32_t slots = h_stats[3];
+  // Exact narrowing: the narrowest storage that holds every value bit for bit
+  // (BF16, then FP16, then FP32); the kernels widen and accumulate in the
+  // vector type, so the arithmetic is unchanged.
+  if (try_narrow) {
+    const int exact = h_stats[2];
+    if (exact & 2) vtype = kValBF16;
+    else if (exact & 4) vtype = kValF16;
+    else if ((exact & 1) && vtype == kValF64) vtype = kValF32;
+  }
+  out->vtype = vtype;
+  out->narrowed = out->vtype != (out->xtype == kValF64 ? kValF64 : kValF32);
   out->slots = slots;
   out->has_columns = h_stats[1] != 0;
   out->batch = static_cast<int32_t>((static_cast<int64_t>(slots) + ns - 1) / ns);
@@ -783,11 +835,16 @@ template <typename XT>
 bcmg_status sliced_relax_sweep(const SlicedView &S, const XT *d, const XT *f, const XT *u,
                                XT *u_out, cudaStream_t s) {
   if (std::is_same<XT, double>::value) {
-    if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
-    return relax_as<double, double>(S, reinterpret_cast<const double *>(d),
-                                    reinterpret_cast<const double *>(f),
-                                    reinterpret_cast<const double *>(u),
-                                    reinterpret_cast<double *>(u_out), s);
+    const double *dd = reinterpret_cast<const double *>(d);
+    const double *fd = reinterpret_cast<const double *>(f);
+    const double *ud = reinterpret_cast<const double *>(u);
+    double *od = reinterpret_cast<double *>(u_out);
+    switch (S.vtype) {
+      case kValF64: return relax_as<double, double>(S, dd, fd, ud, od, s);
+      case kValF32: return relax_as<float, double>(S, dd, fd, ud, od, s);
+      case kValBF16: return relax_as<__nv_bfloat16, double>(S, dd, fd, ud, od, s);
+      default: return relax_as<__half, double>(S, dd, fd, ud, od, s);
+    }
   }
   const float *df = reinterpret_cast<const float *>(d);
   const float *ff = reinterpret_cast<const float *>(f);
@@ -803,10 +860,15 @@ template <typename XT>
 bcmg_status sliced_residual(const SlicedView &S, const XT *f, const XT *u, XT *res,
                             cudaStream_t s) {
   if (std::is_same<XT, double>::value) {
-    if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
-    return residual_as<double, double>(S, reinterpret_cast<const double *>(f),
-                                       reinterpret_cast<const double *>(u),
-                                       reinterpret_cast<double *>(res), s);
+    const double *fd = reinterpret_cast<const double *>(f);
+    const double *ud = reinterpret_cast<const double *>(u);
+    double *rd = reinterpret_cast<double *>(res);
+    switch (S.vtype) {
+      case kValF64: return residual_as<double, double>(S, fd, ud, rd, s);
+      case kValF32: return residual_as<float, double>(S, fd, ud, rd, s);
+      case kValBF16: return residual_as<__nv_bfloat16, double>(S, fd, ud, rd, s);
+      default: return residual_as<__half, double>(S, fd, ud, rd, s);
+    }
   }
   const float *ff = reinterpret_cast<const float *>(f);
   const float *uf = reinterpret_cast<const float *>(u);
@@ -820,15 +882,25 @@ bcmg_status sliced_residual(const SlicedView &S, const XT *f, const XT *u, XT *r
 bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w,
                                  const double *r, const double *q, double *partials,
                                  cudaStream_t s) {
-  if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "FCG SpMV needs FP64 values");
+  if (S.xtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "FCG SpMV needs an FP64 copy");
   EpiFcgDots e{v, r, q, w, partials, {0.0, 0.0, 0.0}};
-  return pipe_launch<double, double>(S, v, e, s);
+  switch (S.vtype) {
+    case kValF64: return pipe_launch<double, double>(S, v, e, s);
+    case kValF32: return pipe_launch<float, double>(S, v, e, s);
+    case kValBF16: return pipe_launch<__nv_bfloat16, double>(S, v, e, s);
+    default: return pipe_launch<__half, double>(S, v, e, s);
+  }
 }
 
 bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStream_t s) {
-  if (S.vtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced SpMV needs FP64 values");
+  if (S.xtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "sliced SpMV needs an FP64 copy");
   EpiSpmv e{y};
-  return pipe_launch<double, double>(S, x, e, s);
+  switch (S.vtype) {
+    case kValF64: return pipe_launch<double, double>(S, x, e, s);
+    case kValF32: return pipe_launch<float, double>(S, x, e, s);
+    case kValBF16: return pipe_launch<__nv_bfloat16, double>(S, x, e, s);
+    default: return pipe_launch<__half, double>(S, x, e, s);
+  }
 }
 
 bcmg_status sliced_wait_status(cudaStream_t s) {

@@ -59,6 +59,7 @@ struct SlicedView {
   int32_t cap_slots = 0;    // slots one pipeline stage holds
   int32_t cols_staged = 0;  // explicit columns exist (and are staged)
   int32_t batch = 0;        // mean slice width (chooses the slot batch size)
+  int xtype = kValF64;      // vector type the copy serves (kValF64 or kValF32)
 };
 
 struct SlicedMat {
@@ -68,14 +69,20 @@ struct SlicedMat {
   void *val = nullptr;
   int vtype = kValF64;
   int32_t cap_slots = 0, batch = 0;
+  int xtype = kValF64;       // vector type served: kValF64 or kValF32
+  bool narrowed = false;     // values stored narrower than xtype (all exact)
   bool has_columns = false;  // scol allocated (some slice is a column slice)
   void release(cudaStream_t s);
   size_t bytes() const;  // device bytes held
   SlicedView view() const;
 };
 
-// Builds the sliced copy of a CSR matrix with values converted to vtype.
-bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s);
+// Builds the sliced copy of a CSR matrix with values converted to vtype
+// (kValF64: a copy for FP64 vectors; otherwise for FP32 vectors).  narrow:
+// store the values in BF16 / FP16 / FP32 instead when every value converts
+// exactly (the kernels widen them, so results are bit-identical).
+bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s,
+                         bool narrow = false);
 template <typename XT>  // u_out = ((-(A u) + f) ./ d) + u
 bcmg_status sliced_relax_sweep(const SlicedView &S, const XT *d, const XT *f, const XT *u,
                                XT *u_out, cudaStream_t s);

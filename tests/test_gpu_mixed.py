@@ -111,3 +111,31 @@ def test_sliced_and_csr_solves_agree():
         x0, i0 = h0.solve(b)
     assert abs(i1.iters - i0.iters) <= 1
     assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) < 1e-7
+
+
+@pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
+def test_exact_value_narrowing_is_bit_identical(prec):
+    """Solve-phase copies store a level's values in BF16 when every value
+    converts exactly (the 27-point stencil's 26 and -1); the kernels widen
+    them, so the solution matches the unnarrowed run bit for bit."""
+    import ctypes as C
+    from bootcmatchg_b200._lib import check, lib
+    A = bc.poisson(27, 32, 32, 32)
+    p = c1_params()
+    b = bc.vector(1, 5, A.n)
+    out = []
+    for narrow in (1, 0):
+        ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0,
+                            narrow_values=narrow)
+        with bc.Handle(A, p, ext) as h:
+            x, info = h.solve(b)
+            slots, cslots = C.c_int64(), C.c_int64()
+            nsl, vb = C.c_int32(), C.c_int32()
+            check(lib.bcmg_level_format(h.ptr, 0, 0, C.byref(slots), C.byref(cslots),
+                                        C.byref(nsl), C.byref(vb)), "level_format")
+        assert info.converged
+        out.append((x, info.iters, vb.value))
+    assert out[0][2] == 2
+    assert out[1][2] == (4 if prec == bc.PREC_MIXED else 8)
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
