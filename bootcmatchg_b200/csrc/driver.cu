@@ -306,6 +306,19 @@ bcmg_status size_buffers_t(bcmg_handle *h, CycleBufs<XT> &B) {
     BCMG_TRY(dev_alloc(&B.res[l], nmax, s));
     B.n[l] = nmax;
   }
+  if (h->prm.cycle_type == 3) {
+    for (auto *v : {&B.kw, &B.kd0, &B.kd1, &B.kv, &B.kv1, &B.kx}) v->resize(L, nullptr);
+    B.kn.resize(L, 0);
+    for (size_t l = 1; l < L; ++l) {
+      if (B.kw[l] && B.n[l] <= B.kn[l]) continue;
+      for (auto *v : {&B.kw, &B.kd0, &B.kd1, &B.kv, &B.kv1, &B.kx}) {
+        dev_free((*v)[l], s);
+        BCMG_TRY(dev_alloc(&(*v)[l], B.n[l], s));
+      }
+      B.kn[l] = B.n[l];
+    }
+    if (!B.kdots) BCMG_TRY(dev_alloc(&B.kdots, 1, s));
+  }
   const int32_t n = h->A0.n;
   if (!B.xk) {
     BCMG_TRY(dev_alloc(&B.xk, n, s));
@@ -330,6 +343,9 @@ void free_buffers_t(CycleBufs<XT> &B, cudaStream_t s) {
   dev_free(B.xadd, s);
   dev_free(B.in0, s);
   dev_free(B.out0, s);
+  for (auto *v : {&B.kw, &B.kd0, &B.kd1, &B.kv, &B.kv1, &B.kx})
+    for (auto &p : *v) dev_free(p, s);
+  dev_free(B.kdots, s);
 }
 
 // The level data a cycle of vector type XT reads.
@@ -384,6 +400,9 @@ struct Lv<float> {
   static const float *p(const DevLevel &l) { return l.p32; }
 };
 
+template <typename XT>
+bcmg_status kcycle_inner_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int c);
+
 // GAMG_cycle (src/SOLVER/GAMG_cycle.cu:25-140); l is 1-based as there.
 // zero[l-1] says the current iterate of level l-1 is identically zero and
 // has not been materialised: the first sweep then reduces to f ./ d.
@@ -409,14 +428,92 @@ bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<
   BCMG_TRY(residual_t<XT>(A, B.rhs[l - 1], B.x[l - 1], B.res[l - 1], s));
   BCMG_TRY(restrict_t<XT>(lv.nc, lv.rptr, lv.ridx, Lv<XT>::p(lv), B.res[l - 1], B.rhs[l], s));
   zero[l] = 1;
-  for (int i = 1; i <= h->grid_sweeps[l - 1]; ++i) {
-    BCMG_TRY(cycle_t<XT>(h, B, k, l + 1, zero));
-    if (l == L - 1) break;
+  if (p.cycle_type == 3) {
+    // K-cycle (GAMG_cycle.cu:88-100): one cycle on the coarsest level, two
+    // inner flexible-CG steps on any other.
+    if (l == L - 1) {
+      BCMG_TRY(cycle_t<XT>(h, B, k, l + 1, zero));
+    } else {
+      BCMG_TRY(kcycle_inner_t<XT>(h, B, k, l));
+      zero[l] = 0;
+    }
+  } else {
+    for (int i = 1; i <= h->grid_sweeps[l - 1]; ++i) {
+      BCMG_TRY(cycle_t<XT>(h, B, k, l + 1, zero));
+      if (l == L - 1) break;
+    }
   }
   BCMG_TRY(prolong_t<XT>(lv.n, lv.agg, Lv<XT>::p(lv), B.x[l], B.x[l - 1], s));
   BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.postrelax_sweeps, false,
                        s));
   return BCMG_OK;
+}
+
+// Relative reduction at which the K-cycle stops after its first inner step
+// (RTOL, src/SOLVER/GAMG_cycle.cu:5).
+constexpr double kKcycleRtol = 0.25;
+
+// inneritkcycle (src/SOLVER/FCG.cu:633-723): two flexible-CG steps on coarse
+// level c (0-based) preconditioned by the cycle from that level on fresh
+// zero iterates (preconditionApplyK, FCG.cu:590-628); the correction lands
+// in x[c], the right-hand side is rhs[c].  The inner scalars are read on the
+// host (the reference's branch on ||w|| decides whether a second cycle runs),
+// so solves with this cycle are not captured in a graph.
+template <typename XT>
+bcmg_status kcycle_inner_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int c) {
+  const DevLevel &lv = h->H[k].lv[c];
+  const MatView A = Lv<XT>::mat(lv);
+  const int32_t n = lv.n;
+  cudaStream_t s = h->stream;
+  XT *w = B.kw[c], *d0 = B.kd0[c], *d1 = B.kd1[c], *v = B.kv[c], *v1 = B.kv1[c];
+  XT *xk = B.kx[c];
+  if (!w || !B.kdots) return set_error(BCMG_ERR_INTERNAL, "K-cycle buffers missing");
+  auto dot = [&](const XT *a, const XT *b, double *out) -> bcmg_status {
+    BCMG_TRY(dot_t<XT>(n, a, b, B.kdots, h->partials, s));
+    BCMG_CUDA(cudaMemcpyAsync(out, B.kdots, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BCMG_CUDA(cudaStreamSynchronize(s));
+    return BCMG_OK;
+  };
+  auto precond_k = [&](const XT *r, XT *d) -> bcmg_status {
+    BCMG_TRY(copy_t<XT>(B.rhs[c], r, n, s));
+    std::vector<char> zero(B.rhs.size(), 0);
+    zero[c] = 1;
+    BCMG_TRY(cycle_t<XT>(h, B, k, c + 1, zero));
+    return copy_t<XT>(d, B.x[c], n, s);
+  };
+  BCMG_TRY(copy_t<XT>(w, B.rhs[c], n, s));
+  double ww = 0, delta_old = 0, tau = 0;
+  BCMG_TRY(dot(w, w, &ww));
+  const double delta0 = std::sqrt(ww);
+  BCMG_TRY(precond_k(w, d0));
+  BCMG_TRY(dot(w, d0, &delta_old));
+  BCMG_TRY(spmv_t<XT>(A, d0, v, s));
+  BCMG_TRY(dot(d0, v, &tau));
+  if (!(delta_old > 0.0) || !(tau > 0.0))
+    return set_error(BCMG_ERR_INDEFINITE,
+                     "K-cycle inner step on level %d: non-positive curvature (%g, %g)", c,
+                     delta_old, tau);
+  double alpha = delta_old / tau;
+  BCMG_TRY(axpy_t<XT>(n, static_cast<XT>(-alpha), v, w, s));
+  BCMG_TRY(dot(w, w, &ww));
+  const double l2 = std::sqrt(ww);
+  BCMG_TRY(fill_t<XT>(xk, n, XT(0), s));
+  if (l2 <= kKcycleRtol * delta0) {
+    BCMG_TRY(axpy_t<XT>(n, static_cast<XT>(alpha), d0, xk, s));
+  } else {
+    BCMG_TRY(precond_k(w, d1));
+    BCMG_TRY(spmv_t<XT>(A, d1, v1, s));
+    double tau1 = 0, tau2 = 0, tau3 = 0;
+    BCMG_TRY(dot(d1, v, &tau1));
+    BCMG_TRY(dot(d1, v1, &tau2));
+    BCMG_TRY(dot(d1, w, &tau3));
+    const double tau4 = tau2 - (tau1 * tau1) / tau;
+    alpha = alpha - (tau1 * tau3) / (tau * tau4);
+    BCMG_TRY(axpy_t<XT>(n, static_cast<XT>(alpha), d0, xk, s));
+    alpha = tau3 / tau4;
+    BCMG_TRY(axpy_t<XT>(n, static_cast<XT>(alpha), d1, xk, s));
+  }
+  return copy_t<XT>(B.x[c], xk, n, s);
 }
 
 template <typename XT>
@@ -766,7 +863,8 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
   BCMG_TRY(fcg_scalars(h->partials, h->scal, true, s));
   BCMG_TRY(fcg_update(n, true, v, d, w, q, x, r, h->partials, h->scal, s));
   double *hs = h->host_scal;
-  const bool graphs = h->ext.use_graphs && h->ext.verbose < 2 && h->stream != nullptr;
+  const bool graphs = h->ext.use_graphs && h->ext.verbose < 2 && h->stream != nullptr &&
+                      h->prm.cycle_type != 3;  // the K-cycle reads its scalars on the host
   g_clock.tick("first_step");
   if (graphs && !h->fcg_exec && build_fcg_graph(h) != BCMG_OK) {
     clear_error();

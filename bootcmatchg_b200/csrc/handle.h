@@ -62,6 +62,12 @@ struct CycleBufs {
   std::vector<XT *> rhs, x, xt, res;
   std::vector<int32_t> n;
   XT *xk = nullptr, *xadd = nullptr, *in0 = nullptr, *out0 = nullptr;
+  // K-cycle (cycle_type 3) inner iterations, per coarse level: residual w,
+  // directions d0/d1, their products v/v1, the correction kx; kdots holds
+  // one device dot product.
+  std::vector<XT *> kw, kd0, kd1, kv, kv1, kx;
+  std::vector<int32_t> kn;  // allocated length of the K-cycle vectors
+  double *kdots = nullptr;
 };
 
 // Multi-right-hand-side solve state (batch.cu), created by the first batched

@@ -386,7 +386,9 @@ bcmg_status bcmg_params_check(const bcmg_params *p) {
     return set_error(BCMG_ERR_PARAM, "No parameter %d for solver_type", p->solver_type);
   if (p->aggrtype != 0 && p->aggrtype != 1)
     return set_error(BCMG_ERR_PARAM, "No parameter %d for aggrtype", p->aggrtype);
-  if (p->cycle_type < 0 || p->cycle_type > 2)
+  // 3 = K-cycle: the reference carries the code (GAMG_cycle.cu:88-100) but its
+  // checkP rejects the value (AMG.cu:508); it is accepted here.
+  if (p->cycle_type < 0 || p->cycle_type > 3)
     return set_error(BCMG_ERR_PARAM, "No parameter %d for cycle_type", p->cycle_type);
   if (p->coarse_solver != 0 && p->coarse_solver != 4)
     return set_error(BCMG_ERR_PARAM, "No parameter %d for coarse_solver", p->coarse_solver);

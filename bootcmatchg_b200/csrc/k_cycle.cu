@@ -9,6 +9,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "reduce.cuh"
 
 namespace bcmg {
 namespace {
@@ -135,6 +136,34 @@ __global__ void k_to_f16(int64_t n, const double *__restrict__ in, __half *out) 
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     out[i] = __double2half(in[i]);
+}
+
+template <int G, typename VT, typename XT>
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_t(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+             const VT *__restrict__ val, const XT *__restrict__ x, XT *__restrict__ y) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  int32_t i = static_cast<int32_t>(t / G);
+  const int lane = threadIdx.x % G;
+  if (i >= n) i = -1;
+  const XT T = row_dot<G, VT, XT>(row, col, val, x, i, lane);
+  if (i >= 0 && lane == 0) y[i] = T;
+}
+
+// a . b with FP64 accumulation, fixed grid and order (deterministic).
+template <typename XT>
+__global__ void __launch_bounds__(kRedThreads)
+    k_dot_t(int64_t n, const XT *__restrict__ a, const XT *__restrict__ b, double *partials) {
+  double v[1] = {0.0};
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    v[0] = fma(static_cast<double>(a[i]), static_cast<double>(b[i]), v[0]);
+  block_partials<1>(v, partials);
+}
+
+__global__ void k_dot_t_final(const double *partials, double *out) {
+  const double s = reduce_partials(partials, 0);
+  if (threadIdx.x == 0) *out = s;
 }
 
 inline int grid_for(int64_t work) {
@@ -349,6 +378,43 @@ bcmg_status convert_values(int64_t n, const double *in, void *out, int vtype, cu
   return BCMG_OK;
 }
 
+template <typename XT>
+bcmg_status spmv_t(const MatView &A, const XT *x, XT *y, cudaStream_t s) {
+  if (A.n <= 0) return BCMG_OK;
+  BCMG_TRY(check_types<XT>(A));
+  if (A.has_sl) return sliced_spmv_t<XT>(A.sl, x, y, s);
+  const int G = group_for(A.nnz, A.n);
+  const int blocks = grid_for(static_cast<int64_t>(A.n) * G);
+#define BCMG_SPMV_G(VT_)                                                                       \
+  switch (G) {                                                                                 \
+    case 4: launch(k_spmv_t<4, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break;  \
+    case 8: launch(k_spmv_t<8, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break;  \
+    case 16: launch(k_spmv_t<16, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break; \
+    default: launch(k_spmv_t<32, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break; \
+  }
+  if (std::is_same<XT, double>::value) {
+    BCMG_SPMV_G(double)
+  } else if (A.vtype == kValF32) {
+    BCMG_SPMV_G(float)
+  } else if (A.vtype == kValBF16) {
+    BCMG_SPMV_G(__nv_bfloat16)
+  } else {
+    BCMG_SPMV_G(__half)
+  }
+#undef BCMG_SPMV_G
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
+template <typename XT>
+bcmg_status dot_t(int64_t n, const XT *a, const XT *b, double *out, double *partials,
+                  cudaStream_t s) {
+  launch(k_dot_t<XT>, kRedBlocks, kRedThreads, 0, s, n, a, b, partials);
+  launch(k_dot_t_final, 1, kRedThreads, 0, s, partials, out);
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
 #define BCMG_INSTANTIATE(XT)                                                               \
   template bcmg_status relax_t<XT>(const MatView &, const XT *, const XT *, XT *, XT *, int, \
                                    bool, cudaStream_t);                                    \
@@ -361,7 +427,10 @@ bcmg_status convert_values(int64_t n, const double *in, void *out, int vtype, cu
   template bcmg_status fill_t<XT>(XT *, int64_t, XT, cudaStream_t);                        \
   template bcmg_status axpy_t<XT>(int64_t, XT, const XT *, XT *, cudaStream_t);            \
   template bcmg_status scale_t<XT>(int64_t, XT, XT *, cudaStream_t);                       \
-  template bcmg_status copy_t<XT>(XT *, const XT *, int64_t, cudaStream_t);
+  template bcmg_status copy_t<XT>(XT *, const XT *, int64_t, cudaStream_t);               \
+  template bcmg_status spmv_t<XT>(const MatView &, const XT *, XT *, cudaStream_t);         \
+  template bcmg_status dot_t<XT>(int64_t, const XT *, const XT *, double *, double *,       \
+                                 cudaStream_t);
 
 BCMG_INSTANTIATE(double)
 BCMG_INSTANTIATE(float)

@@ -352,13 +352,15 @@ struct EpiResidual {  // out = f - T
   __device__ void finish(int, int) {}
 };
 
-struct EpiSpmv {  // out = T
+template <typename XT>
+struct EpiSpmvT {  // out = T
   static constexpr int NV = 0;
-  double *out;
-  __device__ const double *row_vec(int) const { return nullptr; }
-  __device__ void apply(int32_t r, double T, const double *) { out[r] = T; }
+  XT *out;
+  __device__ const XT *row_vec(int) const { return nullptr; }
+  __device__ void apply(int32_t r, XT T, const XT *) { out[r] = T; }
   __device__ void finish(int, int) {}
 };
+using EpiSpmv = EpiSpmvT<double>;
 
 // FCG: w = T with alpha = r.v, beta = w.v, gamma = q.v (v is the gathered
 // vector); per-CTA partial sums in warp order, written to partials[4 b + k].
@@ -657,6 +659,8 @@ template <typename VT>
 bcmg_status warm_f32_vectors(const SlicedView &S) {
   BCMG_TRY((relax_as<VT, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
   BCMG_TRY((residual_as<VT, float>(S, nullptr, nullptr, nullptr, 0, true)));
+  EpiSpmvT<float> e{nullptr};
+  BCMG_TRY((pipe_launch<VT, float>(S, static_cast<const float *>(nullptr), e, 0, true)));
   return BCMG_OK;
 }
 
@@ -900,6 +904,24 @@ bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStr
     case kValF32: return pipe_launch<float, double>(S, x, e, s);
     case kValBF16: return pipe_launch<__nv_bfloat16, double>(S, x, e, s);
     default: return pipe_launch<__half, double>(S, x, e, s);
+  }
+}
+
+template <>
+bcmg_status sliced_spmv_t<double>(const SlicedView &S, const double *x, double *y,
+                                  cudaStream_t s) {
+  return sliced_spmv(S, x, y, s);
+}
+
+template <>
+bcmg_status sliced_spmv_t<float>(const SlicedView &S, const float *x, float *y,
+                                 cudaStream_t s) {
+  EpiSpmvT<float> e{y};
+  switch (S.vtype) {
+    case kValF32: return pipe_launch<float, float>(S, x, e, s);
+    case kValBF16: return pipe_launch<__nv_bfloat16, float>(S, x, e, s);
+    case kValF16: return pipe_launch<__half, float>(S, x, e, s);
+    default: return set_error(BCMG_ERR_INTERNAL, "FP32-vector SpMV on FP64 values");
   }
 }
 

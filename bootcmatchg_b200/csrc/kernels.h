@@ -91,6 +91,8 @@ bcmg_status sliced_residual(const SlicedView &S, const XT *f, const XT *u, XT *r
                             cudaStream_t s);
 // y = A x on a sliced FP64 copy.
 bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStream_t s);
+template <typename XT>  // y = A x on the copy serving XT vectors
+bcmg_status sliced_spmv_t(const SlicedView &S, const XT *x, XT *y, cudaStream_t s);
 // FCG SpMV w = A v fused with alpha = r.v, beta = w.v, gamma = q.v (FP64 values).
 bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w,
                                  const double *r, const double *q, double *partials,
@@ -130,6 +132,11 @@ template <typename XT>
 bcmg_status scale_t(int64_t n, XT a, XT *x, cudaStream_t s);
 template <typename XT>
 bcmg_status copy_t(XT *dst, const XT *src, int64_t n, cudaStream_t s);
+template <typename XT>  // y = A x
+bcmg_status spmv_t(const MatView &A, const XT *x, XT *y, cudaStream_t s);
+template <typename XT>  // *out (device) = a . b, accumulated in FP64 in a fixed order
+bcmg_status dot_t(int64_t n, const XT *a, const XT *b, double *out, double *partials,
+                  cudaStream_t s);
 bcmg_status convert_d2f(int64_t n, const double *in, float *out, cudaStream_t s);
 bcmg_status convert_f2d(int64_t n, const float *in, double *out, cudaStream_t s);
 // FP64 values to FP32 / BF16 / FP16 storage (vtype).

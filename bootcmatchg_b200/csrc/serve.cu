@@ -170,9 +170,11 @@ bool pick(bcmg_server *s, Job *job, std::vector<bcmg_handle *> &victims) {
     auto it = s->cache.find(r->key);
     if (it != s->cache.end() && it->second.busy) continue;  // hierarchy in use
     const bool fresh = it == s->cache.end();
-    // Same-key requests in arrival order join the group.
+    // Same-key requests in arrival order join the group (one at a time with
+    // the K-cycle, which batched solves do not run).
     Group g;
-    for (size_t j = i; j < s->queue.size() && static_cast<int>(g.size()) < s->opt.max_batch; ++j)
+    const int max_group = s->opt.params.cycle_type == 3 ? 1 : s->opt.max_batch;
+    for (size_t j = i; j < s->queue.size() && static_cast<int>(g.size()) < max_group; ++j)
       if (s->queue[j]->key == r->key) g.push_back(s->queue[j]);
     const size_t work = g.size() > 1 ? estimate_batch(r->b.size(), static_cast<int>(g.size())) : 0;
     const size_t need = (fresh ? estimate_setup(r->A, s->opt.ext) : 0) + work;

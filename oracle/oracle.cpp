@@ -59,6 +59,7 @@ struct orc_handle {
   IVec grid_sweeps;
   // cycle work buffers, per level of the deepest hierarchy
   std::vector<Vec> rhs, x, res;
+  int kcycle_status = 0;  // BCMG_ERR_INDEFINITE once a K-cycle inner step broke down
 };
 
 namespace {
@@ -496,6 +497,61 @@ IVec grid_sweeps(int cycle_type, int max_levels) {
   return g;
 }
 
+void cycle(orc_handle &h, int k, int l);
+
+// Relative reduction at which the K-cycle stops after its first inner step
+// (RTOL, src/SOLVER/GAMG_cycle.cu:5).
+constexpr double kKcycleRtol = 0.25;
+
+// inneritkcycle (src/SOLVER/FCG.cu:633-723): two flexible-CG steps on the
+// coarse level c (0-based) preconditioned by the cycle from that level
+// (preconditionApplyK, FCG.cu:590-628, on fresh zero iterates); the result
+// replaces x[c].  rhs[c] holds the right-hand side on entry.
+void kcycle_inner(orc_handle &h, int k, int c) {
+  const Csr &A = *h.H[k].lv[c].A;
+  const int32_t n = A.n;
+  Vec w(h.rhs[c].begin(), h.rhs[c].begin() + n);
+  Vec d0(n), d1(n), v(n), v1(n), xk(n, 0.0);
+  auto precond_k = [&](const Vec &r, Vec &d) {
+    std::copy(r.begin(), r.end(), h.rhs[c].begin());
+    std::fill(h.x[c].begin(), h.x[c].begin() + n, 0.0);
+    cycle(h, k, c + 1);
+    std::copy(h.x[c].begin(), h.x[c].begin() + n, d.begin());
+  };
+  auto axpy = [&](double a, const Vec &x, Vec &y) {
+    for (int32_t i = 0; i < n; ++i) y[i] = a * x[i] + y[i];
+  };
+  const double delta0 = std::sqrt(dot(w.data(), w.data(), n));
+  precond_k(w, d0);
+  const double delta_old = dot(w.data(), d0.data(), n);
+  spmv(A, d0.data(), v.data());
+  const double tau = dot(d0.data(), v.data(), n);
+  if (!(delta_old > 0.0) || !(tau > 0.0)) {
+    // The reference exits the process here (FCG.cu:662-665, 676-679).
+    h.kcycle_status = BCMG_ERR_INDEFINITE;
+    std::fill(h.x[c].begin(), h.x[c].begin() + n, 0.0);
+    return;
+  }
+  double alpha = delta_old / tau;
+  axpy(-alpha, v, w);
+  const double l2 = std::sqrt(dot(w.data(), w.data(), n));
+  if (l2 <= kKcycleRtol * delta0) {
+    axpy(alpha, d0, xk);
+  } else {
+    precond_k(w, d1);
+    spmv(A, d1.data(), v1.data());
+    const double tau1 = dot(d1.data(), v.data(), n);
+    const double tau2 = dot(d1.data(), v1.data(), n);
+    const double tau3 = dot(d1.data(), w.data(), n);
+    const double tau4 = tau2 - (tau1 * tau1) / tau;
+    alpha = alpha - (tau1 * tau3) / (tau * tau4);
+    axpy(alpha, d0, xk);
+    alpha = tau3 / tau4;
+    axpy(alpha, d1, xk);
+  }
+  std::copy(xk.begin(), xk.end(), h.x[c].begin());
+}
+
 // GAMG_cycle (src/SOLVER/GAMG_cycle.cu:25-140), l is 1-based as there.
 void cycle(orc_handle &h, int k, int l) {
   Hierarchy &H = h.H[k];
@@ -520,9 +576,16 @@ void cycle(orc_handle &h, int k, int l) {
   // Rhs_l = R Res (GAMG_cycle.cu:74-79)
   restrict_vec(lv.rptr, lv.ridx, lv.p, res.data(), h.rhs[l].data(), lv.nc);
   std::fill(h.x[l].begin(), h.x[l].begin() + lv.nc, 0.0);
-  for (int i = 1; i <= h.grid_sweeps[l - 1]; ++i) {
-    cycle(h, k, l + 1);
-    if (l == L - 1) break;
+  if (p.cycle_type == 3) {
+    // K-cycle (GAMG_cycle.cu:88-100): the coarsest level is one cycle,
+    // any other coarse level two inner flexible-CG steps.
+    if (l == L - 1) cycle(h, k, l + 1);
+    else kcycle_inner(h, k, l);
+  } else {
+    for (int i = 1; i <= h.grid_sweeps[l - 1]; ++i) {
+      cycle(h, k, l + 1);
+      if (l == L - 1) break;
+    }
   }
   // X += P X_c (_CSR_vector_mul_prolongator, src/matrix/CSR.cu:965-976)
   double *xf = h.x[l - 1].data();
@@ -651,7 +714,9 @@ int fcg(orc_handle &h, const double *b, double *x, int itnlim, bcmg_solve_info *
     info->rel_residual = 0.0;
     return BCMG_OK;
   }
+  h.kcycle_status = 0;
   precond_apply(h, r.data(), v.data());
+  if (h.kcycle_status) return h.kcycle_status;
   spmv(A, v.data(), w.data());
   double alpha = dot(r.data(), v.data(), n);
   double beta = dot(w.data(), v.data(), n);
@@ -675,6 +740,10 @@ int fcg(orc_handle &h, const double *b, double *x, int itnlim, bcmg_solve_info *
     Vec &azp = idx == 0 ? q : w;
     std::fill(z.begin(), z.end(), 0.0);
     precond_apply(h, r.data(), z.data());
+    if (h.kcycle_status) {
+      status = h.kcycle_status;
+      break;
+    }
     spmv(A, z.data(), az.data());
     alpha = dot(r.data(), z.data(), n);
     beta = dot(az.data(), z.data(), n);

@@ -131,7 +131,7 @@ def test_params_default_is_settings_base():
 
 
 @pytest.mark.parametrize("field,value,code", [
-    ("solver_type", 3, "PARAM"), ("cycle_type", 3, "PARAM"), ("relax_type", 1, "PARAM"),
+    ("solver_type", 3, "PARAM"), ("cycle_type", 4, "PARAM"), ("relax_type", 1, "PARAM"),
     ("coarse_solver", 9, "PARAM"), ("aggrtype", 2, "PARAM"), ("aggrtype", 1, "UNSUPPORTED"),
 ])
 def test_params_check(field, value, code):
@@ -332,6 +332,27 @@ def test_oracle_composites_and_cycles(solver_type, cycle_type):
     b = bc.vector(2, 2, A.n)
     x, info, st = h.solve(b)
     assert st == 0 and info["converged"] and info["iters"] < 200
+
+
+def test_oracle_kcycle_converges_in_fewer_iterations():
+    # K-cycle (cycle_type 3): two inner flexible-CG steps per coarse level
+    # (inneritkcycle, FCG.cu:633-723); its own checkP rejects the value, this
+    # build accepts it.  On 7-point Poisson it needs fewer outer iterations
+    # than the V-cycle and still solves to rtol.
+    A = bc.poisson(7, 24, 24, 24)
+    b = bc.vector(1, 3, A.n)
+    iters = {}
+    for ct in (0, 3):
+        p = c1_params()
+        p.cycle_type = ct
+        p.check()
+        h = orc.OracleHandle(A, p)
+        x, info, st = h.solve(b)
+        assert st == 0 and info["converged"]
+        r = b - A.to_scipy() @ x
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-8
+        iters[ct] = info["iters"]
+    assert iters[3] < iters[0]
 
 
 def test_bootstrap_second_hierarchy_uses_same_w():

@@ -286,3 +286,26 @@ def test_cli_matches_reference_format(tmp_path):
     x = np.array([float(s) for s in lines])
     xo, _, _ = orc.OracleHandle(A, bc.Params.init_from_file(str(settings))).solve(np.ones(A.n))
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
+
+
+@pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
+def test_kcycle_matches_oracle(prec):
+    """cycle_type 3 (K-cycle, GAMG_cycle.cu:88-100 + inneritkcycle,
+    FCG.cu:633-723) on the GPU against the oracle's: same hierarchy, the
+    solution within 1e-6 and the outer iteration count within one.  Batched
+    solves refuse the K-cycle."""
+    A = bc.poisson(27, 20, 20, 20)
+    p = c1_params()
+    p.cycle_type = 3
+    b = bc.vector(1, 11, A.n)
+    ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
+    with bc.Handle(A, p, ext) as h:
+        x, info = h.solve(b)
+        with pytest.raises(bc.BcmgError, match="UNSUPPORTED"):
+            h.solve_batch(np.asfortranarray(np.stack([b, b], axis=1)))
+    o = orc.OracleHandle(A, p)
+    xo, oi, st = o.solve(b)
+    assert st == 0 and oi["converged"] and info.converged
+    assert abs(info.iters - oi["iters"]) <= 1
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
+    assert info.true_rel_residual <= 1.05 * p.rtol
