@@ -100,6 +100,9 @@ SIGNATURES = {
                                    C.POINTER(SolveInfo)]),
     "bcmg_precond_apply_batch": (C.c_int, [vp, i32, vp, C.c_int64, vp, C.c_int64]),
     "bcmg_level_relax_batch": (C.c_int, [vp, C.c_int, C.c_int, i32, vp, vp, C.c_int]),
+    "bcmg_save": (C.c_int, [vp, C.c_char_p]),
+    "bcmg_get_params": (C.c_int, [vp, C.POINTER(Params)]),
+    "bcmg_load": (C.c_int, [C.c_char_p, C.POINTER(Ext), C.POINTER(vp)]),
     "bcmg_device_bytes": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
     "bcmg_server_opts_default": (None, [C.POINTER(ServerOpts)]),
     "bcmg_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(vp)]),

@@ -221,6 +221,26 @@ class Handle:
         self.params = params
         return self
 
+    @classmethod
+    def load(cls, path: str, ext: Extensions | None = None) -> "Handle":
+        """A handle from a hierarchy file written by save(); no setup runs."""
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        e = (ext or Extensions()).to_c()
+        check(lib.bcmg_load(str(path).encode(), C.byref(e), C.byref(self._h)), "bcmg_load")
+        n, nnz, nc = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib.bcmg_level_info(self._h, 0, 0, C.byref(n), C.byref(nnz), C.byref(nc)),
+              "level_info")
+        p = _CParams()
+        check(lib.bcmg_get_params(self._h, C.byref(p)), "bcmg_get_params")
+        self.n = n.value
+        self.params = Params._from_c(p)
+        return self
+
+    def save(self, path: str) -> None:
+        """Writes the hierarchies to a file bcmg_load / Handle.load reads."""
+        check(lib.bcmg_save(self._h, str(path).encode()), "bcmg_save")
+
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
             lib.bcmg_destroy(self._h)

@@ -8,6 +8,7 @@
 #include <cfloat>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <initializer_list>
 #include <memory>
@@ -726,15 +727,11 @@ void destroy_handle(bcmg_handle *h) {
   delete h;
 }
 
-bcmg_status setup_common(bcmg_handle *h) {
-  NvtxRange range("bcmg_setup");
-  const auto t0 = Clock::now();
-  BCMG_TRY(csr_validate(h->A0.view(), h->stream));
-  g_clock.start(h->ext.verbose >= 1, h->stream);
+// BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311) and
+// ApplyData::setGridSweeps (src/AMG/AMG.cu:371-394).
+void set_cycle_tables(bcmg_handle *h) {
   const int32_t n = h->A0.n;
-  // BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311).
   h->maxcoarsesize = static_cast<int32_t>(40 * std::pow(static_cast<double>(n), 1. / 3.));
-  // ApplyData::setGridSweeps (src/AMG/AMG.cu:371-394).
   const int ml = std::max(0, h->prm.max_levels - 1);
   h->grid_sweeps.assign(std::max(ml, 1), 1);
   if (h->prm.cycle_type == 1) {
@@ -743,18 +740,31 @@ bcmg_status setup_common(bcmg_handle *h) {
   } else if (h->prm.cycle_type == 2) {
     for (int i = 0; i < ml - 1; ++i) h->grid_sweeps[i] = 2;
   }
-  BCMG_TRY(alloc_work(h));
-  if (h->ext.sliced) BCMG_TRY(sliced_build(h->A0.view(), kValF64, &h->A0.own64, h->stream, h->ext.narrow_values != 0));
-  g_clock.tick("alloc");
-  BCMG_TRY(bootstrap(h));
-  g_clock.tick("other");
+}
+
+// After the hierarchies exist: low-precision and sliced solve copies.
+bcmg_status finish_setup(bcmg_handle *h) {
   h->mixed = h->ext.precision == BCMG_PREC_MIXED;
   if (h->mixed) BCMG_TRY(prepare_mixed(h));
   g_clock.tick("mixed_copies");
   if (h->ext.sliced) BCMG_TRY(prepare_solve_formats(h));
   g_clock.tick("sliced_copies");
   BCMG_CUDA(cudaStreamSynchronize(h->stream));
-  BCMG_TRY(sliced_wait_status(h->stream));
+  return sliced_wait_status(h->stream);
+}
+
+bcmg_status setup_common(bcmg_handle *h) {
+  NvtxRange range("bcmg_setup");
+  const auto t0 = Clock::now();
+  BCMG_TRY(csr_validate(h->A0.view(), h->stream));
+  g_clock.start(h->ext.verbose >= 1, h->stream);
+  set_cycle_tables(h);
+  BCMG_TRY(alloc_work(h));
+  if (h->ext.sliced) BCMG_TRY(sliced_build(h->A0.view(), kValF64, &h->A0.own64, h->stream, h->ext.narrow_values != 0));
+  g_clock.tick("alloc");
+  BCMG_TRY(bootstrap(h));
+  g_clock.tick("other");
+  BCMG_TRY(finish_setup(h));
   h->setup_ms = ms_since(t0);
   g_clock.report("setup");
   return BCMG_OK;
@@ -1005,6 +1015,169 @@ bcmg_status capture_while_loop(cudaStream_t stream,
   return BCMG_OK;
 }
 
+// ---- hierarchy files ---------------------------------------------------------
+// Binary, little-endian: the magic "BCMGHRC1", the 14 settings, the input
+// matrix, then per hierarchy its level data (CSR of levels >= 1, D, M, w, and
+// for every level but the last the aggregates and prolongator values; R's
+// member lists are rebuilt from the aggregates on load).  Each array is an
+// int64 count followed by its raw elements, in the manner of the reference's
+// Vector::dump / Vector::load (src/matrix/vector.cu:468-505).
+constexpr char kHrcMagic[8] = {'B', 'C', 'M', 'G', 'H', 'R', 'C', '1'};
+
+struct FileCloser {
+  void operator()(FILE *f) const {
+    if (f) fclose(f);
+  }
+};
+using File = std::unique_ptr<FILE, FileCloser>;
+
+template <typename T>
+bcmg_status put_array(FILE *f, const T *dev, int64_t count, cudaStream_t s) {
+  if (fwrite(&count, sizeof(count), 1, f) != 1) return set_error(BCMG_ERR_IO, "write failed");
+  if (count <= 0) return BCMG_OK;
+  std::vector<T> host(static_cast<size_t>(count));
+  BCMG_CUDA(cudaMemcpyAsync(host.data(), dev, sizeof(T) * count, cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  if (fwrite(host.data(), sizeof(T), host.size(), f) != host.size())
+    return set_error(BCMG_ERR_IO, "write failed");
+  return BCMG_OK;
+}
+
+template <typename T>
+bcmg_status get_array(FILE *f, T **dev, int64_t expect, cudaStream_t s) {
+  int64_t count = -1;
+  if (fread(&count, sizeof(count), 1, f) != 1 || count != expect)
+    return set_error(BCMG_ERR_IO, "hierarchy file: array of %lld entries where %lld expected",
+                     static_cast<long long>(count), static_cast<long long>(expect));
+  *dev = nullptr;
+  if (count <= 0) return BCMG_OK;
+  std::vector<T> host(static_cast<size_t>(count));
+  if (fread(host.data(), sizeof(T), host.size(), f) != host.size())
+    return set_error(BCMG_ERR_IO, "hierarchy file truncated");
+  BCMG_TRY(dev_alloc(dev, count, s));
+  BCMG_CUDA(cudaMemcpyAsync(*dev, host.data(), sizeof(T) * count, cudaMemcpyHostToDevice, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
+bcmg_status put_scalars(FILE *f, const void *p, size_t bytes) {
+  return fwrite(p, 1, bytes, f) == bytes ? BCMG_OK : set_error(BCMG_ERR_IO, "write failed");
+}
+bcmg_status get_scalars(FILE *f, void *p, size_t bytes) {
+  return fread(p, 1, bytes, f) == bytes ? BCMG_OK
+                                        : set_error(BCMG_ERR_IO, "hierarchy file truncated");
+}
+
+bcmg_status save_hierarchies(const bcmg_handle *h, FILE *f) {
+  cudaStream_t s = h->stream;
+  BCMG_TRY(put_scalars(f, kHrcMagic, sizeof(kHrcMagic)));
+  BCMG_TRY(put_scalars(f, &h->prm, sizeof(h->prm)));
+  const int32_t dims[3] = {h->A0.n, h->A0.nnz, static_cast<int32_t>(h->H.size())};
+  BCMG_TRY(put_scalars(f, dims, sizeof(dims)));
+  BCMG_TRY(put_scalars(f, &h->estimated_ratio, sizeof(double)));
+  BCMG_TRY(put_array(f, h->A0.row, h->A0.n + 1, s));
+  BCMG_TRY(put_array(f, h->A0.col, h->A0.nnz, s));
+  BCMG_TRY(put_array(f, h->A0.val, h->A0.nnz, s));
+  for (const DevHierarchy &H : h->H) {
+    const double stats[3] = {H.op_cmplx, H.op_wcmplx, H.avg_cratio};
+    BCMG_TRY(put_scalars(f, stats, sizeof(stats)));
+    const int32_t L = static_cast<int32_t>(H.lv.size());
+    BCMG_TRY(put_scalars(f, &L, sizeof(L)));
+    for (int32_t l = 0; l < L; ++l) {
+      const DevLevel &lv = H.lv[l];
+      const int32_t ld[3] = {lv.n, lv.nnz, lv.nc};
+      BCMG_TRY(put_scalars(f, ld, sizeof(ld)));
+      if (l > 0) {
+        BCMG_TRY(put_array(f, lv.row, lv.n + 1, s));
+        BCMG_TRY(put_array(f, lv.col, lv.nnz, s));
+        BCMG_TRY(put_array(f, lv.val, lv.nnz, s));
+      }
+      BCMG_TRY(put_array(f, lv.D, lv.n, s));
+      BCMG_TRY(put_array(f, lv.M, lv.n, s));
+      BCMG_TRY(put_array(f, lv.w, lv.n, s));
+      if (lv.nc > 0) {
+        BCMG_TRY(put_array(f, lv.agg, lv.n, s));
+        BCMG_TRY(put_array(f, lv.p, lv.n, s));
+      }
+    }
+  }
+  return BCMG_OK;
+}
+
+bcmg_status load_hierarchies(bcmg_handle *h, FILE *f) {
+  cudaStream_t s = h->stream;
+  int32_t dims[3];
+  BCMG_TRY(get_scalars(f, dims, sizeof(dims)));
+  BCMG_TRY(get_scalars(f, &h->estimated_ratio, sizeof(double)));
+  if (dims[0] <= 0 || dims[1] < dims[0] || dims[2] < 1)
+    return set_error(BCMG_ERR_IO, "hierarchy file: bad sizes");
+  DevLevel &a = h->A0;
+  a.n = dims[0];
+  a.nnz = dims[1];
+  BCMG_TRY(get_array(f, &a.row, a.n + 1, s));
+  BCMG_TRY(get_array(f, &a.col, a.nnz, s));
+  BCMG_TRY(get_array(f, &a.val, a.nnz, s));
+  BCMG_TRY(csr_validate(a.view(), s));
+  set_cycle_tables(h);
+  BCMG_TRY(alloc_work(h));
+  if (h->ext.sliced)
+    BCMG_TRY(sliced_build(a.view(), kValF64, &a.own64, s, h->ext.narrow_values != 0));
+  for (int32_t k = 0; k < dims[2]; ++k) {
+    h->H.emplace_back();
+    DevHierarchy &H = h->H.back();
+    double stats[3];
+    BCMG_TRY(get_scalars(f, stats, sizeof(stats)));
+    H.op_cmplx = stats[0];
+    H.op_wcmplx = stats[1];
+    H.avg_cratio = stats[2];
+    int32_t L = 0;
+    BCMG_TRY(get_scalars(f, &L, sizeof(L)));
+    if (L < 1 || L > 64) return set_error(BCMG_ERR_IO, "hierarchy file: %d levels", L);
+    for (int32_t l = 0; l < L; ++l) {
+      int32_t ld[3];
+      BCMG_TRY(get_scalars(f, ld, sizeof(ld)));
+      H.lv.emplace_back();
+      DevLevel &lv = H.lv.back();
+      lv.n = ld[0];
+      lv.nnz = ld[1];
+      lv.nc = ld[2];
+      if (l == 0) {
+        if (lv.n != a.n || lv.nnz != a.nnz)
+          return set_error(BCMG_ERR_IO, "hierarchy file: level 0 is not the input matrix");
+        lv.row = a.row;
+        lv.col = a.col;
+        lv.val = a.val;
+        lv.own_A = false;
+        if (a.own64.nslices) lv.s64 = &a.own64;
+      } else {
+        if (lv.n <= 0 || lv.nnz < lv.n || lv.n != H.lv[l - 1].nc)
+          return set_error(BCMG_ERR_IO, "hierarchy file: bad size of level %d", l);
+        BCMG_TRY(get_array(f, &lv.row, lv.n + 1, s));
+        BCMG_TRY(get_array(f, &lv.col, lv.nnz, s));
+        BCMG_TRY(get_array(f, &lv.val, lv.nnz, s));
+        BCMG_TRY(csr_validate(lv.view(), s));
+      }
+      BCMG_TRY(get_array(f, &lv.D, lv.n, s));
+      BCMG_TRY(get_array(f, &lv.M, lv.n, s));
+      BCMG_TRY(get_array(f, &lv.w, lv.n, s));
+      const bool last = l == L - 1;
+      if (last != (lv.nc == 0))
+        return set_error(BCMG_ERR_IO, "hierarchy file: level %d coarse size %d", l, lv.nc);
+      if (!last) {
+        if (lv.nc <= 0 || lv.nc > lv.n)
+          return set_error(BCMG_ERR_IO, "hierarchy file: bad coarse size on level %d", l);
+        BCMG_TRY(get_array(f, &lv.agg, lv.n, s));
+        BCMG_TRY(get_array(f, &lv.p, lv.n, s));
+        BCMG_TRY(dev_alloc(&lv.rptr, lv.nc + 1, s));
+        BCMG_TRY(dev_alloc(&lv.ridx, lv.n, s));
+        BCMG_TRY(transpose_agg(lv.n, lv.agg, lv.nc, lv.rptr, lv.ridx, s));
+      }
+    }
+    BCMG_TRY(size_buffers_t<double>(h, h->c64));
+  }
+  return finish_setup(h);
+}
+
 }  // namespace bcmg
 
 using namespace bcmg;
@@ -1123,6 +1296,46 @@ bcmg_status bcmg_device_bytes(const bcmg_handle *h, uint64_t *bytes) {
 
 bcmg_status bcmg_destroy(bcmg_handle *h) {
   destroy_handle(h);
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_get_params(const bcmg_handle *h, bcmg_params *p) {
+  if (!h || !p) return set_error(BCMG_ERR_PARAM, "null argument");
+  *p = h->prm;
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_save(const bcmg_handle *h, const char *path) {
+  clear_error();
+  if (!h || !path) return set_error(BCMG_ERR_PARAM, "null argument");
+  BCMG_CUDA(cudaSetDevice(h->device));
+  File f(fopen(path, "wb"));
+  if (!f) return set_error(BCMG_ERR_IO, "cannot open %s for writing", path);
+  BCMG_TRY(save_hierarchies(h, f.get()));
+  if (fflush(f.get()) != 0) return set_error(BCMG_ERR_IO, "write failed: %s", path);
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_load(const char *path, const bcmg_ext *ext, bcmg_handle **out) {
+  clear_error();
+  if (!path || !out) return set_error(BCMG_ERR_PARAM, "null argument");
+  *out = nullptr;
+  File f(fopen(path, "rb"));
+  if (!f) return set_error(BCMG_ERR_IO, "cannot open %s", path);
+  char magic[sizeof(kHrcMagic)];
+  bcmg_params prm;
+  if (fread(magic, 1, sizeof(magic), f.get()) != sizeof(magic) ||
+      std::memcmp(magic, kHrcMagic, sizeof(magic)) != 0)
+    return set_error(BCMG_ERR_IO, "%s is not a hierarchy file", path);
+  if (fread(&prm, sizeof(prm), 1, f.get()) != 1)
+    return set_error(BCMG_ERR_IO, "hierarchy file truncated");
+  const auto t0 = Clock::now();
+  bcmg_handle *h = nullptr;
+  BCMG_TRY(new_handle(&prm, ext, &h));
+  std::unique_ptr<bcmg_handle, void (*)(bcmg_handle *)> guard(h, destroy_handle);
+  BCMG_TRY(load_hierarchies(h, f.get()));
+  h->setup_ms = ms_since(t0);
+  *out = guard.release();
   return BCMG_OK;
 }
 

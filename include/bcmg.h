@@ -213,6 +213,20 @@ bcmg_status bcmg_batch_config(bcmg_handle *h, int32_t nrhs, int hrc, int level,
 bcmg_status bcmg_device_bytes(const bcmg_handle *h, uint64_t *bytes);
 bcmg_status bcmg_destroy(bcmg_handle *h);
 
+/* ---- hierarchy files -------------------------------------------------------
+ * Save a set-up handle's hierarchies (settings, input matrix, every level's
+ * CSR, D, M, w, aggregates and prolongator values) to a binary file, and
+ * build a handle from such a file without running setup again.  The
+ * reference only dumps single vectors (Vector::dump / Vector::load,
+ * src/matrix/vector.cu:468-505) and rebuilds every hierarchy per solve();
+ * this lets a cache of hierarchies outlive the process.  bcmg_load takes its
+ * own extensions (e.g. a hierarchy built in FP64 mode can be loaded for
+ * mixed-precision solves); NULL selects the defaults.  Little-endian files. */
+bcmg_status bcmg_save(const bcmg_handle *h, const char *path);
+bcmg_status bcmg_load(const char *path, const bcmg_ext *ext, bcmg_handle **out);
+/* The settings a handle was set up (or loaded) with. */
+bcmg_status bcmg_get_params(const bcmg_handle *h, bcmg_params *p);
+
 /* ---- solve server (no counterpart in the reference) ------------------------
  * Continuous batching of solve requests on one GPU: `slots` worker threads
  * with their own CUDA streams run requests from a FIFO queue.  A request

@@ -392,3 +392,13 @@ def test_library_exports_every_declared_symbol():
     for nm in sorted(names):
         assert hasattr(lib, nm), nm
         assert nm in SIGNATURES, nm
+
+
+def test_load_rejects_missing_and_foreign_files(tmp_path):
+    # File checks come before any device work.
+    with pytest.raises(bc.BcmgError, match="IO"):
+        bc.Handle.load(tmp_path / "missing.bin")
+    f = tmp_path / "foreign.bin"
+    f.write_bytes(b"NOTAHRCFILE" + bytes(64))
+    with pytest.raises(bc.BcmgError, match="IO"):
+        bc.Handle.load(f)

@@ -309,3 +309,34 @@ def test_kcycle_matches_oracle(prec):
     assert abs(info.iters - oi["iters"]) <= 1
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
     assert info.true_rel_residual <= 1.05 * p.rtol
+
+
+def test_hierarchy_file_roundtrip(tmp_path):
+    """bcmg_save / bcmg_load: the loaded handle has the same levels bit for bit
+    and solves to the same bits; a hierarchy saved from an FP64 setup also
+    loads for mixed-precision solves."""
+    A = bc.fv2d(64, 64, seed=2)
+    p = c1_params()
+    p.max_hrc, p.conv_ratio, p.solver_type = 2, 0.1, 0
+    b = bc.vector(2, 4, A.n)
+    path = tmp_path / "h.bcmg"
+    with bc.Handle(A, p) as h:
+        x0, i0 = h.solve(b)
+        nh0 = h.num_hierarchies()[0]
+        info0 = h.hierarchy_info(nh0 - 1)
+        lv0 = h.level(nh0 - 1, 1)
+        h.save(path)
+    with bc.Handle.load(path) as h2:
+        assert h2.num_hierarchies()[0] == nh0
+        assert h2.params.max_hrc == 2
+        lv = h2.level(nh0 - 1, 1)
+        assert h2.hierarchy_info(nh0 - 1)["num_levels"] == info0["num_levels"]
+        for a, b_ in ((lv.A.val, lv0.A.val), (lv.A.col, lv0.A.col), (lv.D, lv0.D),
+                      (lv.agg, lv0.agg), (lv.p, lv0.p)):
+            assert np.array_equal(a, b_)
+        x1, i1 = h2.solve(b)
+    assert i1.iters == i0.iters and np.array_equal(x1, x0)
+    ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=10)
+    with bc.Handle.load(path, ext) as h3:
+        x2, i2 = h3.solve(b)
+    assert i2.converged and np.linalg.norm(x2 - x0) / np.linalg.norm(x0) < 1e-6
