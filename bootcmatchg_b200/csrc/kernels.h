@@ -78,9 +78,10 @@ struct SlicedMat {
 };
 
 // Builds the sliced copy of a CSR matrix with values converted to vtype
-// (kValF64: a copy for FP64 vectors; otherwise for FP32 vectors).  narrow:
-// store the values in BF16 / FP16 / FP32 instead when every value converts
-// exactly (the kernels widen them, so results are bit-identical).
+// (kValF64: a copy for FP64 vectors; otherwise for FP32 vectors).  narrow
+// (FP64-vector copies): store the values in BF16 / FP16 / FP32 instead when
+// every value converts exactly (the kernels widen them, so results are
+// bit-identical).
 bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s,
                          bool narrow = false);
 template <typename XT>  // u_out = ((-(A u) + f) ./ d) + u

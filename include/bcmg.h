@@ -99,10 +99,11 @@ typedef struct bcmg_ext {
   int    autotune;        /* batched solves: time the row-kernel shapes of every
                              level once per batch width (default 1); 0 uses a
                              fixed rule.  Results are identical either way.   */
-  int    narrow_values;   /* store a level's solve-phase values in BF16, FP16
-                             or FP32 when every value converts exactly
-                             (default 1); the kernels widen them, so results
-                             are bit-identical with 0.                        */
+  int    narrow_values;   /* store the values of the solve-phase copies that
+                             serve FP64 vectors (FP64 cycle, FCG SpMV) in
+                             BF16, FP16 or FP32 when every value converts
+                             exactly (default 1); the kernels widen them, so
+                             results are bit-identical with 0.               */
 } bcmg_ext;
 
 /* Per-solve report.  residual is the recursive ||r||_2 that FCG returns
