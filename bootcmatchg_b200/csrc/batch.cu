@@ -476,8 +476,9 @@ bcmg_status bcmg_solve_batch(bcmg_handle *h, int32_t nrhs, const double *B, int6
                              double *X, int64_t ldx, int on_device, bcmg_solve_info *infos) {
   clear_error();
   if (!h || !B || !X || nrhs <= 0) return set_error(BCMG_ERR_PARAM, "bad arguments");
-  if (h->prm.cycle_type == 3)
-    return set_error(BCMG_ERR_UNSUPPORTED, "batched solves do not run the K-cycle");
+  if (h->prm.cycle_type == 3 || h->prm.aggrtype == 1)
+    return set_error(BCMG_ERR_UNSUPPORTED,
+                     "batched solves run neither the K-cycle nor smoothed aggregation");
   const int32_t n = h->A0.n;
   if (ldb < n || ldx < n)
     return set_error(BCMG_ERR_PARAM, "leading dimensions must be >= n (%d)", n);
@@ -540,8 +541,9 @@ bcmg_status bcmg_precond_apply_batch(bcmg_handle *h, int32_t nrhs, const double 
                                      int64_t ldr, double *d_Z, int64_t ldz) {
   clear_error();
   if (!h || !d_R || !d_Z || nrhs <= 0) return set_error(BCMG_ERR_PARAM, "bad arguments");
-  if (h->prm.cycle_type == 3)
-    return set_error(BCMG_ERR_UNSUPPORTED, "batched solves do not run the K-cycle");
+  if (h->prm.cycle_type == 3 || h->prm.aggrtype == 1)
+    return set_error(BCMG_ERR_UNSUPPORTED,
+                     "batched solves run neither the K-cycle nor smoothed aggregation");
   const int32_t n = h->A0.n;
   if (ldr < n || ldz < n)
     return set_error(BCMG_ERR_PARAM, "leading dimensions must be >= n (%d)", n);

@@ -47,6 +47,15 @@ void DevLevel::release(cudaStream_t s) {
   dev_free(D32, s);
   dev_free(M32, s);
   dev_free(p32, s);
+  dev_free(Prow, s);
+  dev_free(Pcol, s);
+  dev_free(Pval, s);
+  dev_free(Rrow, s);
+  dev_free(Rcol, s);
+  dev_free(Rval, s);
+  dev_free(Pval32, s);
+  dev_free(Rval32, s);
+  Pnnz = 0;
   own64.release(s);
   ownlo.release(s);
   s64 = slo = nullptr;
@@ -218,6 +227,72 @@ bcmg_status matching_aggregation(bcmg_handle *h, DevLevel &fine, double **w_out,
 }
 
 // adaptiveCoarsening (src/AMG/matchingAggregation.cu:298-423).
+// An FP64 cycle will read the coarse levels: the FP64 solve, or the
+// bootstrap's inner iterations.
+bool wants_coarse_f64(const bcmg_handle *h) {
+  return h->ext.sliced && (h->ext.precision == BCMG_PREC_FP64 || h->prm.max_hrc > 1);
+}
+
+// Smoothed aggregation (aggrtype 1), level by level so that D_j is the
+// diagonal of the already smoothed A_j: S_j = I - omega D_j^{-1} A_j with
+// omega = 4 / (3 ||D_j^{-1} A_j||_inf), P_j = S_j P_tent (P_tent: column
+// agg[i], value p[i] per row), R_j = P_j^T, A_{j+1} = (R_j A_j) P_j.  Every
+// product sums in the canonical order of spgemm.
+bcmg_status smooth_hierarchy(bcmg_handle *h, DevHierarchy &H) {
+  cudaStream_t s = h->stream;
+  const int L = static_cast<int>(H.lv.size());
+  for (int j = 0; j + 1 < L; ++j) {
+    DevLevel &lv = H.lv[j];
+    const CsrView A = lv.view();
+    DevBuf<double> sval;
+    DevBuf<int32_t> trow;
+    BCMG_TRY(sval.alloc(std::max(A.nnz, 1), s));
+    BCMG_TRY(trow.alloc(static_cast<int64_t>(A.n) + 1, s));
+    BCMG_TRY(smoothing_operator(A, lv.D, sval.get(), s));
+    BCMG_TRY(iota(A.n, trow.get(), s));
+    const CsrView S{A.n, A.nnz, A.row, A.col, sval.get()};
+    const CsrView Pt{A.n, A.n, trow.get(), lv.agg, lv.p};
+    BCMG_TRY(dev_alloc(&lv.Prow, static_cast<int64_t>(A.n) + 1, s));
+    BCMG_TRY(spgemm(S, Pt, lv.nc, lv.Prow, &lv.Pcol, &lv.Pval, &lv.Pnnz, s));
+    BCMG_TRY(dev_alloc(&lv.Rrow, static_cast<int64_t>(lv.nc) + 1, s));
+    BCMG_TRY(dev_alloc(&lv.Rcol, std::max(lv.Pnnz, 1), s));
+    BCMG_TRY(dev_alloc(&lv.Rval, std::max(lv.Pnnz, 1), s));
+    BCMG_TRY(csr_transpose(lv.pview(), lv.nc, lv.Rrow, lv.Rcol, lv.Rval, s));
+    DevBuf<int32_t> ra_row, ac_row;
+    BCMG_TRY(ra_row.alloc(static_cast<int64_t>(lv.nc) + 1, s));
+    int32_t *ra_col = nullptr, *ac_col = nullptr;
+    double *ra_val = nullptr, *ac_val = nullptr;
+    int32_t ra_nnz = 0, ac_nnz = 0;
+    BCMG_TRY(spgemm(lv.rview(), A, A.n, ra_row.get(), &ra_col, &ra_val, &ra_nnz, s));
+    DevBuf<int32_t> ra_colb;
+    DevBuf<double> ra_valb;
+    ra_colb.ptr = ra_col;
+    ra_colb.stream = s;
+    ra_valb.ptr = ra_val;
+    ra_valb.stream = s;
+    BCMG_TRY(ac_row.alloc(static_cast<int64_t>(lv.nc) + 1, s));
+    const CsrView RA{lv.nc, ra_nnz, ra_row.get(), ra_col, ra_val};
+    BCMG_TRY(spgemm(RA, lv.pview(), lv.nc, ac_row.get(), &ac_col, &ac_val, &ac_nnz, s));
+    DevLevel &c = H.lv[j + 1];
+    if (c.own_A) {
+      dev_free(c.row, s);
+      dev_free(c.col, s);
+      dev_free(c.val, s);
+    }
+    c.row = ac_row.release();
+    c.col = ac_col;
+    c.val = ac_val;
+    c.nnz = ac_nnz;
+    c.own_A = true;
+    BCMG_TRY(level_prep(c.view(), c.D, c.M, s));
+    c.own64.release(s);
+    if (wants_coarse_f64(h))
+      BCMG_TRY(sliced_build(c.view(), kValF64, &c.own64, s, h->ext.narrow_values != 0));
+  }
+  phase_tick("smoothed aggregation");
+  return BCMG_OK;
+}
+
 bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy &H) {
   cudaStream_t s = h->stream;
   const int maxlevels = h->prm.max_levels;
@@ -252,7 +327,8 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
       BCMG_TRY(level_prep(coarse.view(), coarse.D, coarse.M, s));
       // FP64 sliced copy now if an FP64 cycle will read this level (the FP64
       // solve, or the bootstrap's inner iterations).
-      if (h->ext.sliced && (h->ext.precision == BCMG_PREC_FP64 || h->prm.max_hrc > 1))
+      // (Smoothed aggregation replaces the coarse matrices: built afterwards.)
+      if (h->prm.aggrtype == 0 && wants_coarse_f64(h))
         BCMG_TRY(sliced_build(coarse.view(), kValF64, &coarse.own64, s, h->ext.narrow_values != 0));
       const double size_coarse = coarse.n;
       const double coarse_ratio = fine.n / size_coarse;
@@ -266,6 +342,7 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
     // level, i.e. a smoother-only preconditioner.
     level = 1;
   }
+  if (h->prm.aggrtype == 1) BCMG_TRY(smooth_hierarchy(h, H));
   const double nnz0 = H.lv[0].nnz;
   double c = 0, cw = 0;
   for (size_t i = 0; i < H.lv.size(); ++i) {
@@ -378,6 +455,8 @@ struct Lv<double> {
   static const double *D(const DevLevel &l) { return l.D; }
   static const double *M(const DevLevel &l) { return l.M; }
   static const double *p(const DevLevel &l) { return l.p; }
+  static MatView P(const DevLevel &l) { return mat_f64(l.pview()); }
+  static MatView R(const DevLevel &l) { return mat_f64(l.rview()); }
 };
 template <>
 struct Lv<float> {
@@ -399,6 +478,8 @@ struct Lv<float> {
   static const float *D(const DevLevel &l) { return l.D32; }
   static const float *M(const DevLevel &l) { return l.M32; }
   static const float *p(const DevLevel &l) { return l.p32; }
+  static MatView P(const DevLevel &l) { return mat_f32(l.pview(), l.Pval32); }
+  static MatView R(const DevLevel &l) { return mat_f32(l.rview(), l.Rval32); }
 };
 
 template <typename XT>
@@ -427,7 +508,10 @@ bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<
                        zero[l - 1] != 0, s));
   zero[l - 1] = 0;
   BCMG_TRY(residual_t<XT>(A, B.rhs[l - 1], B.x[l - 1], B.res[l - 1], s));
-  BCMG_TRY(restrict_t<XT>(lv.nc, lv.rptr, lv.ridx, Lv<XT>::p(lv), B.res[l - 1], B.rhs[l], s));
+  if (lv.Prow)
+    BCMG_TRY(spmv_t<XT>(Lv<XT>::R(lv), B.res[l - 1], B.rhs[l], s));
+  else
+    BCMG_TRY(restrict_t<XT>(lv.nc, lv.rptr, lv.ridx, Lv<XT>::p(lv), B.res[l - 1], B.rhs[l], s));
   zero[l] = 1;
   if (p.cycle_type == 3) {
     // K-cycle (GAMG_cycle.cu:88-100): one cycle on the coarsest level, two
@@ -444,7 +528,12 @@ bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<
       if (l == L - 1) break;
     }
   }
-  BCMG_TRY(prolong_t<XT>(lv.n, lv.agg, Lv<XT>::p(lv), B.x[l], B.x[l - 1], s));
+  if (lv.Prow) {
+    BCMG_TRY(spmv_t<XT>(Lv<XT>::P(lv), B.x[l], B.xt[l - 1], s));
+    BCMG_TRY(axpy_t<XT>(lv.n, XT(1), B.xt[l - 1], B.x[l - 1], s));
+  } else {
+    BCMG_TRY(prolong_t<XT>(lv.n, lv.agg, Lv<XT>::p(lv), B.x[l], B.x[l - 1], s));
+  }
   BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.postrelax_sweeps, false,
                        s));
   return BCMG_OK;
@@ -636,6 +725,12 @@ bcmg_status prepare_mixed(bcmg_handle *h) {
       if (lv.p) {
         BCMG_TRY(dev_alloc(&lv.p32, lv.n, s));
         BCMG_TRY(convert_d2f(lv.n, lv.p, lv.p32, s));
+      }
+      if (lv.Prow) {
+        BCMG_TRY(dev_alloc(&lv.Pval32, std::max(lv.Pnnz, 1), s));
+        BCMG_TRY(dev_alloc(&lv.Rval32, std::max(lv.Pnnz, 1), s));
+        BCMG_TRY(convert_d2f(lv.Pnnz, lv.Pval, lv.Pval32, s));
+        BCMG_TRY(convert_d2f(lv.Pnnz, lv.Rval, lv.Rval32, s));
       }
     }
   }
@@ -933,6 +1028,11 @@ size_t level_bytes(const DevLevel &l) {
   if (l.own_lo && l.val_lo) b += (l.vtype_lo == kValF32 ? 4 : 2) * nnz;
   for (const float *v : {l.D32, l.M32, l.p32})
     if (v) b += 4 * n;
+  if (l.Prow) {  // P and R (CSR), FP32 value copies
+    const size_t pn = static_cast<size_t>(l.Pnnz);
+    b += 4 * (n + 1) + 4 * (static_cast<size_t>(l.nc) + 1) + 2 * 12 * pn;
+    if (l.Pval32) b += 2 * 4 * pn;
+  }
   return b + l.own64.bytes() + l.ownlo.bytes();
 }
 
@@ -1308,6 +1408,8 @@ bcmg_status bcmg_get_params(const bcmg_handle *h, bcmg_params *p) {
 bcmg_status bcmg_save(const bcmg_handle *h, const char *path) {
   clear_error();
   if (!h || !path) return set_error(BCMG_ERR_PARAM, "null argument");
+  if (h->prm.aggrtype == 1)
+    return set_error(BCMG_ERR_UNSUPPORTED, "hierarchy files hold unsmoothed aggregation only");
   BCMG_CUDA(cudaSetDevice(h->device));
   File f(fopen(path, "wb"));
   if (!f) return set_error(BCMG_ERR_IO, "cannot open %s for writing", path);
@@ -1329,6 +1431,8 @@ bcmg_status bcmg_load(const char *path, const bcmg_ext *ext, bcmg_handle **out) 
     return set_error(BCMG_ERR_IO, "%s is not a hierarchy file", path);
   if (fread(&prm, sizeof(prm), 1, f.get()) != 1)
     return set_error(BCMG_ERR_IO, "hierarchy file truncated");
+  if (prm.aggrtype != 0)
+    return set_error(BCMG_ERR_IO, "%s: hierarchy file with aggrtype %d", path, prm.aggrtype);
   const auto t0 = Clock::now();
   bcmg_handle *h = nullptr;
   BCMG_TRY(new_handle(&prm, ext, &h));

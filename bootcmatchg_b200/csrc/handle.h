@@ -29,6 +29,15 @@ struct DevLevel {
   int vtype_lo = kValF32;
   bool own_lo = true;
   float *D32 = nullptr, *M32 = nullptr, *p32 = nullptr;
+  // Smoothed aggregation (aggrtype 1): P (n x nc) and R = P^T as CSR
+  // matrices, with FP32 copies of their values for the mixed cycle.  The
+  // cycle uses them instead of agg/p/rptr/ridx when Prow is set.
+  int32_t *Prow = nullptr, *Pcol = nullptr, *Rrow = nullptr, *Rcol = nullptr;
+  double *Pval = nullptr, *Rval = nullptr;
+  float *Pval32 = nullptr, *Rval32 = nullptr;
+  int32_t Pnnz = 0;
+  CsrView pview() const { return CsrView{n, Pnnz, Prow, Pcol, Pval}; }
+  CsrView rview() const { return CsrView{nc, Pnnz, Rrow, Rcol, Rval}; }
   // Sliced solve-phase copies (own64/ownlo owned here; s64/slo may point to
   // the handle's level-0 copies).
   SlicedMat own64, ownlo;

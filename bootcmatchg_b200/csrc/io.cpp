@@ -401,10 +401,6 @@ bcmg_status bcmg_params_check(const bcmg_params *p) {
     return set_error(BCMG_ERR_PARAM, "sweep counts must be >= 0");
   if (p->itnlim < 1) return set_error(BCMG_ERR_PARAM, "itnlim must be >= 1");
   if (!(p->rtol >= 0.0)) return set_error(BCMG_ERR_PARAM, "rtol must be >= 0");
-  if (p->aggrtype == 1)
-    return set_error(BCMG_ERR_UNSUPPORTED,
-                     "aggrtype 1 (smoothed aggregation) is not supported: the "
-                     "reference aborts in CSRm::infinityNorm (CSR.cu:402-404)");
   return BCMG_OK;
 }
 

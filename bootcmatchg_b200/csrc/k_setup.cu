@@ -9,6 +9,8 @@
 // run in a fixed order, so setup is deterministic run to run.
 #include <cfloat>
 #include <climits>
+#include <cmath>
+#include <cstring>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -881,6 +883,233 @@ __global__ void __launch_bounds__(kGalLongThreads)
   }
 }
 
+// ---- general SpGEMM C = X Y (smoothed aggregation) --------------------------
+// Canonical order: row i's terms x_ik y_kj in generation order (k by X's row
+// order, then Y's row order); sorted by (column, generation position), so
+// each column's terms are summed in generation order from the first one.
+
+__global__ void k_sp_terms(int32_t n, const int32_t *__restrict__ xrow,
+                           const int32_t *__restrict__ xcol,
+                           const int32_t *__restrict__ yrow, int32_t *tcount,
+                           unsigned long long *total) {  // total[0] sum, total[1] max
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t t = 0;
+  for (int32_t a = xrow[i]; a < xrow[i + 1]; ++a) {
+    const int32_t k = xcol[a];
+    t += yrow[k + 1] - yrow[k];
+  }
+  tcount[i] = t < INT_MAX ? static_cast<int32_t>(t) : INT_MAX;
+  atomicAdd(total, static_cast<unsigned long long>(t));
+  atomicMax(total + 1, static_cast<unsigned long long>(t));
+}
+
+template <int TEAM>
+__device__ int sp_gather(int32_t i, const int32_t *__restrict__ xrow,
+                         const int32_t *__restrict__ xcol, const double *__restrict__ xval,
+                         const int32_t *__restrict__ yrow, const int32_t *__restrict__ ycol,
+                         const double *__restrict__ yval, int32_t T, GalSmem sm, int cap,
+                         int tid) {
+  if (T > cap) return -1;
+  int base = 0;
+  for (int32_t a = xrow[i]; a < xrow[i + 1]; ++a) {
+    const int32_t k = xcol[a];
+    const double x = xval[a];
+    const int32_t b0 = yrow[k];
+    const int len = yrow[k + 1] - b0;
+    for (int t = tid; t < len; t += TEAM) {
+      const int pos = base + t;
+      sm.key[pos] = (static_cast<unsigned long long>(static_cast<uint32_t>(ycol[b0 + t])) << 32) |
+                    static_cast<uint32_t>(pos);
+      sm.tv[pos] = x * yval[b0 + t];
+    }
+    base += len;
+  }
+  int P2 = 1;
+  while (P2 < T) P2 <<= 1;
+  for (int t = T + tid; t < P2; t += TEAM) sm.key[t] = ~0ull;
+  team_sync<TEAM>();
+  for (int k = 2; k <= P2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < P2 / 2; t += TEAM) {
+        const int i0 = ((t & ~(j - 1)) << 1) | (t & (j - 1));  // j = 2^m
+        const int i1 = i0 + j;
+        const bool asc = (i0 & k) == 0;
+        const unsigned long long a = sm.key[i0], b = sm.key[i1];
+        if ((a > b) == asc) {
+          sm.key[i0] = b;
+          sm.key[i1] = a;
+        }
+      }
+      team_sync<TEAM>();
+    }
+  }
+  return T;
+}
+
+// Runs of the sorted row: (column, sum in generation order), one warp.
+__device__ void sp_emit(const GalSmem &sm, int T, int32_t i, int64_t base, int32_t *tJ,
+                        double *tV, int32_t *runs, int lane) {
+  int carry = 0;
+  for (int b0 = 0; b0 < T; b0 += 32) {
+    const int k = b0 + lane;
+    const bool h = k < T && gal_head(sm, k);
+    const unsigned hm = __ballot_sync(0xffffffffu, h);
+    if (h) {
+      const unsigned long long jj = sm.key[k] >> 32;
+      double s = sm.tv[static_cast<int>(sm.key[k] & 0xffffffffull)];
+      for (int q = k + 1; q < T && (sm.key[q] >> 32) == jj; ++q)
+        s = s + sm.tv[static_cast<int>(sm.key[q] & 0xffffffffull)];
+      const int64_t pos = base + carry + __popc(hm & ((1u << lane) - 1u));
+      tJ[pos] = static_cast<int32_t>(jj);
+      tV[pos] = s;
+    }
+    carry += __popc(hm);
+  }
+  if (lane == 0) runs[i] = carry;
+}
+
+__global__ void __launch_bounds__(kGalWarpsPerBlock * 32)
+    k_sp_rows(int32_t n, const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
+              const double *__restrict__ xval, const int32_t *__restrict__ yrow,
+              const int32_t *__restrict__ ycol, const double *__restrict__ yval,
+              const int32_t *__restrict__ tpos, const int32_t *__restrict__ tcount,
+              int32_t *tJ, double *tV, int32_t *runs, int32_t *long_rows, int32_t *n_long) {
+  extern __shared__ __align__(16) unsigned char gal_dyn[];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int32_t i = blockIdx.x * kGalWarpsPerBlock + wid;
+  if (i >= n) return;
+  GalSmem sm = gal_smem(gal_dyn + static_cast<size_t>(wid) * kGalCap * kGalBytesPerTerm,
+                        kGalCap);
+  const int T = sp_gather<32>(i, xrow, xcol, xval, yrow, ycol, yval, tcount[i], sm, kGalCap,
+                              lane);
+  if (T < 0) {
+    if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
+    return;
+  }
+  sp_emit(sm, T, i, tpos[i], tJ, tV, runs, lane);
+}
+
+// Rows over kGalCap terms, one block each: in shared memory up to
+// kGalCapLong terms, beyond that in this block's slice of a global scratch
+// (huge_cap keys and values per block; the same sort, ordered by
+// __syncthreads).
+__global__ void __launch_bounds__(kGalLongThreads)
+    k_sp_rows_long(const int32_t *__restrict__ long_rows, const int32_t *__restrict__ n_long,
+                   const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
+                   const double *__restrict__ xval, const int32_t *__restrict__ yrow,
+                   const int32_t *__restrict__ ycol, const double *__restrict__ yval,
+                   const int32_t *__restrict__ tpos, const int32_t *__restrict__ tcount,
+                   int32_t *tJ, double *tV, int32_t *runs, unsigned long long *huge_key,
+                   double *huge_val, int huge_cap, int *err) {
+  extern __shared__ __align__(16) unsigned char gal_dyn[];
+  const GalSmem sm = gal_smem(gal_dyn, kGalCapLong);
+  GalSmem gm = sm;
+  if (huge_key) {
+    gm.key = huge_key + static_cast<size_t>(blockIdx.x) * huge_cap;
+    gm.tv = huge_val + static_cast<size_t>(blockIdx.x) * huge_cap;
+  }
+  for (int32_t q = blockIdx.x; q < *n_long; q += gridDim.x) {
+    const int32_t i = long_rows[q];
+    const bool huge = tcount[i] > kGalCapLong;
+    if (huge && !huge_key) {
+      if (threadIdx.x == 0) atomicExch(err, 3);
+      return;
+    }
+    const GalSmem &w = huge ? gm : sm;
+    const int T = sp_gather<kGalLongThreads>(i, xrow, xcol, xval, yrow, ycol, yval, tcount[i],
+                                             w, huge ? huge_cap : kGalCapLong, threadIdx.x);
+    if (T < 0) {
+      if (threadIdx.x == 0) atomicExch(err, 3);
+      return;
+    }
+    if (threadIdx.x < 32) sp_emit(w, T, i, tpos[i], tJ, tV, runs, threadIdx.x);
+    __syncthreads();
+  }
+}
+
+// CSR transpose: counts, a scan, unordered fill, then each row sorted by
+// column (= source row) so the result is canonical.
+__global__ void k_tr_count(int32_t nnz, const int32_t *__restrict__ col, int32_t m,
+                           int32_t *cnt, int *err) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nnz) return;
+  const int32_t c = col[e];
+  if (c < 0 || c >= m) {
+    atomicExch(err, 1);
+    return;
+  }
+  atomicAdd(cnt + c, 1);
+}
+
+__global__ void k_tr_fill(int32_t n, const int32_t *__restrict__ row,
+                          const int32_t *__restrict__ col, const double *__restrict__ val,
+                          int32_t m, const int32_t *__restrict__ trow, int32_t *cursor,
+                          int32_t *tcol, double *tval) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int32_t e = row[i]; e < row[i + 1]; ++e) {
+    const int32_t c = col[e];
+    if (c < 0 || c >= m) continue;
+    const int32_t q = trow[c] + atomicAdd(cursor + c, 1);
+    tcol[q] = i;
+    tval[q] = val[e];
+  }
+}
+
+__global__ void k_tr_sort(int32_t m, const int32_t *__restrict__ trow, int32_t *tcol,
+                          double *tval) {
+  const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  const int32_t b = trow[r], e = trow[r + 1];
+  for (int32_t k = b + 1; k < e; ++k) {
+    const int32_t c = tcol[k];
+    const double v = tval[k];
+    int32_t j = k - 1;
+    while (j >= b && tcol[j] > c) {
+      tcol[j + 1] = tcol[j];
+      tval[j + 1] = tval[j];
+      --j;
+    }
+    tcol[j + 1] = c;
+    tval[j + 1] = v;
+  }
+}
+
+// Smoothing operator S = I - omega D^{-1} A, in two passes:
+// k_smooth_scale writes s = a / d_i and the max absolute row sum (the
+// infinity norm, exact max on non-negative doubles via their bits);
+// k_smooth_omega then applies s = -omega s (+1 on the diagonal).
+__global__ void k_smooth_scale(int32_t n, const int32_t *__restrict__ row,
+                               const double *__restrict__ val, const double *__restrict__ D,
+                               double *sval, unsigned long long *inf_bits) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double rs = 0.0;
+  for (int32_t e = row[i]; e < row[i + 1]; ++e) {
+    const double t = val[e] / D[i];
+    sval[e] = t;
+    rs = rs + fabs(t);
+  }
+  atomicMax(inf_bits, static_cast<unsigned long long>(__double_as_longlong(rs)));
+}
+
+__global__ void k_smooth_omega(int32_t n, const int32_t *__restrict__ row,
+                               const int32_t *__restrict__ col, double omega, double *sval) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int32_t e = row[i]; e < row[i + 1]; ++e) {
+    double t = -omega * sval[e];
+    if (col[e] == i) t = t + 1.0;
+    sval[e] = t;
+  }
+}
+
+__global__ void k_iota(int32_t n, int32_t *x) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= n) x[i] = i;
+}
+
 // Moves each row's runs from its term-sized slot to its final CSR position.
 __global__ void k_gal_compact(int32_t nc, const int32_t *__restrict__ tpos,
                               const int32_t *__restrict__ crow,
@@ -1172,6 +1401,137 @@ bcmg_status compose_p(int32_t n, int32_t *agg, double *p, const int32_t *agg2,
                       const double *p2, cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
   launch(k_compose, ceil_div(n, 256), 256, 0, s, n, agg, p, agg2, p2);
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
+bcmg_status spgemm(const CsrView &X, const CsrView &Y, int32_t m, int32_t *crow,
+                   int32_t **ccol_out, double **cval_out, int32_t *cnnz, cudaStream_t s) {
+  *ccol_out = nullptr;
+  *cval_out = nullptr;
+  *cnnz = 0;
+  const int32_t n = X.n;
+  if (n <= 0) return BCMG_OK;
+  (void)m;
+  DevBuf<int32_t> tcount, tpos, tJ, long_rows, n_long, tmp;
+  DevBuf<double> tV;
+  DevBuf<int> err;
+  BCMG_TRY(tcount.alloc(n, s));
+  BCMG_TRY(tpos.alloc(n + 1, s));
+  BCMG_TRY(long_rows.alloc(n, s));
+  BCMG_TRY(n_long.alloc(1, s));
+  BCMG_TRY(err.alloc(1, s));
+  BCMG_TRY(tmp.alloc(scan_tmp_size(n), s));
+  DevBuf<unsigned long long> total;
+  BCMG_TRY(total.alloc(2, s));
+  BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
+  BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
+  BCMG_CUDA(cudaMemsetAsync(total.get(), 0, 2 * sizeof(unsigned long long), s));
+  launch(k_sp_terms, ceil_div(n, 256), 256, 0, s, n, X.row, X.col, Y.row, tcount.get(),
+         total.get());
+  unsigned long long h_total[2] = {0, 0};
+  BCMG_CUDA(cudaMemcpyAsync(h_total, total.get(), sizeof(h_total), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  if (h_total[0] > static_cast<unsigned long long>(INT_MAX))
+    return set_error(BCMG_ERR_UNSUPPORTED, "sparse product has %llu terms (limit %d)",
+                     h_total[0], INT_MAX);
+  const int32_t terms = static_cast<int32_t>(h_total[0]);
+  // Rows over kGalCapLong terms sort in a global scratch of huge_cap (a power
+  // of two) keys and values per block, at most kHugeScratchBytes in all.
+  constexpr int64_t kHugeScratchBytes = int64_t(1) << 30;
+  int huge_cap = 0, long_grid = std::min(n, kNumSM);
+  DevBuf<unsigned long long> huge_key;
+  DevBuf<double> huge_val;
+  if (h_total[1] > static_cast<unsigned long long>(kGalCapLong)) {
+    int64_t c = 1;
+    while (c < static_cast<int64_t>(h_total[1])) c <<= 1;
+    if (c * 16 > kHugeScratchBytes)
+      return set_error(BCMG_ERR_UNSUPPORTED, "a sparse-product row has %llu terms",
+                       h_total[1]);
+    huge_cap = static_cast<int>(c);
+    long_grid = static_cast<int>(std::min<int64_t>(long_grid, kHugeScratchBytes / (c * 16)));
+    BCMG_TRY(huge_key.alloc(static_cast<int64_t>(long_grid) * huge_cap, s));
+    BCMG_TRY(huge_val.alloc(static_cast<int64_t>(long_grid) * huge_cap, s));
+  }
+  BCMG_TRY(exclusive_scan(tcount.get(), tpos.get(), n, nullptr, tmp.get(), s));
+  BCMG_TRY(tJ.alloc(std::max<int32_t>(terms, 1), s));
+  BCMG_TRY(tV.alloc(std::max<int32_t>(terms, 1), s));
+  const size_t smem_warp = static_cast<size_t>(kGalWarpsPerBlock) * kGalCap * kGalBytesPerTerm;
+  const size_t smem_long = static_cast<size_t>(kGalCapLong) * kGalBytesPerTerm;
+  BCMG_CUDA(cudaFuncSetAttribute(k_sp_rows_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem_long)));
+  launch(k_sp_rows, ceil_div(n, kGalWarpsPerBlock), kGalWarpsPerBlock * 32, smem_warp, s, n,
+         X.row, X.col, X.val, Y.row, Y.col, Y.val, tpos.get(), tcount.get(), tJ.get(), tV.get(),
+         crow, long_rows.get(), n_long.get());
+  launch(k_sp_rows_long, long_grid, kGalLongThreads, smem_long, s, long_rows.get(),
+         n_long.get(), X.row, X.col, X.val, Y.row, Y.col, Y.val, tpos.get(), tcount.get(),
+         tJ.get(), tV.get(), crow, huge_key.get(), huge_val.get(), huge_cap, err.get());
+  BCMG_LAUNCH_CHECK();
+  BCMG_TRY(exclusive_scan(crow, crow, n, crow + n, tmp.get(), s));
+  int h_err = 0;
+  int32_t h_nnz = 0;
+  BCMG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaMemcpyAsync(&h_nnz, crow + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  if (h_err) return set_error(BCMG_ERR_INTERNAL, "sparse product: row over its term capacity");
+  DevBuf<int32_t> ccol;
+  DevBuf<double> cval;
+  BCMG_TRY(ccol.alloc(std::max<int32_t>(h_nnz, 1), s));
+  BCMG_TRY(cval.alloc(std::max<int32_t>(h_nnz, 1), s));
+  launch(k_gal_compact, ceil_div(static_cast<int64_t>(n) * 32, 256), 256, 0, s, n, tpos.get(),
+         crow, tJ.get(), tV.get(), ccol.get(), cval.get());
+  BCMG_LAUNCH_CHECK();
+  *cnnz = h_nnz;
+  *ccol_out = ccol.release();
+  *cval_out = cval.release();
+  return BCMG_OK;
+}
+
+bcmg_status csr_transpose(const CsrView &A, int32_t m, int32_t *trow, int32_t *tcol,
+                          double *tval, cudaStream_t s) {
+  DevBuf<int32_t> cursor, tmp;
+  DevBuf<int> err;
+  BCMG_TRY(cursor.alloc(std::max(m, 1), s));
+  BCMG_TRY(tmp.alloc(scan_tmp_size(m), s));
+  BCMG_TRY(err.alloc(1, s));
+  BCMG_CUDA(cudaMemsetAsync(trow, 0, sizeof(int32_t) * (m + 1), s));
+  BCMG_CUDA(cudaMemsetAsync(cursor.get(), 0, sizeof(int32_t) * std::max(m, 1), s));
+  BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
+  if (A.nnz > 0)
+    launch(k_tr_count, ceil_div(A.nnz, 256), 256, 0, s, A.nnz, A.col, m, trow, err.get());
+  BCMG_TRY(exclusive_scan(trow, trow, m, trow + m, tmp.get(), s));
+  launch(k_tr_fill, ceil_div(A.n, 256), 256, 0, s, A.n, A.row, A.col, A.val, m, trow,
+         cursor.get(), tcol, tval);
+  launch(k_tr_sort, ceil_div(m, 256), 256, 0, s, m, trow, tcol, tval);
+  BCMG_LAUNCH_CHECK();
+  int h_err = 0;
+  BCMG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  if (h_err) return set_error(BCMG_ERR_INTERNAL, "transpose: column outside [0, %d)", m);
+  return BCMG_OK;
+}
+
+bcmg_status smoothing_operator(const CsrView &A, const double *D, double *sval,
+                               cudaStream_t s) {
+  DevBuf<unsigned long long> inf;
+  BCMG_TRY(inf.alloc(1, s));
+  BCMG_CUDA(cudaMemsetAsync(inf.get(), 0, sizeof(unsigned long long), s));
+  launch(k_smooth_scale, ceil_div(A.n, 256), 256, 0, s, A.n, A.row, A.val, D, sval, inf.get());
+  unsigned long long bits = 0;
+  BCMG_CUDA(cudaMemcpyAsync(&bits, inf.get(), sizeof(bits), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  double norm;
+  std::memcpy(&norm, &bits, sizeof(norm));
+  if (!(norm > 0.0) || !std::isfinite(norm))
+    return set_error(BCMG_ERR_INVALID_MATRIX, "smoothed aggregation: bad ||D^-1 A||_inf");
+  const double omega = 4.0 / (3.0 * norm);
+  launch(k_smooth_omega, ceil_div(A.n, 256), 256, 0, s, A.n, A.row, A.col, omega, sval);
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
+bcmg_status iota(int32_t n, int32_t *x, cudaStream_t s) {
+  launch(k_iota, ceil_div(static_cast<int64_t>(n) + 1, 256), 256, 0, s, n, x);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }

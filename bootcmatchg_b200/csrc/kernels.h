@@ -39,6 +39,17 @@ bcmg_status restrict_exact(int32_t nc, const int32_t *rptr, const int32_t *ridx,
                            cudaStream_t s);
 bcmg_status compose_p(int32_t n, int32_t *agg, double *p, const int32_t *agg2,
                       const double *p2, cudaStream_t s);
+// C = X Y (X: n rows, Y: m columns) in the canonical summation order; crow
+// (n+1) caller-allocated, *ccol/*cval allocated on s (*cnnz entries).
+bcmg_status spgemm(const CsrView &X, const CsrView &Y, int32_t m, int32_t *crow,
+                   int32_t **ccol, double **cval, int32_t *cnnz, cudaStream_t s);
+// A^T (A: n x m) into trow (m+1), tcol, tval (nnz), rows sorted by column.
+bcmg_status csr_transpose(const CsrView &A, int32_t m, int32_t *trow, int32_t *tcol,
+                          double *tval, cudaStream_t s);
+// sval = values of S = I - omega D^{-1} A, omega = 4 / (3 ||D^{-1} A||_inf).
+bcmg_status smoothing_operator(const CsrView &A, const double *D, double *sval,
+                               cudaStream_t s);
+bcmg_status iota(int32_t n, int32_t *x, cudaStream_t s);  // x[i] = i, i <= n
 
 // ---- cycle (k_cycle.cu) ----------------------------------------------------
 // Value storage of a level matrix used by the cycle.
@@ -151,6 +162,13 @@ inline MatView mat_f64(const CsrView &A) {
   m.col = A.col;
   m.val = A.val;
   m.vtype = kValF64;
+  return m;
+}
+// A's structure with FP32 values val32.
+inline MatView mat_f32(const CsrView &A, const float *val32) {
+  MatView m = mat_f64(A);
+  m.val = val32;
+  m.vtype = kValF32;
   return m;
 }
 inline bcmg_status fill(double *x, int64_t n, double v, cudaStream_t s) {

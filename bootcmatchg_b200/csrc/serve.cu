@@ -173,7 +173,8 @@ bool pick(bcmg_server *s, Job *job, std::vector<bcmg_handle *> &victims) {
     // Same-key requests in arrival order join the group (one at a time with
     // the K-cycle, which batched solves do not run).
     Group g;
-    const int max_group = s->opt.params.cycle_type == 3 ? 1 : s->opt.max_batch;
+    const bcmg_params &pp = s->opt.params;
+    const int max_group = pp.cycle_type == 3 || pp.aggrtype == 1 ? 1 : s->opt.max_batch;
     for (size_t j = i; j < s->queue.size() && static_cast<int>(g.size()) < max_group; ++j)
       if (s->queue[j]->key == r->key) g.push_back(s->queue[j]);
     const size_t work = g.size() > 1 ? estimate_batch(r->b.size(), static_cast<int>(g.size())) : 0;

@@ -41,6 +41,9 @@ struct Level {
   int32_t nc = 0;
   IVec agg, rptr, ridx;
   Vec p;
+  // Smoothed aggregation (aggrtype 1): the smoothed prolongator and its
+  // transpose replace (agg, p) and the member lists in the cycle.
+  std::shared_ptr<const Csr> P, R;
 };
 
 struct Hierarchy {
@@ -423,6 +426,112 @@ std::shared_ptr<Csr> matching_aggregation(const orc_handle &h, const Csr &A, Vec
   return Ai;
 }
 
+// C = X Y in the canonical order: row i's terms x_ik y_kj are generated by
+// k in X's row order, then by Y's row order; a stable sort by column groups
+// them and each column's terms are summed in generation order from the
+// first term (the GPU kernel follows the same order, so C is bit-identical).
+std::shared_ptr<Csr> spgemm(const Csr &X, const Csr &Y) {
+  auto C = std::make_shared<Csr>();
+  C->n = X.n;
+  C->m = Y.m;
+  C->row.assign(X.n + 1, 0);
+  std::vector<IVec> cols(X.n);
+  std::vector<Vec> vals(X.n);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int32_t i = 0; i < X.n; ++i) {
+    std::vector<std::pair<int32_t, double>> t;
+    for (int32_t a = X.row[i]; a < X.row[i + 1]; ++a) {
+      const int32_t k = X.col[a];
+      const double x = X.val[a];
+      for (int32_t b = Y.row[k]; b < Y.row[k + 1]; ++b) t.emplace_back(Y.col[b], x * Y.val[b]);
+    }
+    std::stable_sort(t.begin(), t.end(),
+                     [](const std::pair<int32_t, double> &u,
+                        const std::pair<int32_t, double> &v) { return u.first < v.first; });
+    for (size_t q = 0; q < t.size();) {
+      double s = t[q].second;
+      size_t e = q + 1;
+      for (; e < t.size() && t[e].first == t[q].first; ++e) s = s + t[e].second;
+      cols[i].push_back(t[q].first);
+      vals[i].push_back(s);
+      q = e;
+    }
+  }
+  for (int32_t i = 0; i < X.n; ++i) C->row[i + 1] = C->row[i] + static_cast<int32_t>(cols[i].size());
+  C->col.reserve(C->row[X.n]);
+  C->val.reserve(C->row[X.n]);
+  for (int32_t i = 0; i < X.n; ++i) {
+    C->col.insert(C->col.end(), cols[i].begin(), cols[i].end());
+    C->val.insert(C->val.end(), vals[i].begin(), vals[i].end());
+  }
+  return C;
+}
+
+// A^T with rows in increasing column order of A (csr2csc).
+std::shared_ptr<Csr> transpose_csr(const Csr &A) {
+  auto T = std::make_shared<Csr>();
+  T->n = A.m;
+  T->m = A.n;
+  T->row.assign(A.m + 1, 0);
+  for (int32_t c : A.col) ++T->row[c + 1];
+  for (int32_t i = 0; i < A.m; ++i) T->row[i + 1] += T->row[i];
+  T->col.resize(A.nnz());
+  T->val.resize(A.nnz());
+  IVec cur(T->row.begin(), T->row.end() - 1);
+  for (int32_t i = 0; i < A.n; ++i)
+    for (int32_t j = A.row[i]; j < A.row[i + 1]; ++j) {
+      const int32_t q = cur[A.col[j]]++;
+      T->col[q] = i;
+      T->val[q] = A.val[j];
+    }
+  return T;
+}
+
+// Smoothed aggregation (adaptiveCoarsening, matchingAggregation.cu:353-390),
+// applied to the built hierarchy: for each level j,
+//   A_s = D_j^{-1} A_j (CSRm::matrixVectorScaling, CSR.cu:519-545),
+//   omega = 4 / (3 ||A_s||_inf) (CSRm::infinityNorm, which the reference
+//           stubs with assert(false), CSR.cu:402-417: the max absolute row sum),
+//   S = I - omega A_s (applyOmega, matchingAggregation.cu:63-88),
+//   P_j = S P_j, R_j = P_j^T, A_{j+1} = (R_j A_j) P_j, and relaxPrepare.
+void smooth_hierarchy(Hierarchy &H) {
+  const int L = static_cast<int>(H.lv.size());
+  for (int j = 0; j + 1 < L; ++j) {
+    Level &lv = H.lv[j];
+    const Csr &A = *lv.A;
+    Csr S = A;
+    double inf = 0.0;
+    for (int32_t i = 0; i < A.n; ++i) {
+      double rs = 0.0;
+      for (int32_t e = A.row[i]; e < A.row[i + 1]; ++e) {
+        S.val[e] = A.val[e] / lv.D[i];
+        rs = rs + std::fabs(S.val[e]);
+      }
+      inf = std::max(inf, rs);
+    }
+    const double omega = 4.0 / (3.0 * inf);
+    for (int32_t i = 0; i < A.n; ++i)
+      for (int32_t e = A.row[i]; e < A.row[i + 1]; ++e) {
+        S.val[e] = -omega * S.val[e];
+        if (A.col[e] == i) S.val[e] = S.val[e] + 1.0;
+      }
+    Csr Pt;
+    Pt.n = A.n;
+    Pt.m = lv.nc;
+    Pt.row.resize(A.n + 1);
+    std::iota(Pt.row.begin(), Pt.row.end(), 0);
+    Pt.col = lv.agg;
+    Pt.val = lv.p;
+    lv.P = spgemm(S, Pt);
+    lv.R = transpose_csr(*lv.P);
+    auto RA = spgemm(*lv.R, A);
+    auto Ac = spgemm(*RA, *lv.P);
+    Level &c = H.lv[j + 1];
+    c.A = Ac;
+    level_prep(*Ac, c.D, c.M);
+  }
+}
+
 // adaptiveCoarsening (matchingAggregation.cu:298-423).
 Hierarchy adaptive_coarsening(const orc_handle &h, const Vec &w_in) {
   Hierarchy H;
@@ -457,6 +566,7 @@ Hierarchy adaptive_coarsening(const orc_handle &h, const Vec &w_in) {
     // level (smoother-only preconditioner) is used instead.
     level = 1;
   }
+  if (h.prm.aggrtype == 1) smooth_hierarchy(H);
   double nnz0 = H.lv[0].A->nnz(), c = 0, cw = 0;
   for (size_t i = 0; i < H.lv.size(); ++i) {
     c += H.lv[i].A->nnz();
@@ -574,7 +684,10 @@ void cycle(orc_handle &h, int k, int l) {
 #pragma omp parallel for schedule(static)
   for (int32_t i = 0; i < n; ++i) res[i] = h.rhs[l - 1][i] - res[i];
   // Rhs_l = R Res (GAMG_cycle.cu:74-79)
-  restrict_vec(lv.rptr, lv.ridx, lv.p, res.data(), h.rhs[l].data(), lv.nc);
+  if (lv.R)
+    spmv(*lv.R, res.data(), h.rhs[l].data());  // Rhs_l = R Res (GAMG_cycle.cu:74-79)
+  else
+    restrict_vec(lv.rptr, lv.ridx, lv.p, res.data(), h.rhs[l].data(), lv.nc);
   std::fill(h.x[l].begin(), h.x[l].begin() + lv.nc, 0.0);
   if (p.cycle_type == 3) {
     // K-cycle (GAMG_cycle.cu:88-100): the coarsest level is one cycle,
@@ -587,11 +700,22 @@ void cycle(orc_handle &h, int k, int l) {
       if (l == L - 1) break;
     }
   }
-  // X += P X_c (_CSR_vector_mul_prolongator, src/matrix/CSR.cu:965-976)
+  // X += P X_c (_CSR_vector_mul_prolongator, src/matrix/CSR.cu:965-976; the
+  // general SpMV with beta = 1 for a smoothed P, GAMG_cycle.cu:116-117)
   double *xf = h.x[l - 1].data();
   const double *xc = h.x[l].data();
+  if (lv.P) {
+    const Csr &P = *lv.P;
 #pragma omp parallel for schedule(static)
-  for (int32_t i = 0; i < n; ++i) xf[i] += lv.p[i] * xc[lv.agg[i]];
+    for (int32_t i = 0; i < n; ++i) {
+      double t = 0.0;
+      for (int32_t e = P.row[i]; e < P.row[i + 1]; ++e) t += P.val[e] * xc[P.col[e]];
+      xf[i] = xf[i] + t;
+    }
+  } else {
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) xf[i] += lv.p[i] * xc[lv.agg[i]];
+  }
   relax(*lv.A, d, h.rhs[l - 1].data(), xf, p.postrelax_sweeps, tmp);
 }
 
@@ -798,7 +922,7 @@ int orc_get_threads(void) { return omp_get_max_threads(); }
 
 int orc_setup(const bcmg_csr *A, const bcmg_params *p, orc_handle **out) {
   if (!A || !p || !out) return BCMG_ERR_PARAM;
-  if (p->aggrtype != 0) return BCMG_ERR_UNSUPPORTED;
+  if (p->aggrtype != 0 && p->aggrtype != 1) return BCMG_ERR_UNSUPPORTED;
   auto h = std::make_unique<orc_handle>();
   h->prm = *p;
   h->A0 = std::make_shared<Csr>(from_bcmg(A));

@@ -132,7 +132,7 @@ def test_params_default_is_settings_base():
 
 @pytest.mark.parametrize("field,value,code", [
     ("solver_type", 3, "PARAM"), ("cycle_type", 4, "PARAM"), ("relax_type", 1, "PARAM"),
-    ("coarse_solver", 9, "PARAM"), ("aggrtype", 2, "PARAM"), ("aggrtype", 1, "UNSUPPORTED"),
+    ("coarse_solver", 9, "PARAM"), ("aggrtype", 2, "PARAM"), ("aggrtype", -1, "PARAM"),
 ])
 def test_params_check(field, value, code):
     p = bc.Params.default()
@@ -353,6 +353,50 @@ def test_oracle_kcycle_converges_in_fewer_iterations():
         assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-8
         iters[ct] = info["iters"]
     assert iters[3] < iters[0]
+
+
+def _level_csr(lv):
+    n = lv["n"]
+    return sp.csr_matrix((lv["val"], lv["col"], lv["row"]), shape=(n, n))
+
+
+def test_oracle_smoothed_aggregation_restates_the_algorithm():
+    # aggrtype 1 (matchingAggregation.cu:353-390): on every level j < L-1,
+    # S = I - omega D^-1 A with omega = 4 / (3 ||D^-1 A||_inf), P = S P_tent,
+    # R = P^T and A_{j+1} = (R A) P, D of the already smoothed A_j.  Checked
+    # against scipy's products of the oracle's own level data, and the
+    # smoothed hierarchy needs fewer iterations than the unsmoothed one.
+    A = bc.poisson(7, 16, 16, 16)
+    b = bc.vector(1, 3, A.n)
+    iters = {}
+    for at in (0, 1):
+        p = c1_params()
+        p.aggrtype = at
+        p.check()
+        h = orc.OracleHandle(A, p)
+        L = h.hierarchy_info(0)["num_levels"]
+        assert L >= 3
+        if at == 1:
+            for j in range(L - 1):
+                f, c = h.level(0, j), h.level(0, j + 1)
+                Af = _level_csr(f)
+                assert np.array_equal(f["D"], Af.diagonal())
+                Dinv = sp.diags(1.0 / f["D"])
+                omega = 4.0 / (3.0 * abs(Dinv @ Af).sum(axis=1).max())
+                S = sp.identity(f["n"]) - omega * (Dinv @ Af)
+                Pt = sp.csr_matrix((f["p"], f["agg"], np.arange(f["n"] + 1)),
+                                   shape=(f["n"], f["n_coarse"]))
+                P = S @ Pt
+                Ac = (P.T @ Af @ P).toarray()
+                got = _level_csr(c).toarray()
+                assert np.abs(got - Ac).max() <= 1e-12 * np.abs(Ac).max(), j
+                assert np.array_equal(c["D"], _level_csr(c).diagonal())
+        x, info, st = h.solve(b)
+        assert st == 0 and info["converged"]
+        r = b - A.to_scipy() @ x
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-8
+        iters[at] = info["iters"]
+    assert iters[1] < iters[0]
 
 
 def test_bootstrap_second_hierarchy_uses_same_w():
