@@ -248,8 +248,10 @@ bcmg_status smooth_hierarchy(bcmg_handle *h, DevHierarchy &H) {
     DevBuf<int32_t> trow;
     BCMG_TRY(sval.alloc(std::max(A.nnz, 1), s));
     BCMG_TRY(trow.alloc(static_cast<int64_t>(A.n) + 1, s));
+    phase_tick("smoothed aggregation");
     BCMG_TRY(smoothing_operator(A, lv.D, sval.get(), s));
     BCMG_TRY(iota(A.n, trow.get(), s));
+    phase_tick("sa smoothing");
     const CsrView S{A.n, A.nnz, A.row, A.col, sval.get()};
     const CsrView Pt{A.n, A.n, trow.get(), lv.agg, lv.p};
     BCMG_TRY(dev_alloc(&lv.Prow, static_cast<int64_t>(A.n) + 1, s));
@@ -257,7 +259,9 @@ bcmg_status smooth_hierarchy(bcmg_handle *h, DevHierarchy &H) {
     BCMG_TRY(dev_alloc(&lv.Rrow, static_cast<int64_t>(lv.nc) + 1, s));
     BCMG_TRY(dev_alloc(&lv.Rcol, std::max(lv.Pnnz, 1), s));
     BCMG_TRY(dev_alloc(&lv.Rval, std::max(lv.Pnnz, 1), s));
+    phase_tick("sa P");
     BCMG_TRY(csr_transpose(lv.pview(), lv.nc, lv.Rrow, lv.Rcol, lv.Rval, s));
+    phase_tick("sa transpose");
     DevBuf<int32_t> ra_row, ac_row;
     BCMG_TRY(ra_row.alloc(static_cast<int64_t>(lv.nc) + 1, s));
     int32_t *ra_col = nullptr, *ac_col = nullptr;
@@ -272,7 +276,9 @@ bcmg_status smooth_hierarchy(bcmg_handle *h, DevHierarchy &H) {
     ra_valb.stream = s;
     BCMG_TRY(ac_row.alloc(static_cast<int64_t>(lv.nc) + 1, s));
     const CsrView RA{lv.nc, ra_nnz, ra_row.get(), ra_col, ra_val};
+    phase_tick("sa RA");
     BCMG_TRY(spgemm(RA, lv.pview(), lv.nc, ac_row.get(), &ac_col, &ac_val, &ac_nnz, s));
+    phase_tick("sa RAP");
     DevLevel &c = H.lv[j + 1];
     if (c.own_A) {
       dev_free(c.row, s);
@@ -931,16 +937,23 @@ bcmg_status build_fcg_graph(bcmg_handle *h) {
       &h->fcg_exec);
 }
 
+// r = b - A x in FP64 on the input matrix, through its sliced copy when
+// there is one.
+bcmg_status residual64(bcmg_handle *h, const double *b, const double *x, double *r) {
+  cudaStream_t s = h->stream;
+  if (h->A0.own64.nslices) return sliced_residual<double>(h->A0.own64.view(), b, x, r, s);
+  BCMG_TRY(copy(r, b, h->A0.n, s));
+  return spmv(h->A0.view(), -1.0, x, 1.0, r, s);
+}
+
 // FCG (flexibileConjugateGradients_v3, src/SOLVER/FCG.cu:433-585) on device
 // vectors h->b (rhs) and h->xs (initial guess in, solution out).
 bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
   const int32_t n = h->A0.n;
   cudaStream_t s = h->stream;
-  const CsrView A = h->A0.view();
   double *x = h->xs, *b = h->b, *r = h->r, *v = h->v, *w = h->w, *d = h->d, *q = h->q;
   // r = b - A x0; delta0 = ||r||; ||b||   (FCG.cu:446-457)
-  BCMG_TRY(copy(r, b, n, s));
-  BCMG_TRY(spmv(A, -1.0, x, 1.0, r, s));
+  BCMG_TRY(residual64(h, b, x, r));
   double delta0 = 0, bnorm = 0;
   BCMG_TRY(norm2(h, r, &delta0));
   BCMG_TRY(norm2(h, b, &bnorm));
@@ -1004,8 +1017,7 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
     return set_error(BCMG_ERR_INDEFINITE,
                      "FCG met non-positive curvature at iteration %d (A not SPD?)", iter);
   // True residual in FP64: ||b - A x|| / ||b - A x0||.
-  BCMG_TRY(copy(h->tmp, b, n, s));
-  BCMG_TRY(spmv(A, -1.0, x, 1.0, h->tmp, s));
+  BCMG_TRY(residual64(h, b, x, h->tmp));
   double tr = 0;
   BCMG_TRY(norm2(h, h->tmp, &tr));
   info->true_rel_residual = tr / delta0;

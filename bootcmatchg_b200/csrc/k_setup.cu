@@ -884,14 +884,247 @@ __global__ void __launch_bounds__(kGalLongThreads)
 }
 
 // ---- general SpGEMM C = X Y (smoothed aggregation) --------------------------
-// Canonical order: row i's terms x_ik y_kj in generation order (k by X's row
-// order, then Y's row order); sorted by (column, generation position), so
-// each column's terms are summed in generation order from the first one.
+// Canonical order: C_ij sums the terms x_ik y_kj in X's row order, from the
+// first term.  Every Y row has distinct columns, so column j gets at most one
+// term per X entry, and this equals summing each column's run of the
+// generation-ordered term list after a stable sort by column.
+// Rows run in three tiers by their distinct column count U: a warp with a
+// shared-memory hash set of kSpWarpHash slots, a block with kSpBlockHash
+// slots, a block with a table in global memory.  A set is used up to half
+// full.  The symbolic pass counts U (sending a row on to the next tier when
+// its set would pass half full); the numeric pass rebuilds the set, sorts its
+// columns, stores each column's rank in the set and accumulates one value per
+// rank, X entry by X entry.
 
-__global__ void k_sp_terms(int32_t n, const int32_t *__restrict__ xrow,
-                           const int32_t *__restrict__ xcol,
-                           const int32_t *__restrict__ yrow, int32_t *tcount,
-                           unsigned long long *total) {  // total[0] sum, total[1] max
+constexpr int kSpWarpHash = 1024;  // warp tier: U <= 512
+constexpr int kSpWarpsPerBlock = 4;
+constexpr int kSpBlockHash = 4096;  // block tier: U <= 2048
+constexpr int kSpThreads = 256;
+
+// The numeric pass takes a row's X entries in chunks of at most CA entries
+// whose Y rows hold at most SB terms in all: their (rank, value) pairs are
+// computed in parallel into shared memory, then added X entry by X entry.
+template <int CA, int SB>
+struct SpStage {
+  double x[CA];
+  double v[SB];
+  int b0[CA];
+  int len[CA];
+  int off[CA + 1];
+  int r[SB];
+};
+using SpStageWarp = SpStage<64, 192>;
+using SpStageBlock = SpStage<256, 2048>;
+constexpr size_t kSpStageWarpBytes = (sizeof(SpStageWarp) + 15) & ~size_t(15);
+constexpr size_t kSpStageBlockBytes = (sizeof(SpStageBlock) + 15) & ~size_t(15);
+
+struct SpTable {
+  double *acc;          // hc/2 values, by rank
+  int *key;             // hc slots, -1 = empty
+  int *rank;            // hc slots
+  int *cols;            // hc/2 sorted columns
+  int *count;           // distinct columns inserted
+  unsigned char *seen;  // hc/2 flags: acc holds a first term
+  int hc;
+};
+
+__host__ __device__ constexpr size_t sp_table_bytes(int hc) {
+  return (static_cast<size_t>(14) * hc + 16 + hc / 2 + 15) & ~static_cast<size_t>(15);
+}
+
+__device__ __forceinline__ SpTable sp_table(unsigned char *base, int hc) {
+  SpTable t;
+  t.hc = hc;
+  t.acc = reinterpret_cast<double *>(base);
+  t.key = reinterpret_cast<int *>(base + 4 * static_cast<size_t>(hc));
+  t.rank = reinterpret_cast<int *>(base + 8 * static_cast<size_t>(hc));
+  t.cols = reinterpret_cast<int *>(base + 12 * static_cast<size_t>(hc));
+  t.count = reinterpret_cast<int *>(base + 14 * static_cast<size_t>(hc));
+  t.seen = base + 14 * static_cast<size_t>(hc) + 16;
+  return t;
+}
+
+__device__ __forceinline__ unsigned sp_hash(int key, int hc) {
+  return (static_cast<unsigned>(key) * 2654435761u) & static_cast<unsigned>(hc - 1);
+}
+
+__device__ __forceinline__ int sp_find(const SpTable &t, int key) {
+  unsigned h = sp_hash(key, t.hc);
+  for (int probe = 0; probe < t.hc; ++probe) {
+    if (t.key[h] == key) return static_cast<int>(h);
+    h = (h + 1) & static_cast<unsigned>(t.hc - 1);
+  }
+  return 0;  // unreachable: the key was inserted
+}
+
+// Inserts the columns of row i of X Y into t; returns their number, or -1 if
+// the set would pass half full.  Ends with the team synchronised.
+template <int TEAM>
+__device__ int sp_collect(const SpTable &t, int32_t i, const int32_t *__restrict__ xrow,
+                          const int32_t *__restrict__ xcol, const int32_t *__restrict__ yrow,
+                          const int32_t *__restrict__ ycol, int tid) {
+  for (int q = tid; q < t.hc; q += TEAM) t.key[q] = -1;
+  if (tid == 0) *t.count = 0;
+  team_sync<TEAM>();
+  const int limit = t.hc / 2;
+  volatile int *cnt = t.count;
+  constexpr int kWarps = TEAM / 32;
+  const int lane = tid & 31;
+  for (int32_t a = xrow[i] + tid / 32; a < xrow[i + 1]; a += kWarps) {
+    const int32_t k = xcol[a];
+    const int32_t b0 = yrow[k], len = yrow[k + 1] - b0;
+    for (int32_t q = lane; q < len; q += 32) {
+      if (*cnt > limit) break;  // (at most TEAM keys past the limit)
+      const int j = ycol[b0 + q];
+      unsigned h = sp_hash(j, t.hc);
+      for (int probe = 0; probe < t.hc; ++probe) {
+        const int prev = atomicCAS(t.key + h, -1, j);
+        if (prev == -1) {
+          atomicAdd(t.count, 1);
+          break;
+        }
+        if (prev == j) break;
+        h = (h + 1) & static_cast<unsigned>(t.hc - 1);
+      }
+    }
+  }
+  team_sync<TEAM>();
+  const int U = *cnt;
+  team_sync<TEAM>();
+  return U > limit ? -1 : U;
+}
+
+// Row i's sorted columns and values into ccol/cval from `base`; t holds the
+// row's set (sp_collect), U its size, st is the team's staging area.
+template <int TEAM, int CA, int SB>
+__device__ void sp_numeric(const SpTable &t, SpStage<CA, SB> &st, int32_t i, int U,
+                           const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
+                           const double *__restrict__ xval, const int32_t *__restrict__ yrow,
+                           const int32_t *__restrict__ ycol, const double *__restrict__ yval,
+                           int32_t base, int32_t *ccol, double *cval, int tid) {
+  static_assert(CA % 32 == 0, "chunk of X entries in whole warps");
+  if (tid == 0) *t.count = 0;
+  team_sync<TEAM>();
+  for (int q = tid; q < t.hc; q += TEAM) {
+    const int j = t.key[q];
+    if (j >= 0) t.cols[atomicAdd(t.count, 1)] = j;
+  }
+  int P2 = 1;
+  while (P2 < U) P2 <<= 1;
+  for (int q = U + tid; q < P2; q += TEAM) t.cols[q] = INT_MAX;
+  team_sync<TEAM>();
+  for (int k = 2; k <= P2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int q = tid; q < P2 / 2; q += TEAM) {
+        const int i0 = ((q & ~(j - 1)) << 1) | (q & (j - 1));  // j = 2^m
+        const int i1 = i0 + j;
+        const bool asc = (i0 & k) == 0;
+        const int u = t.cols[i0], v = t.cols[i1];
+        if ((u > v) == asc) {
+          t.cols[i0] = v;
+          t.cols[i1] = u;
+        }
+      }
+      team_sync<TEAM>();
+    }
+  }
+  for (int r = tid; r < U; r += TEAM) {
+    const int j = t.cols[r];
+    t.rank[sp_find(t, j)] = r;
+    t.seen[r] = 0;
+    ccol[base + r] = j;
+  }
+  team_sync<TEAM>();
+  const int32_t a_end = xrow[i + 1];
+  for (int32_t a0 = xrow[i]; a0 < a_end;) {
+    const int na = a_end - a0 < CA ? static_cast<int>(a_end - a0) : CA;
+    for (int u = tid; u < na; u += TEAM) {
+      const int32_t k = xcol[a0 + u];
+      const int32_t b = yrow[k];
+      st.b0[u] = b;
+      st.len[u] = yrow[k + 1] - b;
+      st.x[u] = xval[a0 + u];
+    }
+    team_sync<TEAM>();
+    if (tid < 32) {  // st.off = exclusive scan of min(len, SB + 1)
+      constexpr int kPer = CA / 32;
+      int loc[kPer];
+      int sum = 0;
+#pragma unroll
+      for (int p = 0; p < kPer; ++p) {
+        const int u = tid * kPer + p;
+        loc[p] = u < na ? min(st.len[u], SB + 1) : 0;
+        sum += loc[p];
+      }
+      int incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (tid >= o) incl += y;
+      }
+      int run = incl - sum;
+#pragma unroll
+      for (int p = 0; p < kPer; ++p) {
+        st.off[tid * kPer + p] = run;
+        run += loc[p];
+      }
+      if (tid == 31) st.off[CA] = incl;
+    }
+    team_sync<TEAM>();
+    if (st.off[1] > SB) {  // one Y row over the stage: added directly
+      const int32_t b0 = st.b0[0], len = st.len[0];
+      const double x = st.x[0];
+      for (int32_t q = tid; q < len; q += TEAM) {
+        const int r = t.rank[sp_find(t, ycol[b0 + q])];
+        const double v = x * yval[b0 + q];
+        t.acc[r] = t.seen[r] ? t.acc[r] + v : v;
+        t.seen[r] = 1;
+      }
+      team_sync<TEAM>();
+      a0 += 1;
+      continue;
+    }
+    int nfit = 1;  // the most X entries whose terms fit the stage
+    {
+      int lo = 1, hi = na;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (st.off[mid] <= SB) lo = mid;
+        else hi = mid - 1;
+      }
+      nfit = lo;
+    }
+    const int total = st.off[nfit];
+    for (int e = tid; e < total; e += TEAM) {
+      int lo = 0, hi = nfit - 1;  // the X entry whose terms hold e
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (st.off[mid] <= e) lo = mid;
+        else hi = mid - 1;
+      }
+      const int32_t b = st.b0[lo] + (e - st.off[lo]);
+      st.r[e] = t.rank[sp_find(t, ycol[b])];
+      st.v[e] = st.x[lo] * yval[b];
+    }
+    team_sync<TEAM>();
+    for (int u = 0; u < nfit; ++u) {
+      for (int e = st.off[u] + tid; e < st.off[u + 1]; e += TEAM) {
+        const int r = st.r[e];
+        const double v = st.v[e];
+        t.acc[r] = t.seen[r] ? t.acc[r] + v : v;
+        t.seen[r] = 1;
+      }
+      team_sync<TEAM>();
+    }
+    a0 += nfit;
+  }
+  for (int r = tid; r < U; r += TEAM) cval[base + r] = t.acc[r];
+  team_sync<TEAM>();
+}
+
+__global__ void k_sp_max_terms(int32_t n, const int32_t *__restrict__ xrow,
+                               const int32_t *__restrict__ xcol,
+                               const int32_t *__restrict__ yrow, unsigned long long *max_terms) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int64_t t = 0;
@@ -899,132 +1132,128 @@ __global__ void k_sp_terms(int32_t n, const int32_t *__restrict__ xrow,
     const int32_t k = xcol[a];
     t += yrow[k + 1] - yrow[k];
   }
-  tcount[i] = t < INT_MAX ? static_cast<int32_t>(t) : INT_MAX;
-  atomicAdd(total, static_cast<unsigned long long>(t));
-  atomicMax(total + 1, static_cast<unsigned long long>(t));
+  atomicMax(max_terms, static_cast<unsigned long long>(t));
 }
 
-template <int TEAM>
-__device__ int sp_gather(int32_t i, const int32_t *__restrict__ xrow,
-                         const int32_t *__restrict__ xcol, const double *__restrict__ xval,
-                         const int32_t *__restrict__ yrow, const int32_t *__restrict__ ycol,
-                         const double *__restrict__ yval, int32_t T, GalSmem sm, int cap,
-                         int tid) {
-  if (T > cap) return -1;
-  int base = 0;
-  for (int32_t a = xrow[i]; a < xrow[i + 1]; ++a) {
+// Symbolic pass, warp tier, every row: ucount[i] = U; rows over the warp
+// set go to `next` with tier[i] = 1.
+__global__ void __launch_bounds__(kSpWarpsPerBlock * 32)
+    k_sp_count_warp(int32_t n, const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
+                    const int32_t *__restrict__ yrow, const int32_t *__restrict__ ycol,
+                    int32_t *ucount, unsigned char *tier, int32_t *next, int32_t *n_next) {
+  extern __shared__ __align__(16) unsigned char sp_dyn[];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int32_t i = blockIdx.x * kSpWarpsPerBlock + wid;
+  if (i >= n) return;
+  const SpTable t = sp_table(sp_dyn + wid * sp_table_bytes(kSpWarpHash), kSpWarpHash);
+  const int U = sp_collect<32>(t, i, xrow, xcol, yrow, ycol, lane);
+  if (lane == 0) {
+    ucount[i] = U < 0 ? 0 : U;
+    tier[i] = U < 0 ? 1 : 0;
+    if (U < 0) next[atomicAdd(n_next, 1)] = i;
+  }
+}
+
+// Symbolic pass, block tiers, over rows[0..*n_rows): the table in shared
+// memory (gtab null, kSpBlockHash slots) or in this block's slice of gtab
+// (ghc slots, sized for every row).  Rows over the set go to `next` with
+// tier[i] = tier_here + 1, or raise err when there is no next tier.
+// A global table's size for one row: a power of two, at least 64, at least
+// twice `bound` (+2), at most ghc.
+__device__ __forceinline__ int sp_row_hc(int64_t bound, int ghc) {
+  int64_t c = 64;
+  while (c < 2 * bound + 2 && c < ghc) c <<= 1;
+  return static_cast<int>(c);
+}
+
+// Terms of row i of X Y (team-wide; ends synchronised).
+__device__ int64_t sp_row_terms(int32_t i, const int32_t *__restrict__ xrow,
+                                const int32_t *__restrict__ xcol,
+                                const int32_t *__restrict__ yrow, unsigned long long *acc) {
+  if (threadIdx.x == 0) *acc = 0;
+  __syncthreads();
+  unsigned long long t = 0;
+  for (int32_t a = xrow[i] + threadIdx.x; a < xrow[i + 1]; a += blockDim.x) {
     const int32_t k = xcol[a];
-    const double x = xval[a];
-    const int32_t b0 = yrow[k];
-    const int len = yrow[k + 1] - b0;
-    for (int t = tid; t < len; t += TEAM) {
-      const int pos = base + t;
-      sm.key[pos] = (static_cast<unsigned long long>(static_cast<uint32_t>(ycol[b0 + t])) << 32) |
-                    static_cast<uint32_t>(pos);
-      sm.tv[pos] = x * yval[b0 + t];
-    }
-    base += len;
+    t += static_cast<unsigned long long>(yrow[k + 1] - yrow[k]);
   }
-  int P2 = 1;
-  while (P2 < T) P2 <<= 1;
-  for (int t = T + tid; t < P2; t += TEAM) sm.key[t] = ~0ull;
-  team_sync<TEAM>();
-  for (int k = 2; k <= P2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int t = tid; t < P2 / 2; t += TEAM) {
-        const int i0 = ((t & ~(j - 1)) << 1) | (t & (j - 1));  // j = 2^m
-        const int i1 = i0 + j;
-        const bool asc = (i0 & k) == 0;
-        const unsigned long long a = sm.key[i0], b = sm.key[i1];
-        if ((a > b) == asc) {
-          sm.key[i0] = b;
-          sm.key[i1] = a;
-        }
-      }
-      team_sync<TEAM>();
-    }
-  }
+  atomicAdd(acc, t);
+  __syncthreads();
+  const int64_t T = static_cast<int64_t>(*acc);
+  __syncthreads();
   return T;
 }
 
-// Runs of the sorted row: (column, sum in generation order), one warp.
-__device__ void sp_emit(const GalSmem &sm, int T, int32_t i, int64_t base, int32_t *tJ,
-                        double *tV, int32_t *runs, int lane) {
-  int carry = 0;
-  for (int b0 = 0; b0 < T; b0 += 32) {
-    const int k = b0 + lane;
-    const bool h = k < T && gal_head(sm, k);
-    const unsigned hm = __ballot_sync(0xffffffffu, h);
-    if (h) {
-      const unsigned long long jj = sm.key[k] >> 32;
-      double s = sm.tv[static_cast<int>(sm.key[k] & 0xffffffffull)];
-      for (int q = k + 1; q < T && (sm.key[q] >> 32) == jj; ++q)
-        s = s + sm.tv[static_cast<int>(sm.key[q] & 0xffffffffull)];
-      const int64_t pos = base + carry + __popc(hm & ((1u << lane) - 1u));
-      tJ[pos] = static_cast<int32_t>(jj);
-      tV[pos] = s;
+__global__ void __launch_bounds__(kSpThreads)
+    k_sp_count_block(const int32_t *__restrict__ rows, const int32_t *__restrict__ n_rows,
+                     const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
+                     const int32_t *__restrict__ yrow, const int32_t *__restrict__ ycol,
+                     int32_t m, int32_t *ucount, unsigned char *tier, int32_t *next,
+                     int32_t *n_next, unsigned char *gtab, int ghc, int tier_here, int *err) {
+  extern __shared__ __align__(16) unsigned char sp_dyn[];
+  __shared__ unsigned long long terms;
+  for (int32_t q = blockIdx.x; q < *n_rows; q += gridDim.x) {
+    const int32_t i = rows[q];
+    SpTable t;
+    if (gtab) {
+      const int64_t T = sp_row_terms(i, xrow, xcol, yrow, &terms);
+      t = sp_table(gtab + blockIdx.x * sp_table_bytes(ghc), sp_row_hc(T < m ? T : m, ghc));
+    } else {
+      t = sp_table(sp_dyn, kSpBlockHash);
     }
-    carry += __popc(hm);
+    const int U = sp_collect<kSpThreads>(t, i, xrow, xcol, yrow, ycol, threadIdx.x);
+    if (threadIdx.x == 0) {
+      ucount[i] = U < 0 ? 0 : U;
+      if (U < 0) {
+        if (next) {
+          tier[i] = static_cast<unsigned char>(tier_here + 1);
+          next[atomicAdd(n_next, 1)] = i;
+        } else {
+          atomicExch(err, 1);
+        }
+      }
+    }
   }
-  if (lane == 0) runs[i] = carry;
 }
 
-__global__ void __launch_bounds__(kGalWarpsPerBlock * 32)
-    k_sp_rows(int32_t n, const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
-              const double *__restrict__ xval, const int32_t *__restrict__ yrow,
-              const int32_t *__restrict__ ycol, const double *__restrict__ yval,
-              const int32_t *__restrict__ tpos, const int32_t *__restrict__ tcount,
-              int32_t *tJ, double *tV, int32_t *runs, int32_t *long_rows, int32_t *n_long) {
-  extern __shared__ __align__(16) unsigned char gal_dyn[];
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int32_t i = blockIdx.x * kGalWarpsPerBlock + wid;
-  if (i >= n) return;
-  GalSmem sm = gal_smem(gal_dyn + static_cast<size_t>(wid) * kGalCap * kGalBytesPerTerm,
-                        kGalCap);
-  const int T = sp_gather<32>(i, xrow, xcol, xval, yrow, ycol, yval, tcount[i], sm, kGalCap,
-                              lane);
-  if (T < 0) {
-    if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
-    return;
-  }
-  sp_emit(sm, T, i, tpos[i], tJ, tV, runs, lane);
-}
-
-// Rows over kGalCap terms, one block each: in shared memory up to
-// kGalCapLong terms, beyond that in this block's slice of a global scratch
-// (huge_cap keys and values per block; the same sort, ordered by
-// __syncthreads).
-__global__ void __launch_bounds__(kGalLongThreads)
-    k_sp_rows_long(const int32_t *__restrict__ long_rows, const int32_t *__restrict__ n_long,
-                   const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
+// Numeric pass, warp tier (rows with tier 0).
+__global__ void __launch_bounds__(kSpWarpsPerBlock * 32)
+    k_sp_fill_warp(int32_t n, const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
                    const double *__restrict__ xval, const int32_t *__restrict__ yrow,
                    const int32_t *__restrict__ ycol, const double *__restrict__ yval,
-                   const int32_t *__restrict__ tpos, const int32_t *__restrict__ tcount,
-                   int32_t *tJ, double *tV, int32_t *runs, unsigned long long *huge_key,
-                   double *huge_val, int huge_cap, int *err) {
-  extern __shared__ __align__(16) unsigned char gal_dyn[];
-  const GalSmem sm = gal_smem(gal_dyn, kGalCapLong);
-  GalSmem gm = sm;
-  if (huge_key) {
-    gm.key = huge_key + static_cast<size_t>(blockIdx.x) * huge_cap;
-    gm.tv = huge_val + static_cast<size_t>(blockIdx.x) * huge_cap;
-  }
-  for (int32_t q = blockIdx.x; q < *n_long; q += gridDim.x) {
-    const int32_t i = long_rows[q];
-    const bool huge = tcount[i] > kGalCapLong;
-    if (huge && !huge_key) {
-      if (threadIdx.x == 0) atomicExch(err, 3);
-      return;
-    }
-    const GalSmem &w = huge ? gm : sm;
-    const int T = sp_gather<kGalLongThreads>(i, xrow, xcol, xval, yrow, ycol, yval, tcount[i],
-                                             w, huge ? huge_cap : kGalCapLong, threadIdx.x);
-    if (T < 0) {
-      if (threadIdx.x == 0) atomicExch(err, 3);
-      return;
-    }
-    if (threadIdx.x < 32) sp_emit(w, T, i, tpos[i], tJ, tV, runs, threadIdx.x);
-    __syncthreads();
+                   const unsigned char *__restrict__ tier, const int32_t *__restrict__ crow,
+                   int32_t *ccol, double *cval) {
+  extern __shared__ __align__(16) unsigned char sp_dyn[];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int32_t i = blockIdx.x * kSpWarpsPerBlock + wid;
+  if (i >= n || tier[i] != 0) return;
+  unsigned char *mine = sp_dyn + wid * (sp_table_bytes(kSpWarpHash) + kSpStageWarpBytes);
+  const SpTable t = sp_table(mine, kSpWarpHash);
+  SpStageWarp &st = *reinterpret_cast<SpStageWarp *>(mine + sp_table_bytes(kSpWarpHash));
+  const int U = sp_collect<32>(t, i, xrow, xcol, yrow, ycol, lane);
+  sp_numeric<32>(t, st, i, U, xrow, xcol, xval, yrow, ycol, yval, crow[i], ccol, cval, lane);
+}
+
+// Numeric pass, block tiers: rows of rows[0..*n_rows) with tier[i] ==
+// tier_here, tables as in k_sp_count_block.
+__global__ void __launch_bounds__(kSpThreads)
+    k_sp_fill_block(const int32_t *__restrict__ rows, const int32_t *__restrict__ n_rows,
+                    const int32_t *__restrict__ xrow, const int32_t *__restrict__ xcol,
+                    const double *__restrict__ xval, const int32_t *__restrict__ yrow,
+                    const int32_t *__restrict__ ycol, const double *__restrict__ yval,
+                    const unsigned char *__restrict__ tier, const int32_t *__restrict__ crow,
+                    int32_t *ccol, double *cval, unsigned char *gtab, int ghc, int tier_here) {
+  extern __shared__ __align__(16) unsigned char sp_dyn[];
+  SpStageBlock &st = *reinterpret_cast<SpStageBlock *>(sp_dyn);
+  for (int32_t q = blockIdx.x; q < *n_rows; q += gridDim.x) {
+    const int32_t i = rows[q];
+    if (tier[i] != tier_here) continue;
+    const SpTable t =
+        gtab ? sp_table(gtab + blockIdx.x * sp_table_bytes(ghc), sp_row_hc(crow[i + 1] - crow[i], ghc))
+             : sp_table(sp_dyn + kSpStageBlockBytes, kSpBlockHash);
+    const int U = sp_collect<kSpThreads>(t, i, xrow, xcol, yrow, ycol, threadIdx.x);
+    sp_numeric<kSpThreads>(t, st, i, U, xrow, xcol, xval, yrow, ycol, yval, crow[i], ccol, cval,
+                           threadIdx.x);
   }
 }
 
@@ -1057,22 +1286,75 @@ __global__ void k_tr_fill(int32_t n, const int32_t *__restrict__ row,
   }
 }
 
-__global__ void k_tr_sort(int32_t m, const int32_t *__restrict__ trow, int32_t *tcol,
-                          double *tval) {
-  const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= m) return;
-  const int32_t b = trow[r], e = trow[r + 1];
-  for (int32_t k = b + 1; k < e; ++k) {
-    const int32_t c = tcol[k];
-    const double v = tval[k];
-    int32_t j = k - 1;
-    while (j >= b && tcol[j] > c) {
-      tcol[j + 1] = tcol[j];
-      tval[j + 1] = tval[j];
-      --j;
+// Sorts key[0..n) ascending with its payload, team-wide: a bitonic network
+// whose comparators all point up (each merge starts by comparing mirrored
+// positions), so positions n..P2 act as +infinity and are never touched.
+template <int TEAM>
+__device__ void sort_up_pairs(int32_t *key, double *val, int n, int tid) {
+  int P2 = 1;
+  while (P2 < n) P2 <<= 1;
+  for (int k = 2; k <= P2; k <<= 1) {
+    const int h = k >> 1;
+    for (int t = tid; t < P2 / 2; t += TEAM) {
+      const int i = (t / h) * k + (t % h);
+      const int j = i ^ (k - 1);
+      if (j < n && key[i] > key[j]) {
+        const int32_t tk = key[i];
+        key[i] = key[j];
+        key[j] = tk;
+        const double tv = val[i];
+        val[i] = val[j];
+        val[j] = tv;
+      }
     }
-    tcol[j + 1] = c;
-    tval[j + 1] = v;
+    team_sync<TEAM>();
+    for (int d = k >> 2; d > 0; d >>= 1) {
+      for (int t = tid; t < P2 / 2; t += TEAM) {
+        const int i = (t / d) * 2 * d + (t % d);
+        const int j = i + d;
+        if (j < n && key[i] > key[j]) {
+          const int32_t tk = key[i];
+          key[i] = key[j];
+          key[j] = tk;
+          const double tv = val[i];
+          val[i] = val[j];
+          val[j] = tv;
+        }
+      }
+      team_sync<TEAM>();
+    }
+  }
+}
+
+constexpr int kTrThreads = 256;
+constexpr int kTrSmem = 8192;  // rows up to this length sort in shared memory
+
+// Sorts every row of the transpose by column (= source row), a block per
+// row: in shared memory up to kTrSmem entries, in place beyond.
+__global__ void __launch_bounds__(kTrThreads)
+    k_tr_sort(int32_t m, const int32_t *__restrict__ trow, int32_t *tcol, double *tval) {
+  extern __shared__ __align__(16) unsigned char tr_dyn[];
+  double *sv = reinterpret_cast<double *>(tr_dyn);
+  int32_t *sk = reinterpret_cast<int32_t *>(tr_dyn + sizeof(double) * kTrSmem);
+  for (int32_t r = blockIdx.x; r < m; r += gridDim.x) {
+    const int32_t b = trow[r];
+    const int len = trow[r + 1] - b;
+    if (len <= 1) continue;
+    if (len <= kTrSmem) {
+      for (int q = threadIdx.x; q < len; q += kTrThreads) {
+        sk[q] = tcol[b + q];
+        sv[q] = tval[b + q];
+      }
+      __syncthreads();
+      sort_up_pairs<kTrThreads>(sk, sv, len, threadIdx.x);
+      for (int q = threadIdx.x; q < len; q += kTrThreads) {
+        tcol[b + q] = sk[q];
+        tval[b + q] = sv[q];
+      }
+      __syncthreads();
+    } else {
+      sort_up_pairs<kTrThreads>(tcol + b, tval + b, len, threadIdx.x);
+    }
   }
 }
 
@@ -1412,75 +1694,99 @@ bcmg_status spgemm(const CsrView &X, const CsrView &Y, int32_t m, int32_t *crow,
   *cnnz = 0;
   const int32_t n = X.n;
   if (n <= 0) return BCMG_OK;
-  (void)m;
-  DevBuf<int32_t> tcount, tpos, tJ, long_rows, n_long, tmp;
-  DevBuf<double> tV;
+  DevBuf<int32_t> list1, list2, counts, tmp;
+  DevBuf<unsigned char> tier;
   DevBuf<int> err;
-  BCMG_TRY(tcount.alloc(n, s));
-  BCMG_TRY(tpos.alloc(n + 1, s));
-  BCMG_TRY(long_rows.alloc(n, s));
-  BCMG_TRY(n_long.alloc(1, s));
+  BCMG_TRY(list1.alloc(n, s));
+  BCMG_TRY(list2.alloc(n, s));
+  BCMG_TRY(counts.alloc(2, s));  // rows in tier 1, tier 2
+  BCMG_TRY(tier.alloc(n, s));
   BCMG_TRY(err.alloc(1, s));
   BCMG_TRY(tmp.alloc(scan_tmp_size(n), s));
-  DevBuf<unsigned long long> total;
-  BCMG_TRY(total.alloc(2, s));
-  BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
+  BCMG_CUDA(cudaMemsetAsync(counts.get(), 0, 2 * sizeof(int32_t), s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
-  BCMG_CUDA(cudaMemsetAsync(total.get(), 0, 2 * sizeof(unsigned long long), s));
-  launch(k_sp_terms, ceil_div(n, 256), 256, 0, s, n, X.row, X.col, Y.row, tcount.get(),
-         total.get());
-  unsigned long long h_total[2] = {0, 0};
-  BCMG_CUDA(cudaMemcpyAsync(h_total, total.get(), sizeof(h_total), cudaMemcpyDeviceToHost, s));
-  BCMG_CUDA(cudaStreamSynchronize(s));
-  if (h_total[0] > static_cast<unsigned long long>(INT_MAX))
-    return set_error(BCMG_ERR_UNSUPPORTED, "sparse product has %llu terms (limit %d)",
-                     h_total[0], INT_MAX);
-  const int32_t terms = static_cast<int32_t>(h_total[0]);
-  // Rows over kGalCapLong terms sort in a global scratch of huge_cap (a power
-  // of two) keys and values per block, at most kHugeScratchBytes in all.
-  constexpr int64_t kHugeScratchBytes = int64_t(1) << 30;
-  int huge_cap = 0, long_grid = std::min(n, kNumSM);
-  DevBuf<unsigned long long> huge_key;
-  DevBuf<double> huge_val;
-  if (h_total[1] > static_cast<unsigned long long>(kGalCapLong)) {
-    int64_t c = 1;
-    while (c < static_cast<int64_t>(h_total[1])) c <<= 1;
-    if (c * 16 > kHugeScratchBytes)
-      return set_error(BCMG_ERR_UNSUPPORTED, "a sparse-product row has %llu terms",
-                       h_total[1]);
-    huge_cap = static_cast<int>(c);
-    long_grid = static_cast<int>(std::min<int64_t>(long_grid, kHugeScratchBytes / (c * 16)));
-    BCMG_TRY(huge_key.alloc(static_cast<int64_t>(long_grid) * huge_cap, s));
-    BCMG_TRY(huge_val.alloc(static_cast<int64_t>(long_grid) * huge_cap, s));
-  }
-  BCMG_TRY(exclusive_scan(tcount.get(), tpos.get(), n, nullptr, tmp.get(), s));
-  BCMG_TRY(tJ.alloc(std::max<int32_t>(terms, 1), s));
-  BCMG_TRY(tV.alloc(std::max<int32_t>(terms, 1), s));
-  const size_t smem_warp = static_cast<size_t>(kGalWarpsPerBlock) * kGalCap * kGalBytesPerTerm;
-  const size_t smem_long = static_cast<size_t>(kGalCapLong) * kGalBytesPerTerm;
-  BCMG_CUDA(cudaFuncSetAttribute(k_sp_rows_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem_long)));
-  launch(k_sp_rows, ceil_div(n, kGalWarpsPerBlock), kGalWarpsPerBlock * 32, smem_warp, s, n,
-         X.row, X.col, X.val, Y.row, Y.col, Y.val, tpos.get(), tcount.get(), tJ.get(), tV.get(),
-         crow, long_rows.get(), n_long.get());
-  launch(k_sp_rows_long, long_grid, kGalLongThreads, smem_long, s, long_rows.get(),
-         n_long.get(), X.row, X.col, X.val, Y.row, Y.col, Y.val, tpos.get(), tcount.get(),
-         tJ.get(), tV.get(), crow, huge_key.get(), huge_val.get(), huge_cap, err.get());
+  const size_t smem_warp = kSpWarpsPerBlock * sp_table_bytes(kSpWarpHash);
+  const size_t smem_warp_fill =
+      kSpWarpsPerBlock * (sp_table_bytes(kSpWarpHash) + kSpStageWarpBytes);
+  const size_t smem_block = sp_table_bytes(kSpBlockHash);
+  const size_t smem_block_fill = kSpStageBlockBytes + sp_table_bytes(kSpBlockHash);
+  BCMG_CUDA(cudaFuncSetAttribute(k_sp_count_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem_warp)));
+  BCMG_CUDA(cudaFuncSetAttribute(k_sp_fill_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem_warp_fill)));
+  BCMG_CUDA(cudaFuncSetAttribute(k_sp_count_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem_block)));
+  BCMG_CUDA(cudaFuncSetAttribute(k_sp_fill_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem_block_fill)));
+  const int warp_grid = ceil_div(n, kSpWarpsPerBlock);
+  const int block_grid = std::min(n, 2 * kNumSM);  // two blocks per SM
+  launch(k_sp_count_warp, warp_grid, kSpWarpsPerBlock * 32, smem_warp, s, n, X.row, X.col,
+         Y.row, Y.col, crow, tier.get(), list1.get(), counts.get());
+  phase_tick("sp count warp");
+  launch(k_sp_count_block, block_grid, kSpThreads, smem_block, s, list1.get(), counts.get(),
+         X.row, X.col, Y.row, Y.col, m, crow, tier.get(), list2.get(), counts.get() + 1,
+         static_cast<unsigned char *>(nullptr), 0, 1, err.get());
   BCMG_LAUNCH_CHECK();
+  int32_t h_counts[2] = {0, 0};
+  BCMG_CUDA(cudaMemcpyAsync(h_counts, counts.get(), sizeof(h_counts), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  phase_tick("sp count block");
+  // Tier 2: a table of ghc slots per block in global memory, ghc a power of
+  // two at least twice the row bound min(terms, m), at most 1 GiB in all.
+  DevBuf<unsigned char> gtab;
+  int ghc = 0, g_grid = 0;
+  if (h_counts[1] > 0) {
+    DevBuf<unsigned long long> maxt;
+    BCMG_TRY(maxt.alloc(1, s));
+    BCMG_CUDA(cudaMemsetAsync(maxt.get(), 0, sizeof(unsigned long long), s));
+    launch(k_sp_max_terms, ceil_div(n, 256), 256, 0, s, n, X.row, X.col, Y.row, maxt.get());
+    unsigned long long h_maxt = 0;
+    BCMG_CUDA(cudaMemcpyAsync(&h_maxt, maxt.get(), sizeof(h_maxt), cudaMemcpyDeviceToHost, s));
+    BCMG_CUDA(cudaStreamSynchronize(s));
+    const int64_t bound = std::min<int64_t>(static_cast<int64_t>(h_maxt), m);
+    int64_t c = kSpBlockHash;
+    while (c < 2 * bound + 2) c <<= 1;
+    constexpr int64_t kTableBudget = int64_t(1) << 30;
+    const int64_t per = static_cast<int64_t>(sp_table_bytes(static_cast<int>(
+        std::min<int64_t>(c, int64_t(1) << 30))));
+    if (c > (int64_t(1) << 26) || per > kTableBudget)
+      return set_error(BCMG_ERR_UNSUPPORTED, "sparse product: a row with %lld columns",
+                       static_cast<long long>(bound));
+    ghc = static_cast<int>(c);
+    const int64_t fit = std::min<int64_t>(kTableBudget / per, std::min(h_counts[1], 4 * kNumSM));
+    g_grid = static_cast<int>(std::max<int64_t>(1, fit));
+    BCMG_TRY(gtab.alloc(per * g_grid, s));
+    launch(k_sp_count_block, g_grid, kSpThreads, 0, s, list2.get(), counts.get() + 1, X.row,
+           X.col, Y.row, Y.col, m, crow, tier.get(), static_cast<int32_t *>(nullptr),
+           static_cast<int32_t *>(nullptr), gtab.get(), ghc, 2, err.get());
+    phase_tick("sp count global");
+  }
   BCMG_TRY(exclusive_scan(crow, crow, n, crow + n, tmp.get(), s));
   int h_err = 0;
   int32_t h_nnz = 0;
   BCMG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaMemcpyAsync(&h_nnz, crow + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   BCMG_CUDA(cudaStreamSynchronize(s));
-  if (h_err) return set_error(BCMG_ERR_INTERNAL, "sparse product: row over its term capacity");
+  if (h_err) return set_error(BCMG_ERR_INTERNAL, "sparse product: row over its table");
+  if (h_nnz < 0) return set_error(BCMG_ERR_UNSUPPORTED, "sparse product over 2^31 entries");
   DevBuf<int32_t> ccol;
   DevBuf<double> cval;
   BCMG_TRY(ccol.alloc(std::max<int32_t>(h_nnz, 1), s));
   BCMG_TRY(cval.alloc(std::max<int32_t>(h_nnz, 1), s));
-  launch(k_gal_compact, ceil_div(static_cast<int64_t>(n) * 32, 256), 256, 0, s, n, tpos.get(),
-         crow, tJ.get(), tV.get(), ccol.get(), cval.get());
+  launch(k_sp_fill_warp, warp_grid, kSpWarpsPerBlock * 32, smem_warp_fill, s, n, X.row, X.col,
+         X.val, Y.row, Y.col, Y.val, tier.get(), crow, ccol.get(), cval.get());
+  phase_tick("sp fill warp");
+  if (h_counts[0] > 0)
+    launch(k_sp_fill_block, block_grid, kSpThreads, smem_block_fill, s, list1.get(), counts.get(),
+           X.row, X.col, X.val, Y.row, Y.col, Y.val, tier.get(), crow, ccol.get(), cval.get(),
+           static_cast<unsigned char *>(nullptr), 0, 1);
+  phase_tick("sp fill block");
+  if (h_counts[1] > 0)
+    launch(k_sp_fill_block, g_grid, kSpThreads, kSpStageBlockBytes, s, list2.get(), counts.get() + 1, X.row,
+           X.col, X.val, Y.row, Y.col, Y.val, tier.get(), crow, ccol.get(), cval.get(),
+           gtab.get(), ghc, 2);
   BCMG_LAUNCH_CHECK();
+  phase_tick("sp fill global");
   *cnnz = h_nnz;
   *ccol_out = ccol.release();
   *cval_out = cval.release();
@@ -1502,7 +1808,11 @@ bcmg_status csr_transpose(const CsrView &A, int32_t m, int32_t *trow, int32_t *t
   BCMG_TRY(exclusive_scan(trow, trow, m, trow + m, tmp.get(), s));
   launch(k_tr_fill, ceil_div(A.n, 256), 256, 0, s, A.n, A.row, A.col, A.val, m, trow,
          cursor.get(), tcol, tval);
-  launch(k_tr_sort, ceil_div(m, 256), 256, 0, s, m, trow, tcol, tval);
+  const size_t tr_smem = static_cast<size_t>(kTrSmem) * (sizeof(double) + sizeof(int32_t));
+  BCMG_CUDA(cudaFuncSetAttribute(k_tr_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tr_smem)));
+  if (m > 0)
+    launch(k_tr_sort, std::min(m, 2 * kNumSM), kTrThreads, tr_smem, s, m, trow, tcol, tval);
   BCMG_LAUNCH_CHECK();
   int h_err = 0;
   BCMG_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
