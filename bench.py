@@ -603,6 +603,25 @@ def run_batch(args):
         torch.cuda.synchronize(dev)
         single.append((g0.elapsed_time(g1), si.iters))
     cfg = [h.batch_config(nrhs, 0, l) for l in range(h.hierarchy_info(0)["num_levels"])]
+    # The plain FP64 path (FP64 hierarchy and cycle, no value narrowing), one
+    # column at a time on its own handle: the denominator of the batching and
+    # mixed-precision gain.
+    ext64 = bc.Extensions(precision=bc.PREC_FP64, narrow_values=0, device=local,
+                          stream=stream.cuda_stream)
+    h64 = bc.Handle.from_device(A.n, A.nnz, row.data_ptr(), col.data_ptr(), val.data_ptr(), p,
+                                ext64)
+    fp64_single = []
+    for j in range(4):
+        with torch.cuda.stream(stream):
+            xs.zero_()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        si = h64.solve_device(Bd[j].data_ptr(), xs.data_ptr())
+        g1.record(stream)
+        torch.cuda.synchronize(dev)
+        fp64_single.append((g0.elapsed_time(g1), si.iters))
+    h64.close()
+    fp64_ms = float(np.median([t for t, _ in fp64_single[1:]]))
     # Roofline: the level-0 batched smoother sweep on 32 interleaved columns.
     W = cfg[0]["width"]
     xdt, xbytes = (torch.float32, 4) if prec == bc.PREC_MIXED else (torch.float64, 8)
@@ -714,6 +733,11 @@ def run_batch(args):
                    "single_rhs_solve_ms_median": single_ms,
                    "single_rhs_solves_per_s": 1e3 / single_ms,
                    "single_rhs_iters": [it for _, it in single],
+                   "fp64_single_rhs_solve_ms_median": fp64_ms,
+                   "fp64_single_rhs_solves_per_s": 1e3 / fp64_ms,
+                   "fp64_single_rhs_iters": [it for _, it in fp64_single],
+                   "batched_mixed_over_fp64_single": (nrhs / (batch_solve_ms / 1e3))
+                   / (1e3 / fp64_ms),
                    "max_true_rel_residual": true_rel, "shapes": cfg,
                    "e2e_steps": e2e_steps},
     }
@@ -721,7 +745,8 @@ def run_batch(args):
     log(f"[bench] {args.workload} {args.precision}: {value:.1f} solves/s "
         f"({ms_max / args.steps:.1f} ms per {nrhs}-column step), solve-only "
         f"{nrhs / (batch_solve_ms / 1e3):.1f} solves/s vs one-at-a-time "
-        f"{1e3 / single_ms:.1f}; sweep {achieved:.0f} GB/s ({achieved / peak:.2f})")
+        f"{1e3 / single_ms:.1f} (plain FP64 {1e3 / fp64_ms:.1f}); sweep {achieved:.0f} GB/s "
+        f"({achieved / peak:.2f})")
     return 0
 
 

@@ -226,6 +226,18 @@ bool pick(bcmg_server *s, Job *job, std::vector<bcmg_handle *> &victims) {
   return false;
 }
 
+// Destroys evicted hierarchies on the calling worker's stream.  A handle
+// keeps the stream of the worker that ran it last (its runs end with a
+// stream synchronize); freeing on that stream could put the frees inside
+// another worker's graph capture on it.
+void destroy_victims(std::vector<bcmg_handle *> &victims, cudaStream_t stream) {
+  for (bcmg_handle *v : victims) {
+    v->stream = stream;
+    bcmg_destroy(v);
+  }
+  victims.clear();
+}
+
 // Runs one job on the worker's stream (no lock held).
 void run_job(bcmg_server *s, Job &job, cudaStream_t stream, bcmg_handle **hp) {
   const auto t0 = Clock::now();
@@ -293,8 +305,7 @@ void worker_main(bcmg_server *s, int slot) {
         if (!victims.empty()) {
           // Free evicted hierarchies before waiting again.
           lk.unlock();
-          for (bcmg_handle *v : victims) bcmg_destroy(v);
-          victims.clear();
+          destroy_victims(victims, stream);
           lk.lock();
           continue;
         }
@@ -302,13 +313,12 @@ void worker_main(bcmg_server *s, int slot) {
       }
       if (job.group.empty()) {
         lk.unlock();
-        for (bcmg_handle *v : victims) bcmg_destroy(v);
+        destroy_victims(victims, stream);
         return;
       }
       if (!job.fresh) h = s->cache[job.key].h;
     }
-    for (bcmg_handle *v : victims) bcmg_destroy(v);
-    victims.clear();
+    destroy_victims(victims, stream);
     run_job(s, job, stream, &h);
     const size_t bytes = h ? handle_bytes(h) : 0;
     {
@@ -356,7 +366,7 @@ void worker_main(bcmg_server *s, int slot) {
       s->cv_done.notify_all();
       s->cv_work.notify_all();
     }
-    for (bcmg_handle *v : victims) bcmg_destroy(v);
+    destroy_victims(victims, stream);
   }
 }
 

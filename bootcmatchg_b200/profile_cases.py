@@ -13,6 +13,8 @@ CASE:
                 plain launch a profiler can see)
   batch_solve   one 32-column batched solve of 7-point Poisson 96^3 (mixed),
                 FCG loop driven from the host
+  setup         one FP64 setup of 27-point Poisson GRID^3 (--grid, default
+                96): matching, aggregation and Galerkin kernels
 
 Each case sets up its hierarchy first and then runs the kernels of interest;
 the kernel names to filter on are k_sl_relax, k_bt_rowop and so on.
@@ -88,11 +90,19 @@ def batch_solve() -> None:
           f"{all(i.converged for i in infos)} solve {infos[0].solve_ms:.1f} ms")
 
 
+def setup(grid: int) -> None:
+    A = bc.poisson(27, grid, grid, grid)
+    with bc.Handle(A, c1_params(), bc.Extensions(precision=bc.PREC_FP64)) as h:
+        info = h.hierarchy_info(0)
+    print(f"levels {info['num_levels']} op_cmplx {info['op_cmplx']:.3f}")
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="profiling workloads")
     ap.add_argument("case", choices=["sweep_fp32", "sweep_fp64", "batch_fp32", "solve_mixed",
-                                     "batch_solve"])
+                                     "batch_solve", "setup"])
     ap.add_argument("--sweeps", type=int, default=3)
+    ap.add_argument("--grid", type=int, default=96)
     a = ap.parse_args(argv)
     if a.case == "sweep_fp32":
         sweeps(bc.PREC_MIXED, a.sweeps)
@@ -102,6 +112,8 @@ def main(argv=None) -> int:
         batch_sweeps(a.sweeps)
     elif a.case == "solve_mixed":
         solve_mixed()
+    elif a.case == "setup":
+        setup(a.grid)
     else:
         batch_solve()
     return 0
