@@ -620,7 +620,11 @@ bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaSt
       launch(kern, cfg.grid, kPipeThreads, cfg.smem, st, S, static_cast<const VT *>(S.val), \
              x, epi, S.cap_slots, S.cols_staged);                                           \
   } while (0)
-  if (S.batch <= 8) BCMG_PIPE_KB(8);
+  // Gathers per batch matched to the mean slice width: 5-point (2-D) and
+  // 7-point (3-D) stencils issue no padding gathers.
+  if (S.batch <= 5) BCMG_PIPE_KB(5);
+  else if (S.batch <= 7) BCMG_PIPE_KB(7);
+  else if (S.batch <= 8) BCMG_PIPE_KB(8);
   else if (S.batch <= 16) BCMG_PIPE_KB(16);
   else BCMG_PIPE_KB(28);
 #undef BCMG_PIPE_KB

@@ -6,11 +6,13 @@ CASE:
   sweep_fp32    level-0 smoother sweeps of 27-point Poisson 128^3, mixed
                 precision (FP32 sliced values)
   sweep_fp64    the same in FP64
+  sweep_fv2d    level-0 smoother sweeps of the 2-D FV 2048^2 matrix (5-point),
+                mixed precision
   batch_fp32    batched smoother sweeps of 7-point Poisson 96^3 on 32
                 interleaved columns (FP32), autotuning off
-  solve_mixed   one complete mixed-precision solve of 27-point Poisson 128^3
-                with the FCG loop driven from the host (every kernel is a
-                plain launch a profiler can see)
+  solve_mixed   one complete mixed-precision solve of 27-point Poisson
+                GRID^3 (--grid, default 128) with the FCG loop driven from the
+                host (every kernel is a plain launch a profiler can see)
   batch_solve   one 32-column batched solve of 7-point Poisson 96^3 (mixed),
                 FCG loop driven from the host
   setup         one FP64 setup of 27-point Poisson GRID^3 (--grid, default
@@ -42,9 +44,9 @@ def c1_params() -> bc.Params:
     return p
 
 
-def sweeps(prec: int, k: int) -> None:
+def sweeps(prec: int, k: int, fv2d: bool = False) -> None:
     import torch
-    A = bc.poisson(27, 128, 128, 128)
+    A = bc.fv2d(2048, 2048, seed=2) if fv2d else bc.poisson(27, 128, 128, 128)
     dt = torch.float32 if prec == bc.PREC_MIXED else torch.float64
     with bc.Handle(A, c1_params(), bc.Extensions(precision=prec, replace_every=10)) as h:
         f = torch.randn(A.n, dtype=dt, device="cuda:0")
@@ -70,8 +72,8 @@ def batch_sweeps(k: int) -> None:
         print(f"{k} batched sweeps: {1e3 * (time.perf_counter() - t0):.3f} ms")
 
 
-def solve_mixed() -> None:
-    A = bc.poisson(27, 128, 128, 128)
+def solve_mixed(grid: int = 128) -> None:
+    A = bc.poisson(27, grid, grid, grid)
     b = bc.vector(1, 1, A.n)
     ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=10, use_graphs=0)
     with bc.Handle(A, c1_params(), ext) as h:
@@ -99,21 +101,25 @@ def setup(grid: int) -> None:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="profiling workloads")
-    ap.add_argument("case", choices=["sweep_fp32", "sweep_fp64", "batch_fp32", "solve_mixed",
+    ap.add_argument("case", choices=["sweep_fp32", "sweep_fp64", "sweep_fv2d", "batch_fp32",
+                                     "solve_mixed",
                                      "batch_solve", "setup"])
     ap.add_argument("--sweeps", type=int, default=3)
-    ap.add_argument("--grid", type=int, default=96)
+    ap.add_argument("--grid", type=int, default=None,
+                    help="grid side for setup (default 96) and solve_mixed (default 128)")
     a = ap.parse_args(argv)
     if a.case == "sweep_fp32":
         sweeps(bc.PREC_MIXED, a.sweeps)
     elif a.case == "sweep_fp64":
         sweeps(bc.PREC_FP64, a.sweeps)
+    elif a.case == "sweep_fv2d":
+        sweeps(bc.PREC_MIXED, a.sweeps, fv2d=True)
     elif a.case == "batch_fp32":
         batch_sweeps(a.sweeps)
     elif a.case == "solve_mixed":
-        solve_mixed()
+        solve_mixed(a.grid or 128)
     elif a.case == "setup":
-        setup(a.grid)
+        setup(a.grid or 96)
     else:
         batch_solve()
     return 0
