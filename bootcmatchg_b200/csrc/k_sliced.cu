@@ -78,9 +78,10 @@ __device__ __forceinline__ __half narrow<__half>(double v) { return __double2hal
 
 // Pass 1: per slice, the longest row and the size of the union of column
 // offsets (merging the 32 sorted rows); chooses the slice kind and width.
+// Also widens offrange[0..1] (min, max) to every offset of an offset slice.
 __global__ void k_slice_shape(int32_t n, int32_t nslices, const int32_t *__restrict__ row,
                               const int32_t *__restrict__ col, int32_t *width,
-                              int32_t *kind) {
+                              int32_t *kind, int32_t *offrange) {
   const int lane = threadIdx.x & 31;
   const int32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   if (s >= nslices) return;
@@ -97,12 +98,15 @@ __global__ void k_slice_shape(int32_t n, int32_t nslices, const int32_t *__restr
   // Merge the sorted offset lists; count distinct offsets up to the cap.
   int32_t pos = b;
   int distinct = 0;
+  int32_t lo = 0, hi = 0;  // smallest and largest offset
   while (distinct <= kMaxOffsetSlots) {
     const int32_t cur = pos < e ? col[pos] - r : INT_MAX;
     int32_t m = cur;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
     if (m == INT_MAX) break;
+    if (distinct == 0) lo = m;
+    hi = m;
     ++distinct;
     if (cur == m) ++pos;
   }
@@ -110,6 +114,10 @@ __global__ void k_slice_shape(int32_t n, int32_t nslices, const int32_t *__restr
     const bool offsets = distinct <= kMaxOffsetSlots && distinct <= maxlen + maxlen / 4 + 2;
     kind[s] = offsets ? 1 : 0;
     width[s] = offsets ? distinct : maxlen;
+    if (offsets && distinct > 0) {
+      atomicMin(offrange, lo);
+      atomicMax(offrange + 1, hi);
+    }
   }
 }
 
@@ -216,16 +224,24 @@ __global__ void k_slice_heads(int32_t nslices, const int32_t *__restrict__ flag,
   if (s < nslices && flag[s]) head[rid[s]] = s;
 }
 
-__global__ void k_slice_meta(int32_t nslices, const int32_t *__restrict__ sptr,
+// meta.z: 0 column slice, 1 offset slice, 2 interior offset slice — every
+// row r of the slice is below n and r + o stays in [0, n) for every offset o
+// in offrange, which bounds every entry of soff (offsets of offset slices,
+// zeros elsewhere), so its gathers need no clamping.
+__global__ void k_slice_meta(int32_t n, int32_t nslices, const int32_t *__restrict__ sptr,
                              const int32_t *__restrict__ width,
                              const int32_t *__restrict__ kind,
                              const int32_t *__restrict__ flag,
                              const int32_t *__restrict__ rid,
-                             const int32_t *__restrict__ head, int4 *meta) {
+                             const int32_t *__restrict__ head,
+                             const int32_t *__restrict__ offrange, int4 *meta) {
   const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslices) return;
   const int32_t h = head[rid[s] + flag[s] - 1];
-  meta[s] = make_int4(sptr[s], width[s], kind[s], sptr[h]);
+  const int64_t r0 = static_cast<int64_t>(s) * 32, r1 = r0 + 31;
+  const bool interior =
+      kind[s] == 1 && r1 < n && r0 + offrange[0] >= 0 && r1 + offrange[1] < n;
+  meta[s] = make_int4(sptr[s], width[s], interior ? 2 : kind[s], sptr[h]);
 }
 
 // ---- pipeline primitives (mbarrier + bulk async copy) ---------------------
@@ -306,7 +322,7 @@ __device__ __forceinline__ double gather(const double *x, int32_t i) {
 template <typename VT, typename XT, int KB>
 __device__ __forceinline__ XT slice_row_sum(const VT *v, const int32_t *cidx,
                                             const int32_t *off, int W, int32_t r, int32_t hi,
-                                            const XT *__restrict__ x) {
+                                            bool interior, const XT *__restrict__ x) {
   const int lane = threadIdx.x & 31;
   XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
   for (int k = 0; k < W; k += KB) {
@@ -314,6 +330,10 @@ __device__ __forceinline__ XT slice_row_sum(const VT *v, const int32_t *cidx,
     if (cidx) {
 #pragma unroll
       for (int q = 0; q < KB; ++q) xv[q] = gather(x, min(max(cidx[(k + q) * 32], 0), hi));
+    } else if (KB <= 8 && interior) {  // narrow stencils are issue-bound
+      const int32_t offl = __ldg(off + k + lane);
+#pragma unroll
+      for (int q = 0; q < KB; ++q) xv[q] = gather(x, r + __shfl_sync(0xffffffffu, offl, q));
     } else {
       const int32_t offl = __ldg(off + k + lane);
 #pragma unroll
@@ -543,11 +563,11 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
             m.z ? nullptr
                 : (cols_staged ? reinterpret_cast<const int32_t *>(base + L.cols) + rel
                                : S.scol + static_cast<int64_t>(m.x) * 32 + lane);
-        T = slice_row_sum<VT, XT, KB>(v, ci, S.soff + m.w, m.y, r, hi, x);
+        T = slice_row_sum<VT, XT, KB>(v, ci, S.soff + m.w, m.y, r, hi, m.z == 2, x);
       } else {
         const int64_t at = static_cast<int64_t>(m.x) * 32 + lane;
         T = slice_row_sum<VT, XT, KB>(val + at, m.z ? nullptr : S.scol + at, S.soff + m.w, m.y,
-                                      r, hi, x);
+                                      r, hi, m.z == 2, x);
       }
       if (r < S.n) epi.apply(r, T, rv);
     }
@@ -733,7 +753,9 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
   out->nslices = ns;
   out->xtype = vtype == kValF64 ? kValF64 : kValF32;
   out->vtype = vtype;
-  DevBuf<int32_t> width, kind, stats, tmp;
+  DevBuf<int32_t> width, kind, stats, tmp, offrange;
+  BCMG_TRY(offrange.alloc(2, s));
+  BCMG_CUDA(cudaMemsetAsync(offrange.get(), 0, 2 * sizeof(int32_t), s));  // 0 in the range
   BCMG_TRY(dev_alloc(&out->sptr, ns + 1, s));
   BCMG_TRY(dev_alloc(&out->meta, ns, s));
   BCMG_TRY(width.alloc(ns, s));
@@ -742,7 +764,7 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
   BCMG_TRY(tmp.alloc(scan_tmp_size(ns), s));
   const int blocks = ceil_div(ns, kWarpsPerBlock);
   launch(k_slice_shape, blocks, kWarpsPerBlock * 32, 0, s, n, ns, A.row, A.col, width.get(),
-         kind.get());
+         kind.get(), offrange.get());
   BCMG_TRY(exclusive_scan(width.get(), out->sptr, ns, out->sptr + ns, tmp.get(), s));
   BCMG_CUDA(cudaMemsetAsync(stats.get(), 0, 2 * sizeof(int32_t), s));
   // Only copies that serve FP64 vectors are narrowed: FP64 -> BF16 cuts the
@@ -827,8 +849,8 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
            kind.get(), out->soff, flag.get());
     BCMG_TRY(exclusive_scan(flag.get(), rid.get(), ns, rid.get() + ns, tmp.get(), s));
     launch(k_slice_heads, ceil_div(ns, 256), 256, 0, s, ns, flag.get(), rid.get(), head.get());
-    launch(k_slice_meta, ceil_div(ns, 256), 256, 0, s, ns, out->sptr, width.get(), kind.get(),
-           flag.get(), rid.get(), head.get(), out->meta);
+    launch(k_slice_meta, ceil_div(ns, 256), 256, 0, s, n, ns, out->sptr, width.get(),
+           kind.get(), flag.get(), rid.get(), head.get(), offrange.get(), out->meta);
     BCMG_LAUNCH_CHECK();
   }
   // Stage capacity: the largest chunk, capped so two stages fit in shared
