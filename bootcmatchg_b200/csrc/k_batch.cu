@@ -17,6 +17,7 @@
 #include <cuda_fp16.h>
 
 #include <cfloat>
+#include <type_traits>
 
 #include "batch.h"
 #include "common.cuh"
@@ -136,8 +137,16 @@ __global__ void __launch_bounds__(256)
   if (!valid) return;
   Cols<XT, V> res;
   if (MODE == kModeRelax) {
+    if (std::is_same<XT, float>::value) {
+      // The FP32 cycle multiplies by one reciprocal per row (within an ulp
+      // of dividing; the cycle is an inexact preconditioner either way).
+      const XT rdi = XT(1) / di;
 #pragma unroll
-    for (int v = 0; v < V; ++v) res.v[v] = ((-acc[v] + fv.v[v]) / di) + uv.v[v];
+      for (int v = 0; v < V; ++v) res.v[v] = ((-acc[v] + fv.v[v]) * rdi) + uv.v[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) res.v[v] = ((-acc[v] + fv.v[v]) / di) + uv.v[v];
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < V; ++v) res.v[v] = fv.v[v] - acc[v];
