@@ -639,6 +639,7 @@ struct GalSmem {
   double *tv;
   int32_t *ti;
   int32_t *tj;
+  int32_t *heads;  // first position of each run (gal_emit)
 };
 
 __device__ __forceinline__ GalSmem gal_smem(unsigned char *base, int cap) {
@@ -647,9 +648,10 @@ __device__ __forceinline__ GalSmem gal_smem(unsigned char *base, int cap) {
   s.tv = reinterpret_cast<double *>(base + sizeof(unsigned long long) * cap);
   s.ti = reinterpret_cast<int32_t *>(base + 16 * cap);
   s.tj = reinterpret_cast<int32_t *>(base + 20 * cap);
+  s.heads = reinterpret_cast<int32_t *>(base + 24 * cap);
   return s;
 }
-constexpr int kGalBytesPerTerm = 24;
+constexpr int kGalBytesPerTerm = 28;
 
 template <int TEAM>
 __device__ __forceinline__ void team_sync() {
@@ -722,8 +724,8 @@ __device__ __forceinline__ bool gal_head(const GalSmem &sm, int k) {
   return k == 0 || (sm.key[k] >> 32) != (sm.key[k - 1] >> 32);
 }
 
-// Sums the run starting at head position k; returns false if the run is
-// longer than kGalMaxRun.
+// Sums the run of len terms starting at sorted position k; returns false if
+// the run is longer than kGalMaxRun.
 // Canonical-order compare-exchange of two run terms (a before b after it).
 __device__ __forceinline__ void gal_cx(int &ia, int32_t &mna, int32_t &mxa, int32_t &ta, int &ib,
                                        int32_t &mnb, int32_t &mxb, int32_t &tb) {
@@ -736,10 +738,8 @@ __device__ __forceinline__ void gal_cx(int &ia, int32_t &mna, int32_t &mxa, int3
   }
 }
 
-__device__ bool gal_run_sum(const GalSmem &sm, int k, int T, int32_t *J, double *sum) {
+__device__ bool gal_run_sum(const GalSmem &sm, int k, int len, int32_t *J, double *sum) {
   const unsigned long long jj = sm.key[k] >> 32;
-  int len = 1;
-  while (len <= 4 && k + len < T && (sm.key[k + len] >> 32) == jj) ++len;
   if (len <= 4) {
     // Runs of at most four terms (pairwise aggregates: |I| |J| <= 4): a
     // four-input sorting network on (min(i,j), max(i,j), i) in registers;
@@ -768,12 +768,10 @@ __device__ bool gal_run_sum(const GalSmem &sm, int k, int T, int32_t *J, double 
     *sum = s;
     return true;
   }
+  if (len > kGalMaxRun) return false;
   int idx[kGalMaxRun];
-  int r = 0;
-  for (int q = k; q < T && (sm.key[q] >> 32) == jj; ++q) {
-    if (r == kGalMaxRun) return false;
-    idx[r++] = static_cast<int>(sm.key[q] & 0xffffffffull);
-  }
+  const int r = len;
+  for (int q = 0; q < r; ++q) idx[q] = static_cast<int>(sm.key[k + q] & 0xffffffffull);
   // Insertion sort of the run by (min(i,j), max(i,j), i).
   for (int a = 1; a < r; ++a) {
     const int x = idx[a];
@@ -813,28 +811,32 @@ __global__ void k_gal_terms(int32_t nc, const int32_t *__restrict__ row,
 }
 
 // Writes the runs of a sorted coarse row: (J, sum) at tJ/tV[base + rank] and
-// the number of runs in runs[I].  Run by one warp.
+// the number of runs in runs[I].  Run by one warp: the run heads are listed
+// first, then each lane sums whole runs.
 __device__ void gal_emit(const GalSmem &sm, int T, int32_t I, int64_t base, int32_t *tJ,
                          double *tV, int32_t *runs, int *err, int lane) {
-  int carry = 0;
+  int nr = 0;
   for (int b0 = 0; b0 < T; b0 += 32) {
     const int k = b0 + lane;
     const bool h = k < T && gal_head(sm, k);
     const unsigned hm = __ballot_sync(0xffffffffu, h);
-    if (h) {
-      int32_t J;
-      double sum;
-      if (gal_run_sum(sm, k, T, &J, &sum)) {
-        const int64_t pos = base + carry + __popc(hm & ((1u << lane) - 1u));
-        tJ[pos] = J;
-        tV[pos] = sum;
-      } else {
-        atomicExch(err, 2);
-      }
-    }
-    carry += __popc(hm);
+    if (h) sm.heads[nr + __popc(hm & ((1u << lane) - 1u))] = k;
+    nr += __popc(hm);
   }
-  if (lane == 0) runs[I] = carry;
+  __syncwarp();
+  for (int r = lane; r < nr; r += 32) {
+    const int k = sm.heads[r];
+    const int len = (r + 1 < nr ? sm.heads[r + 1] : T) - k;
+    int32_t J;
+    double sum;
+    if (gal_run_sum(sm, k, len, &J, &sum)) {
+      tJ[base + r] = J;
+      tV[base + r] = sum;
+    } else {
+      atomicExch(err, 2);
+    }
+  }
+  if (lane == 0) runs[I] = nr;
 }
 
 // Sort-and-reduce pass, one warp per coarse row; rows over kGalCap terms
