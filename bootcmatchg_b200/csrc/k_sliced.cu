@@ -436,11 +436,12 @@ struct __align__(16) StageCtl {
   int32_t slot0, staged, rows_staged, pad;
 };
 
-// Resident CTAs per SM the register budget is sized for: FP64 vectors keep
-// two CTAs (16 consumer warps), FP32 vectors four (more would spill).
+// Resident CTAs per SM the register budget is sized for: FP64 vectors three
+// (24 consumer warps, with at most 14 gathers per batch), FP32 vectors four
+// (more would spill).
 template <typename XT>
 constexpr int pipe_min_blocks() {
-  return sizeof(XT) == 8 ? 2 : 4;
+  return sizeof(XT) == 8 ? 3 : 4;
 }
 
 template <typename VT, typename XT, typename Epi, int KB>
@@ -641,12 +642,21 @@ bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaSt
              x, epi, S.cap_slots, S.cols_staged);                                           \
   } while (0)
   // Gathers per batch matched to the mean slice width: 5-point (2-D) and
-  // 7-point (3-D) stencils issue no padding gathers.
-  if (S.batch <= 5) BCMG_PIPE_KB(5);
-  else if (S.batch <= 7) BCMG_PIPE_KB(7);
-  else if (S.batch <= 8) BCMG_PIPE_KB(8);
-  else if (S.batch <= 16) BCMG_PIPE_KB(16);
-  else BCMG_PIPE_KB(28);
+  // 7-point (3-D) stencils issue no padding gathers.  FP64 vectors take at
+  // most 14 gathers per batch (two batches cover a 27-point row), which keeps
+  // three CTAs per SM in the register file.
+  if constexpr (sizeof(XT) == 8) {
+    if (S.batch <= 5) BCMG_PIPE_KB(5);
+    else if (S.batch <= 7) BCMG_PIPE_KB(7);
+    else if (S.batch <= 8) BCMG_PIPE_KB(8);
+    else BCMG_PIPE_KB(14);
+  } else {
+    if (S.batch <= 5) BCMG_PIPE_KB(5);
+    else if (S.batch <= 7) BCMG_PIPE_KB(7);
+    else if (S.batch <= 8) BCMG_PIPE_KB(8);
+    else if (S.batch <= 16) BCMG_PIPE_KB(16);
+    else BCMG_PIPE_KB(28);
+  }
 #undef BCMG_PIPE_KB
   if (!warm_only) BCMG_LAUNCH_CHECK();
   return BCMG_OK;
