@@ -922,8 +922,11 @@ bcmg_status fcg_iteration(bcmg_handle *h, cudaGraphConditionalHandle cond, bool 
   BCMG_TRY(fcg_scalars(h->partials, h->scal, false, s));
   BCMG_TRY(fcg_update(A.n, false, h->v, h->d, h->w, h->q, h->xs, h->r, h->partials, h->scal,
                       s));
-  if (h->ext.replace_every > 0)
-    BCMG_TRY(fcg_replace(A, h->b, h->xs, h->r, h->partials, h->scal, h->ext.replace_every, s));
+  if (h->ext.replace_every > 0) {
+    const SlicedView S64 = h->A0.own64.view();
+    BCMG_TRY(fcg_replace(A, h->A0.own64.nslices ? &S64 : nullptr, h->b, h->xs, h->r,
+                         h->partials, h->scal, h->ext.replace_every, s));
+  }
   BCMG_TRY(fcg_continue(h->scal, cond, use_cond, s));
   return BCMG_OK;
 }

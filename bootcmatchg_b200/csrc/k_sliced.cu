@@ -355,6 +355,7 @@ __device__ __forceinline__ XT slice_row_sum(const VT *v, const int32_t *cidx,
 template <typename XT>
 struct EpiRelax {  // out = ((-T + f) / d) + u
   static constexpr int NV = 3;
+  __device__ bool active() const { return true; }
   const XT *f, *d, *u;
   XT *out;
   __device__ const XT *row_vec(int i) const { return i == 0 ? f : (i == 1 ? d : u); }
@@ -365,6 +366,7 @@ struct EpiRelax {  // out = ((-T + f) / d) + u
 template <typename XT>
 struct EpiResidual {  // out = f - T
   static constexpr int NV = 1;
+  __device__ bool active() const { return true; }
   const XT *f;
   XT *out;
   __device__ const XT *row_vec(int) const { return f; }
@@ -375,6 +377,7 @@ struct EpiResidual {  // out = f - T
 template <typename XT>
 struct EpiSpmvT {  // out = T
   static constexpr int NV = 0;
+  __device__ bool active() const { return true; }
   XT *out;
   __device__ const XT *row_vec(int) const { return nullptr; }
   __device__ void apply(int32_t r, XT T, const XT *) { out[r] = T; }
@@ -386,6 +389,7 @@ using EpiSpmv = EpiSpmvT<double>;
 // vector); per-CTA partial sums in warp order, written to partials[4 b + k].
 struct EpiFcgDots {
   static constexpr int NV = 3;
+  __device__ bool active() const { return true; }
   const double *v, *r, *q;  // q == nullptr: no gamma
   double *w, *partials;
   double acc[3];
@@ -413,6 +417,39 @@ struct EpiFcgDots {
       partials[blockIdx.x * 4 + lane] = s;
       for (int b = blockIdx.x + gridDim.x; b < kRedBlocks; b += gridDim.x)
         partials[b * 4 + lane] = 0.0;
+    }
+  }
+};
+
+// Residual replacement (mixed precision): r = b - A x with per-CTA partial
+// sums of ||r||^2 (as EpiFcgDots, partial 0), only when the device flag
+// scal[kReplace] is set; otherwise every CTA returns at once.
+struct EpiReplace {
+  static constexpr int NV = 1;
+  const double *b;
+  double *r, *partials;
+  const double *scal;
+  double acc[1];
+  __device__ bool active() const { return scal[kReplace] != 0.0; }
+  __device__ const double *row_vec(int) const { return b; }
+  __device__ void apply(int32_t row, double T, const double *rv) {
+    const double ri = rv[0] - T;
+    r[row] = ri;
+    acc[0] = fma(ri, ri, acc[0]);
+  }
+  __device__ void finish(int wid, int lane) {
+    __shared__ double red[kPipeWarps];
+    double a = acc[0];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) red[wid] = a;
+    asm volatile("bar.sync 1, %0;" ::"n"(kPipeWarps * 32) : "memory");
+    if (wid == 0 && lane == 0) {
+      double t = 0.0;
+      for (int w2 = 0; w2 < kPipeWarps; ++w2) t += red[w2];
+      partials[blockIdx.x * 4] = t;
+      for (int b2 = blockIdx.x + gridDim.x; b2 < kRedBlocks; b2 += gridDim.x)
+        partials[b2 * 4] = 0.0;
     }
   }
 };
@@ -452,6 +489,7 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
   __shared__ __align__(8) uint64_t full[kPipeStages], empty[kPipeStages];
   __shared__ StageCtl ctl[kPipeStages];
   constexpr int NVS = Epi::NV > 0 ? Epi::NV : 1;
+  if (!epi.active()) return;  // uniform: a device flag read by every thread
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int32_t nchunks = (S.nslices + kPipeWarps - 1) / kPipeWarps;
   const StageLayout L(cap_slots, sizeof(VT), sizeof(XT), cols_staged != 0, Epi::NV);
@@ -686,6 +724,8 @@ bcmg_status warm_f64_vectors(const SlicedView &S) {
   BCMG_TRY((pipe_launch<VT, double>(S, static_cast<const double *>(nullptr), e1, 0, true)));
   EpiFcgDots e2{};
   BCMG_TRY((pipe_launch<VT, double>(S, static_cast<const double *>(nullptr), e2, 0, true)));
+  EpiReplace e3{};
+  BCMG_TRY((pipe_launch<VT, double>(S, static_cast<const double *>(nullptr), e3, 0, true)));
   return BCMG_OK;
 }
 
@@ -932,6 +972,18 @@ bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w
     case kValF32: return pipe_launch<float, double>(S, v, e, s);
     case kValBF16: return pipe_launch<__nv_bfloat16, double>(S, v, e, s);
     default: return pipe_launch<__half, double>(S, v, e, s);
+  }
+}
+
+bcmg_status sliced_replace(const SlicedView &S, const double *b, const double *x, double *r,
+                           double *partials, const double *scal, cudaStream_t s) {
+  if (S.xtype != kValF64) return set_error(BCMG_ERR_INTERNAL, "replacement needs an FP64 copy");
+  EpiReplace e{b, r, partials, scal, {0.0}};
+  switch (S.vtype) {
+    case kValF64: return pipe_launch<double, double>(S, x, e, s);
+    case kValF32: return pipe_launch<float, double>(S, x, e, s);
+    case kValBF16: return pipe_launch<__nv_bfloat16, double>(S, x, e, s);
+    default: return pipe_launch<__half, double>(S, x, e, s);
   }
 }
 

@@ -320,9 +320,15 @@ bcmg_status fcg_update(int64_t n, bool first, const double *z, double *zp,
   return BCMG_OK;
 }
 
-bcmg_status fcg_replace(const CsrView &A, const double *b, const double *x, double *r,
-                        double *partials, double *scal, int every, cudaStream_t s) {
+bcmg_status fcg_replace(const CsrView &A, const SlicedView *S, const double *b, const double *x,
+                        double *r, double *partials, double *scal, int every, cudaStream_t s) {
   launch(k_replace_flag, 1, 1, 0, s, scal, every);
+  if (S && S->nslices) {
+    BCMG_TRY(sliced_replace(*S, b, x, r, partials, scal, s));
+    launch(k_norm_final_if, 1, kThreads, 0, s, partials, scal);
+    BCMG_LAUNCH_CHECK();
+    return BCMG_OK;
+  }
   const int G = group_for(A.nnz, A.n);
   switch (G) {
     case 4: launch(k_true_residual<4>, kRedBlocks, kThreads, 0, s, A.n, A.row, A.col, A.val, b, x, r, scal, partials); break;

@@ -224,8 +224,13 @@ bcmg_status fcg_update(int64_t n, bool first, const double *z, double *zp,
                        double *partials, double *scal, cudaStream_t s);
 // Residual replacement: if iteration kIter+1 is a multiple of `every` or the
 // recursive norm reached the target, r = b - A x and ||r|| recomputed (FP64).
-bcmg_status fcg_replace(const CsrView &A, const double *b, const double *x, double *r,
-                        double *partials, double *scal, int every, cudaStream_t s);
+// With S (an FP64-vector sliced copy of A) the product runs on it.
+bcmg_status fcg_replace(const CsrView &A, const SlicedView *S, const double *b, const double *x,
+                        double *r, double *partials, double *scal, int every, cudaStream_t s);
+// r = b - A x and the ||r||^2 partials on the sliced copy when scal[kReplace]
+// is set (fcg_replace).
+bcmg_status sliced_replace(const SlicedView &S, const double *b, const double *x, double *r,
+                           double *partials, const double *scal, cudaStream_t s);
 // Counts the iteration and evaluates the loop condition (into the graph's
 // WHILE condition when use_cond).
 bcmg_status fcg_continue(double *scal, cudaGraphConditionalHandle cond, bool use_cond,
