@@ -40,6 +40,35 @@ inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
   kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
 }
 
+// Programmatic dependent launch (solve-phase kernels): a kernel launched with
+// launch_pdl may begin while the previous kernel on its stream is still
+// running.  Every such kernel calls pdl_wait() first — it returns once the
+// previous grid has completed and its writes are visible (a no-op for a
+// normal launch) — and pdl_trigger() to let the next one start launching;
+// a grid can only start after every CTA of its predecessor has triggered or
+// exited, so those CTAs are all resident already.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, Args &&...args) {
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 
 // Lanes per row for row-group kernels, from the average row length.

@@ -47,6 +47,8 @@ __global__ void __launch_bounds__(kThreads)
     k_relax_t(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
               const VT *__restrict__ val, const XT *__restrict__ d,
               const XT *__restrict__ f, const XT *__restrict__ u, XT *__restrict__ u_out) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   int32_t i = static_cast<int32_t>(t / G);
   const int lane = threadIdx.x % G;
@@ -59,6 +61,8 @@ __global__ void __launch_bounds__(kThreads)
 template <typename XT>
 __global__ void k_relax_zero_t(int32_t n, const XT *__restrict__ d, const XT *__restrict__ f,
                                XT *__restrict__ u_out) {
+  pdl_wait();
+  pdl_trigger();
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) u_out[i] = f[i] / d[i];
 }
@@ -68,6 +72,8 @@ __global__ void __launch_bounds__(kThreads)
     k_residual_t(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
                  const VT *__restrict__ val, const XT *__restrict__ f,
                  const XT *__restrict__ u, XT *__restrict__ res) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   int32_t i = static_cast<int32_t>(t / G);
   const int lane = threadIdx.x % G;
@@ -80,6 +86,8 @@ template <typename XT>
 __global__ void k_restrict_t(int32_t nc, const int32_t *__restrict__ rptr,
                              const int32_t *__restrict__ ridx, const XT *__restrict__ p,
                              const XT *__restrict__ x, XT *__restrict__ y) {
+  pdl_wait();
+  pdl_trigger();
   const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= nc) return;
   XT s = XT(0);
@@ -94,12 +102,16 @@ template <typename XT>
 __global__ void k_prolong_t(int32_t n, const int32_t *__restrict__ agg,
                             const XT *__restrict__ p, const XT *__restrict__ xc,
                             XT *__restrict__ xf) {
+  pdl_wait();
+  pdl_trigger();
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) xf[i] = fma(p[i], xc[agg[i]], xf[i]);
 }
 
 template <typename XT>
 __global__ void k_fill_t(XT *x, int64_t n, XT v) {
+  pdl_wait();
+  pdl_trigger();
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     x[i] = v;
@@ -107,6 +119,8 @@ __global__ void k_fill_t(XT *x, int64_t n, XT v) {
 
 template <typename XT>
 __global__ void k_axpy_t(int64_t n, XT a, const XT *__restrict__ x, XT *__restrict__ y) {
+  pdl_wait();
+  pdl_trigger();
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     y[i] = fma(a, x[i], y[i]);
@@ -114,6 +128,8 @@ __global__ void k_axpy_t(int64_t n, XT a, const XT *__restrict__ x, XT *__restri
 
 template <typename XT>
 __global__ void k_scale_t(int64_t n, XT a, XT *x) {
+  pdl_wait();
+  pdl_trigger();
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     x[i] = x[i] * a;
@@ -121,6 +137,8 @@ __global__ void k_scale_t(int64_t n, XT a, XT *x) {
 
 template <typename From, typename To>
 __global__ void k_convert(int64_t n, const From *__restrict__ in, To *__restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     out[i] = static_cast<To>(in[i]);
@@ -142,6 +160,8 @@ template <int G, typename VT, typename XT>
 __global__ void __launch_bounds__(kThreads)
     k_spmv_t(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
              const VT *__restrict__ val, const XT *__restrict__ x, XT *__restrict__ y) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   int32_t i = static_cast<int32_t>(t / G);
   const int lane = threadIdx.x % G;
@@ -154,6 +174,8 @@ __global__ void __launch_bounds__(kThreads)
 template <typename XT>
 __global__ void __launch_bounds__(kRedThreads)
     k_dot_t(int64_t n, const XT *__restrict__ a, const XT *__restrict__ b, double *partials) {
+  pdl_wait();
+  pdl_trigger();
   double v[1] = {0.0};
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -162,6 +184,8 @@ __global__ void __launch_bounds__(kRedThreads)
 }
 
 __global__ void k_dot_t_final(const double *partials, double *out) {
+  pdl_wait();
+  pdl_trigger();
   const double s = reduce_partials(partials, 0);
   if (threadIdx.x == 0) *out = s;
 }
@@ -180,10 +204,10 @@ void launch_relax(int G, int blocks, cudaStream_t s, const MatView &A, const XT 
                   const XT *f, const XT *src, XT *dst) {
   const VT *val = static_cast<const VT *>(A.val);
   switch (G) {
-    case 4: launch(k_relax_t<4, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
-    case 8: launch(k_relax_t<8, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
-    case 16: launch(k_relax_t<16, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
-    default: launch(k_relax_t<32, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
+    case 4: launch_pdl(k_relax_t<4, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
+    case 8: launch_pdl(k_relax_t<8, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
+    case 16: launch_pdl(k_relax_t<16, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
+    default: launch_pdl(k_relax_t<32, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, d, f, src, dst); break;
   }
 }
 
@@ -192,10 +216,10 @@ void launch_residual(int G, int blocks, cudaStream_t s, const MatView &A, const 
                      const XT *u, XT *res) {
   const VT *val = static_cast<const VT *>(A.val);
   switch (G) {
-    case 4: launch(k_residual_t<4, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
-    case 8: launch(k_residual_t<8, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
-    case 16: launch(k_residual_t<16, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
-    default: launch(k_residual_t<32, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
+    case 4: launch_pdl(k_residual_t<4, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
+    case 8: launch_pdl(k_residual_t<8, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
+    case 16: launch_pdl(k_residual_t<16, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
+    default: launch_pdl(k_residual_t<32, VT, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, val, f, u, res); break;
   }
 }
 
@@ -264,7 +288,7 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
   int left = k;
   if (zero_start) {
     cur = (k % 2 == 1) ? u : u_tmp;
-    launch(k_relax_zero_t<XT>, ceil_div(n, kThreads), kThreads, 0, s, n, d, f, cur);
+    launch_pdl(k_relax_zero_t<XT>, ceil_div(n, kThreads), kThreads, 0, s, n, d, f, cur);
     --left;
   } else if (k % 2 == 1) {
     BCMG_CUDA(cudaMemcpyAsync(u_tmp, u, sizeof(XT) * n, cudaMemcpyDeviceToDevice, s));
@@ -299,7 +323,7 @@ template <typename XT>
 bcmg_status restrict_t(int32_t nc, const int32_t *rptr, const int32_t *ridx, const XT *p,
                        const XT *x, XT *y, cudaStream_t s) {
   if (nc <= 0) return BCMG_OK;
-  launch(k_restrict_t<XT>, ceil_div(nc, kThreads), kThreads, 0, s, nc, rptr, ridx, p, x, y);
+  launch_pdl(k_restrict_t<XT>, ceil_div(nc, kThreads), kThreads, 0, s, nc, rptr, ridx, p, x, y);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -308,7 +332,7 @@ template <typename XT>
 bcmg_status prolong_t(int32_t n, const int32_t *agg, const XT *p, const XT *xc, XT *xf,
                       cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
-  launch(k_prolong_t<XT>, ceil_div(n, kThreads), kThreads, 0, s, n, agg, p, xc, xf);
+  launch_pdl(k_prolong_t<XT>, ceil_div(n, kThreads), kThreads, 0, s, n, agg, p, xc, xf);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -316,7 +340,7 @@ bcmg_status prolong_t(int32_t n, const int32_t *agg, const XT *p, const XT *xc, 
 template <typename XT>
 bcmg_status fill_t(XT *x, int64_t n, XT v, cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
-  launch(k_fill_t<XT>, stream_grid(n), kThreads, 0, s, x, n, v);
+  launch_pdl(k_fill_t<XT>, stream_grid(n), kThreads, 0, s, x, n, v);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -324,7 +348,7 @@ bcmg_status fill_t(XT *x, int64_t n, XT v, cudaStream_t s) {
 template <typename XT>
 bcmg_status axpy_t(int64_t n, XT a, const XT *x, XT *y, cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
-  launch(k_axpy_t<XT>, stream_grid(n), kThreads, 0, s, n, a, x, y);
+  launch_pdl(k_axpy_t<XT>, stream_grid(n), kThreads, 0, s, n, a, x, y);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -332,7 +356,7 @@ bcmg_status axpy_t(int64_t n, XT a, const XT *x, XT *y, cudaStream_t s) {
 template <typename XT>
 bcmg_status scale_t(int64_t n, XT a, XT *x, cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
-  launch(k_scale_t<XT>, stream_grid(n), kThreads, 0, s, n, a, x);
+  launch_pdl(k_scale_t<XT>, stream_grid(n), kThreads, 0, s, n, a, x);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -346,14 +370,14 @@ bcmg_status copy_t(XT *dst, const XT *src, int64_t n, cudaStream_t s) {
 
 bcmg_status convert_d2f(int64_t n, const double *in, float *out, cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
-  launch(k_convert<double, float>, stream_grid(n), kThreads, 0, s, n, in, out);
+  launch_pdl(k_convert<double, float>, stream_grid(n), kThreads, 0, s, n, in, out);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
 bcmg_status convert_f2d(int64_t n, const float *in, double *out, cudaStream_t s) {
   if (n <= 0) return BCMG_OK;
-  launch(k_convert<float, double>, stream_grid(n), kThreads, 0, s, n, in, out);
+  launch_pdl(k_convert<float, double>, stream_grid(n), kThreads, 0, s, n, in, out);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -362,7 +386,7 @@ bcmg_status convert_values(int64_t n, const double *in, void *out, int vtype, cu
   if (n <= 0) return BCMG_OK;
   switch (vtype) {
     case kValF32:
-      launch(k_convert<double, float>, stream_grid(n), kThreads, 0, s, n, in,
+      launch_pdl(k_convert<double, float>, stream_grid(n), kThreads, 0, s, n, in,
              static_cast<float *>(out));
       break;
     case kValBF16:
@@ -387,10 +411,10 @@ bcmg_status spmv_t(const MatView &A, const XT *x, XT *y, cudaStream_t s) {
   const int blocks = grid_for(static_cast<int64_t>(A.n) * G);
 #define BCMG_SPMV_G(VT_)                                                                       \
   switch (G) {                                                                                 \
-    case 4: launch(k_spmv_t<4, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break;  \
-    case 8: launch(k_spmv_t<8, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break;  \
-    case 16: launch(k_spmv_t<16, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break; \
-    default: launch(k_spmv_t<32, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break; \
+    case 4: launch_pdl(k_spmv_t<4, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break;  \
+    case 8: launch_pdl(k_spmv_t<8, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break;  \
+    case 16: launch_pdl(k_spmv_t<16, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break; \
+    default: launch_pdl(k_spmv_t<32, VT_, XT>, blocks, kThreads, 0, s, A.n, A.row, A.col, static_cast<const VT_ *>(A.val), x, y); break; \
   }
   if (std::is_same<XT, double>::value) {
     BCMG_SPMV_G(double)
@@ -409,8 +433,8 @@ bcmg_status spmv_t(const MatView &A, const XT *x, XT *y, cudaStream_t s) {
 template <typename XT>
 bcmg_status dot_t(int64_t n, const XT *a, const XT *b, double *out, double *partials,
                   cudaStream_t s) {
-  launch(k_dot_t<XT>, kRedBlocks, kRedThreads, 0, s, n, a, b, partials);
-  launch(k_dot_t_final, 1, kRedThreads, 0, s, partials, out);
+  launch_pdl(k_dot_t<XT>, kRedBlocks, kRedThreads, 0, s, n, a, b, partials);
+  launch_pdl(k_dot_t_final, 1, kRedThreads, 0, s, partials, out);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }

@@ -485,6 +485,8 @@ template <typename VT, typename XT, typename Epi, int KB>
 __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
     k_sl_pipe(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ x, Epi epi,
               int cap_slots, int cols_staged) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kPipeStages], empty[kPipeStages];
   __shared__ StageCtl ctl[kPipeStages];
@@ -676,7 +678,7 @@ bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaSt
     auto kern = k_sl_pipe<VT, XT, Epi, KB_>;                                                \
     BCMG_TRY(pipe_cfg(kern, L.bytes, nchunks, &cfg));                                       \
     if (!warm_only)                                                                         \
-      launch(kern, cfg.grid, kPipeThreads, cfg.smem, st, S, static_cast<const VT *>(S.val), \
+      launch_pdl(kern, cfg.grid, kPipeThreads, cfg.smem, st, S, static_cast<const VT *>(S.val), \
              x, epi, S.cap_slots, S.cols_staged);                                           \
   } while (0)
   // Gathers per batch matched to the mean slice width: 5-point (2-D) and

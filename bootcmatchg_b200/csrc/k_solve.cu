@@ -52,6 +52,8 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void __launch_bounds__(kThreads)
     k_dot_partials(int64_t n, const double *__restrict__ a, const double *__restrict__ b,
                    double *partials) {
+  pdl_wait();
+  pdl_trigger();
   double v[1] = {0.0};
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -60,6 +62,8 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void k_dot_final(const double *partials, double *out) {
+  pdl_wait();
+  pdl_trigger();
   const double s = reduce_partials(partials, 0);
   if (threadIdx.x == 0) *out = s;
 }
@@ -73,6 +77,8 @@ __global__ void __launch_bounds__(kThreads)
                     const double *__restrict__ v, double *__restrict__ w,
                     const double *__restrict__ r, const double *__restrict__ q,
                     double *partials) {
+  pdl_wait();
+  pdl_trigger();
   double acc[3] = {0.0, 0.0, 0.0};
   const int lane = threadIdx.x % G;
   const int64_t groups = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
@@ -96,6 +102,8 @@ __global__ void __launch_bounds__(kThreads)
 // FCG scalar recurrences (FCG.cu:475-478 for the first step, :531-534 in
 // the loop), kept on the device.
 __global__ void k_fcg_scalars(const double *partials, double *scal, int first) {
+  pdl_wait();
+  pdl_trigger();
   const double alpha = reduce_partials(partials, 0);
   const double beta = reduce_partials(partials, 1);
   const double gamma = reduce_partials(partials, 2);
@@ -142,6 +150,8 @@ __global__ void __launch_bounds__(kThreads)
                  double *__restrict__ azp, double *__restrict__ x,
                  double *__restrict__ r, const double *__restrict__ scal,
                  double *partials) {
+  pdl_wait();
+  pdl_trigger();
   double acc[1] = {0.0};
   const double theta = scal[kTheta];
   const double theta2 = first ? theta : scal[kTheta2];
@@ -163,6 +173,8 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void k_norm_final(const double *partials, double *scal) {
+  pdl_wait();
+  pdl_trigger();
   const double s = reduce_partials(partials, 0);
   if (threadIdx.x == 0) scal[kNorm] = sqrt(s);
 }
@@ -171,6 +183,8 @@ __global__ void k_norm_final(const double *partials, double *scal) {
 // FCG.cu:497-565 continues (||r|| > rtol delta0 and iter < itnlim and no
 // breakdown).  Inside a graph the decision drives the WHILE node.
 __global__ void k_fcg_continue(double *scal, cudaGraphConditionalHandle cond, int use_cond) {
+  pdl_wait();
+  pdl_trigger();
   const double iter = scal[kIter] + 1.0;
   scal[kIter] = iter;
   const bool go = scal[kNorm] > scal[kTarget] && iter < scal[kItnlim] && scal[kIndef] == 0.0;
@@ -183,6 +197,8 @@ __global__ void k_fcg_continue(double *scal, cudaGraphConditionalHandle cond, in
 // multiple of `every` or when the recursive norm has reached the target, so
 // convergence is always decided on the true residual.
 __global__ void k_replace_flag(double *scal, int every) {
+  pdl_wait();
+  pdl_trigger();
   const int i = static_cast<int>(scal[kIter]) + 1;
   const bool due = (every > 0 && i % every == 0) || scal[kNorm] <= scal[kTarget];
   scal[kReplace] = due ? 1.0 : 0.0;
@@ -215,6 +231,8 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void k_norm_final_if(const double *partials, double *scal) {
+  pdl_wait();
+  pdl_trigger();
   if (scal[kReplace] == 0.0) return;
   const double s = reduce_partials(partials, 0);
   if (threadIdx.x == 0) scal[kNorm] = sqrt(s);
@@ -275,8 +293,8 @@ bcmg_status spmv(const CsrView &A, double alpha, const double *x, double beta, d
 
 bcmg_status dot_dev(int64_t n, const double *a, const double *b, double *out,
                     double *partials, cudaStream_t s) {
-  launch(k_dot_partials, kRedBlocks, kThreads, 0, s, n, a, b, partials);
-  launch(k_dot_final, 1, kThreads, 0, s, partials, out);
+  launch_pdl(k_dot_partials, kRedBlocks, kThreads, 0, s, n, a, b, partials);
+  launch_pdl(k_dot_final, 1, kThreads, 0, s, partials, out);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -288,24 +306,24 @@ bcmg_status fcg_spmv_dots(const CsrView &A, const double *v, double *w, const do
   const int32_t n = A.n;
   const int G = group_for(A.nnz, n);
   switch (G) {
-    case 4: launch(k_fcg_spmv_dots<4>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
-    case 8: launch(k_fcg_spmv_dots<8>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
-    case 16: launch(k_fcg_spmv_dots<16>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
-    default: launch(k_fcg_spmv_dots<32>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    case 4: launch_pdl(k_fcg_spmv_dots<4>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    case 8: launch_pdl(k_fcg_spmv_dots<8>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    case 16: launch_pdl(k_fcg_spmv_dots<16>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
+    default: launch_pdl(k_fcg_spmv_dots<32>, kRedBlocks, kThreads, 0, s, n, A.row, A.col, A.val, v, w, r, q, partials); break;
   }
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
 bcmg_status fcg_scalars(double *partials, double *scal, bool first, cudaStream_t s) {
-  launch(k_fcg_scalars, 1, kThreads, 0, s, partials, scal, first ? 1 : 0);
+  launch_pdl(k_fcg_scalars, 1, kThreads, 0, s, partials, scal, first ? 1 : 0);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
 bcmg_status fcg_continue(double *scal, cudaGraphConditionalHandle cond, bool use_cond,
                          cudaStream_t s) {
-  launch(k_fcg_continue, 1, 1, 0, s, scal, cond, use_cond ? 1 : 0);
+  launch_pdl(k_fcg_continue, 1, 1, 0, s, scal, cond, use_cond ? 1 : 0);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
@@ -313,19 +331,19 @@ bcmg_status fcg_continue(double *scal, cudaGraphConditionalHandle cond, bool use
 bcmg_status fcg_update(int64_t n, bool first, const double *z, double *zp,
                        const double *az, double *azp, double *x, double *r,
                        double *partials, double *scal, cudaStream_t s) {
-  launch(k_fcg_update, kRedBlocks, kThreads, 0, s, n, first ? 1 : 0, z, zp, az, azp, x, r,
+  launch_pdl(k_fcg_update, kRedBlocks, kThreads, 0, s, n, first ? 1 : 0, z, zp, az, azp, x, r,
                                                scal, partials);
-  launch(k_norm_final, 1, kThreads, 0, s, partials, scal);
+  launch_pdl(k_norm_final, 1, kThreads, 0, s, partials, scal);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
 bcmg_status fcg_replace(const CsrView &A, const SlicedView *S, const double *b, const double *x,
                         double *r, double *partials, double *scal, int every, cudaStream_t s) {
-  launch(k_replace_flag, 1, 1, 0, s, scal, every);
+  launch_pdl(k_replace_flag, 1, 1, 0, s, scal, every);
   if (S && S->nslices) {
     BCMG_TRY(sliced_replace(*S, b, x, r, partials, scal, s));
-    launch(k_norm_final_if, 1, kThreads, 0, s, partials, scal);
+    launch_pdl(k_norm_final_if, 1, kThreads, 0, s, partials, scal);
     BCMG_LAUNCH_CHECK();
     return BCMG_OK;
   }
@@ -336,7 +354,7 @@ bcmg_status fcg_replace(const CsrView &A, const SlicedView *S, const double *b, 
     case 16: launch(k_true_residual<16>, kRedBlocks, kThreads, 0, s, A.n, A.row, A.col, A.val, b, x, r, scal, partials); break;
     default: launch(k_true_residual<32>, kRedBlocks, kThreads, 0, s, A.n, A.row, A.col, A.val, b, x, r, scal, partials); break;
   }
-  launch(k_norm_final_if, 1, kThreads, 0, s, partials, scal);
+  launch_pdl(k_norm_final_if, 1, kThreads, 0, s, partials, scal);
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
