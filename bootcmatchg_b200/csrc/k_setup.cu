@@ -244,6 +244,24 @@ __device__ __forceinline__ void sort_row_regs(int32_t i, int32_t b, int T, doubl
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) nu += __shfl_xor_sync(0xffffffffu, nu, o);
+  if (E == 1) {
+    // All usable weights equal (a constant-coefficient stencil under w = 1):
+    // the order is usable entries by offset descending, then the rest by
+    // offset descending — positions from two ballots, no sort.
+    const bool usable = wv[0] > 0.0;
+    const unsigned U = __ballot_sync(0xffffffffu, usable);
+    const unsigned Vd = __ballot_sync(0xffffffffu, tv[0] >= 0);
+    const double wref = __shfl_sync(0xffffffffu, wv[0], U ? __ffs(U) - 1 : 0);
+    if (__all_sync(0xffffffffu, !usable || wv[0] == wref)) {
+      if (lane < T) {
+        const unsigned above = static_cast<unsigned>((0xffffffffull << (lane + 1)) & 0xffffffffull);
+        const int pos = usable ? __popc(U & above) : __popc(U) + __popc(Vd & ~U & above);
+        put_sorted(b, pos, lane, wv[0], col, sW, scol, inv);
+      }
+      if (lane == 0) ucnt[i] = nu;
+      return;
+    }
+  }
   warp_bitonic<E>(wv, tv, lane);
 #pragma unroll
   for (int e = 0; e < E; ++e) {
