@@ -124,6 +124,8 @@ SIGNATURES = {
                                     C.POINTER(C.c_int64), i32p, i32p]),
     "bcmg_k_pair_aggregate": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i32p, vp, vp,
                                         vp, vp]),
+    "bcmg_k_spgemm": (C.c_int, [i32, i32, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp, i32p,
+                                vp, vp, vp]),
     "bcmg_k_galerkin": (C.c_int, [i32, i32, vp, vp, vp, i32, vp, vp, vp, i32p, vp, vp,
                                   vp]),
     "bcmg_k_relax": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, C.c_int, vp]),

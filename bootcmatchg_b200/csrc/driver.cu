@@ -1613,6 +1613,33 @@ bcmg_status bcmg_k_pair_aggregate(int32_t n, int32_t nnz, const int32_t *d_row,
   return BCMG_OK;
 }
 
+bcmg_status bcmg_k_spgemm(int32_t n, int32_t m, int32_t x_nnz, const int32_t *d_xrow,
+                          const int32_t *d_xcol, const double *d_xval, int32_t y_n,
+                          int32_t y_nnz, const int32_t *d_yrow, const int32_t *d_ycol,
+                          const double *d_yval, int32_t *d_crow, int32_t *c_nnz,
+                          int32_t *d_ccol, double *d_cval, void *stream) {
+  clear_error();
+  if (n <= 0 || m <= 0 || y_n <= 0 || !d_xrow || !d_xcol || !d_xval || !d_yrow || !d_ycol ||
+      !d_yval || !d_crow)
+    return set_error(BCMG_ERR_PARAM, "bad arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const CsrView X{n, x_nnz, d_xrow, d_xcol, d_xval};
+  const CsrView Y{y_n, y_nnz, d_yrow, d_ycol, d_yval};
+  int32_t *ccol = nullptr;
+  double *cval = nullptr;
+  int32_t cnnz = 0;
+  BCMG_TRY(spgemm(X, Y, m, d_crow, &ccol, &cval, &cnnz, s));
+  if (c_nnz) *c_nnz = cnnz;
+  if (d_ccol && d_cval && cnnz > 0) {
+    BCMG_CUDA(cudaMemcpyAsync(d_ccol, ccol, sizeof(int32_t) * cnnz, cudaMemcpyDeviceToDevice, s));
+    BCMG_CUDA(cudaMemcpyAsync(d_cval, cval, sizeof(double) * cnnz, cudaMemcpyDeviceToDevice, s));
+  }
+  dev_free(ccol, s);
+  dev_free(cval, s);
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  return BCMG_OK;
+}
+
 bcmg_status bcmg_k_galerkin(int32_t n, int32_t nnz, const int32_t *d_row,
                             const int32_t *d_col, const double *d_val, int32_t n_coarse,
                             const int32_t *d_agg, const double *d_p, int32_t *d_crow,

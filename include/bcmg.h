@@ -340,6 +340,18 @@ bcmg_status bcmg_k_galerkin(int32_t n, int32_t nnz, const int32_t *d_row,
                             const double *d_p, int32_t *d_crow,
                             int32_t *c_nnz, int32_t *d_ccol, double *d_cval,
                             void *stream);
+/* C = X Y for device CSR matrices (X: n rows, x_nnz entries; Y: y_n rows,
+ * m columns, rows with distinct columns), each entry summed over X's row
+ * order from the first term — the products of smoothed aggregation
+ * (CSRm::CSRCSR_product, src/matrix/CSR.cu:1069-1082, whose cuSPARSE order
+ * is unspecified; matchingAggregation.cu:372-384).  Rows come out sorted by
+ * column.  Call with d_crow (n+1) only to get *c_nnz; then again with
+ * d_ccol/d_cval of that size. */
+bcmg_status bcmg_k_spgemm(int32_t n, int32_t m, int32_t x_nnz, const int32_t *d_xrow,
+                          const int32_t *d_xcol, const double *d_xval, int32_t y_n,
+                          int32_t y_nnz, const int32_t *d_yrow, const int32_t *d_ycol,
+                          const double *d_yval, int32_t *d_crow, int32_t *c_nnz,
+                          int32_t *d_ccol, double *d_cval, void *stream);
 /* k Jacobi / l1-Jacobi sweeps u <- u + (f - A u) ./ d
  * (_jacobi_it, src/AMG/relaxation.cu:176-209).  d is D (Jacobi) or the
  * absolute row sums (l1).  u is updated in place. */

@@ -1071,6 +1071,22 @@ int orc_galerkin(int32_t n, int32_t nnz, const int32_t *row, const int32_t *col,
   return BCMG_OK;
 }
 
+// C = X Y in the canonical order of spgemm (X: n rows; Y: yn rows, m columns).
+int orc_spgemm(int32_t n, int32_t xnnz, const int32_t *xrow, const int32_t *xcol,
+               const double *xval, int32_t yn, int32_t m, int32_t ynnz, const int32_t *yrow,
+               const int32_t *ycol, const double *yval, int32_t *crow, int32_t *c_nnz,
+               int32_t *ccol, double *cval) {
+  Csr X = wrap(n, xnnz, xrow, xcol, xval);
+  Csr Y = wrap(yn, ynnz, yrow, ycol, yval);
+  Y.m = m;
+  auto C = spgemm(X, Y);
+  if (crow) std::copy(C->row.begin(), C->row.end(), crow);
+  if (c_nnz) *c_nnz = C->nnz();
+  if (ccol) std::copy(C->col.begin(), C->col.end(), ccol);
+  if (cval) std::copy(C->val.begin(), C->val.end(), cval);
+  return BCMG_OK;
+}
+
 int orc_relax(int32_t n, const int32_t *row, const int32_t *col, const double *val,
               const double *d, const double *f, double *u, int k) {
   Csr A = wrap(n, row[n], row, col, val);

@@ -60,6 +60,7 @@ _SIG = {
     "orc_pair_aggregate": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i32p, vp, vp, vp]),
     "orc_galerkin": (C.c_int, [i32, i32, vp, vp, vp, i32, vp, vp, vp, i32p, vp, vp]),
     "orc_relax": (C.c_int, [i32, vp, vp, vp, vp, vp, vp, C.c_int]),
+    "orc_spgemm": (C.c_int, [i32, i32, vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, i32p, vp, vp]),
     "orc_spmv": (C.c_int, [i32, vp, vp, vp, C.c_double, vp, C.c_double, vp]),
     "orc_greedy_match": (C.c_int, [i32, vp, vp, vp, vp]),
 }
@@ -206,6 +207,18 @@ def galerkin(A, agg, p, nc):
     _check(olib.orc_galerkin(A.n, A.nnz, _ptr(A.row), _ptr(A.col), _ptr(A.val), nc, _ptr(agg),
                              _ptr(p), _ptr(crow), C.byref(cnnz), _ptr(ccol), _ptr(cval)),
            "galerkin")
+    return crow, ccol, cval
+
+
+def spgemm(X, Y, m):
+    """C = X Y (Y has m columns) in the canonical summation order."""
+    crow = np.zeros(X.n + 1, np.int32)
+    cnnz = C.c_int32()
+    args = (X.n, X.nnz, _ptr(X.row), _ptr(X.col), _ptr(X.val), Y.n, m, Y.nnz, _ptr(Y.row),
+            _ptr(Y.col), _ptr(Y.val), _ptr(crow), C.byref(cnnz))
+    _check(olib.orc_spgemm(*args, None, None), "spgemm")
+    ccol, cval = np.zeros(cnnz.value, np.int32), np.zeros(cnnz.value)
+    _check(olib.orc_spgemm(*args, _ptr(ccol), _ptr(cval)), "spgemm")
     return crow, ccol, cval
 
 

@@ -399,6 +399,29 @@ def test_oracle_smoothed_aggregation_restates_the_algorithm():
     assert iters[1] < iters[0]
 
 
+def rows_with_lengths(lengths, ncols, seed):
+    """CSR with the given row lengths, distinct sorted columns, N(0,1) values."""
+    rng = np.random.default_rng(seed)
+    row = np.zeros(len(lengths) + 1, np.int32)
+    row[1:] = np.cumsum(lengths)
+    col = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lengths])
+    val = rng.standard_normal(int(row[-1]))
+    return bc.CsrMatrix(len(lengths), row, col.astype(np.int32), val, ncols)
+
+
+def test_oracle_spgemm_matches_scipy():
+    # The canonical-order product of smoothed aggregation: structure equal to
+    # scipy's, values within rounding of it.
+    X = rows_with_lengths([3, 40, 0, 17, 120], 900, 5)
+    Y = rows_with_lengths([9] * 900, 1500, 6)
+    crow, ccol, cval = orc.spgemm(X, Y, 1500)
+    ref = (sp.csr_matrix((X.val, X.col, X.row), shape=(5, 900)) @
+           sp.csr_matrix((Y.val, Y.col, Y.row), shape=(900, 1500))).tocsr()
+    ref.sort_indices()
+    assert np.array_equal(crow, ref.indptr) and np.array_equal(ccol, ref.indices)
+    np.testing.assert_allclose(cval, ref.data, rtol=1e-12, atol=1e-12)
+
+
 def test_bootstrap_second_hierarchy_uses_same_w():
     # After hierarchy 1 the inner iterations are skipped (bootstrap.cu:68-75),
     # so hierarchy 2 is built from w = 1 again: it equals hierarchy 1.

@@ -373,3 +373,30 @@ def test_smoothed_aggregation_matches_oracle(case):
         assert info.converged and abs(info.iters - oi["iters"]) <= 1, (info.iters, oi["iters"])
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6
         assert info.true_rel_residual <= 1.05 * p.rtol
+
+
+def test_spgemm_tiers_match_oracle():
+    """bcmg_k_spgemm bit for bit against the oracle's canonical-order product,
+    with product rows in every tier of the kernel: up to 512 distinct
+    columns (a warp, shared memory), up to 2,048 (a block, shared memory)
+    and beyond (a block, global memory)."""
+    from test_cpu_oracle import rows_with_lengths
+    rng = np.random.default_rng(8)
+    lengths = rng.choice([10, 60, 300], size=240)
+    X = rows_with_lengths(lengths, 4000, 9)
+    Y = rows_with_lengths([25] * 4000, 6000, 10)
+    crow_o, ccol_o, cval_o = orc.spgemm(X, Y, 6000)
+    assert np.diff(crow_o).max() > 2048 and np.diff(crow_o).min() < 512
+    xr, xc, xv = dev(X.row), dev(X.col), dev(X.val)
+    yr, yc, yv = dev(Y.row), dev(Y.col), dev(Y.val)
+    crow = torch.zeros(X.n + 1, dtype=torch.int32, device="cuda")
+    nnz = C.c_int32()
+    args = (X.n, 6000, X.nnz, P(xr), P(xc), P(xv), Y.n, Y.nnz, P(yr), P(yc), P(yv), P(crow),
+            C.byref(nnz))
+    check(lib.bcmg_k_spgemm(*args, None, None, None), "spgemm")
+    ccol = torch.zeros(nnz.value, dtype=torch.int32, device="cuda")
+    cval = torch.zeros(nnz.value, dtype=torch.float64, device="cuda")
+    check(lib.bcmg_k_spgemm(*args, P(ccol), P(cval), None), "spgemm")
+    assert np.array_equal(crow.cpu().numpy(), crow_o)
+    assert np.array_equal(ccol.cpu().numpy(), ccol_o)
+    assert np.array_equal(cval.cpu().numpy(), cval_o)
