@@ -715,7 +715,9 @@ def run_batch(args):
                    "l2": "interleaved 32-column blocks (%.0f MB each in FP32) exceed "
                          "the 126 MB L2; no flush" % (A.n * nrhs * 4 / 1e6),
                    "step": "setup (shared hierarchy) + batched FCG of all columns + "
-                           "teardown"},
+                           "teardown",
+                   "autotune": "row-kernel shapes timed once per level shape and width in "
+                               "the process (warm-up steps), reused by later setups"},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),

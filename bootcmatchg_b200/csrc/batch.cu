@@ -19,6 +19,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -194,6 +197,19 @@ bcmg_status tune_level(bcmg_handle *h, const MatView &A, const XT *d, XT *f, XT 
   return st;
 }
 
+// Tuned shapes by (rows, entries, value type, vector bytes, width), kept for
+// the process: a level of the same shape (a repeated matrix, a server's next
+// request) takes the earlier choice instead of timing the candidates again.
+struct TuneKey {
+  int32_t n, nnz;
+  int vtype, xbytes, W;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(n, nnz, vtype, xbytes, W) < std::tie(o.n, o.nnz, o.vtype, o.xbytes, o.W);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, BtCfg> g_tuned;
+
 template <typename XT>
 bcmg_status tune_all(bcmg_handle *h, BatchState &S, CycleBufs<XT> &B) {
   const int W = S.W;
@@ -202,6 +218,15 @@ bcmg_status tune_all(bcmg_handle *h, BatchState &S, CycleBufs<XT> &B) {
     DevHierarchy &H = h->H[k];
     for (size_t l = 0; l < H.lv.size(); ++l) {
       DevLevel &lv = H.lv[l];
+      const TuneKey key{lv.n, lv.nnz, BtLv<XT>::mat(lv).vtype, static_cast<int>(sizeof(XT)), W};
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+          S.cfg[k][l] = it->second;
+          continue;
+        }
+      }
       const int64_t cnt = static_cast<int64_t>(lv.n) * W;
       XT *f = l == 0 ? B.res[0] : B.rhs[l];
       XT *u = l == 0 ? B.xt[0] : B.x[l];
@@ -213,6 +238,8 @@ bcmg_status tune_all(bcmg_handle *h, BatchState &S, CycleBufs<XT> &B) {
       BCMG_TRY(fill_t<XT>(u, cnt, XT(0), s));
       const XT *d = BtLv<XT>::M(lv) ? BtLv<XT>::M(lv) : BtLv<XT>::D(lv);
       BCMG_TRY(tune_level<XT>(h, BtLv<XT>::mat(lv), d, f, u, out, W, &S.cfg[k][l]));
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tuned[key] = S.cfg[k][l];
     }
   }
   return BCMG_OK;
