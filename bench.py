@@ -12,7 +12,9 @@ does (src/SOLVER/solver.cu:20-129).
          buffers: host->device copies of A, b and x0 and the device->host copy
          of x are inside the timed region.
   roofline  the dominant kernel (level-0 l1-Jacobi sweep) timed live with CUDA
-         events; algorithmic bytes from the sweep formula in DESIGN.md.
+         events; algorithmic bytes = stored values (slots x 32 x value bytes)
+         + explicit columns + 16 B of metadata per 32-row slice + u, f, d read
+         and u' written (4 n x vector bytes).
   cpu_baseline  the CPU oracle (multithreaded FP64 restatement of the same
          method) on a bounded sample of the same workload.
 
@@ -183,6 +185,13 @@ def aggregate_over_ranks(ms_local, steps, units_per_step, world, dist=None, devi
 
 
 # ---------------------------------------------------------------------------
+def clock_dir():
+    """Where the nvidia-smi clock samples of the timed region go
+    (BCMG_CLOCK_DIR, else the system temporary directory)."""
+    import tempfile
+    return os.environ.get("BCMG_CLOCK_DIR") or tempfile.gettempdir()
+
+
 def run_cpu_baseline(bc, orc, A, b, p, iters_hint, threads):
     """Oracle on a bounded sample: full setup + 3 FCG iterations, scaled to a
     complete solve with the same iteration count as the GPU FP64 run."""
@@ -303,8 +312,7 @@ def run_ours(args):
     if not info.converged:
         raise SystemExit(f"warm-up solve did not converge: {info}")
 
-    sampler = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else ".", f"clocks_rank{rank}.csv"))
+    sampler = ClockSampler(os.path.join(clock_dir(), f"clocks_rank{rank}.csv"))
     barrier()
     torch.cuda.synchronize(dev)
     sampler.start()
@@ -554,8 +562,7 @@ def run_batch(args):
         infos = step()
     if not all(i.converged for i in infos):
         raise SystemExit("warm-up batch did not converge")
-    sampler = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else ".", f"clocks_rank{rank}.csv"))
+    sampler = ClockSampler(os.path.join(clock_dir(), f"clocks_rank{rank}.csv"))
     barrier()
     torch.cuda.synchronize(dev)
     sampler.start()
