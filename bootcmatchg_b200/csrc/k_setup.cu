@@ -407,18 +407,17 @@ __global__ void k_sym_keys(int32_t n, const int32_t *__restrict__ row,
   }
 }
 
-// Suitor with symmetric weights: offer[y] = index of the current suitor's
-// entry in y's sorted row (kNoSuitor if none); a smaller index is a better
-// offer,
-// so one atomicMin both tests and installs an offer.  Same proposal chains
-// and resume points as k_suitor; exits at once when *nonsym is set.
-constexpr int32_t kNoSuitor = INT_MAX;  // above any entry index (nnz < 2^31)
-
+// Suitor with symmetric weights: offer[y] = (index of the current suitor's
+// entry in y's sorted row) << 32 | suitor (kNoOffer if none); a smaller
+// index is a better offer and identifies the proposer, so one 64-bit
+// atomicMin both tests and installs an offer and returns the displaced
+// proposer.  Same proposal chains and resume points as k_suitor; exits at
+// once when *nonsym is set.
 __global__ void __launch_bounds__(256)
     k_suitor_sym(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ ucnt,
                  const int32_t *__restrict__ scol, const int32_t *__restrict__ key,
-                 int32_t *next, int32_t *offer, int64_t limit, const int *__restrict__ nonsym,
-                 int *err) {
+                 int32_t *next, unsigned long long *offer, int64_t limit,
+                 const int *__restrict__ nonsym, int *err) {
   const int32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= n || *nonsym) return;
   volatile int32_t *vnext = next;
@@ -427,15 +426,26 @@ __global__ void __launch_bounds__(256)
   while (true) {
     int32_t k = vnext[cur];
     const int32_t e = row[cur] + ucnt[cur];
-    int32_t old = kNoSuitor, y = -1;
+    unsigned long long old = kNoOffer;
     bool found = false;
+    int32_t yk = 0, mk = 0;  // the candidate at k, loaded one step ahead
+    if (k < e) {
+      yk = scol[k];
+      mk = key[k];
+    }
     while (k < e) {
       if (++steps > limit) {
         atomicExch(err, 1);
         return;
       }
-      y = scol[k];
-      const int32_t mine = key[k];
+      const int32_t y = yk;
+      const unsigned long long mine =
+          (static_cast<unsigned long long>(static_cast<uint32_t>(mk)) << 32) |
+          static_cast<uint32_t>(cur);
+      if (k + 1 < e) {
+        yk = scol[k + 1];
+        mk = key[k + 1];
+      }
       old = atomicMin(offer + y, mine);
       if (old > mine) {
         found = true;
@@ -444,8 +454,8 @@ __global__ void __launch_bounds__(256)
       ++k;
     }
     vnext[cur] = found ? k + 1 : e;
-    if (!found || old == kNoSuitor) return;
-    cur = scol[old];  // the displaced proposer
+    if (!found || old == kNoOffer) return;
+    cur = static_cast<int32_t>(old & 0xffffffffull);  // the displaced proposer
   }
 }
 
@@ -506,29 +516,21 @@ __global__ void __launch_bounds__(256)
 
 // Resume points at each row's start; no offers yet.
 __global__ void k_init_match(int32_t n, const int32_t *__restrict__ row, int32_t *next,
-                             unsigned long long *offer, int32_t *offer_sym) {
+                             unsigned long long *offer) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   next[i] = row[i];
   offer[i] = kNoOffer;
-  offer_sym[i] = kNoSuitor;
 }
 
 // Suitor array from whichever matcher ran.
-__global__ void k_offer_to_suitor(int32_t n, const int32_t *__restrict__ row,
-                                  const int32_t *__restrict__ scol,
-                                  const unsigned long long *__restrict__ offer,
-                                  const int32_t *__restrict__ offer_sym,
-                                  const int *__restrict__ nonsym, int32_t *s) {
+// Both matchers keep the proposer in the offer's low 32 bits.
+__global__ void k_offer_to_suitor(int32_t n, const unsigned long long *__restrict__ offer,
+                                  int32_t *s) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (*nonsym) {
-    const unsigned long long o = offer[i];
-    s[i] = o == kNoOffer ? -1 : static_cast<int32_t>(o & 0xffffffffull);
-  } else {
-    const int32_t o = offer_sym[i];
-    s[i] = o == kNoSuitor ? -1 : scol[o];
-  }
+  const unsigned long long o = offer[i];
+  s[i] = o == kNoOffer ? -1 : static_cast<int32_t>(o & 0xffffffffull);
 }
 
 // unsymFix pass 1 (_setSymPair, src/AMG/unsymMatching.cu:32-50).
@@ -1521,14 +1523,13 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   phase_tick("weights");
   // Preference-sorted rows, then the suitor proposals.
   DevBuf<double> sW;
-  DevBuf<int32_t> scol, inv, ucnt, key, offer_sym, next, long_rows, n_long;
+  DevBuf<int32_t> scol, inv, ucnt, key, next, long_rows, n_long;
   DevBuf<int> nonsym;
   BCMG_TRY(sW.alloc(A.nnz, s));
   BCMG_TRY(scol.alloc(A.nnz, s));
   BCMG_TRY(inv.alloc(A.nnz, s));
   BCMG_TRY(key.alloc(A.nnz, s));
   BCMG_TRY(ucnt.alloc(n, s));
-  BCMG_TRY(offer_sym.alloc(n, s));
   BCMG_TRY(next.alloc(n, s));
   BCMG_TRY(long_rows.alloc(n, s));
   BCMG_TRY(n_long.alloc(1, s));
@@ -1559,15 +1560,14 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   phase_tick("sort_prefs");
   // Both matchers are launched; the one that does not apply (by *nonsym)
   // returns at once, so no host round trip decides between them.
-  launch(k_init_match, nb, T, 0, s, n, A.row, next.get(), offer.get(), offer_sym.get());
+  launch(k_init_match, nb, T, 0, s, n, A.row, next.get(), offer.get());
   const int64_t limit = 8 * static_cast<int64_t>(A.nnz) + 1024;
   launch(k_suitor_sym, nb, T, 0, s, n, A.row, ucnt.get(), scol.get(), key.get(), next.get(),
-         offer_sym.get(), limit, nonsym.get(), err.get());
+         offer.get(), limit, nonsym.get(), err.get());
   launch(k_suitor, nb, T, 0, s, n, A.row, scol.get(), sW.get(), next.get(), offer.get(), limit,
          nonsym.get(), err.get());
   BCMG_LAUNCH_CHECK();
-  launch(k_offer_to_suitor, nb, T, 0, s, n, A.row, scol.get(), offer.get(), offer_sym.get(),
-         nonsym.get(), sv.get());
+  launch(k_offer_to_suitor, nb, T, 0, s, n, offer.get(), sv.get());
   phase_tick("suitor");
 
   // unsymFix.
