@@ -74,3 +74,25 @@ def test_single_rank_needs_no_process_group():
     import bench
     ms, value = bench.aggregate_over_ranks(12.5, steps=4, units_per_step=1, world=1)
     assert ms == 12.5 and value == pytest.approx(4 / 0.0125)
+
+
+def test_reference_arm_json_line():
+    """bench.py --impl reference on the CPU: one JSON line with the metric of
+    the GPU arm, the CPU baseline it times and an e2e block without
+    transfers."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1")
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                          "--workload", "poisson7_32", "--steps", "1", "--warmup", "1"],
+                         capture_output=True, text=True, check=True, env=env, timeout=600)
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "solves/s"
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] in ("port", "reference")
+    assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": "solves/s",
+                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert line["config"]["workload"] == "poisson7_32"
