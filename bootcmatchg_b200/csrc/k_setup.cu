@@ -386,13 +386,20 @@ __global__ void k_sym_keys(int32_t n, const int32_t *__restrict__ row,
     const int32_t pa = inv[a];
     const double wya = sW[by + pa];
     if (x == y || !(wya > 0.0)) continue;
-    // the entry (x, y): binary search of y in row x (columns increasing)
+    // the entry (x, y): first the mirrored position (a symmetric stencil
+    // row of the same length holds y at index len - 1 - (a - by)), else a
+    // binary search of y in row x (columns increasing)
     int32_t lo = row[x], hi = row[x + 1] - 1;
     const int32_t bx = lo;
-    while (lo < hi) {
-      const int32_t mid = (lo + hi) >> 1;
-      if (col[mid] < y) lo = mid + 1;
-      else hi = mid;
+    const int32_t guess = hi - (a - by);
+    if (hi - lo == ey - 1 - by && col[guess] == y) {
+      lo = hi = guess;
+    } else {
+      while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (col[mid] < y) lo = mid + 1;
+        else hi = mid;
+      }
     }
     if (lo > hi || col[lo] != y) {
       atomicExch(nonsym, 1);
