@@ -379,14 +379,14 @@ def test_spgemm_tiers_match_oracle():
     """bcmg_k_spgemm bit for bit against the oracle's canonical-order product,
     with product rows in every tier of the kernel: up to 512 distinct
     columns (a warp, shared memory), up to 2,048 (a block, shared memory)
-    and beyond (a block, global memory)."""
+    and beyond (a block, global memory), plus empty and one-entry rows."""
     from test_cpu_oracle import rows_with_lengths
     rng = np.random.default_rng(8)
-    lengths = rng.choice([10, 60, 300], size=240)
+    lengths = rng.choice([0, 1, 10, 60, 300], size=240, p=[0.05, 0.05, 0.3, 0.3, 0.3])
     X = rows_with_lengths(lengths, 4000, 9)
     Y = rows_with_lengths([25] * 4000, 6000, 10)
     crow_o, ccol_o, cval_o = orc.spgemm(X, Y, 6000)
-    assert np.diff(crow_o).max() > 2048 and np.diff(crow_o).min() < 512
+    assert np.diff(crow_o).max() > 2048 and np.diff(crow_o).min() == 0
     xr, xc, xv = dev(X.row), dev(X.col), dev(X.val)
     yr, yc, yv = dev(Y.row), dev(Y.col), dev(Y.val)
     crow = torch.zeros(X.n + 1, dtype=torch.int32, device="cuda")
