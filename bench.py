@@ -16,11 +16,14 @@ does (src/SOLVER/solver.cu:20-129).
          + explicit columns + 16 B of metadata per 32-row slice + u, f, d read
          and u' written (4 n x vector bytes).
   cpu_baseline  the CPU oracle (multithreaded FP64 restatement of the same
-         method) on a bounded sample of the same workload.
+         method): one complete, timed solve of the workload on all host
+         threads, plus a 1-thread figure (setup timed in full, FCG iterations
+         from a timed sample); its solution also gives detail.err_vs_oracle.
 
---impl reference times the CPU implementation of the path (the oracle; the
-reference itself has no CPU path and its CUDA build needs cuSPARSE routines
-removed from CUDA 11+) on the host cores.
+--impl reference times the CPU implementation of the path on the host cores:
+the oracle (the reference has no CPU path, and its own GPU solve stopped with
+an illegal memory access on these inputs, so it is not run); every step is
+one complete solve.  It loads no product library.
 
 Multi-GPU: one solve never shards (global dots every iteration), so N GPUs
 run N independent replicas ("scaling": "weak"); value = all solves / the
@@ -43,6 +46,8 @@ if ROOT not in sys.path:
 
 import numpy as np  # noqa: E402
 
+import workloads as wl  # noqa: E402  (seeded synthetic inputs; not the product)
+
 METRIC = "solves/s to rtol 1e-8, mixed vs FP64 AMG-FCG"
 BATCH_RHS = 32
 
@@ -51,41 +56,49 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def c1_settings(bc):
-    p = bc.Params.default()
-    p.solver_type, p.max_hrc, p.conv_ratio = 0, 1, 0.8
-    p.aggrsweeps, p.aggrtype, p.max_levels, p.cycle_type = 2, 0, 20, 0
-    p.relax_type, p.coarse_solver = 4, 4
-    p.prerelax_sweeps, p.postrelax_sweeps, p.relaxnumber_coarse = 4, 4, 16
-    p.itnlim, p.rtol = 1000, 1e-8
-    return p
+def c1_settings():
+    """The 7-point Poisson 32^3 settings (single hierarchy, aggrsweeps 2,
+    unsmoothed, 20 levels, V-cycle, l1 smoother and l1 coarse solver, 4/4
+    sweeps, 16 coarse sweeps, itnlim 1000, rtol 1e-8); the other workloads
+    take them for every field they do not name.  A plain namespace, so the
+    CPU arm never loads the product library; the GPU arms convert it with
+    product_params()."""
+    import types
+    return types.SimpleNamespace(
+        solver_type=0, max_hrc=1, conv_ratio=0.8, matchtype=3, aggrsweeps=2, aggrtype=0,
+        max_levels=20, cycle_type=0, coarse_solver=4, relax_type=4, prerelax_sweeps=4,
+        postrelax_sweeps=4, itnlim=1000, rtol=1e-8, relaxnumber_coarse=16)
 
 
-def make_workload(bc, name):
+def product_params(bc, p):
+    return bc.Params(**vars(p))
+
+
+def make_workload(name):
     """Synthetic inputs with the shapes and distributions of the configs."""
-    p = c1_settings(bc)
+    p = c1_settings()
     if name == "poisson27_128":
-        A = bc.poisson(27, 128, 128, 128)
-        b = bc.vector(1, 1, A.n)
+        A = wl.poisson(27, 128, 128, 128)
+        b = wl.vector(1, 1, A.n)
         desc = "3-D 27-point Poisson 128^3 (center 26, neighbours -1), b ~ N(0,1) seed 1"
     elif name == "poisson7_32":
-        A = bc.poisson(7, 32, 32, 32)
-        b = bc.vector(0, 0, A.n)
+        A = wl.poisson(7, 32, 32, 32)
+        b = wl.vector(0, 0, A.n)
         desc = "3-D 7-point Poisson 32^3, Dirichlet, b = 1"
     elif name == "fv2d_2048":
-        A = bc.fv2d(2048, 2048, seed=2, aniso=1e-3)
-        b = bc.vector(2, 2, A.n)
+        A = wl.fv2d(2048, 2048, seed=2, aniso=1e-3)
+        b = wl.vector(2, 2, A.n)
         p.max_hrc, p.conv_ratio, p.solver_type = 3, 0.5, 0
         desc = ("2-D anisotropic FV -div(K grad u) 2048^2, K=exp(2g), g boxed N(0,1), "
                 "y-faces x1e-3, bootstrap max_hrc 3 rho 0.5, b ~ U[-1,1] seed 2")
     elif name == "poisson7_96":
-        A = bc.poisson(7, 96, 96, 96)
-        b = bc.vector(1, 3, A.n)
+        A = wl.poisson(7, 96, 96, 96)
+        b = wl.vector(1, 3, A.n)
         desc = "3-D 7-point Poisson 96^3, b ~ N(0,1) seed 3"
     elif name == "poisson7_96_x32":
-        A = bc.poisson(7, 96, 96, 96)
+        A = wl.poisson(7, 96, 96, 96)
         # 32 right-hand sides: one N(0,1) stream from seed 3, column-major.
-        b = np.asfortranarray(bc.vector(1, 3, A.n * BATCH_RHS).reshape(A.n, BATCH_RHS,
+        b = np.asfortranarray(wl.vector(1, 3, A.n * BATCH_RHS).reshape(A.n, BATCH_RHS,
                                                                        order="F"))
         desc = ("3-D 7-point Poisson 96^3 with 32 simultaneous right-hand sides "
                 "~ N(0,1) seed 3 (column-major), one shared hierarchy")
@@ -192,69 +205,121 @@ def clock_dir():
     return os.environ.get("BCMG_CLOCK_DIR") or tempfile.gettempdir()
 
 
-def run_cpu_baseline(bc, orc, A, b, p, iters_hint, threads):
-    """Oracle on a bounded sample: full setup + 3 FCG iterations, scaled to a
-    complete solve with the same iteration count as the GPU FP64 run."""
+def oracle_full_solve(orc, A, b, p, threads):
+    """One complete oracle solve (bootstrap setup + FCG from x0 = 0 to rtol)
+    on `threads` host threads, timed on the host clock."""
     orc.set_threads(threads)
     t0 = time.perf_counter()
     h = orc.OracleHandle(A, p)
-    setup_s = time.perf_counter() - t0
-    k = 3
-    # itnlim=k runs the first FCG step plus k loop passes: k+1 preconditioned
-    # iterations, the unit the reference's num_iter counts (FCG.cu:569).
-    it_s = h.fcg_sample(b, k) / (k + 1)
-    h.close()
-    per_solve = setup_s + iters_hint * it_s
-    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": (f"oracle setup ({setup_s:.2f} s) + {k} FCG iterations "
-                       f"({it_s:.3f} s each), scaled to {iters_hint} iterations"),
-            "setup_s": setup_s, "iter_s": it_s}
+    t1 = time.perf_counter()
+    x, info, st = h.solve(b)
+    t2 = time.perf_counter()
+    if st != 0 or not info["converged"]:
+        raise RuntimeError(f"oracle solve did not converge (status {st}, {info})")
+    return {"x": x, "iters": info["iters"], "setup_s": t1 - t0, "solve_s": t2 - t1,
+            "total_s": t2 - t0, "handle": h}
+
+
+def one_core_figure(orc, A, b, p, iters):
+    """The 1-thread figure beside the all-core one: 1-thread setup, timed in
+    full, plus a timed 2-iteration FCG sample scaled to `iters` iterations
+    (a complete 1-thread solve of the large workloads takes minutes)."""
+    orc.set_threads(1)
+    try:
+        t0 = time.perf_counter()
+        h = orc.OracleHandle(A, p)
+        setup_s = time.perf_counter() - t0
+        # itnlim=1 = first FCG step + one loop pass: 2 preconditioned
+        # iterations, the unit the reference's num_iter counts (FCG.cu:569).
+        it_s = h.fcg_sample(b, 1) / 2
+        h.close()
+    finally:
+        orc.set_threads(os.cpu_count() or 1)
+    per = setup_s + iters * it_s
+    return {"value": 1.0 / per, "unit": "solves/s", "cores": 1,
+            "sample": (f"1-thread setup ({setup_s:.2f} s, timed) + a timed 2-iteration FCG "
+                       f"sample ({it_s:.3f} s per iteration) scaled to {iters} iterations")}
+
+
+def run_cpu_baseline(orc, A, b, p, threads, nrhs=1):
+    """The oracle on the host cores: one complete, timed solve of the
+    workload (setup + FCG to convergence) on all threads; for nrhs > 1 the
+    setup is shared and every column's solve is counted at that one column's
+    solve time.  Also returns the oracle's solution for the error figure."""
+    full = oracle_full_solve(orc, A, b, p, threads)
+    full["handle"].close()
+    per = (full["setup_s"] + nrhs * full["solve_s"]) / nrhs
+    sample = (f"one complete oracle solve timed on {threads} threads: setup "
+              f"{full['setup_s']:.2f} s + {full['iters']} FCG iterations {full['solve_s']:.2f} s")
+    if nrhs > 1:
+        sample += f"; one setup shared by {nrhs} right-hand sides, each at that solve time"
+    out = {"value": 1.0 / per, "unit": "solves/s", "cores": threads, "kind": "port",
+           "sample": sample, "setup_s": full["setup_s"], "solve_s": full["solve_s"],
+           "iters": full["iters"]}
+    out["one_core"] = one_core_figure(orc, A, b, p, full["iters"])
+    return out, full["x"]
 
 
 def run_reference(args):
-    """CPU implementation of the path (the oracle) on the box's host cores."""
+    """The reference's method on the host cores: the multithreaded FP64 CPU
+    oracle (the reference has no CPU path of its own, and its GPU solve is not
+    run: it stopped with an illegal memory access on these inputs).  One step
+    = one complete solve (setup + FCG to rtol) of the workload, timed on the
+    host clock; the multi-right-hand-side workload shares one setup among its
+    32 columns and solves every column."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import bootcmatchg_b200 as bc
     from oracle import oracle as orc
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
-    A, b, p, desc = make_workload(bc, args.workload)
-    nrhs = 1
-    if b.ndim == 2:
-        # Multi-right-hand-side workload: one setup shared by all columns;
-        # column 0's iteration count stands for every column.
-        nrhs = b.shape[1]
-        b = np.ascontiguousarray(b[:, 0])
-    t0 = time.perf_counter()
-    h = orc.OracleHandle(A, p)
-    setup_s = time.perf_counter() - t0
-    # One full solve (untimed) gives the iteration count of this workload.
-    x, info, _ = h.solve(b)
-    iters = info["iters"]
+    if args.workload == "serve_stream":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the served stream has no CPU counterpart: the oracle solves "
+                          "one request at a time and the reference has no server"}))
+        return 0
+    A, b, p, desc = make_workload(args.workload)
+    cols = [b] if b.ndim == 1 else [np.ascontiguousarray(b[:, j]) for j in range(b.shape[1])]
+    nrhs = len(cols)
+
+    def step():
+        t0 = time.perf_counter()
+        h = orc.OracleHandle(A, p)
+        iters = []
+        for c in cols:
+            x, info, st = h.solve(c)
+            if st != 0 or not info["converged"]:
+                raise RuntimeError(f"oracle solve did not converge: {info}")
+            iters.append(info["iters"])
+        h.close()
+        return time.perf_counter() - t0, iters
+
     for _ in range(args.warmup):
-        h.fcg_sample(b, 1)
-    # itnlim=1 = first FCG step + one loop pass = 2 preconditioned iterations.
-    samples = [h.fcg_sample(b, 1) / 2 for _ in range(args.steps)]
-    it_s = statistics.median(samples)
-    per_solve = (setup_s + nrhs * iters * it_s) / nrhs
-    value = 1.0 / per_solve
-    sample = (f"setup {setup_s:.2f} s once + {iters} iterations x median of {args.steps} "
-              f"two-iteration samples ({it_s:.3f} s per iteration)")
+        step()
+    times, iters = [], []
+    for _ in range(args.steps):
+        t, it = step()
+        times.append(t)
+        iters = it
+    total = sum(times)
+    value = args.steps * nrhs / total
+    sample = (f"{args.steps} complete oracle solves (setup + FCG to rtol) timed on {threads} "
+              f"threads, median {statistics.median(times):.2f} s")
     if nrhs > 1:
-        sample += f"; one setup shared by {nrhs} right-hand sides"
+        sample = (f"{args.steps} steps of one oracle setup + {nrhs} complete column solves, "
+                  f"timed on {threads} threads, median {statistics.median(times):.2f} s")
+    one = one_core_figure(orc, A, cols[0], p, iters[0])
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": it_s * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "description": desc,
-                       "params": params_dict(p), "n": A.n, "nnz": A.nnz},
+                       "params": params_dict(p), "n": A.n, "nnz": A.nnz, "nrhs": nrhs},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads,
-                             "kind": "port", "sample": sample},
+                             "kind": "port", "sample": sample, "one_core": one},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "detail": {"iters": iters, "setup_s": setup_s, "iter_s": it_s}}
+            "detail": {"iters": iters, "step_s": times}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -277,7 +342,8 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    A, b_h, p, desc = make_workload(bc, args.workload)
+    A, b_h, p_plain, desc = make_workload(args.workload)
+    p = product_params(bc, p_plain)
     prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
     stream = torch.cuda.Stream(device=dev)
     # The anisotropic FV workload stores its coarse levels in BF16 (FP32
@@ -361,12 +427,14 @@ def run_ours(args):
     ext64 = bc.Extensions(precision=bc.PREC_FP64, device=local, stream=stream.cuda_stream,
                           narrow_values=0)
     compare = {}
+    x64 = None
     if prec == bc.PREC_MIXED:
         ext_saved = ext
         ext = ext64
         step()
         fp64_ms, fp64_infos = timed_ms(step, args.steps)
         ext = ext_saved
+        x64 = x.cpu().numpy()
         compare["fp64_full_solve"] = {"solves_per_s": 1e3 / fp64_ms, "ms_per_solve": fp64_ms,
                                       "iters": fp64_infos[-1].iters,
                                       "setup_ms": fp64_infos[-1].setup_ms}
@@ -432,7 +500,7 @@ def run_ours(args):
     xbytes = 4 if prec == bc.PREC_MIXED else 8
     with torch.cuda.stream(stream):
         f = torch.from_numpy(b_h).to(dev).to(xdt)
-        u = torch.from_numpy(bc.vector(1, 5, A.n)).to(dev).to(xdt)
+        u = torch.from_numpy(wl.vector(1, 5, A.n)).to(dev).to(xdt)
     stream.synchronize()
     sweeps = 20
     check(lib.bcmg_level_relax(h.ptr, 0, 0, C.c_void_p(f.data_ptr()), C.c_void_p(u.data_ptr()),
@@ -459,11 +527,18 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     traffic = committed_traffic("k_sl_pipe", f"{args.workload}:{args.precision}")
 
-    cpu = None
+    cpu, err = None, {}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as orc
         try:
-            cpu = run_cpu_baseline(bc, orc, A, b_h, p, info.iters, os.cpu_count() or 1)
+            cpu, x_orc = run_cpu_baseline(orc, A, b_h, p_plain, os.cpu_count() or 1)
+            # error of the GPU solutions against the FP64 oracle's solution of
+            # the same PCG + AMG (same settings, same right-hand side)
+            nrm = np.linalg.norm(x_orc)
+            err["err_vs_oracle"] = float(np.linalg.norm(xs - x_orc) / nrm)
+            if x64 is not None:
+                err["fp64_err_vs_oracle"] = float(np.linalg.norm(x64 - x_orc) / nrm)
+            err["oracle_iters"] = cpu["iters"]
         except Exception as exc:  # the baseline never blocks the GPU line
             cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {exc}"}
@@ -498,7 +573,7 @@ def run_ours(args):
         "clocks": clocks,
         "detail": {"iters": info.iters, "setup_ms": info.setup_ms, "solve_ms": info.solve_ms,
                    "rel_residual": info.rel_residual, "true_rel_residual": true_rel,
-                   "e2e_steps": e2e_steps, "compare": compare,
+                   **err, "e2e_steps": e2e_steps, "compare": compare,
                    "level0_cycle_value_bytes": vbytes.value},
     }
     print(json.dumps(line), flush=True)
@@ -529,7 +604,8 @@ def run_batch(args):
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    A, B_h, p, desc = make_workload(bc, args.workload)
+    A, B_h, p_plain, desc = make_workload(args.workload)
+    p = product_params(bc, p_plain)
     nrhs = B_h.shape[1]
     prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
     stream = torch.cuda.Stream(device=dev)
@@ -691,17 +767,14 @@ def run_batch(args):
     h2d = (A.n + 1) * 4 + A.nnz * 12 + 2 * A.n * nrhs * 8
     d2h = A.n * nrhs * 8
 
-    cpu = None
+    cpu, err = None, {}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as orc
         try:
-            one = run_cpu_baseline(bc, orc, A, B_h[:, 0].copy(), p, infos[0].iters,
-                                   os.cpu_count() or 1)
-            # setup once for all columns, then every column's iterations
-            per_batch = one["setup_s"] + sum(i.iters for i in infos) * one["iter_s"]
-            cpu = {"value": nrhs / per_batch, "unit": "solves/s", "cores": one["cores"],
-                   "kind": "port",
-                   "sample": one["sample"] + f"; one setup shared by {nrhs} columns"}
+            cpu, x_orc = run_cpu_baseline(orc, A, B_h[:, 0].copy(), p_plain,
+                                          os.cpu_count() or 1, nrhs=nrhs)
+            err["err_vs_oracle_column0"] = float(np.linalg.norm(X[:, 0] - x_orc)
+                                                 / np.linalg.norm(x_orc))
         except Exception as exc:
             cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {exc}"}
@@ -747,7 +820,7 @@ def run_batch(args):
                    "fp64_single_rhs_iters": [it for _, it in fp64_single],
                    "batched_mixed_over_fp64_single": (nrhs / (batch_solve_ms / 1e3))
                    / (1e3 / fp64_ms),
-                   "max_true_rel_residual": true_rel, "shapes": cfg,
+                   "max_true_rel_residual": true_rel, **err, "shapes": cfg,
                    "e2e_steps": e2e_steps},
     }
     print(json.dumps(line), flush=True)
@@ -759,7 +832,7 @@ def run_batch(args):
     return 0
 
 
-def serve_requests(bc, count, seed):
+def serve_requests(count, seed):
     """The serving stream: per request a matrix spec and a right-hand-side
     seed.  New matrices are 7-point or 27-point 3-D Poisson grids with side
     log-uniform in [16, 160] or random geometric graph Laplacians (unit
@@ -786,10 +859,10 @@ def serve_requests(bc, count, seed):
     return reqs
 
 
-def make_matrix(bc, spec):
+def make_matrix(spec):
     if spec[0] == "poisson":
-        return bc.poisson(spec[1], spec[2], spec[2], spec[2])
-    return bc.rgg(spec[1], seed=spec[2])
+        return wl.poisson(spec[1], spec[2], spec[2], spec[2])
+    return wl.rgg(spec[1], seed=spec[2])
 
 
 def run_serve(args):
@@ -806,10 +879,10 @@ def run_serve(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0  # replicas of the stream add nothing: one GPU per server
-    p = c1_settings(bc)
+    p = product_params(bc, c1_settings())
     prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
     ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
-    reqs = serve_requests(bc, args.requests, 11)
+    reqs = serve_requests(args.requests, 11)
     rng = np.random.default_rng(12)
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, len(reqs)))
     # Host matrices are generated ahead of their arrival by a thread pool and
@@ -826,7 +899,7 @@ def run_serve(args):
         while ahead < min(upto, len(reqs)):
             key = reqs[ahead][0]
             if key not in futures:
-                futures[key] = pool.submit(make_matrix, bc, key[1])
+                futures[key] = pool.submit(make_matrix, key[1])
             ahead += 1
     srv = bc.Server(p, ext, slots=args.slots, mem_cap_gb=150.0, cache_cap_gb=60.0,
                     max_batch=32)
@@ -847,7 +920,7 @@ def run_serve(args):
     for i, (key, rseed) in enumerate(reqs):
         prefetch(i + 48)
         A = futures[key].result()
-        b = bc.vector(1, rseed, A.n)
+        b = wl.vector(1, rseed, A.n)
         now = time.perf_counter() - t0
         if arrivals[i] > now:
             time.sleep(arrivals[i] - now)
@@ -902,6 +975,83 @@ def run_serve(args):
     return 0
 
 
+# ---- profiling cases (--case): small fixed workloads for ncu --------------
+def run_case(args):
+    """Small, fixed workloads for profiling single kernels under ncu.
+
+    sweep_fp32   level-0 smoother sweeps (--sweeps, default 3) of 27-point
+                 Poisson 128^3, mixed precision (FP32 sliced values)
+    sweep_fp64   the same in FP64
+    sweep_fv2d   level-0 smoother sweeps of the 2-D FV 2048^2 matrix
+                 (5-point), mixed precision
+    batch_fp32   batched smoother sweeps of 7-point Poisson 96^3 on 32
+                 interleaved columns (FP32), autotuning off
+    solve_mixed  one complete mixed-precision solve of 27-point Poisson
+                 GRID^3 (--grid, default 128), FCG loop driven from the host
+                 (every kernel is a plain launch a profiler can see)
+    batch_solve  one 32-column batched solve of 7-point Poisson 96^3 (mixed),
+                 FCG loop driven from the host
+    setup        one FP64 setup of 27-point Poisson GRID^3 (--grid, default
+                 96): matching, aggregation and Galerkin kernels
+
+    Each case sets up its hierarchy first and then runs the kernels of
+    interest; filter on kernel names such as k_sl_pipe or k_bt_rowop."""
+    import torch
+
+    import bootcmatchg_b200 as bc
+    from bootcmatchg_b200._lib import check, lib
+
+    p = product_params(bc, c1_settings())
+    case, k = args.case, args.sweeps
+    if case in ("sweep_fp32", "sweep_fp64", "sweep_fv2d"):
+        prec = bc.PREC_FP64 if case == "sweep_fp64" else bc.PREC_MIXED
+        A = wl.fv2d(2048, 2048, seed=2) if case == "sweep_fv2d" else wl.poisson(27, 128, 128, 128)
+        dt = torch.float32 if prec == bc.PREC_MIXED else torch.float64
+        with bc.Handle(A, p, bc.Extensions(precision=prec, replace_every=10)) as h:
+            f = torch.randn(A.n, dtype=dt, device="cuda:0")
+            u = torch.zeros(A.n, dtype=dt, device="cuda:0")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            check(lib.bcmg_level_relax(h.ptr, 0, 0, C.c_void_p(f.data_ptr()),
+                                       C.c_void_p(u.data_ptr()), k), "bcmg_level_relax")
+            print(f"{k} sweeps: {1e3 * (time.perf_counter() - t0):.3f} ms")
+    elif case == "batch_fp32":
+        A = wl.poisson(7, 96, 96, 96)
+        ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=10, autotune=0)
+        with bc.Handle(A, p, ext) as h:
+            f = torch.randn(A.n * 32, dtype=torch.float32, device="cuda:0")
+            u = torch.zeros(A.n * 32, dtype=torch.float32, device="cuda:0")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            check(lib.bcmg_level_relax_batch(h.ptr, 0, 0, 32, C.c_void_p(f.data_ptr()),
+                                             C.c_void_p(u.data_ptr()), k), "relax_batch")
+            print(f"{k} batched sweeps: {1e3 * (time.perf_counter() - t0):.3f} ms")
+    elif case == "solve_mixed":
+        g = args.grid or 128
+        A = wl.poisson(27, g, g, g)
+        b = wl.vector(1, 1, A.n)
+        ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=10, use_graphs=0)
+        with bc.Handle(A, p, ext) as h:
+            x, info = h.solve(b)
+        print(f"iters {info.iters} converged {info.converged} setup {info.setup_ms:.1f} ms "
+              f"solve {info.solve_ms:.1f} ms")
+    elif case == "batch_solve":
+        A = wl.poisson(7, 96, 96, 96)
+        B = np.asfortranarray(wl.vector(1, 3, A.n * 32).reshape(A.n, 32, order="F"))
+        ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=10, use_graphs=0)
+        with bc.Handle(A, p, ext) as h:
+            X, infos = h.solve_batch(B)
+        print(f"iters {max(i.iters for i in infos)} converged "
+              f"{all(i.converged for i in infos)} solve {infos[0].solve_ms:.1f} ms")
+    elif case == "setup":
+        g = args.grid or 96
+        A = wl.poisson(27, g, g, g)
+        with bc.Handle(A, p, bc.Extensions(precision=bc.PREC_FP64)) as h:
+            info = h.hierarchy_info(0)
+        print(f"levels {info['num_levels']} op_cmplx {info['op_cmplx']:.3f}")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -916,7 +1066,14 @@ def main():
     ap.add_argument("--slots", type=int, default=4, help="serve_stream: solves in flight")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["sweep_fp32", "sweep_fp64", "sweep_fv2d", "batch_fp32",
+                                       "solve_mixed", "batch_solve", "setup"],
+                    help="run one small profiling case instead of the benchmark")
+    ap.add_argument("--sweeps", type=int, default=3, help="--case: sweeps per launch")
+    ap.add_argument("--grid", type=int, default=None, help="--case setup/solve_mixed: side")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)
     if args.warmup < 3:
         log("[bench] warm-up raised to the minimum of 3 steps")
         args.warmup = 3

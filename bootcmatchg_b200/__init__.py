@@ -4,14 +4,14 @@ The product is libbcmg.so (C ABI in include/bcmg.h); this package binds it.
 """
 from .api import (CsrMatrix, Extensions, Handle, LevelData, Params, RequestResult, Server,
                   SolveResult, ERR_ALLOC, ERR_PARAM, ERR_PENDING,
-                  PREC_FP64, PREC_MIXED, STORE_BF16, STORE_FP16, STORE_FP32, fv2d,
-                  poisson, read_matrix_from_file, rgg, solve, vector, write_matrix_mm)
+                  PREC_FP64, PREC_MIXED, STORE_BF16, STORE_FP16, STORE_FP32,
+                  read_matrix_from_file, solve, write_matrix_mm)
 from ._lib import LIB_PATH, BcmgError, lib
 
 __all__ = [
     "CsrMatrix", "Extensions", "Handle", "LevelData", "Params", "RequestResult", "Server",
     "SolveResult", "ERR_ALLOC", "ERR_PARAM", "ERR_PENDING",
-    "PREC_FP64", "PREC_MIXED", "STORE_BF16", "STORE_FP16", "STORE_FP32", "fv2d",
-    "poisson", "read_matrix_from_file", "rgg", "solve", "vector", "write_matrix_mm",
+    "PREC_FP64", "PREC_MIXED", "STORE_BF16", "STORE_FP16", "STORE_FP32",
+    "read_matrix_from_file", "solve", "write_matrix_mm",
     "LIB_PATH", "BcmgError", "lib",
 ]

@@ -131,11 +131,6 @@ SIGNATURES = {
     "bcmg_k_relax": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, C.c_int, vp]),
     "bcmg_k_relax_noalloc": (C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, C.c_int, vp]),
     "bcmg_k_spmv": (C.c_int, [i32, i32, vp, vp, vp, C.c_double, vp, C.c_double, vp, vp]),
-    "bcmg_gen_poisson": (C.c_int, [C.c_int, i32, i32, i32, C.POINTER(Csr)]),
-    "bcmg_gen_fv2d": (C.c_int, [i32, i32, C.c_uint64, C.c_double, C.POINTER(Csr)]),
-    "bcmg_gen_rgg": (C.c_int, [i32, C.c_uint64, C.c_double, C.c_double, C.c_double,
-                               C.c_double, C.POINTER(Csr)]),
-    "bcmg_gen_vector": (C.c_int, [C.c_int, C.c_uint64, i32, vp]),
 }
 
 

@@ -59,6 +59,14 @@ class CsrMatrix:
         return sp.csr_matrix((self.val, self.col, self.row), shape=(self.n, self.m))
 
     @staticmethod
+    def of(A) -> "CsrMatrix":
+        """A itself, or a CsrMatrix over the n/row/col/val(/m) fields of any
+        host CSR object (no copy when the arrays already have the dtypes)."""
+        if isinstance(A, CsrMatrix):
+            return A
+        return CsrMatrix(A.n, A.row, A.col, A.val, getattr(A, "m", -1))
+
+    @staticmethod
     def from_scipy(a) -> "CsrMatrix":
         a = a.tocsr()
         a.sort_indices()
@@ -84,7 +92,7 @@ def read_matrix_from_file(path: str, m_type: int = 0) -> CsrMatrix:
 
 
 def write_matrix_mm(path: str, A: CsrMatrix) -> None:
-    c = A.as_c()
+    c = CsrMatrix.of(A).as_c()
     check(lib.bcmg_write_matrix_mm(path.encode(), C.byref(c)), "write_matrix_mm")
 
 
@@ -199,6 +207,7 @@ class Handle:
     def __init__(self, A: CsrMatrix, params: Params, ext: Extensions | None = None):
         self._h = C.c_void_p()
         ext = ext or Extensions()
+        A = CsrMatrix.of(A)
         c = A.as_c()
         p = params.to_c()
         e = ext.to_c()
@@ -378,6 +387,7 @@ class Server:
         self._live = {}  # ticket -> objects that must outlive the request
 
     def submit(self, A: CsrMatrix, b: np.ndarray, key: int = 0) -> int:
+        A = CsrMatrix.of(A)
         c = A.as_c()
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(A.n)
@@ -426,37 +436,10 @@ def solve(A: CsrMatrix, params: Params, rhs: np.ndarray,
     x0 = 0, teardown."""
     rhs = np.ascontiguousarray(rhs, dtype=np.float64)
     x = np.zeros(A.n)
-    c = A.as_c()
+    c = CsrMatrix.of(A).as_c()
     p = params.to_c()
     e = (ext or Extensions()).to_c()
     info = SolveInfo()
     check(lib.bcmg_solve_legacy(C.byref(c), C.byref(p), C.byref(e), _ptr(rhs), _ptr(x),
                                 C.byref(info)), "solve")
     return x, SolveResult.from_c(info)
-
-
-# ---- synthetic inputs -----------------------------------------------------
-def poisson(stencil: int, nx: int, ny: int, nz: int = 1) -> CsrMatrix:
-    c = Csr()
-    check(lib.bcmg_gen_poisson(stencil, nx, ny, nz, C.byref(c)), "gen_poisson")
-    return _take(c)
-
-
-def fv2d(nx: int, ny: int, seed: int = 2, aniso: float = 1e-3) -> CsrMatrix:
-    c = Csr()
-    check(lib.bcmg_gen_fv2d(nx, ny, seed, aniso, C.byref(c)), "gen_fv2d")
-    return _take(c)
-
-
-def rgg(n: int, seed: int, mean_degree: float = 12.0, wlo: float = 0.5, whi: float = 2.0,
-        shift: float = 1e-3) -> CsrMatrix:
-    c = Csr()
-    check(lib.bcmg_gen_rgg(n, seed, mean_degree, wlo, whi, shift, C.byref(c)), "gen_rgg")
-    return _take(c)
-
-
-def vector(kind: int, seed: int, n: int) -> np.ndarray:
-    """kind 0: ones, 1: standard normal, 2: uniform [-1, 1]."""
-    out = np.zeros(n)
-    check(lib.bcmg_gen_vector(kind, seed, n, _ptr(out)), "gen_vector")
-    return out

@@ -378,26 +378,6 @@ bcmg_status bcmg_k_spmv(int32_t n, int32_t nnz, const int32_t *d_row,
                         double alpha, const double *d_x, double beta,
                         double *d_y, void *stream);
 
-/* ---- synthetic inputs (shared by tests, bench and the CPU baseline) ------
- * Deterministic generators: splitmix64 + Box-Muller with fixed seeds.
- * stencil 7 or 27: 3-D Poisson on nx*ny*nz with Dirichlet boundary unknowns
- * eliminated (diag 6 / 26, neighbours -1), x-fastest ordering; stencil 5:
- * 2-D 5-point Poisson on nx*ny (nz ignored). */
-bcmg_status bcmg_gen_poisson(int stencil, int32_t nx, int32_t ny, int32_t nz,
-                             bcmg_csr *out);
-/* 2-D cell-centred finite-volume -div(K grad u) on nx*ny cells: K = exp(2 g),
- * g = 3x3 box filter (edge-clamped) of a standard normal field from seed;
- * harmonic face coefficients, y faces scaled by aniso, Dirichlet boundary
- * through half-cell faces 2 K. */
-bcmg_status bcmg_gen_fv2d(int32_t nx, int32_t ny, uint64_t seed, double aniso,
-                          bcmg_csr *out);
-/* Random geometric graph Laplacian in the unit cube: n points, radius for the
- * given mean degree, edge weights uniform [wlo, whi], L = D - W + shift I. */
-bcmg_status bcmg_gen_rgg(int32_t n, uint64_t seed, double mean_degree,
-                         double wlo, double whi, double shift, bcmg_csr *out);
-/* kind 0: ones; 1: standard normal; 2: uniform [-1, 1]. */
-bcmg_status bcmg_gen_vector(int kind, uint64_t seed, int32_t n, double *out);
-
 #ifdef __cplusplus
 }
 #endif

@@ -96,3 +96,29 @@ def test_reference_arm_json_line():
     assert line["e2e"] == {"value": line["value"], "unit": "solves/s",
                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] == "poisson7_32"
+    assert "one complete oracle solve" in line["cpu_baseline"]["sample"] or \
+        "complete oracle solves" in line["cpu_baseline"]["sample"]
+    assert line["cpu_baseline"]["one_core"]["cores"] == 1
+
+
+def test_reference_arm_loads_no_product_library():
+    """The reference arm runs the oracle only: neither the product package
+    nor libbcmg.so is loaded in its process."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import runpy, sys\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'poisson7_32',"
+        " '--steps', '1', '--warmup', '3']\n"
+        "try:\n"
+        f"    runpy.run_path({os.path.join(root, 'bench.py')!r}, run_name='__main__')\n"
+        "except SystemExit as e:\n"
+        "    assert not e.code, e.code\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('PRODUCT_LOADED' if ('libbcmg.so' in maps or 'bootcmatchg_b200' in sys.modules)"
+        " else 'NO_PRODUCT')\n")
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                         check=True, env=env, timeout=600, cwd=root)
+    assert out.stdout.strip().splitlines()[-1] == "NO_PRODUCT"

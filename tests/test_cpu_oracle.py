@@ -11,6 +11,7 @@ import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
 import bootcmatchg_b200 as bc
+import workloads as wl
 from helpers import c1_params, random_sym_graph
 from oracle import oracle as orc
 
@@ -29,35 +30,35 @@ def is_valid_matching(A, m):
 
 
 def test_generators_shapes():
-    A = bc.poisson(7, 32, 32, 32)
+    A = wl.poisson(7, 32, 32, 32)
     assert (A.n, A.nnz) == (32768, 223232)
-    B = bc.poisson(27, 8, 8, 8)
+    B = wl.poisson(27, 8, 8, 8)
     assert B.n == 512 and B.nnz == 512 * 27 - 6 * 64 * 9 + 12 * 8 * 3 - 8 * 1
     S = B.to_scipy()
     assert (S - S.T).nnz == 0
     assert np.all(S.diagonal() == 26.0)
-    P5 = bc.poisson(5, 6, 5)
+    P5 = wl.poisson(5, 6, 5)
     assert P5.n == 30 and P5.nnz == 30 * 5 - 2 * 6 - 2 * 5
-    F = bc.fv2d(16, 16, seed=2)
+    F = wl.fv2d(16, 16, seed=2)
     SF = F.to_scipy()
     assert abs(SF - SF.T).max() == 0.0
     rs = np.asarray(SF.sum(axis=1)).ravel().reshape(16, 16)
     assert np.all(rs[0, :] > 0) and np.all(rs[:, 0] > 0)  # Dirichlet boundary faces
     assert np.all(np.abs(rs[1:-1, 1:-1]) <= 1e-12 * SF.diagonal().max())
-    G = bc.rgg(3000, seed=5)
+    G = wl.rgg(3000, seed=5)
     SG = G.to_scipy()
     assert abs(SG - SG.T).max() == 0.0
     deg = np.diff(G.row) - 1
     assert 8 < deg.mean() < 13
-    v = bc.vector(1, 1, 100000)
+    v = wl.vector(1, 1, 100000)
     assert abs(v.mean()) < 0.02 and abs(v.std() - 1) < 0.02
-    u = bc.vector(2, 2, 100000)
+    u = wl.vector(2, 2, 100000)
     assert u.min() >= -1 and u.max() < 1 and abs(u.mean()) < 0.02
-    assert np.array_equal(bc.vector(1, 7, 10), bc.vector(1, 7, 10))
+    assert np.array_equal(wl.vector(1, 7, 10), wl.vector(1, 7, 10))
 
 
 def test_matrix_market_roundtrip(tmp_path):
-    A = bc.fv2d(10, 9, seed=3)
+    A = wl.fv2d(10, 9, seed=3)
     path = str(tmp_path / "a.mtx")
     bc.write_matrix_mm(path, A)
     B = bc.read_matrix_from_file(path)
@@ -156,7 +157,7 @@ def test_params_file_errors(tmp_path):
 # ---- weights --------------------------------------------------------------
 def test_weights_formula():
     A = random_sym_graph(300, 6, seed=1, int_weights=False)
-    w = bc.vector(1, 3, A.n)
+    w = wl.vector(1, 3, A.n)
     r = orc.pair_aggregate(A, w)
     S = A.to_scipy().tocoo()
     d = A.to_scipy().diagonal()
@@ -178,7 +179,7 @@ def test_weights_formula():
 @pytest.mark.parametrize("seed,intw", [(1, True), (2, True), (3, False), (4, True)])
 def test_suitor_equals_greedy_and_valid(seed, intw):
     A = random_sym_graph(2000, 8, seed=seed, int_weights=intw)
-    w = np.ones(A.n) if intw else bc.vector(1, seed, A.n)
+    w = np.ones(A.n) if intw else wl.vector(1, seed, A.n)
     r = orc.pair_aggregate(A, w)
     g = orc.greedy_match(A, r["W"])
     assert np.array_equal(r["match"], g)
@@ -220,7 +221,7 @@ def test_matching_known_answer_ties():
 
 def test_aggregation_invariants():
     A = random_sym_graph(3000, 7, seed=11, int_weights=False)
-    w = bc.vector(1, 4, A.n)
+    w = wl.vector(1, 4, A.n)
     w[::97] = 0.0  # bad singles / bad pairs
     r = orc.pair_aggregate(A, w)
     agg, p, nc = r["agg"], r["p"], r["nc"]
@@ -264,7 +265,7 @@ def test_unsymfix_lockstep_on_asymmetric_weights():
 @pytest.mark.parametrize("seed", [1, 2])
 def test_galerkin_matches_scipy_and_is_symmetric(seed):
     A = random_sym_graph(2500, 8, seed=seed, int_weights=False)
-    w = bc.vector(1, seed, A.n)
+    w = wl.vector(1, seed, A.n)
     r = orc.pair_aggregate(A, w)
     crow, ccol, cval = orc.galerkin(A, r["agg"], r["p"], r["nc"])
     Cm = sp.csr_matrix((cval, ccol, crow), shape=(r["nc"], r["nc"]))
@@ -285,11 +286,11 @@ def test_galerkin_matches_scipy_and_is_symmetric(seed):
 
 # ---- smoother, hierarchy, solve ----------------------------------------------
 def test_relax_matches_numpy():
-    A = bc.poisson(7, 10, 9, 8)
+    A = wl.poisson(7, 10, 9, 8)
     S = A.to_scipy()
     d = np.asarray(abs(S).sum(axis=1)).ravel()
-    f = bc.vector(1, 1, A.n)
-    u0 = bc.vector(2, 2, A.n)
+    f = wl.vector(1, 1, A.n)
+    u0 = wl.vector(2, 2, A.n)
     u = u0.copy()
     for _ in range(3):
         u = ((-(S @ u) + f) / d) + u
@@ -297,7 +298,7 @@ def test_relax_matches_numpy():
 
 
 def test_maxcoarsesize_and_levels_32cube():
-    A = bc.poisson(7, 32, 32, 32)
+    A = wl.poisson(7, 32, 32, 32)
     h = orc.OracleHandle(A, c1_params())
     info = h.hierarchy_info(0)
     # maxcoarsesize = (int)(40 * pow(32768, 1/3)) = 1279 (pow lands below 32)
@@ -308,8 +309,8 @@ def test_maxcoarsesize_and_levels_32cube():
 
 
 def test_oracle_solve_matches_direct():
-    A = bc.poisson(7, 14, 13, 12)
-    b = bc.vector(1, 1, A.n)
+    A = wl.poisson(7, 14, 13, 12)
+    b = wl.vector(1, 1, A.n)
     h = orc.OracleHandle(A, c1_params())
     x, info, st = h.solve(b)
     assert st == 0 and info["converged"]
@@ -322,14 +323,14 @@ def test_oracle_solve_matches_direct():
 @pytest.mark.parametrize("solver_type", [0, 1, 2])
 @pytest.mark.parametrize("cycle_type", [0, 1, 2])
 def test_oracle_composites_and_cycles(solver_type, cycle_type):
-    A = bc.fv2d(40, 40, seed=2)
+    A = wl.fv2d(40, 40, seed=2)
     p = c1_params()
     p.solver_type, p.cycle_type, p.max_hrc, p.conv_ratio = solver_type, cycle_type, 3, 0.1
     p.relax_type, p.coarse_solver = 0, 4
     h = orc.OracleHandle(A, p)
     nh, est = h.num_hierarchies()
     assert nh == 3
-    b = bc.vector(2, 2, A.n)
+    b = wl.vector(2, 2, A.n)
     x, info, st = h.solve(b)
     assert st == 0 and info["converged"] and info["iters"] < 200
 
@@ -339,8 +340,8 @@ def test_oracle_kcycle_converges_in_fewer_iterations():
     # (inneritkcycle, FCG.cu:633-723); its own checkP rejects the value, this
     # build accepts it.  On 7-point Poisson it needs fewer outer iterations
     # than the V-cycle and still solves to rtol.
-    A = bc.poisson(7, 24, 24, 24)
-    b = bc.vector(1, 3, A.n)
+    A = wl.poisson(7, 24, 24, 24)
+    b = wl.vector(1, 3, A.n)
     iters = {}
     for ct in (0, 3):
         p = c1_params()
@@ -366,8 +367,8 @@ def test_oracle_smoothed_aggregation_restates_the_algorithm():
     # R = P^T and A_{j+1} = (R A) P, D of the already smoothed A_j.  Checked
     # against scipy's products of the oracle's own level data, and the
     # smoothed hierarchy needs fewer iterations than the unsmoothed one.
-    A = bc.poisson(7, 16, 16, 16)
-    b = bc.vector(1, 3, A.n)
+    A = wl.poisson(7, 16, 16, 16)
+    b = wl.vector(1, 3, A.n)
     iters = {}
     for at in (0, 1):
         p = c1_params()
@@ -425,7 +426,7 @@ def test_oracle_spgemm_matches_scipy():
 def test_bootstrap_second_hierarchy_uses_same_w():
     # After hierarchy 1 the inner iterations are skipped (bootstrap.cu:68-75),
     # so hierarchy 2 is built from w = 1 again: it equals hierarchy 1.
-    A = bc.poisson(7, 12, 12, 12)
+    A = wl.poisson(7, 12, 12, 12)
     p = c1_params()
     p.max_hrc, p.conv_ratio = 2, 0.5
     h = orc.OracleHandle(A, p)
@@ -439,7 +440,7 @@ def test_bootstrap_second_hierarchy_uses_same_w():
 
 
 def test_already_converged_returns_zero_iterations():
-    A = bc.poisson(7, 6, 6, 6)
+    A = wl.poisson(7, 6, 6, 6)
     h = orc.OracleHandle(A, c1_params())
     x, info, st = h.solve(np.zeros(A.n))
     assert st == 0 and info["iters"] == 0

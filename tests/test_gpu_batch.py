@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import bootcmatchg_b200 as bc
+import workloads as wl
 from helpers import c1_params
 from oracle import oracle as orc
 
@@ -25,7 +26,7 @@ def rhs_block(n, seeds, zero_cols=()):
     B = np.zeros((n, len(seeds)), order="F")
     for j, s in enumerate(seeds):
         if j not in zero_cols:
-            B[:, j] = bc.vector(1, s, n)
+            B[:, j] = wl.vector(1, s, n)
     return B
 
 
@@ -47,7 +48,7 @@ def check_column(A, b, x, info, rtol, x0=None):
 
 @pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
 def test_batch_matches_oracle_and_single(prec):
-    A = bc.poisson(7, 16, 16, 16)
+    A = wl.poisson(7, 16, 16, 16)
     p = c1_params()
     B = rhs_block(A.n, [11, 12, 13, 14, 15], zero_cols=(3,))
     ext = bc.Extensions(precision=prec, replace_every=10 if prec == bc.PREC_MIXED else 0)
@@ -70,7 +71,7 @@ def test_batch_matches_oracle_and_single(prec):
 
 @pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
 def test_autotune_does_not_change_bits(prec):
-    A = bc.poisson(27, 14, 14, 14)
+    A = wl.poisson(27, 14, 14, 14)
     p = c1_params()
     B = rhs_block(A.n, list(range(20, 28)))
     out = []
@@ -91,7 +92,7 @@ def test_autotune_does_not_change_bits(prec):
 
 def test_batch_is_reproducible_and_device_path_agrees():
     import torch
-    A = bc.poisson(7, 18, 18, 18)
+    A = wl.poisson(7, 18, 18, 18)
     p = c1_params()
     nrhs, ld = 6, A.n + 5
     B = rhs_block(A.n, list(range(40, 40 + nrhs)))
@@ -111,7 +112,7 @@ def test_batch_is_reproducible_and_device_path_agrees():
 
 
 def test_more_columns_than_one_group():
-    A = bc.poisson(7, 12, 12, 12)
+    A = wl.poisson(7, 12, 12, 12)
     p = c1_params()
     B = rhs_block(A.n, list(range(100, 140)))  # 32 + 8 (padded) columns
     with bc.Handle(A, p) as h:
@@ -126,7 +127,7 @@ def test_more_columns_than_one_group():
 
 @pytest.mark.parametrize("solver_type", [0, 1, 2])
 def test_batch_bootstrap_composites(solver_type):
-    A = bc.fv2d(48, 48, seed=3)
+    A = wl.fv2d(48, 48, seed=3)
     p = c1_params()
     p.max_hrc, p.conv_ratio, p.solver_type = 3, 0.1, solver_type
     B = rhs_block(A.n, [7, 8, 9])
@@ -141,10 +142,10 @@ def test_batch_bootstrap_composites(solver_type):
 
 
 def test_batch_initial_guess_and_itnlim():
-    A = bc.poisson(7, 14, 14, 14)
+    A = wl.poisson(7, 14, 14, 14)
     p = c1_params()
     B = rhs_block(A.n, [3, 4])
-    X0 = np.asfortranarray(np.stack([bc.vector(2, 5, A.n), np.zeros(A.n)], axis=1))
+    X0 = np.asfortranarray(np.stack([wl.vector(2, 5, A.n), np.zeros(A.n)], axis=1))
     with bc.Handle(A, p) as h:
         X, infos = h.solve_batch(B, X0)
         for j in range(2):
@@ -161,7 +162,7 @@ def test_batch_initial_guess_and_itnlim():
 
 def test_precond_apply_batch_matches_single():
     import torch
-    A = bc.poisson(27, 12, 12, 12)
+    A = wl.poisson(27, 12, 12, 12)
     p = c1_params()
     n, nrhs = A.n, 4
     dev = torch.device("cuda:0")
@@ -180,7 +181,7 @@ def test_precond_apply_batch_matches_single():
 
 
 def test_batch_errors():
-    A = bc.poisson(7, 8, 8, 8)
+    A = wl.poisson(7, 8, 8, 8)
     with bc.Handle(A, c1_params()) as h:
         B = np.zeros((A.n, 2))
         X = np.zeros((A.n, 2))

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import bootcmatchg_b200 as bc
+import workloads as wl
 from helpers import c1_params
 from oracle import oracle as orc
 
@@ -19,9 +20,9 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("storage", [bc.STORE_FP32, bc.STORE_BF16, bc.STORE_FP16])
 @pytest.mark.parametrize("case", ["poisson27_24", "fv2d_96"])
 def test_mixed_solve_meets_fp64_tolerance(case, storage):
-    A = bc.poisson(27, 24, 24, 24) if case == "poisson27_24" else bc.fv2d(96, 96, seed=2)
+    A = wl.poisson(27, 24, 24, 24) if case == "poisson27_24" else wl.fv2d(96, 96, seed=2)
     p = c1_params()
-    b = bc.vector(1, 1, A.n)
+    b = wl.vector(1, 1, A.n)
     ext = bc.Extensions(precision=bc.PREC_MIXED, coarse_storage=storage, replace_every=10)
     with bc.Handle(A, p, ext) as h:
         x, info = h.solve(b)
@@ -39,10 +40,10 @@ def test_mixed_solve_meets_fp64_tolerance(case, storage):
 
 
 def test_mixed_bootstrap_composite():
-    A = bc.fv2d(80, 80, seed=2)
+    A = wl.fv2d(80, 80, seed=2)
     p = c1_params()
     p.max_hrc, p.conv_ratio, p.solver_type = 3, 0.1, 1
-    b = bc.vector(2, 2, A.n)
+    b = wl.vector(2, 2, A.n)
     ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=5)
     with bc.Handle(A, p, ext) as h, bc.Handle(A, p) as h64:
         assert h.num_hierarchies() == h64.num_hierarchies()
@@ -54,9 +55,9 @@ def test_mixed_bootstrap_composite():
 
 @pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
 def test_graph_loop_equals_host_loop(prec):
-    A = bc.poisson(7, 20, 20, 20)
+    A = wl.poisson(7, 20, 20, 20)
     p = c1_params()
-    b = bc.vector(1, 4, A.n)
+    b = wl.vector(1, 4, A.n)
     e1 = bc.Extensions(precision=prec, use_graphs=1, replace_every=7 if prec else 0)
     e0 = bc.Extensions(precision=prec, use_graphs=0, replace_every=7 if prec else 0)
     with bc.Handle(A, p, e1) as h1, bc.Handle(A, p, e0) as h0:
@@ -68,7 +69,7 @@ def test_graph_loop_equals_host_loop(prec):
 
 
 def test_itnlim_respected():
-    A = bc.poisson(7, 16, 16, 16)
+    A = wl.poisson(7, 16, 16, 16)
     p = c1_params()
     p.itnlim, p.rtol = 3, 1e-14
     with bc.Handle(A, p) as h:
@@ -84,13 +85,13 @@ def test_sliced_level_relax_matches_oracle(case):
     import ctypes as C
     import torch
     from bootcmatchg_b200._lib import check, lib
-    A = bc.poisson(27, 20, 20, 20) if case == "poisson27_20" else bc.rgg(20000, seed=3)
+    A = wl.poisson(27, 20, 20, 20) if case == "poisson27_20" else wl.rgg(20000, seed=3)
     p = c1_params()
     with bc.Handle(A, p) as h:
         L = h.hierarchy_info()["num_levels"]
         for level in range(min(3, L)):
             lv = h.level(0, level)
-            f, u0 = bc.vector(1, level + 1, lv.n), bc.vector(2, level + 2, lv.n)
+            f, u0 = wl.vector(1, level + 1, lv.n), wl.vector(2, level + 2, lv.n)
             ft = torch.from_numpy(f).cuda()
             ut = torch.from_numpy(u0).cuda()
             check(lib.bcmg_level_relax(h.ptr, 0, level, C.c_void_p(ft.data_ptr()),
@@ -102,9 +103,9 @@ def test_sliced_level_relax_matches_oracle(case):
 
 
 def test_sliced_and_csr_solves_agree():
-    A = bc.rgg(30000, seed=2)
+    A = wl.rgg(30000, seed=2)
     p = c1_params()
-    b = bc.vector(1, 8, A.n)
+    b = wl.vector(1, 8, A.n)
     with bc.Handle(A, p, bc.Extensions(sliced=1)) as h1, \
             bc.Handle(A, p, bc.Extensions(sliced=0)) as h0:
         x1, i1 = h1.solve(b)
@@ -122,9 +123,9 @@ def test_exact_value_narrowing_is_bit_identical(prec):
     cycle's FP32 copy is not narrowed."""
     import ctypes as C
     from bootcmatchg_b200._lib import check, lib
-    A = bc.poisson(27, 32, 32, 32)
+    A = wl.poisson(27, 32, 32, 32)
     p = c1_params()
-    b = bc.vector(1, 5, A.n)
+    b = wl.vector(1, 5, A.n)
     out = []
     for narrow in (1, 0):
         ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0,

@@ -16,6 +16,7 @@ import pytest
 import scipy.sparse as sp
 
 import bootcmatchg_b200 as bc
+import workloads as wl
 from bootcmatchg_b200._lib import check, lib
 from helpers import c1_params, random_sym_graph
 from oracle import oracle as orc
@@ -82,14 +83,14 @@ def star(n_leaves):
 
 
 CASES = {
-    "poisson7_16": lambda: (bc.poisson(7, 16, 16, 16), None),
-    "poisson27_10": lambda: (bc.poisson(27, 10, 10, 10), None),
-    "poisson5_40": lambda: (bc.poisson(5, 40, 40), None),
-    "fv2d_64": lambda: (bc.fv2d(64, 64, seed=2), None),
-    "rgg_20000": lambda: (bc.rgg(20000, seed=4), None),
+    "poisson7_16": lambda: (wl.poisson(7, 16, 16, 16), None),
+    "poisson27_10": lambda: (wl.poisson(27, 10, 10, 10), None),
+    "poisson5_40": lambda: (wl.poisson(5, 40, 40), None),
+    "fv2d_64": lambda: (wl.fv2d(64, 64, seed=2), None),
+    "rgg_20000": lambda: (wl.rgg(20000, seed=4), None),
     "rand_int_ties": lambda: (random_sym_graph(5000, 8, seed=3, int_weights=True), None),
     "rand_float_w": lambda: (random_sym_graph(5000, 8, seed=4, int_weights=False),
-                             bc.vector(1, 9, 5000)),
+                             wl.vector(1, 9, 5000)),
     "asymmetric": lambda: (asym(random_sym_graph(4000, 8, seed=6, int_weights=False), 1),
                            None),
     "zero_w_entries": lambda: (random_sym_graph(3000, 6, seed=8, int_weights=False),
@@ -126,10 +127,10 @@ def test_galerkin_parity(case):
 
 
 def test_relax_and_spmv_parity():
-    A = bc.poisson(27, 12, 11, 10)
+    A = wl.poisson(27, 12, 11, 10)
     S = A.to_scipy()
     d = np.asarray(abs(S).sum(axis=1)).ravel()
-    f, u0 = bc.vector(1, 1, A.n), bc.vector(2, 2, A.n)
+    f, u0 = wl.vector(1, 1, A.n), wl.vector(2, 2, A.n)
     row, col, val = dev(A.row), dev(A.col), dev(A.val)
     dd, ff, uu = dev(d), dev(f), dev(u0)
     for k in (1, 2, 3):
@@ -138,7 +139,7 @@ def test_relax_and_spmv_parity():
                                None), "relax")
         np.testing.assert_allclose(uu.cpu().numpy(), orc.relax(A, d, f, u0, k), rtol=1e-13,
                                    atol=1e-13)
-    x, y0 = bc.vector(1, 3, A.n), bc.vector(1, 4, A.n)
+    x, y0 = wl.vector(1, 3, A.n), wl.vector(1, 4, A.n)
     xx, yy = dev(x), dev(y0)
     check(lib.bcmg_k_spmv(A.n, A.nnz, P(row), P(col), P(val), 2.0, P(xx), -0.5, P(yy), None),
           "spmv")
@@ -164,10 +165,10 @@ def compare_hierarchies(h, o, hrc=0, ohrc=None):
 
 
 HIER_CASES = {
-    "poisson7_32": lambda: bc.poisson(7, 32, 32, 32),
-    "poisson27_20": lambda: bc.poisson(27, 20, 20, 20),
-    "fv2d_128": lambda: bc.fv2d(128, 128, seed=2),
-    "rgg_30000": lambda: bc.rgg(30000, seed=11),
+    "poisson7_32": lambda: wl.poisson(7, 32, 32, 32),
+    "poisson27_20": lambda: wl.poisson(27, 20, 20, 20),
+    "fv2d_128": lambda: wl.fv2d(128, 128, seed=2),
+    "rgg_30000": lambda: wl.rgg(30000, seed=11),
 }
 
 
@@ -175,7 +176,7 @@ HIER_CASES = {
 def test_hierarchy_and_solve_parity(case):
     A = HIER_CASES[case]()
     p = c1_params()
-    b = bc.vector(1, 1, A.n)
+    b = wl.vector(1, 1, A.n)
     with bc.Handle(A, p) as h:
         o = orc.OracleHandle(A, p)
         compare_hierarchies(h, o)
@@ -192,11 +193,11 @@ def test_hierarchy_and_solve_parity(case):
 @pytest.mark.parametrize("solver_type", [0, 1, 2])
 @pytest.mark.parametrize("cycle_type", [0, 1, 2])
 def test_bootstrap_composites_cycles(solver_type, cycle_type):
-    A = bc.fv2d(64, 64, seed=2)
+    A = wl.fv2d(64, 64, seed=2)
     p = c1_params()
     p.solver_type, p.cycle_type, p.max_hrc, p.conv_ratio = solver_type, cycle_type, 3, 0.1
     p.relax_type, p.coarse_solver = 0, 4
-    b = bc.vector(2, 2, A.n)
+    b = wl.vector(2, 2, A.n)
     with bc.Handle(A, p) as h:
         o = orc.OracleHandle(A, p)
         nh, est = h.num_hierarchies()
@@ -214,7 +215,7 @@ def test_bootstrap_composites_cycles(solver_type, cycle_type):
                                    atol=1e-12 * np.abs(gw).max())
         compare_hierarchies(h, orc.OracleHandle(A, p, w=gw), 2, 0)
         # one preconditioner application from a nonzero guess
-        r0, z0 = bc.vector(1, 5, A.n), bc.vector(1, 6, A.n)
+        r0, z0 = wl.vector(1, 5, A.n), wl.vector(1, 6, A.n)
         rt, zt = dev(r0), dev(z0)
         h.precond_apply_device(rt.data_ptr(), zt.data_ptr())
         zo = o.precond_apply(r0, z0)
@@ -227,7 +228,7 @@ def test_bootstrap_composites_cycles(solver_type, cycle_type):
 
 
 def test_setup_is_deterministic():
-    A = bc.rgg(20000, seed=3)
+    A = wl.rgg(20000, seed=3)
     p = c1_params()
     with bc.Handle(A, p) as h1, bc.Handle(A, p) as h2:
         L = h1.hierarchy_info()["num_levels"]
@@ -252,7 +253,7 @@ def test_edge_cases():
     x, info = bc.solve(D, p, np.ones(n))
     np.testing.assert_allclose(x, 1 / np.linspace(1, 2, n), rtol=1e-12)
     # zero right-hand side: already converged
-    B = bc.poisson(7, 8, 8, 8)
+    B = wl.poisson(7, 8, 8, 8)
     x, info = bc.solve(B, p, np.zeros(B.n))
     assert info.iters == 0 and np.all(x == 0)
 
@@ -265,7 +266,7 @@ def test_errors():
 
 
 def test_cli_matches_reference_format(tmp_path):
-    A = bc.poisson(7, 10, 10, 10)
+    A = wl.poisson(7, 10, 10, 10)
     mtx = tmp_path / "a.mtx"
     bc.write_matrix_mm(str(mtx), A)
     settings = tmp_path / "settings"
@@ -290,10 +291,10 @@ def test_kcycle_matches_oracle(prec):
     FCG.cu:633-723) on the GPU against the oracle's: same hierarchy, the
     solution within 1e-6 and the outer iteration count within one.  Batched
     solves refuse the K-cycle."""
-    A = bc.poisson(27, 20, 20, 20)
+    A = wl.poisson(27, 20, 20, 20)
     p = c1_params()
     p.cycle_type = 3
-    b = bc.vector(1, 11, A.n)
+    b = wl.vector(1, 11, A.n)
     ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
     with bc.Handle(A, p, ext) as h:
         x, info = h.solve(b)
@@ -311,10 +312,10 @@ def test_hierarchy_file_roundtrip(tmp_path):
     """bcmg_save / bcmg_load: the loaded handle has the same levels bit for bit
     and solves to the same bits; a hierarchy saved from an FP64 setup also
     loads for mixed-precision solves."""
-    A = bc.fv2d(64, 64, seed=2)
+    A = wl.fv2d(64, 64, seed=2)
     p = c1_params()
     p.max_hrc, p.conv_ratio, p.solver_type = 2, 0.1, 0
-    b = bc.vector(2, 4, A.n)
+    b = wl.vector(2, 4, A.n)
     path = tmp_path / "h.bcmg"
     with bc.Handle(A, p) as h:
         x0, i0 = h.solve(b)
@@ -339,10 +340,10 @@ def test_hierarchy_file_roundtrip(tmp_path):
 
 
 SMOOTHED_CASES = {
-    "poisson7_20": lambda: bc.poisson(7, 20, 20, 20),
-    "poisson27_12": lambda: bc.poisson(27, 12, 12, 12),
-    "fv2d_64": lambda: bc.fv2d(64, 64, seed=2),
-    "rgg_20000": lambda: bc.rgg(20000, seed=11),
+    "poisson7_20": lambda: wl.poisson(7, 20, 20, 20),
+    "poisson27_12": lambda: wl.poisson(27, 12, 12, 12),
+    "fv2d_64": lambda: wl.fv2d(64, 64, seed=2),
+    "rgg_20000": lambda: wl.rgg(20000, seed=11),
 }
 
 
@@ -356,7 +357,7 @@ def test_smoothed_aggregation_matches_oracle(case):
     A = SMOOTHED_CASES[case]()
     p = c1_params()
     p.aggrtype = 1
-    b = bc.vector(1, 7, A.n)
+    b = wl.vector(1, 7, A.n)
     o = orc.OracleHandle(A, p)
     xo, oi, st = o.solve(b)
     assert st == 0 and oi["converged"]

@@ -14,19 +14,20 @@ import numpy as np
 import pytest
 
 import bootcmatchg_b200 as bc
+import workloads as wl
 from helpers import c1_params
 
 pytestmark = pytest.mark.gpu
 
 
 def mix():
-    mats = [bc.poisson(7, 10, 10, 10), bc.poisson(27, 8, 8, 8), bc.rgg(2000, seed=7),
-            bc.fv2d(24, 24, seed=2), bc.poisson(7, 20, 20, 20)]
+    mats = [wl.poisson(7, 10, 10, 10), wl.poisson(27, 8, 8, 8), wl.rgg(2000, seed=7),
+            wl.fv2d(24, 24, seed=2), wl.poisson(7, 20, 20, 20)]
     rng = np.random.default_rng(5)
     reqs = []
     for k in range(24):
         m = int(rng.integers(0, len(mats)))
-        reqs.append((m, bc.vector(1, 1000 + k, mats[m].n)))
+        reqs.append((m, wl.vector(1, 1000 + k, mats[m].n)))
     return mats, reqs
 
 
@@ -58,8 +59,8 @@ def test_same_alone_and_in_the_mix():
 
 def test_grouped_requests_match_their_single_solves():
     p = c1_params()
-    A = bc.poisson(7, 16, 16, 16)
-    bs = [bc.vector(1, 2000 + k, A.n) for k in range(12)]
+    A = wl.poisson(7, 16, 16, 16)
+    bs = [wl.vector(1, 2000 + k, A.n) for k in range(12)]
     with bc.Server(p, slots=1, max_batch=32) as srv:
         first = srv.submit(A, bs[0], key=7)
         tickets = [srv.submit(A, b, key=7) for b in bs[1:]]  # queue behind the setup
@@ -91,8 +92,8 @@ def test_cache_budget_evicts_and_keeps_results():
 
 def test_admission_rejects_what_cannot_fit():
     p = c1_params()
-    small = bc.poisson(7, 8, 8, 8)
-    big = bc.poisson(7, 64, 64, 64)  # ~0.14 GB estimated
+    small = wl.poisson(7, 8, 8, 8)
+    big = wl.poisson(7, 64, 64, 64)  # ~0.14 GB estimated
     with bc.Server(p, slots=2, mem_cap_gb=0.05) as srv:
         tb = srv.submit(big, np.ones(big.n), key=1)
         ts = srv.submit(small, np.ones(small.n), key=2)
@@ -107,7 +108,7 @@ def test_admission_rejects_what_cannot_fit():
 
 def test_wait_timeout_and_stats():
     p = c1_params()
-    A = bc.poisson(7, 40, 40, 40)
+    A = wl.poisson(7, 40, 40, 40)
     with bc.Server(p, slots=1) as srv:
         t = srv.submit(A, np.ones(A.n), key=3)
         polls = 0

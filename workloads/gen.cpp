@@ -1,4 +1,7 @@
-// Deterministic synthetic inputs for the solve path (host code).
+// Deterministic synthetic inputs for the solve path (host code): the
+// workload generators shared by the tests, bench.py's GPU arm and its CPU
+// baseline.  Built as its own library (libworkloads.so) so that neither the
+// product library nor the CPU oracle carries them.
 //
 // The reference ships no test matrices (its only sample, pi8grid6.mtx, is
 // absent), so every workload is generated here from fixed seeds with one
@@ -7,14 +10,52 @@
 // rows in x-fastest lexicographic order for grids.
 #include <algorithm>
 #include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
 
-#include "host_util.h"
+extern "C" {
+/* Same layout as bcmg_csr: 0-based CSR, int32 indices, FP64 values. */
+typedef struct {
+  int32_t n, m, nnz;
+  int32_t *row;
+  int32_t *col;
+  double *val;
+} wl_csr;
+}
 
-namespace bcmg {
+namespace wl {
 namespace {
+
+enum { WL_OK = 0, WL_ERR_PARAM = 1, WL_ERR_ALLOC = 3 };
+
+thread_local char g_err[256];
+
+int set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define WL_TRY(expr)           \
+  do {                         \
+    int _st = (expr);          \
+    if (_st != WL_OK) return _st; \
+  } while (0)
+
+void csr_free(wl_csr *c) {
+  if (!c) return;
+  std::free(c->row);
+  std::free(c->col);
+  std::free(c->val);
+  c->row = c->col = nullptr;
+  c->val = nullptr;
+}
 
 struct SplitMix64 {
   uint64_t s;
@@ -50,38 +91,41 @@ struct Normal {
   }
 };
 
-bcmg_status alloc_csr(int32_t n, int64_t nnz, bcmg_csr *out) {
-  if (nnz > INT32_MAX) return set_error(BCMG_ERR_PARAM, "nnz %lld exceeds int32", (long long)nnz);
+int alloc_csr(int32_t n, int64_t nnz, wl_csr *out) {
+  if (nnz > INT32_MAX) return set_error(WL_ERR_PARAM, "nnz %lld exceeds int32", (long long)nnz);
   out->n = out->m = n;
   out->nnz = static_cast<int32_t>(nnz);
   out->row = static_cast<int32_t *>(malloc(sizeof(int32_t) * (n + 1)));
   out->col = static_cast<int32_t *>(malloc(sizeof(int32_t) * (nnz > 0 ? nnz : 1)));
   out->val = static_cast<double *>(malloc(sizeof(double) * (nnz > 0 ? nnz : 1)));
   if (!out->row || !out->col || !out->val) {
-    bcmg_csr_free(out);
-    return set_error(BCMG_ERR_ALLOC, "host allocation failed");
+    csr_free(out);
+    return set_error(WL_ERR_ALLOC, "host allocation failed");
   }
-  return BCMG_OK;
+  return WL_OK;
 }
 
 }  // namespace
-}  // namespace bcmg
+}  // namespace wl
 
-using namespace bcmg;
+using namespace wl;
 
 extern "C" {
 
-bcmg_status bcmg_gen_poisson(int stencil, int32_t nx, int32_t ny, int32_t nz,
-                             bcmg_csr *out) {
-  if (!out) return set_error(BCMG_ERR_PARAM, "null output");
+const char *wl_last_error(void) { return g_err; }
+
+void wl_csr_free(wl_csr *c) { csr_free(c); }
+
+int wl_poisson(int stencil, int32_t nx, int32_t ny, int32_t nz, wl_csr *out) {
+  if (!out) return set_error(WL_ERR_PARAM, "null output");
   std::memset(out, 0, sizeof(*out));
   if (stencil == 5) nz = 1;
   if (nx <= 0 || ny <= 0 || nz <= 0)
-    return set_error(BCMG_ERR_PARAM, "grid sizes must be positive");
+    return set_error(WL_ERR_PARAM, "grid sizes must be positive");
   if (stencil != 5 && stencil != 7 && stencil != 27)
-    return set_error(BCMG_ERR_PARAM, "stencil must be 5, 7 or 27");
+    return set_error(WL_ERR_PARAM, "stencil must be 5, 7 or 27");
   const int64_t n64 = static_cast<int64_t>(nx) * ny * nz;
-  if (n64 > INT32_MAX) return set_error(BCMG_ERR_PARAM, "grid too large for int32");
+  if (n64 > INT32_MAX) return set_error(WL_ERR_PARAM, "grid too large for int32");
   const int32_t n = static_cast<int32_t>(n64);
   // Offsets in increasing linear-index order so rows come out sorted.
   std::vector<int> ox, oy, oz;
@@ -119,20 +163,19 @@ bcmg_status bcmg_gen_poisson(int stencil, int32_t nx, int32_t ny, int32_t nz,
         }
         row[r + 1] = static_cast<int32_t>(col.size());
       }
-  BCMG_TRY(alloc_csr(n, static_cast<int64_t>(col.size()), out));
+  WL_TRY(alloc_csr(n, static_cast<int64_t>(col.size()), out));
   std::memcpy(out->row, row.data(), sizeof(int32_t) * (n + 1));
   std::memcpy(out->col, col.data(), sizeof(int32_t) * col.size());
   std::memcpy(out->val, val.data(), sizeof(double) * val.size());
-  return BCMG_OK;
+  return WL_OK;
 }
 
-bcmg_status bcmg_gen_fv2d(int32_t nx, int32_t ny, uint64_t seed, double aniso,
-                          bcmg_csr *out) {
-  if (!out) return set_error(BCMG_ERR_PARAM, "null output");
+int wl_fv2d(int32_t nx, int32_t ny, uint64_t seed, double aniso, wl_csr *out) {
+  if (!out) return set_error(WL_ERR_PARAM, "null output");
   std::memset(out, 0, sizeof(*out));
-  if (nx <= 0 || ny <= 0) return set_error(BCMG_ERR_PARAM, "grid sizes must be positive");
+  if (nx <= 0 || ny <= 0) return set_error(WL_ERR_PARAM, "grid sizes must be positive");
   const int64_t n64 = static_cast<int64_t>(nx) * ny;
-  if (n64 * 5 > INT32_MAX) return set_error(BCMG_ERR_PARAM, "grid too large");
+  if (n64 * 5 > INT32_MAX) return set_error(WL_ERR_PARAM, "grid too large");
   const int32_t n = static_cast<int32_t>(n64);
   std::vector<double> g0(n), g(n), K(n);
   Normal nrm(seed);
@@ -170,18 +213,18 @@ bcmg_status bcmg_gen_fv2d(int32_t nx, int32_t ny, uint64_t seed, double aniso,
       if (y < ny - 1) { col.push_back(c + nx); val.push_back(-fn); }
       row[c + 1] = static_cast<int32_t>(col.size());
     }
-  BCMG_TRY(alloc_csr(n, static_cast<int64_t>(col.size()), out));
+  WL_TRY(alloc_csr(n, static_cast<int64_t>(col.size()), out));
   std::memcpy(out->row, row.data(), sizeof(int32_t) * (n + 1));
   std::memcpy(out->col, col.data(), sizeof(int32_t) * col.size());
   std::memcpy(out->val, val.data(), sizeof(double) * val.size());
-  return BCMG_OK;
+  return WL_OK;
 }
 
-bcmg_status bcmg_gen_rgg(int32_t n, uint64_t seed, double mean_degree, double wlo,
-                         double whi, double shift, bcmg_csr *out) {
-  if (!out) return set_error(BCMG_ERR_PARAM, "null output");
+int wl_rgg(int32_t n, uint64_t seed, double mean_degree, double wlo, double whi,
+           double shift, wl_csr *out) {
+  if (!out) return set_error(WL_ERR_PARAM, "null output");
   std::memset(out, 0, sizeof(*out));
-  if (n <= 1 || !(mean_degree > 0)) return set_error(BCMG_ERR_PARAM, "bad RGG sizes");
+  if (n <= 1 || !(mean_degree > 0)) return set_error(WL_ERR_PARAM, "bad RGG sizes");
   // Radius so that the expected number of neighbours in the (unbounded)
   // unit-density ball is mean_degree: n * 4/3 pi r^3 = mean_degree.
   const double r = std::cbrt(mean_degree / (static_cast<double>(n) * 4.0 / 3.0 *
@@ -236,7 +279,7 @@ bcmg_status bcmg_gen_rgg(int32_t n, uint64_t seed, double mean_degree, double wl
   }
   int64_t nnz = n;
   for (int32_t i = 0; i < n; ++i) nnz += static_cast<int64_t>(adj[i].size());
-  BCMG_TRY(alloc_csr(n, nnz, out));
+  WL_TRY(alloc_csr(n, nnz, out));
   int64_t w = 0;
   out->row[0] = 0;
   for (int32_t i = 0; i < n; ++i) {
@@ -261,11 +304,11 @@ bcmg_status bcmg_gen_rgg(int32_t n, uint64_t seed, double mean_degree, double wl
     }
     out->row[i + 1] = static_cast<int32_t>(w);
   }
-  return BCMG_OK;
+  return WL_OK;
 }
 
-bcmg_status bcmg_gen_vector(int kind, uint64_t seed, int32_t n, double *out) {
-  if (!out || n < 0) return set_error(BCMG_ERR_PARAM, "bad vector arguments");
+int wl_vector(int kind, uint64_t seed, int32_t n, double *out) {
+  if (!out || n < 0) return set_error(WL_ERR_PARAM, "bad vector arguments");
   if (kind == 0) {
     for (int32_t i = 0; i < n; ++i) out[i] = 1.0;
   } else if (kind == 1) {
@@ -275,9 +318,9 @@ bcmg_status bcmg_gen_vector(int kind, uint64_t seed, int32_t n, double *out) {
     SplitMix64 rng(seed);
     for (int32_t i = 0; i < n; ++i) out[i] = 2.0 * rng.uniform() - 1.0;
   } else {
-    return set_error(BCMG_ERR_PARAM, "unknown vector kind %d", kind);
+    return set_error(WL_ERR_PARAM, "unknown vector kind %d", kind);
   }
-  return BCMG_OK;
+  return WL_OK;
 }
 
 }  // extern "C"
