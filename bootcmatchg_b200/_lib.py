@@ -44,7 +44,7 @@ class Ext(C.Structure):
                 ("replace_every", C.c_int), ("use_graphs", C.c_int), ("device", C.c_int),
                 ("verbose", C.c_int), ("max_device_seconds", C.c_double),
                 ("stream", C.c_void_p), ("sliced", C.c_int), ("autotune", C.c_int),
-                ("narrow_values", C.c_int)]
+                ("narrow_values", C.c_int), ("match_step_limit", C.c_int64)]
 
 
 class SolveInfo(C.Structure):
@@ -78,6 +78,10 @@ SIGNATURES = {
     "bcmg_status_string": (C.c_char_p, [C.c_int]),
     "bcmg_version": (C.c_char_p, []),
     "bcmg_kernel_launches": (C.c_ulonglong, []),
+    "bcmg_set_max_device_seconds": (C.c_int, [vp, C.c_double]),
+    "bcmg_debug_fail_alloc": (C.c_int, [C.c_int64]),
+    "bcmg_wait_selftest": (C.c_int, [C.c_int, C.c_double]),
+    "bcmg_debug_alloc_stats": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "bcmg_read_matrix": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(Csr)]),
     "bcmg_write_matrix_mm": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
     "bcmg_csr_free": (None, [C.POINTER(Csr)]),

@@ -151,7 +151,8 @@ class Extensions:
     use_graphs: int = 1
     device: int = 0
     verbose: int = 0
-    max_device_seconds: float = 60.0
+    max_device_seconds: float = 2.0  # bound on each pipelined-pass wait
+    match_step_limit: int = 0  # per-thread matching step bound (0: 8 nnz + 1024)
     stream: int = 0  # cudaStream_t as an integer (0: the handle makes its own)
     sliced: int = 1  # solve on the sliced copies of the levels
     autotune: int = 1  # batched solves: time the row-kernel shapes per level
@@ -326,6 +327,11 @@ class Handle:
         b = C.c_uint64()
         check(lib.bcmg_device_bytes(self._h, C.byref(b)), "bcmg_device_bytes")
         return b.value
+
+    def set_max_device_seconds(self, seconds: float) -> None:
+        """Bound on each wait of the handle's pipelined row passes."""
+        check(lib.bcmg_set_max_device_seconds(self._h, seconds),
+              "bcmg_set_max_device_seconds")
 
     def set_stream(self, stream_ptr: int) -> None:
         check(lib.bcmg_set_stream(self._h, C.c_void_p(stream_ptr)), "bcmg_set_stream")

@@ -30,6 +30,22 @@ constexpr uint64_t kNoOffer = ~0ull;
 
 // Kernel launches issued by this library (bcmg_kernel_launches()).
 extern std::atomic<unsigned long long> g_kernel_launches;
+// Device allocations made by dev_alloc and not yet freed, all made so far
+// (bcmg_debug_alloc_stats), and the countdown of an injected allocation
+// failure (bcmg_debug_fail_alloc; -1: none armed).
+extern std::atomic<long long> g_live_allocs;
+extern std::atomic<long long> g_made_allocs;
+extern std::atomic<long long> g_fail_alloc_countdown;
+
+// True for the one allocation an armed bcmg_debug_fail_alloc picks (the
+// countdown then disarms itself).
+inline bool injected_alloc_failure() {
+  long long c = g_fail_alloc_countdown.load(std::memory_order_relaxed);
+  while (c >= 0)
+    if (g_fail_alloc_countdown.compare_exchange_weak(c, c - 1, std::memory_order_relaxed))
+      return c == 0;
+  return false;
+}
 
 // Every kernel of the library is launched through here so launches are
 // counted.
@@ -85,6 +101,10 @@ template <typename T>
 bcmg_status dev_alloc(T **p, int64_t count, cudaStream_t s) {
   *p = nullptr;
   if (count <= 0) return BCMG_OK;
+  if (injected_alloc_failure())
+    return set_error(BCMG_ERR_ALLOC,
+                     "device allocation of %lld bytes failed: injected by bcmg_debug_fail_alloc",
+                     static_cast<long long>(sizeof(T) * count));
   cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(p),
                                   sizeof(T) * static_cast<size_t>(count), s);
   if (e != cudaSuccess) {
@@ -94,12 +114,17 @@ bcmg_status dev_alloc(T **p, int64_t count, cudaStream_t s) {
                      "device allocation of %lld bytes failed: %s",
                      static_cast<long long>(sizeof(T) * count), cudaGetErrorString(e));
   }
+  g_live_allocs.fetch_add(1, std::memory_order_relaxed);
+  g_made_allocs.fetch_add(1, std::memory_order_relaxed);
   return BCMG_OK;
 }
 
 template <typename T>
 void dev_free(T *&p, cudaStream_t s) {
-  if (p) cudaFreeAsync(p, s);
+  if (p) {
+    cudaFreeAsync(p, s);
+    g_live_allocs.fetch_sub(1, std::memory_order_relaxed);
+  }
   p = nullptr;
 }
 
@@ -135,8 +160,7 @@ struct DevBuf {
     return dev_alloc(&ptr, n, s);
   }
   void reset() {
-    if (ptr) cudaFreeAsync(ptr, stream);
-    ptr = nullptr;
+    dev_free(ptr, stream);
     count = 0;
   }
   T *get() const { return ptr; }

@@ -20,6 +20,25 @@
 namespace bcmg {
 
 std::atomic<unsigned long long> g_kernel_launches{0};
+std::atomic<long long> g_live_allocs{0};
+std::atomic<long long> g_made_allocs{0};
+std::atomic<long long> g_fail_alloc_countdown{-1};
+
+// Bound on each wait of a pipelined row pass, from the handle's extensions.
+unsigned long long wait_ns_of(const bcmg_handle *h) {
+  const double sec = h->ext.max_device_seconds;
+  if (!(sec > 0.0)) return kDefaultWaitNs;
+  const double ns = sec * 1e9;
+  if (ns >= 1.8e19) return ~0ull;
+  return ns < 1.0 ? 1ull : static_cast<unsigned long long>(ns);
+}
+
+// A sliced solve copy of this handle: its narrowing rule and wait bound.
+bcmg_status build_sliced(bcmg_handle *h, const CsrView &A, int vtype, SlicedMat *out,
+                         cudaStream_t s) {
+  out->wait_ns = wait_ns_of(h);
+  return sliced_build(A, vtype, out, s, h->ext.narrow_values != 0);
+}
 
 // NVTX range for the lifetime of a scope (profilers filter on these names).
 struct NvtxRange {
@@ -154,6 +173,21 @@ bcmg_status matching_aggregation(bcmg_handle *h, DevLevel &fine, double **w_out,
   double *cur_w = fine.w;
   DevLevel inter;  // intermediate coarse matrix between sweeps
   bool have_inter = false;
+  // On an early return the intermediate matrix and smooth vector are freed
+  // here; on success they become `coarse` and *w_out.
+  struct Scratch {
+    DevLevel &inter;
+    bool &have_inter;
+    double *&cur_w;
+    const double *w_in;
+    cudaStream_t s;
+    bool handed_over = false;
+    ~Scratch() {
+      if (handed_over) return;
+      if (have_inter) inter.release(s);
+      if (cur_w != w_in) dev_free(cur_w, s);
+    }
+  } scratch{inter, have_inter, cur_w, w_in, s};
   DevBuf<int32_t> agg_acc;
   DevBuf<double> p_acc;
   int32_t nc_acc = 0;
@@ -165,7 +199,7 @@ bcmg_status matching_aggregation(bcmg_handle *h, DevLevel &fine, double **w_out,
     BCMG_TRY(p_i.alloc(cur.n, s));
     g_clock.tick("other");
     BCMG_TRY(pair_aggregate(cur, cur_w, agg_i.get(), p_i.get(), &nci, nullptr, nullptr,
-                            nullptr, s));
+                            nullptr, s, h->ext.match_step_limit));
     g_clock.tick("match+aggregate");
     BCMG_TRY(rptr_i.alloc(nci + 1, s));
     BCMG_TRY(ridx_i.alloc(cur.n, s));
@@ -223,6 +257,7 @@ bcmg_status matching_aggregation(bcmg_handle *h, DevLevel &fine, double **w_out,
   BCMG_TRY(transpose_agg(fine.n, fine.agg, nc_acc, fine.rptr, fine.ridx, s));
   coarse = inter;
   *w_out = cur_w;
+  scratch.handed_over = true;
   return BCMG_OK;
 }
 
@@ -293,7 +328,7 @@ bcmg_status smooth_hierarchy(bcmg_handle *h, DevHierarchy &H) {
     BCMG_TRY(level_prep(c.view(), c.D, c.M, s));
     c.own64.release(s);
     if (wants_coarse_f64(h))
-      BCMG_TRY(sliced_build(c.view(), kValF64, &c.own64, s, h->ext.narrow_values != 0));
+      BCMG_TRY(build_sliced(h, c.view(), kValF64, &c.own64, s));
   }
   phase_tick("smoothed aggregation");
   return BCMG_OK;
@@ -302,20 +337,24 @@ bcmg_status smooth_hierarchy(bcmg_handle *h, DevHierarchy &H) {
 bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy &H) {
   cudaStream_t s = h->stream;
   const int maxlevels = h->prm.max_levels;
-  DevLevel l0;
-  l0.n = h->A0.n;
-  l0.nnz = h->A0.nnz;
-  l0.row = h->A0.row;
-  l0.col = h->A0.col;
-  l0.val = h->A0.val;
-  l0.own_A = false;
-  if (h->A0.own64.nslices) l0.s64 = &h->A0.own64;
-  BCMG_TRY(dev_alloc(&l0.D, l0.n, s));
-  BCMG_TRY(dev_alloc(&l0.M, l0.n, s));
-  BCMG_TRY(dev_alloc(&l0.w, l0.n, s));
-  BCMG_TRY(copy(l0.w, w_in, l0.n, s));
-  BCMG_TRY(level_prep(l0.view(), l0.D, l0.M, s));
-  H.lv.push_back(l0);
+  // Every level is owned by H before its arrays are allocated, so a failure
+  // part-way leaves nothing that H.release would not free.
+  H.lv.emplace_back();
+  {
+    DevLevel &l0 = H.lv.back();
+    l0.n = h->A0.n;
+    l0.nnz = h->A0.nnz;
+    l0.row = h->A0.row;
+    l0.col = h->A0.col;
+    l0.val = h->A0.val;
+    l0.own_A = false;
+    if (h->A0.own64.nslices) l0.s64 = &h->A0.own64;
+    BCMG_TRY(dev_alloc(&l0.D, l0.n, s));
+    BCMG_TRY(dev_alloc(&l0.M, l0.n, s));
+    BCMG_TRY(dev_alloc(&l0.w, l0.n, s));
+    BCMG_TRY(copy(l0.w, w_in, l0.n, s));
+    BCMG_TRY(level_prep(l0.view(), l0.D, l0.M, s));
+  }
   double normw = 0;
   BCMG_TRY(anorm(h, w_in, &normw));
   int ftcoarse = 1;
@@ -323,11 +362,13 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
   int level = 0;
   if (normw > DBL_EPSILON) {
     for (level = 1; level < maxlevels;) {
-      DevLevel &fine = H.lv[level - 1];
       double *w = nullptr;
-      DevLevel coarse;
-      BCMG_TRY(matching_aggregation(h, fine, &w, &ftcoarse, coarse));
-      coarse.w = w;
+      DevLevel built;
+      BCMG_TRY(matching_aggregation(h, H.lv[level - 1], &w, &ftcoarse, built));
+      built.w = w;
+      const double fine_n = H.lv[level - 1].n;
+      H.lv.push_back(built);  // (invalidates references into H.lv)
+      DevLevel &coarse = H.lv.back();
       BCMG_TRY(dev_alloc(&coarse.D, coarse.n, s));
       BCMG_TRY(dev_alloc(&coarse.M, coarse.n, s));
       BCMG_TRY(level_prep(coarse.view(), coarse.D, coarse.M, s));
@@ -335,11 +376,10 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
       // solve, or the bootstrap's inner iterations).
       // (Smoothed aggregation replaces the coarse matrices: built afterwards.)
       if (h->prm.aggrtype == 0 && wants_coarse_f64(h))
-        BCMG_TRY(sliced_build(coarse.view(), kValF64, &coarse.own64, s, h->ext.narrow_values != 0));
+        BCMG_TRY(build_sliced(h, coarse.view(), kValF64, &coarse.own64, s));
       const double size_coarse = coarse.n;
-      const double coarse_ratio = fine.n / size_coarse;
+      const double coarse_ratio = fine_n / size_coarse;
       avcoarseratio += coarse_ratio;
-      H.lv.push_back(coarse);
       ++level;
       if (size_coarse <= static_cast<double>(ftcoarse * h->maxcoarsesize)) break;
     }
@@ -750,8 +790,8 @@ bcmg_status prepare_mixed(bcmg_handle *h) {
 bcmg_status prepare_solve_formats(bcmg_handle *h) {
   cudaStream_t s = h->stream;
   DevLevel &a = h->A0;
-  if (!a.own64.nslices) BCMG_TRY(sliced_build(a.view(), kValF64, &a.own64, s, h->ext.narrow_values != 0));
-  if (h->mixed && !a.ownlo.nslices) BCMG_TRY(sliced_build(a.view(), kValF32, &a.ownlo, s, h->ext.narrow_values != 0));
+  if (!a.own64.nslices) BCMG_TRY(build_sliced(h, a.view(), kValF64, &a.own64, s));
+  if (h->mixed && !a.ownlo.nslices) BCMG_TRY(build_sliced(h, a.view(), kValF32, &a.ownlo, s));
   for (auto &H : h->H) {
     for (size_t l = 0; l < H.lv.size(); ++l) {
       DevLevel &lv = H.lv[l];
@@ -761,9 +801,9 @@ bcmg_status prepare_solve_formats(bcmg_handle *h) {
         continue;
       }
       if (h->mixed) {
-        if (!lv.ownlo.nslices) BCMG_TRY(sliced_build(lv.view(), lv.vtype_lo, &lv.ownlo, s, h->ext.narrow_values != 0));
+        if (!lv.ownlo.nslices) BCMG_TRY(build_sliced(h, lv.view(), lv.vtype_lo, &lv.ownlo, s));
       } else {
-        if (!lv.own64.nslices) BCMG_TRY(sliced_build(lv.view(), kValF64, &lv.own64, s, h->ext.narrow_values != 0));
+        if (!lv.own64.nslices) BCMG_TRY(build_sliced(h, lv.view(), kValF64, &lv.own64, s));
       }
     }
   }
@@ -861,7 +901,7 @@ bcmg_status setup_common(bcmg_handle *h) {
   g_clock.start(h->ext.verbose >= 1, h->stream);
   set_cycle_tables(h);
   BCMG_TRY(alloc_work(h));
-  if (h->ext.sliced) BCMG_TRY(sliced_build(h->A0.view(), kValF64, &h->A0.own64, h->stream, h->ext.narrow_values != 0));
+  if (h->ext.sliced) BCMG_TRY(build_sliced(h, h->A0.view(), kValF64, &h->A0.own64, h->stream));
   g_clock.tick("alloc");
   BCMG_TRY(bootstrap(h));
   g_clock.tick("other");
@@ -965,6 +1005,8 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
   info->rel_residual = delta0 > 0 ? 1.0 : 0.0;
   info->converged = 0;
   if (delta0 <= DBL_EPSILON * bnorm) {
+    // (a residual pass that gave up would make r meaningless)
+    BCMG_TRY(sliced_wait_status(s));
     // The reference exits the process here (FCG.cu:459-462).
     info->converged = 1;
     info->rel_residual = 0.0;
@@ -1236,7 +1278,7 @@ bcmg_status load_hierarchies(bcmg_handle *h, FILE *f) {
   set_cycle_tables(h);
   BCMG_TRY(alloc_work(h));
   if (h->ext.sliced)
-    BCMG_TRY(sliced_build(a.view(), kValF64, &a.own64, s, h->ext.narrow_values != 0));
+    BCMG_TRY(build_sliced(h, a.view(), kValF64, &a.own64, s));
   for (int32_t k = 0; k < dims[2]; ++k) {
     h->H.emplace_back();
     DevHierarchy &H = h->H.back();
@@ -1401,6 +1443,50 @@ bcmg_status bcmg_solve_legacy(const bcmg_csr *A, const bcmg_params *p, const bcm
 
 unsigned long long bcmg_kernel_launches(void) {
   return g_kernel_launches.load(std::memory_order_relaxed);
+}
+
+bcmg_status bcmg_set_max_device_seconds(bcmg_handle *h, double seconds) {
+  clear_error();
+  if (!h || !(seconds > 0.0))
+    return set_error(BCMG_ERR_PARAM, "need a handle and a positive bound in seconds");
+  h->ext.max_device_seconds = seconds;
+  const unsigned long long ns = wait_ns_of(h);
+  h->A0.own64.wait_ns = h->A0.ownlo.wait_ns = ns;
+  for (auto &H : h->H)
+    for (auto &lv : H.lv) lv.own64.wait_ns = lv.ownlo.wait_ns = ns;
+  // The captured FCG loop holds the old bound in its kernel parameters; the
+  // next solve captures it again.
+  if (h->fcg_exec) {
+    BCMG_CUDA(cudaSetDevice(h->device));
+    BCMG_CUDA(cudaStreamSynchronize(h->stream));
+    cudaGraphExecDestroy(h->fcg_exec);
+    h->fcg_exec = nullptr;
+  }
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_wait_selftest(int device, double seconds) {
+  clear_error();
+  if (!(seconds > 0.0) || seconds > 10.0)
+    return set_error(BCMG_ERR_PARAM, "bound must be in (0, 10] seconds");
+  BCMG_CUDA(cudaSetDevice(device));
+  cudaStream_t s = nullptr;
+  BCMG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const bcmg_status st = wait_selftest(static_cast<unsigned long long>(seconds * 1e9), s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return st;
+}
+
+bcmg_status bcmg_debug_fail_alloc(int64_t after) {
+  g_fail_alloc_countdown.store(after < 0 ? -1 : after, std::memory_order_relaxed);
+  return BCMG_OK;
+}
+
+bcmg_status bcmg_debug_alloc_stats(int64_t *live, int64_t *made) {
+  if (live) *live = g_live_allocs.load(std::memory_order_relaxed);
+  if (made) *made = g_made_allocs.load(std::memory_order_relaxed);
+  return BCMG_OK;
 }
 
 bcmg_status bcmg_device_bytes(const bcmg_handle *h, uint64_t *bytes) {

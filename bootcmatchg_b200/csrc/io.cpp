@@ -459,11 +459,12 @@ void bcmg_ext_default(bcmg_ext *e) {
   e->use_graphs = 1;
   e->device = 0;
   e->verbose = 0;
-  e->max_device_seconds = 60.0;
+  e->max_device_seconds = 2.0;
   e->stream = nullptr;
   e->sliced = 1;
   e->autotune = 1;
   e->narrow_values = 1;
+  e->match_step_limit = 0;
 }
 
 }  // extern "C"

@@ -16,7 +16,11 @@
 // the host that name is a stand-in, not a device address), so the device
 // address is looked up with cudaGetSymbolAddress once per device, with that
 // device current, on the first call made on the device; that first call
-// should therefore happen before any stream capture.  All calls share the
+// should therefore happen before any stream capture.  The address stays
+// cached per device ordinal for the rest of the process, so the entry point
+// must not be used after the device was reset (cudaDeviceReset) or its
+// primary context destroyed; `stream` must belong to the current device.
+// Each call synchronises `stream` before it returns.  All calls share the
 // one buffer: calls whose work overlaps on the GPU (other streams, other
 // host threads) race on it and must be serialised by the caller.  The
 // ping-pong buffer is fully written before it is read, so nothing has to be

@@ -1489,7 +1489,7 @@ bcmg_status level_prep(const CsrView &A, double *D, double *M, cudaStream_t s) {
 // Matching::suitor (src/AMG/matching.cu:476-502).
 bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, double *p,
                            int32_t *nc_out, double *W_out, int32_t *s_out,
-                           int32_t *m_out, cudaStream_t s) {
+                           int32_t *m_out, cudaStream_t s, int64_t step_limit) {
   const int32_t n = A.n;
   if (n <= 0) {
     *nc_out = 0;
@@ -1568,7 +1568,8 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   // Both matchers are launched; the one that does not apply (by *nonsym)
   // returns at once, so no host round trip decides between them.
   launch(k_init_match, nb, T, 0, s, n, A.row, next.get(), offer.get());
-  const int64_t limit = 8 * static_cast<int64_t>(A.nnz) + 1024;
+  const int64_t limit =
+      step_limit > 0 ? step_limit : 8 * static_cast<int64_t>(A.nnz) + 1024;
   launch(k_suitor_sym, nb, T, 0, s, n, A.row, ucnt.get(), scol.get(), key.get(), next.get(),
          offer.get(), limit, nonsym.get(), err.get());
   launch(k_suitor, nb, T, 0, s, n, A.row, scol.get(), sW.get(), next.get(), offer.get(), limit,

@@ -51,7 +51,10 @@ constexpr int kPipeStages = 2;
 constexpr int kPipeThreads = (kPipeWarps + 1) * 32;
 constexpr int kSlotPad = 32;                       // >= the largest slot batch
 constexpr size_t kMaxStageBytes = 108 * 1024;      // two stages fit in 227 KB
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
+// A CTA leaves only after the copies it issued have landed: the producer's
+// final drain waits at least this long, whatever bound the handle sets on the
+// pipeline's other waits (S.wait_ns).
+constexpr unsigned long long kDrainLimitNs = 2000000000ull;
 
 // Set by a pipeline wait that ran out (a bulk copy that never landed).
 __device__ int g_sliced_wait_error;
@@ -276,13 +279,31 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Waits for the phase with the given parity; false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+// Waits (one thread) for the phase with the given parity; false after
+// limit_ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity,
+                                          unsigned long long limit_ns) {
   if (mbar_test(b, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_test(b, parity))
-    if (global_ns() - t0 > kWaitLimitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   return true;
+}
+// The same for a whole converged warp, with one outcome for all its lanes:
+// true once every lane has seen the phase complete, false when lane 0's
+// clock passes limit_ns first.  (Lanes that decided differently would leave
+// the full-warp shuffles of the row sums unmatched.)
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *b, uint32_t parity,
+                                               unsigned long long limit_ns) {
+  bool seen = mbar_test(b, parity);
+  if (__all_sync(0xffffffffu, seen)) return true;
+  const unsigned long long t0 = global_ns();
+  while (true) {
+    seen = seen || mbar_test(b, parity);
+    if (__all_sync(0xffffffffu, seen)) return true;
+    const int late = (global_ns() - t0 > limit_ns) ? 1 : 0;
+    if (__shfl_sync(0xffffffffu, late, 0)) return false;
+  }
 }
 // Global -> shared bulk copy (16-byte aligned, size a multiple of 16).
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
@@ -521,7 +542,8 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
       const int32_t q1 = cn < nchunks ? __ldg(S.sptr + min((cn + 1) * kPipeWarps, S.nslices)) : 0;
       const int st = j % kPipeStages;
       if (j >= kPipeStages &&
-          !mbar_wait(&empty[st], static_cast<uint32_t>(((j / kPipeStages) - 1) & 1))) {
+          !mbar_wait(&empty[st], static_cast<uint32_t>(((j / kPipeStages) - 1) & 1),
+                     S.wait_ns)) {
         atomicExch(&g_sliced_wait_error, 1);
         break;
       }
@@ -560,7 +582,8 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
       const int jj = j - 1 - k;
       const int st = jj % kPipeStages;
       if ((armed >> st) & 1u) {
-        if (!mbar_wait(&full[st], static_cast<uint32_t>((jj / kPipeStages) & 1)))
+        if (!mbar_wait(&full[st], static_cast<uint32_t>((jj / kPipeStages) & 1),
+                       S.wait_ns > kDrainLimitNs ? S.wait_ns : kDrainLimitNs))
           atomicExch(&g_sliced_wait_error, 1);
       }
     }
@@ -572,8 +595,9 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
   int32_t c = blockIdx.x;
   for (int j = 0; c < nchunks; ++j, c += gridDim.x) {
     const int st = j % kPipeStages;
-    if (!mbar_wait(&full[st], static_cast<uint32_t>((j / kPipeStages) & 1))) {
-      atomicExch(&g_sliced_wait_error, 1);
+    if (!mbar_wait_warp(&full[st], static_cast<uint32_t>((j / kPipeStages) & 1),
+                        S.wait_ns)) {
+      if (lane == 0) atomicExch(&g_sliced_wait_error, 1);
       break;
     }
     const StageCtl cl = ctl[st];
@@ -616,6 +640,36 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
     if (lane == 0) mbar_arrive(&empty[st]);
   }
   epi.finish(wid, lane);
+}
+
+// Self-test of the bounded pipeline waits with the pipeline's own wait
+// functions: one CTA; lane 0 of warp 0 (the producer) stages one real bulk
+// copy on barrier 0 and drains it; warp 1 (a consumer) waits on barrier 1,
+// which nothing ever arms, until limit_ns runs out, and reports that as a
+// pipelined pass does.  flags bit 0: the consumer gave up; bit 1: the copy
+// landed before the producer left.
+__global__ void k_wait_selftest(const int4 *__restrict__ src, unsigned long long limit_ns,
+                                int *flags) {
+  __shared__ __align__(128) int4 buf[16];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (wid == 0) {
+    if (lane != 0) return;
+    mbar_arrive_tx(&bar[0], sizeof(buf));
+    bulk_load(buf, src, sizeof(buf), &bar[0]);
+    if (mbar_wait(&bar[0], 0, kDrainLimitNs)) atomicOr(flags, 2);
+    return;
+  }
+  if (!mbar_wait_warp(&bar[1], 0, limit_ns) && lane == 0) {
+    atomicOr(flags, 1);
+    atomicExch(&g_sliced_wait_error, 1);
+  }
 }
 
 // ---- launch configuration ----------------------------------------------------
@@ -772,7 +826,8 @@ void SlicedMat::release(cudaStream_t s) {
   dev_free(meta, s);
   dev_free(scol, s);
   dev_free(soff, s);
-  if (val) cudaFreeAsync(val, s);
+  char *vp = static_cast<char *>(val);
+  dev_free(vp, s);
   val = nullptr;
   nslices = 0;
   has_columns = false;
@@ -792,6 +847,7 @@ SlicedView SlicedMat::view() const {
   v.cols_staged = has_columns ? 1 : 0;
   v.batch = batch;
   v.xtype = xtype;
+  v.wait_ns = wait_ns;
   return v;
 }
 
@@ -857,7 +913,11 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
   out->batch = static_cast<int32_t>((static_cast<int64_t>(slots) + ns - 1) / ns);
   const size_t vb = value_bytes(vtype);
   const int64_t padded = static_cast<int64_t>(slots) + kSlotPad;
-  BCMG_CUDA(cudaMallocAsync(&out->val, vb * static_cast<size_t>(padded) * 32, s));
+  {
+    char *vp = nullptr;
+    BCMG_TRY(dev_alloc(&vp, static_cast<int64_t>(vb) * padded * 32, s));
+    out->val = vp;
+  }
   BCMG_CUDA(cudaMemsetAsync(static_cast<char *>(out->val) + vb * static_cast<size_t>(slots) * 32,
                             0, vb * kSlotPad * 32, s));
   // Explicit columns are only read in column slices; a matrix made of offset
@@ -1016,6 +1076,23 @@ bcmg_status sliced_spmv_t<float>(const SlicedView &S, const float *x, float *y,
     case kValF16: return pipe_launch<__half, float>(S, x, e, s);
     default: return set_error(BCMG_ERR_INTERNAL, "FP32-vector SpMV on FP64 values");
   }
+}
+
+bcmg_status wait_selftest(unsigned long long limit_ns, cudaStream_t s) {
+  DevBuf<int4> src;
+  DevBuf<int> flags;
+  BCMG_TRY(src.alloc(16, s));
+  BCMG_TRY(flags.alloc(1, s));
+  BCMG_CUDA(cudaMemsetAsync(src.get(), 0, sizeof(int4) * 16, s));
+  BCMG_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int), s));
+  launch(k_wait_selftest, 1, 64, 0, s, src.get(), limit_ns, flags.get());
+  BCMG_LAUNCH_CHECK();
+  int h_flags = 0;
+  BCMG_CUDA(cudaMemcpyAsync(&h_flags, flags.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  BCMG_CUDA(cudaStreamSynchronize(s));
+  if (!(h_flags & 2)) return set_error(BCMG_ERR_INTERNAL, "self-test copy did not drain");
+  if (!(h_flags & 1)) return set_error(BCMG_ERR_INTERNAL, "self-test wait did not give up");
+  return sliced_wait_status(s);
 }
 
 bcmg_status sliced_wait_status(cudaStream_t s) {

@@ -24,9 +24,12 @@ void phase_tick(const char *name);
 
 // ---- setup (k_setup.cu; FP64, no FMA contraction) -------------------------
 bcmg_status level_prep(const CsrView &A, double *D, double *M, cudaStream_t s);
+// step_limit bounds the steps of each matching thread (0: 8 nnz + 1024); a
+// thread that runs out makes it return BCMG_ERR_DEVICE_TIMEOUT.
 bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg,
                            double *p, int32_t *nc, double *W_out,
-                           int32_t *s_out, int32_t *m_out, cudaStream_t s);
+                           int32_t *s_out, int32_t *m_out, cudaStream_t s,
+                           int64_t step_limit = 0);
 bcmg_status transpose_agg(int32_t n, const int32_t *agg, int32_t nc,
                           int32_t *rptr, int32_t *ridx, cudaStream_t s);
 // A_c = P^T A P into crow (nc+1, caller-allocated) and *ccol/*cval
@@ -60,6 +63,10 @@ enum ValType { kValF64 = 0, kValF32 = 1, kValBF16 = 2, kValF16 = 3 };
 // offsets soff[base + k] (base = the first slice of a run of slices with the
 // same offsets); kind 0 = explicit columns scol[32 first + 32 k + lane].
 // Values, columns and offsets are padded past the last slot.
+// Default bound on each wait of a pipelined row pass for its staged copies
+// (bcmg_ext.max_device_seconds overrides it per handle).
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;
+
 struct SlicedView {
   int32_t n = 0, nslices = 0;
   const int32_t *sptr = nullptr;  // first slot of each slice (nslices + 1)
@@ -71,6 +78,7 @@ struct SlicedView {
   int32_t cols_staged = 0;  // explicit columns exist (and are staged)
   int32_t batch = 0;        // mean slice width (chooses the slot batch size)
   int xtype = kValF64;      // vector type the copy serves (kValF64 or kValF32)
+  unsigned long long wait_ns = kDefaultWaitNs;  // bound on each pipeline wait
 };
 
 struct SlicedMat {
@@ -83,6 +91,7 @@ struct SlicedMat {
   int xtype = kValF64;       // vector type served: kValF64 or kValF32
   bool narrowed = false;     // values stored narrower than xtype (all exact)
   bool has_columns = false;  // scol allocated (some slice is a column slice)
+  unsigned long long wait_ns = kDefaultWaitNs;  // copied into every view
   void release(cudaStream_t s);
   size_t bytes() const;  // device bytes held
   SlicedView view() const;
@@ -112,6 +121,10 @@ bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w
 // BCMG_ERR_DEVICE_TIMEOUT (and the flag cleared) if a sliced row pass gave up
 // waiting for its staged copies since the last call; synchronises s.
 bcmg_status sliced_wait_status(cudaStream_t s);
+// Runs a pipeline wait that nothing completes, bounded by limit_ns, beside a
+// real staged copy that must drain: BCMG_ERR_DEVICE_TIMEOUT (reported through
+// sliced_wait_status) when both behave, BCMG_ERR_INTERNAL otherwise.
+bcmg_status wait_selftest(unsigned long long limit_ns, cudaStream_t s);
 
 struct MatView {
   int32_t n = 0, nnz = 0;

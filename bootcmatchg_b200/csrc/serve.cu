@@ -113,6 +113,7 @@ struct bcmg_server {
   std::unordered_map<uint64_t, bcmg::Entry> cache;
   size_t cache_bytes = 0;  // every entry, idle, busy or being built
   size_t work_bytes = 0;   // batch work blocks of running groups
+  size_t pending_bytes = 0;  // evicted hierarchies not destroyed yet
   int running = 0;
   uint64_t next_ticket = 1, use_clock = 0;
   bool stop = false;
@@ -133,7 +134,14 @@ struct Job {
   size_t work = 0;     // batch work bytes reserved
 };
 
-size_t resident(const bcmg_server *s) { return s->cache_bytes + s->work_bytes; }
+// Evicted hierarchies still hold their memory until a worker has destroyed
+// them outside the lock, so they count as resident until then.
+size_t resident(const bcmg_server *s) {
+  return s->cache_bytes + s->work_bytes + s->pending_bytes;
+}
+
+// An evicted hierarchy and the bytes it was charged.
+using Victims = std::vector<std::pair<bcmg_handle *, size_t>>;
 
 size_t idle_bytes(const bcmg_server *s, uint64_t keep) {
   size_t b = 0;
@@ -145,8 +153,7 @@ size_t idle_bytes(const bcmg_server *s, uint64_t keep) {
 // Evicts idle entries (other than `keep`), least recently used first, until
 // `need` more bytes fit under `cap` or none is left.  The handles go to
 // `victims` to be destroyed outside the lock.
-void evict_for(bcmg_server *s, size_t need, size_t cap, uint64_t keep,
-               std::vector<bcmg_handle *> &victims) {
+void evict_for(bcmg_server *s, size_t need, size_t cap, uint64_t keep, Victims &victims) {
   while (resident(s) + need > cap) {
     auto best = s->cache.end();
     for (auto it = s->cache.begin(); it != s->cache.end(); ++it) {
@@ -155,14 +162,15 @@ void evict_for(bcmg_server *s, size_t need, size_t cap, uint64_t keep,
     }
     if (best == s->cache.end()) return;
     s->cache_bytes -= best->second.bytes;
-    victims.push_back(best->second.h);
+    s->pending_bytes += best->second.bytes;
+    victims.emplace_back(best->second.h, best->second.bytes);
     s->cache.erase(best);
     ++s->st.evictions;
   }
 }
 
 // Picks the next job under the lock, or returns false.
-bool pick(bcmg_server *s, Job *job, std::vector<bcmg_handle *> &victims) {
+bool pick(bcmg_server *s, Job *job, Victims &victims) {
   const size_t cap = static_cast<size_t>(s->opt.mem_cap_gb * 1e9);
   bool blocked = false;  // an earlier request is waiting for memory
   for (size_t i = 0; i < s->queue.size(); ++i) {
@@ -230,12 +238,20 @@ bool pick(bcmg_server *s, Job *job, std::vector<bcmg_handle *> &victims) {
 // keeps the stream of the worker that ran it last (its runs end with a
 // stream synchronize); freeing on that stream could put the frees inside
 // another worker's graph capture on it.
-void destroy_victims(std::vector<bcmg_handle *> &victims, cudaStream_t stream) {
-  for (bcmg_handle *v : victims) {
-    v->stream = stream;
-    bcmg_destroy(v);
+// Called without the lock; takes it to release the victims' bytes once they
+// are freed (and wakes the workers that may wait for that room).
+void destroy_victims(bcmg_server *s, Victims &victims, cudaStream_t stream) {
+  if (victims.empty()) return;
+  size_t freed = 0;
+  for (auto &v : victims) {
+    v.first->stream = stream;
+    bcmg_destroy(v.first);
+    freed += v.second;
   }
   victims.clear();
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->pending_bytes -= freed;
+  s->cv_work.notify_all();
 }
 
 // Runs one job on the worker's stream (no lock held).
@@ -295,7 +311,7 @@ void worker_main(bcmg_server *s, int slot) {
   cudaStream_t stream = s->streams[slot];
   for (;;) {
     Job job;
-    std::vector<bcmg_handle *> victims;
+    Victims victims;
     bcmg_handle *h = nullptr;
     {
       std::unique_lock<std::mutex> lk(s->mu);
@@ -305,7 +321,7 @@ void worker_main(bcmg_server *s, int slot) {
         if (!victims.empty()) {
           // Free evicted hierarchies before waiting again.
           lk.unlock();
-          destroy_victims(victims, stream);
+          destroy_victims(s, victims, stream);
           lk.lock();
           continue;
         }
@@ -313,12 +329,12 @@ void worker_main(bcmg_server *s, int slot) {
       }
       if (job.group.empty()) {
         lk.unlock();
-        destroy_victims(victims, stream);
+        destroy_victims(s, victims, stream);
         return;
       }
       if (!job.fresh) h = s->cache[job.key].h;
     }
-    destroy_victims(victims, stream);
+    destroy_victims(s, victims, stream);
     run_job(s, job, stream, &h);
     const size_t bytes = h ? handle_bytes(h) : 0;
     {
@@ -359,14 +375,15 @@ void worker_main(bcmg_server *s, int slot) {
             best = jt;
         if (best == s->cache.end()) break;
         s->cache_bytes -= best->second.bytes;
-        victims.push_back(best->second.h);
+        s->pending_bytes += best->second.bytes;
+        victims.emplace_back(best->second.h, best->second.bytes);
         s->cache.erase(best);
         ++s->st.evictions;
       }
       s->cv_done.notify_all();
       s->cv_work.notify_all();
     }
-    destroy_victims(victims, stream);
+    destroy_victims(s, victims, stream);
   }
 }
 

@@ -92,7 +92,11 @@ typedef struct bcmg_ext {
   int    use_graphs;      /* capture the FCG iteration in a CUDA graph         */
   int    device;          /* CUDA device ordinal                               */
   int    verbose;         /* 0 quiet, 1 #META lines, 2 per-iteration residual  */
-  double max_device_seconds; /* bound on any single device loop (matching)     */
+  double max_device_seconds; /* bound, in seconds, on each wait of a pipelined
+                             row pass for its staged copies (default 2); a
+                             wait that runs out makes the call return
+                             BCMG_ERR_DEVICE_TIMEOUT and leaves the handle
+                             usable (bcmg_set_max_device_seconds changes it) */
   void  *stream;          /* cudaStream_t to run on from setup on (NULL: the
                              handle creates its own); the caller keeps it alive */
   int    sliced;          /* solve on the sliced copies of the levels (default 1) */
@@ -104,6 +108,10 @@ typedef struct bcmg_ext {
                              BF16, FP16 or FP32 when every value converts
                              exactly (default 1); the kernels widen them, so
                              results are bit-identical with 0.               */
+  int64_t match_step_limit; /* bound on the steps (proposals and displacements)
+                             of each suitor-matching thread; 0 (default): 8 nnz
+                             + 1024 of the level.  A thread that runs out makes
+                             setup return BCMG_ERR_DEVICE_TIMEOUT.           */
 } bcmg_ext;
 
 /* Per-solve report.  residual is the recursive ||r||_2 that FCG returns
@@ -129,6 +137,29 @@ const char *bcmg_status_string(int status);
 const char *bcmg_version(void);
 /* Number of CUDA kernels this library has launched in this process. */
 unsigned long long bcmg_kernel_launches(void);
+
+/* ---- failure detection (no counterpart in the reference, which exit()s or
+ * asserts: src/utility/utils.h:36-71) ---------------------------------------
+ * Every device-side wait of the library is bounded.  This changes the bound
+ * of a handle's pipelined row passes (bcmg_ext.max_device_seconds); the next
+ * solve recaptures its CUDA graph with it.  seconds > 0. */
+bcmg_status bcmg_set_max_device_seconds(bcmg_handle *h, double seconds);
+/* Self-test of that mechanism on `device`: a pipeline wait that nothing ever
+ * completes, bounded by `seconds` (0 < seconds <= 10), beside a real staged
+ * copy that must land before its kernel exits.  Returns
+ * BCMG_ERR_DEVICE_TIMEOUT -- what a solve returns when one of its waits runs
+ * out -- when the wait gave up and the copy drained, BCMG_ERR_INTERNAL if
+ * either did not happen.  The device stays usable either way. */
+bcmg_status bcmg_wait_selftest(int device, double seconds);
+/* Host-side failure injection for tests of the error paths: the device
+ * allocation that follows `after` further successful ones fails with
+ * BCMG_ERR_ALLOC, as an out-of-memory cudaMallocAsync would (one shot,
+ * process-wide; after < 0 disarms).  Nothing reaches the GPU. */
+bcmg_status bcmg_debug_fail_alloc(int64_t after);
+/* Device allocations of the library: *live held right now over all handles
+ * (a failed call leaves it where it found it), *made since the library was
+ * loaded.  Either pointer may be NULL. */
+bcmg_status bcmg_debug_alloc_stats(int64_t *live, int64_t *made);
 
 /* ---- matrix input (replaces readMatrixFromFile, src/matrix/matrixIO.cu:4) --
  * m_type 0: Matrix Market coordinate real/integer, general or symmetric
@@ -366,7 +397,10 @@ bcmg_status bcmg_k_relax(int32_t n, int32_t nnz, const int32_t *d_row,
  * process-lifetime device buffer of 1,048,576 doubles (8 MiB on every GPU
  * that loads the library): n above that is rejected with BCMG_ERR_PARAM.
  * The first call on a device looks the buffer up and should come before any
- * stream capture; calls that overlap on the GPU share the buffer and race. */
+ * stream capture; the address stays cached for the process, so do not call
+ * it after resetting the device or destroying its primary context.  stream
+ * must belong to the current device, and each call synchronises it before
+ * returning.  Calls that overlap on the GPU share the buffer and race. */
 bcmg_status bcmg_k_relax_noalloc(int32_t n, int32_t nnz, const int32_t *d_row,
                                  const int32_t *d_col, const double *d_val,
                                  const double *d_d, const double *d_f, double *d_u,
