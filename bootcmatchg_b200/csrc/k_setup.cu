@@ -367,15 +367,20 @@ __global__ void __launch_bounds__(256)
 
 // Symmetric weights: receiver y ranks proposers x by (W_xy, x) descending,
 // which for W_xy = W_yx is y's own preference order, so an offer can be the
-// proposer's position in y's sorted row.  key[k] (for sorted entry k of row x
-// pointing to y) = the index of x's entry in y's sorted row (row[y] plus the
-// position; offers at one receiver compare like positions).  Any usable entry whose
-// transposed entry is missing or carries a different weight (bit for bit)
-// sets *nonsym, and the general matcher runs instead.
+// proposer's position in y's sorted row.  For sorted usable entry k of row x
+// pointing to y, E[k] packs what a proposal through it needs in one word:
+// bits 0-31 y, bits 32-62 the index of x's entry in y's sorted row (row[y]
+// plus the position; offers at one receiver compare like these indices), bit
+// 63 set when k is x's last usable entry.  Any usable entry whose transposed
+// entry is missing or carries a different weight (bit for bit) sets *nonsym,
+// and the general matcher runs instead.
+constexpr unsigned long long kLastEntry = 1ull << 63;
+
 template <int G>
 __global__ void k_sym_keys(int32_t n, const int32_t *__restrict__ row,
                            const int32_t *__restrict__ col, const double *__restrict__ sW,
-                           const int32_t *__restrict__ inv, int32_t *key, int *nonsym) {
+                           const int32_t *__restrict__ inv, const int32_t *__restrict__ ucnt,
+                           unsigned long long *E, int *nonsym) {
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int32_t y = static_cast<int32_t>(t / G);
   const int lane = threadIdx.x % G;
@@ -410,59 +415,54 @@ __global__ void k_sym_keys(int32_t n, const int32_t *__restrict__ row,
       atomicExch(nonsym, 1);
       continue;
     }
-    key[bx + pb] = by + pa;
+    E[bx + pb] = (pb == ucnt[x] - 1 ? kLastEntry : 0ull) |
+                 (static_cast<unsigned long long>(static_cast<uint32_t>(by + pa)) << 32) |
+                 static_cast<uint32_t>(y);
   }
 }
 
-// Suitor with symmetric weights: offer[y] = (index of the current suitor's
-// entry in y's sorted row) << 32 | suitor (kNoOffer if none); a smaller
-// index is a better offer and identifies the proposer, so one 64-bit
-// atomicMin both tests and installs an offer and returns the displaced
-// proposer.  Same proposal chains and resume points as k_suitor; exits at
-// once when *nonsym is set.
+// Suitor with symmetric weights.  offer[y] = (index of the current suitor's
+// entry in y's sorted row) << 32 | (the suitor's own sorted entry index k of
+// that proposal, bit 31 set if k is its last usable entry), kNoOffer if
+// none.  The high half orders offers (smaller is better, unique per
+// proposer), so one 64-bit atomicMin tests and installs an offer and returns
+// the displaced one; the low half says where the displaced proposer resumes
+// (k + 1, its candidates before k having rejected it for good), so taking a
+// displaced proposer over costs one load of E[k + 1] and no per-vertex state.
+// Proposer v starts at its first sorted entry; the thread's next candidate is
+// loaded while the atomic is in flight.  Exits at once when *nonsym is set.
 __global__ void __launch_bounds__(256)
     k_suitor_sym(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ ucnt,
-                 const int32_t *__restrict__ scol, const int32_t *__restrict__ key,
-                 int32_t *next, unsigned long long *offer, int64_t limit,
-                 const int *__restrict__ nonsym, int *err) {
-  const int32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= n || *nonsym) return;
-  volatile int32_t *vnext = next;
-  int32_t cur = gid;
+                 const unsigned long long *__restrict__ E, unsigned long long *offer,
+                 int64_t limit, const int *__restrict__ nonsym, int *err) {
+  const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n || *nonsym) return;
+  if (ucnt[v] <= 0) return;
+  uint32_t k = static_cast<uint32_t>(row[v]);
+  unsigned long long ek = E[k];
   int64_t steps = 0;
   while (true) {
-    int32_t k = vnext[cur];
-    const int32_t e = row[cur] + ucnt[cur];
-    unsigned long long old = kNoOffer;
-    bool found = false;
-    int32_t yk = 0, mk = 0;  // the candidate at k, loaded one step ahead
-    if (k < e) {
-      yk = scol[k];
-      mk = key[k];
+    if (++steps > limit) {
+      atomicExch(err, 1);
+      return;
     }
-    while (k < e) {
-      if (++steps > limit) {
-        atomicExch(err, 1);
-        return;
-      }
-      const int32_t y = yk;
-      const unsigned long long mine =
-          (static_cast<unsigned long long>(static_cast<uint32_t>(mk)) << 32) |
-          static_cast<uint32_t>(cur);
-      if (k + 1 < e) {
-        yk = scol[k + 1];
-        mk = key[k + 1];
-      }
-      old = atomicMin(offer + y, mine);
-      if (old > mine) {
-        found = true;
-        break;
-      }
-      ++k;
+    const bool last = (ek & kLastEntry) != 0;
+    const uint32_t y = static_cast<uint32_t>(ek);
+    const unsigned long long mine = (ek & 0x7fffffff00000000ull) | k |
+                                    (last ? 0x80000000ull : 0ull);
+    unsigned long long en = 0;
+    if (!last) en = E[k + 1];  // in flight with the atomic
+    const unsigned long long old = atomicMin(offer + y, mine);
+    if (old > mine) {
+      if (old == kNoOffer) return;
+      if (old & 0x80000000ull) return;  // the displaced proposer has no candidate left
+      k = static_cast<uint32_t>(old & 0x7fffffffull) + 1u;
+      ek = E[k];
+      continue;
     }
-    vnext[cur] = found ? k + 1 : e;
-    if (!found || old == kNoOffer) return;
-    cur = static_cast<int32_t>(old & 0xffffffffull);  // the displaced proposer
+    if (last) return;
+    ++k;
+    ek = en;
   }
 }
 
@@ -530,14 +530,21 @@ __global__ void k_init_match(int32_t n, const int32_t *__restrict__ row, int32_t
   offer[i] = kNoOffer;
 }
 
-// Suitor array from whichever matcher ran.
-// Both matchers keep the proposer in the offer's low 32 bits.
+// Suitor array from whichever matcher ran: the general matcher keeps the
+// proposer in the offer's low 32 bits; the symmetric one keeps the index of
+// the proposer's entry in the receiver's own sorted row in the high half,
+// whose column is the proposer.
 __global__ void k_offer_to_suitor(int32_t n, const unsigned long long *__restrict__ offer,
-                                  int32_t *s) {
+                                  const int32_t *__restrict__ scol,
+                                  const int *__restrict__ nonsym, int32_t *s) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned long long o = offer[i];
-  s[i] = o == kNoOffer ? -1 : static_cast<int32_t>(o & 0xffffffffull);
+  if (o == kNoOffer) {
+    s[i] = -1;
+    return;
+  }
+  s[i] = *nonsym ? static_cast<int32_t>(o & 0xffffffffull) : scol[o >> 32];
 }
 
 // unsymFix pass 1 (_setSymPair, src/AMG/unsymMatching.cu:32-50).
@@ -1530,12 +1537,13 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   phase_tick("weights");
   // Preference-sorted rows, then the suitor proposals.
   DevBuf<double> sW;
-  DevBuf<int32_t> scol, inv, ucnt, key, next, long_rows, n_long;
+  DevBuf<int32_t> scol, inv, ucnt, next, long_rows, n_long;
+  DevBuf<unsigned long long> E;
   DevBuf<int> nonsym;
   BCMG_TRY(sW.alloc(A.nnz, s));
   BCMG_TRY(scol.alloc(A.nnz, s));
   BCMG_TRY(inv.alloc(A.nnz, s));
-  BCMG_TRY(key.alloc(A.nnz, s));
+  BCMG_TRY(E.alloc(A.nnz, s));
   BCMG_TRY(ucnt.alloc(n, s));
   BCMG_TRY(next.alloc(n, s));
   BCMG_TRY(long_rows.alloc(n, s));
@@ -1558,10 +1566,10 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
     BCMG_LAUNCH_CHECK();
   }
   switch (G) {
-    case 4: launch(k_sym_keys<4>, ceil_div(static_cast<int64_t>(n) * 4, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
-    case 8: launch(k_sym_keys<8>, ceil_div(static_cast<int64_t>(n) * 8, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
-    case 16: launch(k_sym_keys<16>, ceil_div(static_cast<int64_t>(n) * 16, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
-    default: launch(k_sym_keys<32>, ceil_div(static_cast<int64_t>(n) * 32, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), key.get(), nonsym.get()); break;
+    case 4: launch(k_sym_keys<4>, ceil_div(static_cast<int64_t>(n) * 4, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
+    case 8: launch(k_sym_keys<8>, ceil_div(static_cast<int64_t>(n) * 8, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
+    case 16: launch(k_sym_keys<16>, ceil_div(static_cast<int64_t>(n) * 16, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
+    default: launch(k_sym_keys<32>, ceil_div(static_cast<int64_t>(n) * 32, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
   }
   BCMG_LAUNCH_CHECK();
   phase_tick("sort_prefs");
@@ -1570,12 +1578,12 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   launch(k_init_match, nb, T, 0, s, n, A.row, next.get(), offer.get());
   const int64_t limit =
       step_limit > 0 ? step_limit : 8 * static_cast<int64_t>(A.nnz) + 1024;
-  launch(k_suitor_sym, nb, T, 0, s, n, A.row, ucnt.get(), scol.get(), key.get(), next.get(),
-         offer.get(), limit, nonsym.get(), err.get());
+  launch(k_suitor_sym, nb, T, 0, s, n, A.row, ucnt.get(), E.get(), offer.get(), limit,
+         nonsym.get(), err.get());
   launch(k_suitor, nb, T, 0, s, n, A.row, scol.get(), sW.get(), next.get(), offer.get(), limit,
          nonsym.get(), err.get());
   BCMG_LAUNCH_CHECK();
-  launch(k_offer_to_suitor, nb, T, 0, s, n, offer.get(), sv.get());
+  launch(k_offer_to_suitor, nb, T, 0, s, n, offer.get(), scol.get(), nonsym.get(), sv.get());
   phase_tick("suitor");
 
   // unsymFix.
