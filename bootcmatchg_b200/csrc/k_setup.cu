@@ -430,13 +430,18 @@ __global__ void k_sym_keys(int32_t n, const int32_t *__restrict__ row,
 // (k + 1, its candidates before k having rejected it for good), so taking a
 // displaced proposer over costs one load of E[k + 1] and no per-vertex state.
 // Proposer v starts at its first sorted entry; the thread's next candidate is
-// loaded while the atomic is in flight.  Exits at once when *nonsym is set.
+// loaded while the atomic is in flight.  Threads take the proposers from the
+// highest id down: on tied weights a receiver prefers the higher proposer,
+// so the winners tend to arrive first and fewer offers are displaced (the
+// final state does not depend on the order).  Exits at once when *nonsym is
+// set.
 __global__ void __launch_bounds__(256)
     k_suitor_sym(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ ucnt,
                  const unsigned long long *__restrict__ E, unsigned long long *offer,
                  int64_t limit, const int *__restrict__ nonsym, int *err) {
-  const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n || *nonsym) return;
+  const int32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n || *nonsym) return;
+  const int32_t v = n - 1 - gid;
   if (ucnt[v] <= 0) return;
   uint32_t k = static_cast<uint32_t>(row[v]);
   unsigned long long ek = E[k];
@@ -873,10 +878,12 @@ __device__ void gal_emit(const GalSmem &sm, int T, int32_t I, int64_t base, int3
   if (lane == 0) runs[I] = nr;
 }
 
-// Sort-and-reduce pass, one warp per coarse row; rows over kGalCap terms
-// are queued for k_gal_rows_long.
+// Sort-and-reduce pass, one warp per coarse row, over the rows queued by
+// k_gal_rows_reg (grid-stride); rows over kGalCap terms are queued for
+// k_gal_rows_long.
 __global__ void __launch_bounds__(kGalWarpsPerBlock * 32)
-    k_gal_rows(int32_t nc, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+    k_gal_rows(const int32_t *__restrict__ queue, const int32_t *__restrict__ n_queue,
+               const int32_t *__restrict__ row, const int32_t *__restrict__ col,
                const double *__restrict__ val, const int32_t *__restrict__ agg,
                const double *__restrict__ p, const int32_t *__restrict__ rptr,
                const int32_t *__restrict__ ridx, const int32_t *__restrict__ tpos,
@@ -884,16 +891,191 @@ __global__ void __launch_bounds__(kGalWarpsPerBlock * 32)
                int *err) {
   extern __shared__ __align__(16) unsigned char gal_dyn[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int32_t I = blockIdx.x * kGalWarpsPerBlock + wid;
-  if (I >= nc) return;
   GalSmem sm = gal_smem(gal_dyn + static_cast<size_t>(wid) * kGalCap * kGalBytesPerTerm,
                         kGalCap);
-  const int T = gal_gather<32>(I, row, col, val, agg, p, rptr, ridx, sm, kGalCap, lane);
-  if (T < 0) {
-    if (lane == 0) long_rows[atomicAdd(n_long, 1)] = I;
+  const int32_t nq = *n_queue;
+  for (int32_t q = blockIdx.x * kGalWarpsPerBlock + wid; q < nq;
+       q += gridDim.x * kGalWarpsPerBlock) {
+    const int32_t I = queue[q];
+    const int T = gal_gather<32>(I, row, col, val, agg, p, rptr, ridx, sm, kGalCap, lane);
+    if (T < 0) {
+      if (lane == 0) long_rows[atomicAdd(n_long, 1)] = I;
+      continue;
+    }
+    gal_emit(sm, T, I, tpos[I], tJ, tV, runs, err, lane);
+    __syncwarp();
+  }
+}
+
+// Coarse rows of at most kGalRegTerms terms, one warp per row with the terms
+// in registers, two per lane (slot t = lane + 32 r): keys J << 6 | t (J below
+// 2^26) go through a 64-key bitonic network of shuffles, the terms' values
+// and fine (i, j) wait in shared memory by slot, and the lane at each run head
+// sums its run in the canonical order.  Same output as k_gal_rows, at a
+// fraction of its instructions; longer rows, and aggregates of more than 32
+// members, are queued for it.
+constexpr int kGalRegTerms = 64;
+constexpr int kGalRegWarps = 8;
+struct GalRegSmem {
+  double v[kGalRegTerms];
+  int32_t ti[kGalRegTerms];
+  int32_t tj[kGalRegTerms];
+  int32_t sidx[kGalRegTerms];
+};
+
+__global__ void __launch_bounds__(kGalRegWarps * 32)
+    k_gal_rows_reg(int32_t nc, const int32_t *__restrict__ row,
+                   const int32_t *__restrict__ col, const double *__restrict__ val,
+                   const int32_t *__restrict__ agg, const double *__restrict__ p,
+                   const int32_t *__restrict__ rptr, const int32_t *__restrict__ ridx,
+                   const int32_t *__restrict__ tpos, int32_t *tJ, double *tV,
+                   int32_t *runs, int32_t *mid_rows, int32_t *n_mid, int *err) {
+  __shared__ GalRegSmem smem[kGalRegWarps];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int32_t I = blockIdx.x * kGalRegWarps + wid;
+  if (I >= nc) return;
+  GalRegSmem &sm = smem[wid];
+  const int32_t kb = rptr[I];
+  const int M = rptr[I + 1] - kb;
+  // Members (ascending): row start, length, p, and the exclusive prefix of
+  // the lengths (each member's first slot).
+  int32_t mi = 0, mb = 0, ml = 0;
+  double mp = 0.0;
+  if (lane < M) {
+    mi = ridx[kb + lane];
+    mb = row[mi];
+    ml = row[mi + 1] - mb;
+    mp = p[mi];
+  }
+  int32_t incl = ml;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int32_t T = __shfl_sync(0xffffffffu, incl, 31);
+  if (M > 32 || T > kGalRegTerms) {
+    if (lane == 0) mid_rows[atomicAdd(n_mid, 1)] = I;
     return;
   }
-  gal_emit(sm, T, I, tpos[I], tJ, tV, runs, err, lane);
+  const int32_t first = incl - ml;
+  uint32_t key[2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int t = lane + 32 * r;
+    // the member holding slot t: the last one whose first slot is <= t
+    int m = 0;
+    for (int q = 1; q < M; ++q)
+      if (__shfl_sync(0xffffffffu, first, q) <= t) m = q;
+    const int32_t b = __shfl_sync(0xffffffffu, mb, m);
+    const int32_t f = __shfl_sync(0xffffffffu, first, m);
+    const int32_t i = __shfl_sync(0xffffffffu, mi, m);
+    const double pi = __shfl_sync(0xffffffffu, mp, m);
+    key[r] = 0xffffffffu;
+    if (t < T) {
+      const int32_t e = b + (t - f);
+      const int32_t j = col[e];
+      sm.v[t] = (pi * p[j]) * val[e];
+      sm.ti[t] = i;
+      sm.tj[t] = j;
+      key[r] = (static_cast<uint32_t>(agg[j]) << 6) | static_cast<uint32_t>(t);
+    }
+  }
+  // Ascending bitonic sort of the 64 keys (position lane + 32 r).
+#pragma unroll
+  for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j == 32) {
+        const uint32_t a = key[0], b = key[1];
+        key[0] = min(a, b);
+        key[1] = max(a, b);
+      } else {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const uint32_t o = __shfl_xor_sync(0xffffffffu, key[r], j);
+          const int pos = lane + 32 * r;
+          const bool lower = (pos & j) == 0;
+          const bool asc = (pos & k) == 0;
+          key[r] = (lower == asc) ? min(key[r], o) : max(key[r], o);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+    if (lane + 32 * r < T) sm.sidx[lane + 32 * r] = static_cast<int32_t>(key[r] & 63u);
+  __syncwarp();
+  // Run heads and their ranks.
+  const uint32_t J0 = key[0] >> 6, J1 = key[1] >> 6;
+  const uint32_t up0 = __shfl_up_sync(0xffffffffu, J0, 1);
+  const uint32_t up1 = __shfl_up_sync(0xffffffffu, J1, 1);
+  const uint32_t last0 = __shfl_sync(0xffffffffu, J0, 31);
+  const bool h0 = lane < T && (lane == 0 || J0 != up0);
+  const bool h1 = lane + 32 < T && J1 != (lane == 0 ? last0 : up1);
+  const unsigned b0 = __ballot_sync(0xffffffffu, h0), b1 = __ballot_sync(0xffffffffu, h1);
+  const unsigned long long H = static_cast<unsigned long long>(b0) |
+                               (static_cast<unsigned long long>(b1) << 32);
+  const int nr = __popcll(H);
+  const int64_t base = tpos[I];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    if (!(r == 0 ? h0 : h1)) continue;
+    const int q = lane + 32 * r;
+    const unsigned long long after = q < 63 ? (H >> (q + 1)) : 0ull;
+    const int len = (after ? q + 1 + __ffsll(static_cast<long long>(after)) - 1 : T) - q;
+    const int rank = __popcll(H & ((1ull << q) - 1ull));
+    int32_t Jv = static_cast<int32_t>(r == 0 ? J0 : J1);
+    double sum = 0.0;
+    if (len <= 4) {
+      int id[4];
+      int32_t mn[4], mx[4], ti[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const bool ok = a < len;
+        id[a] = ok ? sm.sidx[q + a] : 0;
+        const int32_t x = ok ? sm.ti[id[a]] : INT_MAX, y = ok ? sm.tj[id[a]] : INT_MAX;
+        ti[a] = x;
+        mn[a] = min(x, y);
+        mx[a] = max(x, y);
+      }
+      gal_cx(id[0], mn[0], mx[0], ti[0], id[1], mn[1], mx[1], ti[1]);
+      gal_cx(id[2], mn[2], mx[2], ti[2], id[3], mn[3], mx[3], ti[3]);
+      gal_cx(id[0], mn[0], mx[0], ti[0], id[2], mn[2], mx[2], ti[2]);
+      gal_cx(id[1], mn[1], mx[1], ti[1], id[3], mn[3], mx[3], ti[3]);
+      gal_cx(id[1], mn[1], mx[1], ti[1], id[2], mn[2], mx[2], ti[2]);
+      sum = sm.v[id[0]];
+#pragma unroll
+      for (int a = 1; a < 4; ++a)
+        if (a < len) sum = sum + sm.v[id[a]];
+    } else if (len <= kGalMaxRun) {
+      int idx[kGalMaxRun];
+      for (int a = 0; a < len; ++a) idx[a] = sm.sidx[q + a];
+      for (int a = 1; a < len; ++a) {  // insertion sort by (min, max, i)
+        const int x = idx[a];
+        const int32_t xi = sm.ti[x], xj = sm.tj[x];
+        const int32_t xmn = min(xi, xj), xmx = max(xi, xj);
+        int c = a - 1;
+        while (c >= 0) {
+          const int y = idx[c];
+          const int32_t yi = sm.ti[y], yj = sm.tj[y];
+          const int32_t ymn = min(yi, yj), ymx = max(yi, yj);
+          if (!(ymn > xmn || (ymn == xmn && (ymx > xmx || (ymx == xmx && yi > xi))))) break;
+          idx[c + 1] = idx[c];
+          --c;
+        }
+        idx[c + 1] = x;
+      }
+      sum = sm.v[idx[0]];
+      for (int a = 1; a < len; ++a) sum = sum + sm.v[idx[a]];
+    } else {
+      atomicExch(err, 2);
+      continue;
+    }
+    tJ[base + rank] = Jv;
+    tV[base + rank] = sum;
+  }
+  if (lane == 0) runs[I] = nr;
 }
 
 // The queued long rows, one block per row (grid-stride over the queue).
@@ -1655,7 +1837,7 @@ bcmg_status galerkin(const CsrView &A, const int32_t *agg, const double *p, int3
   *cval_out = nullptr;
   *cnnz = 0;
   if (nc <= 0) return BCMG_OK;
-  DevBuf<int32_t> tpos, tJ, long_rows, n_long, tmp;
+  DevBuf<int32_t> tpos, tJ, long_rows, n_long, mid_rows, n_mid, tmp;
   DevBuf<double> tV;
   DevBuf<int> err;
   BCMG_TRY(tpos.alloc(nc + 1, s));
@@ -1663,9 +1845,12 @@ bcmg_status galerkin(const CsrView &A, const int32_t *agg, const double *p, int3
   BCMG_TRY(tV.alloc(std::max<int32_t>(A.nnz, 1), s));
   BCMG_TRY(long_rows.alloc(nc, s));
   BCMG_TRY(n_long.alloc(1, s));
+  BCMG_TRY(mid_rows.alloc(static_cast<int64_t>(nc) + 1, s));  // (iota writes nc + 1)
+  BCMG_TRY(n_mid.alloc(1, s));
   BCMG_TRY(err.alloc(1, s));
   BCMG_TRY(tmp.alloc(scan_tmp_size(nc), s));
   BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
+  BCMG_CUDA(cudaMemsetAsync(n_mid.get(), 0, sizeof(int32_t), s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
   launch(k_gal_terms, ceil_div(nc, 256), 256, 0, s, nc, A.row, rptr, ridx, tpos.get());
   BCMG_TRY(exclusive_scan(tpos.get(), tpos.get(), nc, tpos.get() + nc, tmp.get(), s));
@@ -1674,9 +1859,19 @@ bcmg_status galerkin(const CsrView &A, const int32_t *agg, const double *p, int3
   const size_t smem_long = static_cast<size_t>(kGalCapLong) * kGalBytesPerTerm;
   BCMG_CUDA(cudaFuncSetAttribute(k_gal_rows_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem_long)));
-  launch(k_gal_rows, ceil_div(nc, kGalWarpsPerBlock), kGalWarpsPerBlock * 32, smem_warp, s, nc,
-         A.row, A.col, A.val, agg, p, rptr, ridx, tpos.get(), tJ.get(), tV.get(), crow,
-         long_rows.get(), n_long.get(), err.get());
+  if (nc < (1 << 26)) {
+    // Short rows in registers; the rest queued for the shared-memory sort.
+    launch(k_gal_rows_reg, ceil_div(nc, kGalRegWarps), kGalRegWarps * 32, 0, s, nc, A.row,
+           A.col, A.val, agg, p, rptr, ridx, tpos.get(), tJ.get(), tV.get(), crow,
+           mid_rows.get(), n_mid.get(), err.get());
+  } else {
+    BCMG_TRY(iota(nc, mid_rows.get(), s));
+    BCMG_CUDA(cudaMemcpyAsync(n_mid.get(), &nc, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  }
+  launch(k_gal_rows, std::min(ceil_div(nc, kGalWarpsPerBlock), 16 * kNumSM),
+         kGalWarpsPerBlock * 32, smem_warp, s, mid_rows.get(), n_mid.get(), A.row, A.col, A.val,
+         agg, p, rptr, ridx, tpos.get(), tJ.get(), tV.get(), crow, long_rows.get(),
+         n_long.get(), err.get());
   launch(k_gal_rows_long, std::min(nc, kNumSM), kGalLongThreads, smem_long, s, long_rows.get(),
          n_long.get(), A.row, A.col, A.val, agg, p, rptr, ridx, tpos.get(), tJ.get(), tV.get(),
          crow, err.get());
