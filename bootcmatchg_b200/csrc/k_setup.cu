@@ -77,6 +77,11 @@ __device__ __forceinline__ unsigned group_mask() {
 // src/AMG/matching.cu:319-329,401-431).  Grid-stride over rows, block
 // reduction, one atomicMin per block: non-negative doubles order like their
 // bit patterns, so the global min is an integer atomicMin (exact, order-free).
+// A group of G lanes takes kMinRows rows at a time with the loads of each
+// stage issued for all of them together (the pass is bound by the latency of
+// the gathers of C and w, not by bandwidth).
+constexpr int kMinRows = 2;
+
 template <int G>
 __global__ void __launch_bounds__(256)
     k_ah_min(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
@@ -86,15 +91,50 @@ __global__ void __launch_bounds__(256)
   const int lane = threadIdx.x % G;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
   double m = DBL_MAX;
-  for (int64_t gi = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G; gi < n;
-       gi += stride) {
-    const int32_t i = static_cast<int32_t>(gi);
-    const double ci = C[i], wi = w[i];
-    for (int32_t j = row[i] + lane; j < row[i + 1]; j += G) {
-      const int32_t c = col[j];
-      if (c == i) continue;
-      const double ah = fabs(ah_value(val[j], ci, C[c], wi, w[c]));
-      if (ah < m) m = ah;
+  for (int64_t g0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G; g0 < n;
+       g0 += kMinRows * stride) {
+    int32_t i[kMinRows], b[kMinRows], e[kMinRows], c[kMinRows];
+    double ci[kMinRows], wi[kMinRows], a[kMinRows], cc[kMinRows], wc[kMinRows];
+#pragma unroll
+    for (int u = 0; u < kMinRows; ++u) {
+      const int64_t r = g0 + u * stride;
+      i[u] = r < n ? static_cast<int32_t>(r) : -1;
+      b[u] = e[u] = 0;
+      ci[u] = wi[u] = 0.0;
+      if (i[u] >= 0) {
+        b[u] = row[i[u]];
+        e[u] = row[i[u] + 1];
+        ci[u] = C[i[u]];
+        wi[u] = w[i[u]];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kMinRows; ++u) {
+      const int32_t j = b[u] + lane;
+      c[u] = j < e[u] ? col[j] : -1;
+      a[u] = j < e[u] ? val[j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kMinRows; ++u) {
+      cc[u] = wc[u] = 0.0;
+      if (c[u] >= 0) {
+        cc[u] = C[c[u]];
+        wc[u] = w[c[u]];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kMinRows; ++u) {
+      if (c[u] >= 0 && c[u] != i[u]) {
+        const double ah = fabs(ah_value(a[u], ci[u], cc[u], wi[u], wc[u]));
+        if (ah < m) m = ah;
+      }
+      // entries past the first G of a long row
+      for (int32_t j = b[u] + lane + G; j < e[u]; j += G) {
+        const int32_t cj = col[j];
+        if (cj == i[u]) continue;
+        const double ah = fabs(ah_value(val[j], ci[u], C[cj], wi[u], w[cj]));
+        if (ah < m) m = ah;
+      }
     }
   }
 #pragma unroll
@@ -376,48 +416,131 @@ __global__ void __launch_bounds__(256)
 // and the general matcher runs instead.
 constexpr unsigned long long kLastEntry = 1ull << 63;
 
+// One group of G lanes takes kKeyRows receiver rows at a time (one measured
+// best: the full grid keeps more warps resident than interleaved rows with
+// their registers do).  Usability comes from the sorted position
+// (pa < ucnt[y]); the symmetry test compares the two values bit for bit,
+// which is the same as comparing the two weights (both are computed from
+// them by the same commutative expression).
+constexpr int kKeyRows = 1;
+
 template <int G>
-__global__ void k_sym_keys(int32_t n, const int32_t *__restrict__ row,
-                           const int32_t *__restrict__ col, const double *__restrict__ sW,
-                           const int32_t *__restrict__ inv, const int32_t *__restrict__ ucnt,
-                           unsigned long long *E, int *nonsym) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int32_t y = static_cast<int32_t>(t / G);
+__device__ __forceinline__ void sym_key_entry(int32_t y, int32_t by, int32_t ey, int32_t a,
+                                              int32_t x, int32_t pa, double va,
+                                              const int32_t *__restrict__ row,
+                                              const int32_t *__restrict__ col,
+                                              const double *__restrict__ val,
+                                              const int32_t *__restrict__ inv,
+                                              const int32_t *__restrict__ ucnt,
+                                              unsigned long long *E, int *nonsym) {
+  // the entry (x, y): first the mirrored position (a symmetric stencil row
+  // of the same length holds y at index len - 1 - (a - by)), else a binary
+  // search of y in row x (columns increasing)
+  const int32_t bx = row[x], ex = row[x + 1];
+  const int32_t ux = ucnt[x];
+  int32_t lo = bx, hi = ex - 1;
+  const int32_t guess = hi - (a - by);
+  if (hi - lo == ey - 1 - by && col[guess] == y) {
+    lo = hi = guess;
+  } else {
+    while (lo < hi) {
+      const int32_t mid = (lo + hi) >> 1;
+      if (col[mid] < y) lo = mid + 1;
+      else hi = mid;
+    }
+  }
+  if (lo > hi || col[lo] != y ||
+      __double_as_longlong(val[lo]) != __double_as_longlong(va)) {
+    atomicExch(nonsym, 1);
+    return;
+  }
+  const int32_t pb = inv[lo];
+  E[bx + pb] = (pb == ux - 1 ? kLastEntry : 0ull) |
+               (static_cast<unsigned long long>(static_cast<uint32_t>(by + pa)) << 32) |
+               static_cast<uint32_t>(y);
+}
+
+template <int G>
+__global__ void __launch_bounds__(256)
+    k_sym_keys(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+               const double *__restrict__ val, const int32_t *__restrict__ inv,
+               const int32_t *__restrict__ ucnt, unsigned long long *E, int *nonsym) {
   const int lane = threadIdx.x % G;
-  if (y >= n) return;
-  const int32_t by = row[y], ey = row[y + 1];
-  for (int32_t a = by + lane; a < ey; a += G) {
-    const int32_t x = col[a];
-    const int32_t pa = inv[a];
-    const double wya = sW[by + pa];
-    if (x == y || !(wya > 0.0)) continue;
-    // the entry (x, y): first the mirrored position (a symmetric stencil
-    // row of the same length holds y at index len - 1 - (a - by)), else a
-    // binary search of y in row x (columns increasing)
-    int32_t lo = row[x], hi = row[x + 1] - 1;
-    const int32_t bx = lo;
-    const int32_t guess = hi - (a - by);
-    if (hi - lo == ey - 1 - by && col[guess] == y) {
-      lo = hi = guess;
-    } else {
-      while (lo < hi) {
-        const int32_t mid = (lo + hi) >> 1;
-        if (col[mid] < y) lo = mid + 1;
-        else hi = mid;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
+  for (int64_t g0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G; g0 < n;
+       g0 += kKeyRows * stride) {
+    int32_t y[kKeyRows], by[kKeyRows], ey[kKeyRows], uy[kKeyRows];
+    int32_t a[kKeyRows], x[kKeyRows], pa[kKeyRows];
+    int32_t bx[kKeyRows], ex[kKeyRows], ux[kKeyRows], g[kKeyRows];
+    double va[kKeyRows];
+    bool ok[kKeyRows];
+#pragma unroll
+    for (int u = 0; u < kKeyRows; ++u) {
+      const int64_t r = g0 + u * stride;
+      y[u] = r < n ? static_cast<int32_t>(r) : -1;
+      by[u] = ey[u] = uy[u] = 0;
+      if (y[u] >= 0) {
+        by[u] = row[y[u]];
+        ey[u] = row[y[u] + 1];
+        uy[u] = ucnt[y[u]];
       }
     }
-    if (lo > hi || col[lo] != y) {
-      atomicExch(nonsym, 1);
-      continue;
+#pragma unroll
+    for (int u = 0; u < kKeyRows; ++u) {
+      a[u] = by[u] + lane;
+      x[u] = -1;
+      pa[u] = 0;
+      va[u] = 0.0;
+      if (a[u] < ey[u]) {
+        x[u] = col[a[u]];
+        pa[u] = inv[a[u]];
+        va[u] = val[a[u]];
+      }
+      ok[u] = x[u] >= 0 && x[u] != y[u] && pa[u] < uy[u];
     }
-    const int32_t pb = inv[lo];
-    if (__double_as_longlong(sW[bx + pb]) != __double_as_longlong(wya)) {
-      atomicExch(nonsym, 1);
-      continue;
+#pragma unroll
+    for (int u = 0; u < kKeyRows; ++u) {
+      bx[u] = ex[u] = ux[u] = 0;
+      if (ok[u]) {
+        bx[u] = row[x[u]];
+        ex[u] = row[x[u] + 1];
+        ux[u] = ucnt[x[u]];
+      }
     }
-    E[bx + pb] = (pb == ucnt[x] - 1 ? kLastEntry : 0ull) |
-                 (static_cast<unsigned long long>(static_cast<uint32_t>(by + pa)) << 32) |
-                 static_cast<uint32_t>(y);
+    // the mirrored-position guess for every row at once
+#pragma unroll
+    for (int u = 0; u < kKeyRows; ++u) {
+      g[u] = -1;
+      if (ok[u] && ex[u] - 1 - bx[u] == ey[u] - 1 - by[u]) {
+        const int32_t guess = ex[u] - 1 - (a[u] - by[u]);
+        if (col[guess] == y[u] &&
+            __double_as_longlong(val[guess]) == __double_as_longlong(va[u]))
+          g[u] = guess;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kKeyRows; ++u) {
+      if (ok[u]) {
+        if (g[u] >= 0) {
+          const int32_t pb = inv[g[u]];
+          E[bx[u] + pb] =
+              (pb == ux[u] - 1 ? kLastEntry : 0ull) |
+              (static_cast<unsigned long long>(static_cast<uint32_t>(by[u] + pa[u])) << 32) |
+              static_cast<uint32_t>(y[u]);
+        } else {
+          sym_key_entry<G>(y[u], by[u], ey[u], a[u], x[u], pa[u], va[u], row, col, val, inv,
+                           ucnt, E, nonsym);
+        }
+      }
+      // entries past the first G of a long row
+      for (int32_t aa = by[u] + lane + G; aa < ey[u]; aa += G) {
+        const int32_t xx = col[aa];
+        const int32_t pp = inv[aa];
+        if (xx == y[u] || pp >= uy[u]) continue;
+        sym_key_entry<G>(y[u], by[u], ey[u], aa, xx, pp, val[aa], row, col, val, inv, ucnt, E,
+                         nonsym);
+      }
+    }
   }
 }
 
@@ -1747,11 +1870,15 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
            scol.get(), inv.get(), ucnt.get(), err.get());
     BCMG_LAUNCH_CHECK();
   }
+  // every lane group its kKeyRows rows
+  auto key_blocks = [&](int g) {
+    return ceil_div(static_cast<int64_t>(n) * g, static_cast<int64_t>(T) * kKeyRows);
+  };
   switch (G) {
-    case 4: launch(k_sym_keys<4>, ceil_div(static_cast<int64_t>(n) * 4, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
-    case 8: launch(k_sym_keys<8>, ceil_div(static_cast<int64_t>(n) * 8, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
-    case 16: launch(k_sym_keys<16>, ceil_div(static_cast<int64_t>(n) * 16, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
-    default: launch(k_sym_keys<32>, ceil_div(static_cast<int64_t>(n) * 32, T), T, 0, s, n, A.row, A.col, sW.get(), inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
+    case 4: launch(k_sym_keys<4>, key_blocks(4), T, 0, s, n, A.row, A.col, A.val, inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
+    case 8: launch(k_sym_keys<8>, key_blocks(8), T, 0, s, n, A.row, A.col, A.val, inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
+    case 16: launch(k_sym_keys<16>, key_blocks(16), T, 0, s, n, A.row, A.col, A.val, inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
+    default: launch(k_sym_keys<32>, key_blocks(32), T, 0, s, n, A.row, A.col, A.val, inv.get(), ucnt.get(), E.get(), nonsym.get()); break;
   }
   BCMG_LAUNCH_CHECK();
   phase_tick("sort_prefs");
