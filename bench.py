@@ -95,6 +95,12 @@ def make_workload(name):
         A = wl.poisson(7, 96, 96, 96)
         b = wl.vector(1, 3, A.n)
         desc = "3-D 7-point Poisson 96^3, b ~ N(0,1) seed 3"
+    elif name == "rgg_2m":
+        A = wl.rgg(2_000_000, seed=4)
+        b = wl.vector(1, 4, A.n)
+        desc = ("random geometric graph Laplacian, 2,000,000 points in the unit cube, mean "
+                "degree 12, weights U[0.5, 2], shift 1e-3 (the largest graphs of the served "
+                "stream), b ~ N(0,1) seed 4")
     elif name == "poisson7_96_x32":
         A = wl.poisson(7, 96, 96, 96)
         # 32 right-hand sides: one N(0,1) stream from seed 3, column-major.
@@ -703,6 +709,20 @@ def run_batch(args):
         g1.record(stream)
         torch.cuda.synchronize(dev)
         fp64_single.append((g0.elapsed_time(g1), si.iters))
+    # The same plain FP64 path batched: all columns in one solve on the FP64
+    # handle (warmed once), so batching and precision gains are separable.
+    with torch.cuda.stream(stream):
+        Xd.zero_()
+    h64.solve_batch_device(nrhs, Bd.data_ptr(), A.n, Xd.data_ptr(), A.n)
+    with torch.cuda.stream(stream):
+        Xd.zero_()
+    torch.cuda.synchronize(dev)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    infos64 = h64.solve_batch_device(nrhs, Bd.data_ptr(), A.n, Xd.data_ptr(), A.n)
+    g1.record(stream)
+    torch.cuda.synchronize(dev)
+    fp64_batch_ms = g0.elapsed_time(g1)
     h64.close()
     fp64_ms = float(np.median([t for t, _ in fp64_single[1:]]))
     # Roofline: the level-0 batched smoother sweep on 32 interleaved columns.
@@ -818,6 +838,10 @@ def run_batch(args):
                    "fp64_single_rhs_solve_ms_median": fp64_ms,
                    "fp64_single_rhs_solves_per_s": 1e3 / fp64_ms,
                    "fp64_single_rhs_iters": [it for _, it in fp64_single],
+                   "fp64_batch_solve_ms": fp64_batch_ms,
+                   "fp64_batch_solves_per_s": nrhs / (fp64_batch_ms / 1e3),
+                   "fp64_batch_iters": [i.iters for i in infos64],
+                   "batched_mixed_over_fp64_batched": fp64_batch_ms / batch_solve_ms,
                    "batched_mixed_over_fp64_single": (nrhs / (batch_solve_ms / 1e3))
                    / (1e3 / fp64_ms),
                    "max_true_rel_residual": true_rel, **err, "shapes": cfg,
@@ -865,26 +889,14 @@ def make_matrix(spec):
     return wl.rgg(spec[1], seed=spec[2])
 
 
-def run_serve(args):
-    """Serving stream: requests with Poisson arrivals at args.rate per second
-    go to a bcmg_server (continuous batching, hierarchy cache, admission under
-    a 150 GB footprint cap).  value = completed solves / (last completion -
-    first submission); latency = submission -> solution on the host."""
+def serve_once(bc, lib, p, ext, reqs, rate, slots):
+    """One pass of the request stream through a fresh bcmg_server at `rate`
+    Poisson arrivals per second; returns its throughput and latencies."""
     import threading
     from concurrent.futures import ThreadPoolExecutor
 
-    import bootcmatchg_b200 as bc
-    from bootcmatchg_b200._lib import lib
-
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0  # replicas of the stream add nothing: one GPU per server
-    p = product_params(bc, c1_settings())
-    prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
-    ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
-    reqs = serve_requests(args.requests, 11)
     rng = np.random.default_rng(12)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, len(reqs)))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
     # Host matrices are generated ahead of their arrival by a thread pool and
     # kept while a later request may reuse them.
     pool = ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4))
@@ -901,8 +913,7 @@ def run_serve(args):
             if key not in futures:
                 futures[key] = pool.submit(make_matrix, key[1])
             ahead += 1
-    srv = bc.Server(p, ext, slots=args.slots, mem_cap_gb=150.0, cache_cap_gb=60.0,
-                    max_batch=32)
+    srv = bc.Server(p, ext, slots=slots, mem_cap_gb=150.0, cache_cap_gb=60.0, max_batch=32)
     l0 = lib.bcmg_kernel_launches()
     results = [None] * len(reqs)
     lag = []
@@ -936,42 +947,71 @@ def run_serve(args):
             futures[key] = None
     for th in threads:
         th.join()
-    t_end = time.perf_counter()
+    wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
     pool.shutdown()
-    launches = lib.bcmg_kernel_launches() - l0
     lat = np.array([r.latency_ms for r in results])
     qms = np.array([r.queue_ms for r in results])
-    conv = sum(r.solve.converged for r in results)
-    wall = t_end - t0
-    value = len(reqs) / wall
+    return {"rate_per_s": rate, "solves_per_s": len(reqs) / wall, "wall_s": wall,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99)), "mean": float(lat.mean()),
+                           "max": float(lat.max())},
+            "queue_ms": {"p50": float(np.percentile(qms, 50)),
+                         "p99": float(np.percentile(qms, 99))},
+            "converged": int(sum(r.solve.converged for r in results)),
+            "arrival_lag_ms_p99": 1e3 * float(np.percentile(lag, 99)),
+            "groups": int(sum(1 for r in results if r.group > 1)),
+            "cache_hits": int(sum(r.cache_hit for r in results)),
+            "launches": int(lib.bcmg_kernel_launches() - l0), "server": st}
+
+
+def run_serve(args):
+    """Serving stream: the requests go to a bcmg_server (continuous batching,
+    hierarchy cache, admission under a 150 GB footprint cap) with Poisson
+    arrivals, once per rate of --rate (a comma-separated list).  value = the
+    throughput at the highest rate (completed solves / (last completion -
+    first submission)); latency = submission -> solution on the host, p50 and
+    p99 at every rate."""
+    import bootcmatchg_b200 as bc
+    from bootcmatchg_b200._lib import lib
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0  # replicas of the stream add nothing: one GPU per server
+    p = product_params(bc, c1_settings())
+    prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
+    ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
+    reqs = serve_requests(args.requests, 11)
+    rates = sorted(float(r) for r in str(args.rate).split(","))
+    runs = []
+    for rate in rates:
+        r = serve_once(bc, lib, p, ext, reqs, rate, args.slots)
+        runs.append(r)
+        log(f"[bench] serve_stream {len(reqs)} requests at {rate}/s: "
+            f"{r['solves_per_s']:.1f} solves/s, latency p50 {r['latency_ms']['p50']:.1f} ms "
+            f"p99 {r['latency_ms']['p99']:.1f} ms, queue p50 {r['queue_ms']['p50']:.1f} ms, "
+            f"{r['converged']}/{len(reqs)} converged, setups {r['server']['setups']}, "
+            f"hits {r['server']['cache_hits']}, batches {r['server']['batches']}")
+    top = runs[-1]
     line = {
-        "metric": "solves/s to rtol 1e-8 and p50/p99 latency, served stream", "value": value,
-        "unit": "solves/s", "n_gpus": 1, "steps": len(reqs), "warmup": 0,
-        "ms_per_step": 1e3 * wall / len(reqs), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64" if prec else "f64", "data": "synthetic",
-        "config": {"workload": "serve_stream", "requests": len(reqs), "rate_per_s": args.rate,
+        "metric": "solves/s to rtol 1e-8 and p50/p99 latency, served stream",
+        "value": top["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "steps": len(reqs), "warmup": 0, "ms_per_step": 1e3 * top["wall_s"] / len(reqs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if prec else "f64", "data": "synthetic",
+        "config": {"workload": "serve_stream", "requests": len(reqs), "rates_per_s": rates,
                    "slots": args.slots, "mem_cap_gb": 150, "cache_cap_gb": 60,
                    "max_batch": 32, "precision": args.precision,
                    "description": serve_requests.__doc__.split("\n\n")[0].replace("\n", " ")},
-        "latency_ms": {"p50": float(np.percentile(lat, 50)),
-                       "p99": float(np.percentile(lat, 99)), "mean": float(lat.mean()),
-                       "max": float(lat.max())},
-        "queue_ms": {"p50": float(np.percentile(qms, 50)), "p99": float(np.percentile(qms, 99))},
-        "e2e": {"value": value, "unit": "solves/s",
+        "latency_ms": top["latency_ms"], "queue_ms": top["queue_ms"],
+        "by_rate": [{k: v for k, v in r.items() if k != "server"} | {"server": r["server"]}
+                    for r in runs],
+        "e2e": {"value": top["solves_per_s"], "unit": "solves/s",
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
-        "gpu_launches": int(launches),
-        "detail": {"converged": int(conv), "server": st,
-                   "arrival_lag_ms_p99": 1e3 * float(np.percentile(lag, 99)),
-                   "groups": int(sum(1 for r in results if r.group > 1)),
-                   "cache_hits": int(sum(r.cache_hit for r in results))},
+        "gpu_launches": int(sum(r["launches"] for r in runs)),
     }
     print(json.dumps(line), flush=True)
-    log(f"[bench] serve_stream rate {args.rate}/s: {value:.1f} solves/s, latency p50 "
-        f"{line['latency_ms']['p50']:.1f} ms p99 {line['latency_ms']['p99']:.1f} ms, "
-        f"{conv}/{len(reqs)} converged, setups {st['setups']}, hits {st['cache_hits']}, "
-        f"batches {st['batches']}")
     return 0
 
 
@@ -1059,10 +1099,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="poisson27_128",
-                    choices=["poisson27_128", "poisson7_32", "fv2d_2048", "poisson7_96",
+                    choices=["poisson27_128", "poisson7_32", "fv2d_2048", "poisson7_96", "rgg_2m",
                              "poisson7_96_x32", "serve_stream"])
     ap.add_argument("--requests", type=int, default=300, help="serve_stream: requests")
-    ap.add_argument("--rate", type=float, default=20.0, help="serve_stream: arrivals per s")
+    ap.add_argument("--rate", default="20", help="serve_stream: arrivals per s (a comma list "
+                    "runs the stream once per rate)")
     ap.add_argument("--slots", type=int, default=4, help="serve_stream: solves in flight")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
