@@ -550,10 +550,9 @@ bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<
     return BCMG_OK;
   }
   const XT *d = p.relax_type == 0 ? Lv<XT>::D(lv) : Lv<XT>::M(lv);
-  BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.prerelax_sweeps,
-                       zero[l - 1] != 0, s));
+  BCMG_TRY(relax_residual_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1],
+                                p.prerelax_sweeps, zero[l - 1] != 0, B.res[l - 1], s));
   zero[l - 1] = 0;
-  BCMG_TRY(residual_t<XT>(A, B.rhs[l - 1], B.x[l - 1], B.res[l - 1], s));
   if (lv.Prow)
     BCMG_TRY(spmv_t<XT>(Lv<XT>::R(lv), B.res[l - 1], B.rhs[l], s));
   else

@@ -277,6 +277,9 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
   const int32_t n = A.n;
   if (n <= 0) return BCMG_OK;
   BCMG_TRY(check_types<XT>(A));
+  // A small level held by one thread-block cluster: all sweeps in one launch.
+  if (A.has_sl && A.sl.cl_size > 0 && k >= 2)
+    return sliced_cluster<XT>(A.sl, d, f, u, k, zero_start, nullptr, s);
   if (k <= 0) {
     if (zero_start) BCMG_TRY(fill_t<XT>(u, n, XT(0), s));
     return BCMG_OK;
@@ -306,6 +309,17 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
   }
   BCMG_LAUNCH_CHECK();
   return BCMG_OK;
+}
+
+template <typename XT>
+bcmg_status relax_residual_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp,
+                             int k, bool zero_start, XT *res, cudaStream_t s) {
+  if (A.n > 0 && A.has_sl && A.sl.cl_size > 0 && k >= 1) {
+    BCMG_TRY(check_types<XT>(A));
+    return sliced_cluster<XT>(A.sl, d, f, u, k, zero_start, res, s);
+  }
+  BCMG_TRY(relax_t<XT>(A, d, f, u, u_tmp, k, zero_start, s));
+  return residual_t<XT>(A, f, u, res, s);
 }
 
 template <typename XT>
@@ -442,6 +456,8 @@ bcmg_status dot_t(int64_t n, const XT *a, const XT *b, double *out, double *part
 #define BCMG_INSTANTIATE(XT)                                                               \
   template bcmg_status relax_t<XT>(const MatView &, const XT *, const XT *, XT *, XT *, int, \
                                    bool, cudaStream_t);                                    \
+  template bcmg_status relax_residual_t<XT>(const MatView &, const XT *, const XT *, XT *,  \
+                                            XT *, int, bool, XT *, cudaStream_t);          \
   template bcmg_status residual_t<XT>(const MatView &, const XT *, const XT *, XT *,       \
                                       cudaStream_t);                                       \
   template bcmg_status restrict_t<XT>(int32_t, const int32_t *, const int32_t *, const XT *, \

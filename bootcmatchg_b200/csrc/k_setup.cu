@@ -260,17 +260,16 @@ __device__ __forceinline__ void warp_bitonic(double (&wv)[E], int32_t (&tv)[E], 
   }
 }
 
+// A row's weights in registers (entry t at lane t % 32, register t / 32);
+// -1 and offset -1 past the row's end.
 template <int E>
-__device__ __forceinline__ void sort_row_regs(int32_t i, int32_t b, int T, double ci, double wi,
-                                              const int32_t *__restrict__ col,
-                                              const double *__restrict__ val,
-                                              const double *__restrict__ w,
-                                              const double *__restrict__ C, double den,
-                                              double *W_out, double *sW, int32_t *scol,
-                                              int32_t *inv, int32_t *ucnt, int lane) {
-  double wv[E];
-  int32_t tv[E];
-  int nu = 0;
+__device__ __forceinline__ void row_weights(int32_t i, int32_t b, int T, double ci, double wi,
+                                            const int32_t *__restrict__ col,
+                                            const double *__restrict__ val,
+                                            const double *__restrict__ w,
+                                            const double *__restrict__ C, double den,
+                                            double *W_out, double (&wv)[E], int32_t (&tv)[E],
+                                            int lane) {
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     const int t = e * 32 + lane;
@@ -279,9 +278,20 @@ __device__ __forceinline__ void sort_row_regs(int32_t i, int32_t b, int T, doubl
     if (t < T) {
       wv[e] = match_weight(i, b + t, ci, wi, col, val, w, C, den, W_out);
       tv[e] = t;
-      nu += wv[e] > 0.0 ? 1 : 0;
     }
   }
+}
+
+// Orders one row from its weights in registers and writes sW, scol, inv and
+// ucnt.
+template <int E>
+__device__ __forceinline__ void order_row(int32_t i, int32_t b, int T, double (&wv)[E],
+                                          int32_t (&tv)[E], const int32_t *__restrict__ col,
+                                          double *sW, int32_t *scol, int32_t *inv,
+                                          int32_t *ucnt, int lane) {
+  int nu = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) nu += wv[e] > 0.0 ? 1 : 0;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) nu += __shfl_xor_sync(0xffffffffu, nu, o);
   if (E == 1) {
@@ -311,11 +321,52 @@ __device__ __forceinline__ void sort_row_regs(int32_t i, int32_t b, int T, doubl
   if (lane == 0) ucnt[i] = nu;
 }
 
+template <int E>
+__device__ __forceinline__ void sort_row_regs(int32_t i, int32_t b, int T, double ci, double wi,
+                                              const int32_t *__restrict__ col,
+                                              const double *__restrict__ val,
+                                              const double *__restrict__ w,
+                                              const double *__restrict__ C, double den,
+                                              double *W_out, double *sW, int32_t *scol,
+                                              int32_t *inv, int32_t *ucnt, int lane) {
+  double wv[E];
+  int32_t tv[E];
+  row_weights<E>(i, b, T, ci, wi, col, val, w, C, den, W_out, wv, tv, lane);
+  order_row<E>(i, b, T, wv, tv, col, sW, scol, inv, ucnt, lane);
+}
+
 // Computes each row's matching weights and sorts the row into preference
 // order: sW, scol, the inverse permutation inv (original offset -> sorted
 // position) and the number of usable entries per row (ucnt).  One warp per
-// row, in registers; rows longer than kSortRegMax are queued for
+// kSortRowsPerWarp consecutive rows, in registers: when both rows have at
+// most 32 entries their weights (and the gathers behind them) are computed
+// before either is ordered, so the two rows' dependent loads overlap (the
+// pass is latency-bound); rows longer than kSortRegMax are queued for
 // k_sort_prefs_long.
+constexpr int kSortRowsPerWarp = 2;
+
+__device__ __forceinline__ void sort_one_row(int32_t i, const int32_t *__restrict__ row,
+                                             const int32_t *__restrict__ col,
+                                             const double *__restrict__ val,
+                                             const double *__restrict__ w,
+                                             const double *__restrict__ C, double den,
+                                             double *W_out, double *sW, int32_t *scol,
+                                             int32_t *inv, int32_t *ucnt, int32_t *long_rows,
+                                             int32_t *n_long, int lane) {
+  const int32_t b = row[i], T = row[i + 1] - b;
+  if (T > kSortRegMax) {
+    if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
+    return;
+  }
+  const double ci = C[i], wi = w[i];
+  if (T <= 32)
+    sort_row_regs<1>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+  else if (T <= 64)
+    sort_row_regs<2>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+  else
+    sort_row_regs<4>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+}
+
 __global__ void __launch_bounds__(kSortWarps * 32)
     k_sort_prefs(int32_t n, const int32_t *__restrict__ row, const int32_t *__restrict__ col,
                  const double *__restrict__ val, const double *__restrict__ w,
@@ -324,21 +375,28 @@ __global__ void __launch_bounds__(kSortWarps * 32)
                  int32_t *scol, int32_t *inv, int32_t *ucnt, int32_t *long_rows,
                  int32_t *n_long) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int32_t i = blockIdx.x * kSortWarps + wid;
-  if (i >= n) return;
-  const int32_t b = row[i], T = row[i + 1] - b;
-  if (T > kSortRegMax) {
-    if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
+  const int32_t i0 = (blockIdx.x * kSortWarps + wid) * kSortRowsPerWarp;
+  if (i0 >= n) return;
+  const double den = 0.999 * __longlong_as_double(static_cast<long long>(*min_bits));
+  const int32_t i1 = i0 + 1;
+  const int32_t b0 = row[i0], e0 = row[i0 + 1];
+  const int32_t e1 = i1 < n ? row[i1 + 1] : e0;
+  const int T0 = e0 - b0, T1 = e1 - e0;
+  if (i1 < n && T0 <= 32 && T1 <= 32) {
+    const double ci0 = C[i0], wi0 = w[i0], ci1 = C[i1], wi1 = w[i1];
+    double w0[1], w1[1];
+    int32_t t0[1], t1[1];
+    row_weights<1>(i0, b0, T0, ci0, wi0, col, val, w, C, den, W_out, w0, t0, lane);
+    row_weights<1>(i1, e0, T1, ci1, wi1, col, val, w, C, den, W_out, w1, t1, lane);
+    order_row<1>(i0, b0, T0, w0, t0, col, sW, scol, inv, ucnt, lane);
+    order_row<1>(i1, e0, T1, w1, t1, col, sW, scol, inv, ucnt, lane);
     return;
   }
-  const double den = 0.999 * __longlong_as_double(static_cast<long long>(*min_bits));
-  const double ci = C[i], wi = w[i];
-  if (T <= 32)
-    sort_row_regs<1>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
-  else if (T <= 64)
-    sort_row_regs<2>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
-  else
-    sort_row_regs<4>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+  sort_one_row(i0, row, col, val, w, C, den, W_out, sW, scol, inv, ucnt, long_rows, n_long,
+               lane);
+  if (i1 < n)
+    sort_one_row(i1, row, col, val, w, C, den, W_out, sW, scol, inv, ucnt, long_rows, n_long,
+                 lane);
 }
 
 // Same for the queued long rows, one block per row in shared memory: each
@@ -1857,7 +1915,8 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
   BCMG_CUDA(cudaMemsetAsync(nonsym.get(), 0, sizeof(int), s));
-  launch(k_sort_prefs, ceil_div(n, kSortWarps), kSortWarps * 32, 0, s, n, A.row, A.col, A.val,
+  launch(k_sort_prefs, ceil_div(n, kSortWarps * kSortRowsPerWarp), kSortWarps * 32, 0, s, n,
+         A.row, A.col, A.val,
          w, C.get(), minb.get(), W_out, sW.get(), scol.get(), inv.get(), ucnt.get(),
          long_rows.get(), n_long.get());
   {

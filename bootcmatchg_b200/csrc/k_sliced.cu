@@ -26,6 +26,7 @@
 // keeps a full row's gathers in flight.  Every wait is bounded; a wait that
 // runs out sets a device error word (sliced_wait_status) and the kernel
 // returns without touching the stage.
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -672,6 +673,164 @@ __global__ void k_wait_selftest(const int4 *__restrict__ src, unsigned long long
   }
 }
 
+// ---- small levels on one thread-block cluster ---------------------------------
+// A level whose sliced copy fits in the shared memory of a cluster of at most
+// kClusterMax CTAs runs all its sweeps (and the residual after them) in one
+// launch: CTA q loads slices [q spc, (q + 1) spc) -- values, explicit
+// columns, metadata, f, d and its rows of the iterate -- once, and every pass
+// reads the iterate of the other CTAs through distributed shared memory, with
+// a cluster barrier between passes.  The row sums repeat slice_row_sum
+// operation for operation (same gather indices, same partial sums, same
+// batch size), so the results are those of the separate launches bit for
+// bit, while the level costs one launch instead of one per pass.
+namespace cg = cooperative_groups;
+
+constexpr int kClusterWarps = 16;
+constexpr int kClusterThreads = kClusterWarps * 32;
+constexpr int kClusterMax = 8;  // the portable cluster size
+constexpr size_t kClusterSmem = 220 * 1024;
+// A pass costs about one dependent shared-memory gather chain per slot of
+// the busiest warp; beyond this many slots a separate launch per sweep over
+// the whole GPU is faster (27-point stencils: one 32-row slice per warp).
+constexpr int32_t kClusterWarpSlots = 32;
+
+// One CTA's shared memory: the same offsets in every CTA of the cluster, so
+// a remote CTA's iterate sits where the local one does.
+struct ClusterLayout {
+  uint32_t vals, cols, meta, x0, x1, f, d, bytes;
+  __host__ __device__ ClusterLayout(int slots, int vbytes, bool cols_on, int spc, int xbytes) {
+    vals = 0;
+    cols = vals + ((static_cast<uint32_t>(slots) * 32u * vbytes + 15u) & ~15u);
+    meta = cols + (cols_on ? static_cast<uint32_t>(slots) * 32u * 4u : 0u);
+    const uint32_t rows = static_cast<uint32_t>(spc) * 32u * xbytes;
+    x0 = meta + static_cast<uint32_t>(spc) * 16u;
+    x1 = x0 + rows;
+    f = x1 + rows;
+    d = f + rows;
+    bytes = d + rows;
+  }
+};
+
+template <typename XT>
+struct ClusterArgs {
+  const XT *f, *d;
+  XT *u;      // the iterate: read unless zero_start, written at the end
+  XT *res;    // f - A u after the sweeps (nullptr: none)
+  int k;      // sweeps
+  int zero_start;
+};
+
+// slice_row_sum with the gathers served by the cluster's shared memory.
+template <typename VT, typename XT, int KB, typename Gather>
+__device__ __forceinline__ XT cluster_row_sum(const VT *v, const int32_t *cidx,
+                                              const int32_t *off, int W, int32_t r, int32_t hi,
+                                              bool interior, const Gather &g) {
+  const int lane = threadIdx.x & 31;
+  XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
+  for (int k = 0; k < W; k += KB) {
+    XT xv[KB];
+    if (cidx) {
+#pragma unroll
+      for (int q = 0; q < KB; ++q) xv[q] = g(min(max(cidx[(k + q) * 32], 0), hi));
+    } else if (KB <= 8 && interior) {
+      const int32_t offl = __ldg(off + k + lane);
+#pragma unroll
+      for (int q = 0; q < KB; ++q) xv[q] = g(r + __shfl_sync(0xffffffffu, offl, q));
+    } else {
+      const int32_t offl = __ldg(off + k + lane);
+#pragma unroll
+      for (int q = 0; q < KB; ++q)
+        xv[q] = g(min(max(r + __shfl_sync(0xffffffffu, offl, q), 0), hi));
+    }
+#pragma unroll
+    for (int q = 0; q < KB; ++q)
+      if (k + q < W)
+        t[q & 3] = fma(static_cast<XT>(widen(v[(k + q) * 32])), xv[q], t[q & 3]);
+  }
+  return (t[0] + t[1]) + (t[2] + t[3]);
+}
+
+template <typename VT, typename XT, int KB>
+__global__ void __launch_bounds__(kClusterThreads)
+    k_sl_cluster(SlicedView S, ClusterArgs<XT> a) {
+  pdl_wait();
+  pdl_trigger();
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(128) unsigned char smem[];
+  const ClusterLayout L(S.cl_slots, sizeof(VT), S.cols_staged != 0, S.cl_spc, sizeof(XT));
+  __shared__ __align__(8) uint64_t loaded;
+  const int q = static_cast<int>(cl.block_rank());
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  // slices per CTA are a power of two: a row's owner is a shift away
+  const int32_t spc = S.cl_spc, rows_cta = spc * 32;
+  const int rshift = __ffs(rows_cta) - 1;
+  const int32_t s0 = min(q * spc, S.nslices), s1 = min(s0 + spc, S.nslices);
+  const int32_t r0 = s0 * 32, nrow = max(0, min(s1 * 32, S.n) - r0);
+  const int32_t p0 = S.sptr[s0], p1 = S.sptr[s1];
+  VT *sv = reinterpret_cast<VT *>(smem + L.vals);
+  int32_t *sc = reinterpret_cast<int32_t *>(smem + L.cols);
+  int4 *sm = reinterpret_cast<int4 *>(smem + L.meta);
+  XT *xb0 = reinterpret_cast<XT *>(smem + L.x0), *xb1 = reinterpret_cast<XT *>(smem + L.x1);
+  XT *sf = reinterpret_cast<XT *>(smem + L.f), *sd = reinterpret_cast<XT *>(smem + L.d);
+  const VT *val = static_cast<const VT *>(S.val);
+  // The CTA's slots plus the padding a batch may read past its last slice
+  // (the global copy is padded the same way; those values are never used),
+  // its columns and metadata: bulk async copies under one mbarrier (all
+  // 16-byte multiples at 16-byte aligned addresses).
+  const uint32_t nsl = static_cast<uint32_t>(p1 - p0 + kSlotPad) * 32u;
+  if (tid == 0) {
+    mbar_init(&loaded, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const uint32_t vbytes = nsl * sizeof(VT), cbytes = S.cols_staged ? nsl * 4u : 0u;
+    const uint32_t mbytes = static_cast<uint32_t>(s1 - s0) * 16u;
+    mbar_arrive_tx(&loaded, vbytes + cbytes + mbytes);
+    bulk_load(sv, val + static_cast<int64_t>(p0) * 32, vbytes, &loaded);
+    if (cbytes) bulk_load(sc, S.scol + static_cast<int64_t>(p0) * 32, cbytes, &loaded);
+    bulk_load(sm, S.meta + s0, mbytes, &loaded);
+  }
+  for (int32_t i = tid; i < nrow; i += kClusterThreads) {
+    const XT fi = a.f[r0 + i], di = a.d[r0 + i];
+    sf[i] = fi;
+    sd[i] = di;
+    xb0[i] = a.zero_start ? fi / di : a.u[r0 + i];
+  }
+  __syncthreads();  // (the barrier's initialisation before anyone waits on it)
+  if (!mbar_wait(&loaded, 0, kDrainLimitNs)) atomicExch(&g_sliced_wait_error, 1);
+  cl.sync();
+  const int32_t hi = S.n - 1;
+  const int sweeps = a.k - (a.zero_start ? 1 : 0);
+  const int passes = sweeps + (a.res ? 1 : 0);
+  int cur = 0;
+  for (int p = 0; p < passes; ++p) {
+    const bool resid = p == sweeps;
+    XT *xc = cur ? xb1 : xb0;
+    XT *xn = cur ? xb0 : xb1;
+    auto gath = [&](int32_t j) -> XT {
+      const int owner = j >> rshift;
+      const XT *base = cl.map_shared_rank(xc, owner);
+      return base[j & (rows_cta - 1)];
+    };
+    for (int32_t ls = wid; ls < s1 - s0; ls += kClusterWarps) {
+      const int4 m = sm[ls];
+      const int32_t r = (s0 + ls) * 32 + lane;
+      const int64_t rel = static_cast<int64_t>(m.x - p0) * 32 + lane;
+      const XT T = cluster_row_sum<VT, XT, KB>(sv + rel, m.z ? nullptr : sc + rel,
+                                               S.soff + m.w, m.y, r, hi, m.z == 2, gath);
+      if (r < S.n) {
+        const int32_t rl = r - r0;
+        if (resid)
+          a.res[r] = sf[rl] - T;
+        else
+          xn[rl] = ((-T + sf[rl]) / sd[rl]) + xc[rl];
+      }
+    }
+    cl.sync();  // every read of this pass's iterate is done before the next
+    if (!resid) cur ^= 1;
+  }
+  const XT *xf = cur ? xb1 : xb0;
+  for (int32_t i = tid; i < nrow; i += kClusterThreads) a.u[r0 + i] = xf[i];
+}
+
 // ---- launch configuration ----------------------------------------------------
 
 struct PipeCfg {
@@ -756,6 +915,82 @@ bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaSt
   return BCMG_OK;
 }
 
+// One cluster launch (k_sl_cluster): a grid of exactly one cluster, the
+// gather batch chosen as pipe_launch chooses it (the partial sums depend on
+// it).  The shared-memory attribute is set on first use, which sliced_build
+// makes happen outside any stream capture.
+template <typename VT, typename XT, int KB>
+bcmg_status cluster_launch_kb(const SlicedView &S, const ClusterArgs<XT> &a, cudaStream_t st,
+                              bool warm_only) {
+  auto kern = k_sl_cluster<VT, XT, KB>;
+  {
+    static std::mutex mu;
+    static bool attr_set = false;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!attr_set) {
+      BCMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kClusterSmem)));
+      attr_set = true;
+    }
+  }
+  if (warm_only) return BCMG_OK;
+  const ClusterLayout L(S.cl_slots, sizeof(VT), S.cols_staged != 0, S.cl_spc, sizeof(XT));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(S.cl_size);
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = L.bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = S.cl_size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 2;
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  BCMG_CUDA(cudaLaunchKernelEx(&cfg, kern, S, a));
+  return BCMG_OK;
+}
+
+template <typename VT, typename XT>
+bcmg_status cluster_launch(const SlicedView &S, const ClusterArgs<XT> &a, cudaStream_t st,
+                           bool warm_only = false) {
+  if constexpr (sizeof(XT) == 8) {
+    if (S.batch <= 5) return cluster_launch_kb<VT, XT, 5>(S, a, st, warm_only);
+    if (S.batch <= 7) return cluster_launch_kb<VT, XT, 7>(S, a, st, warm_only);
+    if (S.batch <= 8) return cluster_launch_kb<VT, XT, 8>(S, a, st, warm_only);
+    return cluster_launch_kb<VT, XT, 14>(S, a, st, warm_only);
+  } else {
+    if (S.batch <= 5) return cluster_launch_kb<VT, XT, 5>(S, a, st, warm_only);
+    if (S.batch <= 7) return cluster_launch_kb<VT, XT, 7>(S, a, st, warm_only);
+    if (S.batch <= 8) return cluster_launch_kb<VT, XT, 8>(S, a, st, warm_only);
+    if (S.batch <= 16) return cluster_launch_kb<VT, XT, 16>(S, a, st, warm_only);
+    return cluster_launch_kb<VT, XT, 28>(S, a, st, warm_only);
+  }
+}
+
+template <typename XT>
+bcmg_status cluster_dispatch(const SlicedView &S, const ClusterArgs<XT> &a, cudaStream_t st,
+                             bool warm_only) {
+  if constexpr (sizeof(XT) == 8) {
+    switch (S.vtype) {
+      case kValF64: return cluster_launch<double, double>(S, a, st, warm_only);
+      case kValF32: return cluster_launch<float, double>(S, a, st, warm_only);
+      case kValBF16: return cluster_launch<__nv_bfloat16, double>(S, a, st, warm_only);
+      default: return cluster_launch<__half, double>(S, a, st, warm_only);
+    }
+  } else {
+    switch (S.vtype) {
+      case kValF32: return cluster_launch<float, float>(S, a, st, warm_only);
+      case kValBF16: return cluster_launch<__nv_bfloat16, float>(S, a, st, warm_only);
+      case kValF16: return cluster_launch<__half, float>(S, a, st, warm_only);
+      default: return set_error(BCMG_ERR_INTERNAL, "FP32-vector cluster passes on FP64 values");
+    }
+  }
+}
+
 template <typename VT, typename XT>
 bcmg_status relax_as(const SlicedView &S, const XT *d, const XT *f, const XT *u, XT *u_out,
                      cudaStream_t st, bool warm_only = false) {
@@ -794,7 +1029,14 @@ bcmg_status warm_f32_vectors(const SlicedView &S) {
   return BCMG_OK;
 }
 
+bcmg_status warm_cluster(const SlicedView &S) {
+  if (S.cl_size <= 0) return BCMG_OK;
+  if (S.xtype == kValF64) return cluster_dispatch<double>(S, ClusterArgs<double>{}, 0, true);
+  return cluster_dispatch<float>(S, ClusterArgs<float>{}, 0, true);
+}
+
 bcmg_status warm_kernels(const SlicedView &S) {
+  BCMG_TRY(warm_cluster(S));
   if (S.xtype == kValF64) {
     switch (S.vtype) {
       case kValF64: return warm_f64_vectors<double>(S);
@@ -829,6 +1071,7 @@ void SlicedMat::release(cudaStream_t s) {
   char *vp = static_cast<char *>(val);
   dev_free(vp, s);
   val = nullptr;
+  cl_size = cl_spc = cl_slots = 0;
   nslices = 0;
   has_columns = false;
 }
@@ -848,6 +1091,9 @@ SlicedView SlicedMat::view() const {
   v.batch = batch;
   v.xtype = xtype;
   v.wait_ns = wait_ns;
+  v.cl_size = cl_size;
+  v.cl_spc = cl_spc;
+  v.cl_slots = cl_slots;
   return v;
 }
 
@@ -972,6 +1218,35 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
   const int32_t cap_max =
       static_cast<int32_t>((kMaxStageBytes - fixed) / per_slot) - kSlotPad;
   out->cap_slots = std::max<int32_t>(1, std::min<int32_t>(h_stats[0], cap_max));
+  // Small levels: the cluster that holds the whole copy, if one does.
+  out->cl_size = out->cl_spc = out->cl_slots = 0;
+  if (ns <= kClusterMax * 64) {
+    std::vector<int32_t> h_sptr(static_cast<size_t>(ns) + 1);
+    BCMG_CUDA(cudaMemcpyAsync(h_sptr.data(), out->sptr, sizeof(int32_t) * (ns + 1),
+                              cudaMemcpyDeviceToHost, s));
+    BCMG_CUDA(cudaStreamSynchronize(s));
+    int32_t spc = 1;  // a power of two with at most kClusterMax CTAs
+    while (static_cast<int64_t>(spc) * kClusterMax < ns) spc <<= 1;
+    const int32_t csize = ceil_div(ns, spc);
+    int32_t cap = 0, warp_slots = 0;
+    for (int32_t q = 0; q < csize; ++q) {
+      const int32_t s0 = q * spc, s1 = std::min(s0 + spc, ns);
+      cap = std::max(cap, h_sptr[s1] - h_sptr[s0]);
+      for (int32_t w = 0; w < kClusterWarps; ++w) {
+        int32_t t = 0;
+        for (int32_t i = s0 + w; i < s1; i += kClusterWarps) t += h_sptr[i + 1] - h_sptr[i];
+        warp_slots = std::max(warp_slots, t);
+      }
+    }
+    cap += kSlotPad;
+    const ClusterLayout CL(cap, static_cast<int>(vb), out->has_columns, spc,
+                           out->xtype == kValF64 ? 8 : 4);
+    if (CL.bytes <= kClusterSmem && warp_slots <= kClusterWarpSlots) {
+      out->cl_size = csize;
+      out->cl_spc = spc;
+      out->cl_slots = cap;
+    }
+  }
   BCMG_TRY(warm_kernels(out->view()));
   return BCMG_OK;
 }
@@ -1077,6 +1352,25 @@ bcmg_status sliced_spmv_t<float>(const SlicedView &S, const float *x, float *y,
     default: return set_error(BCMG_ERR_INTERNAL, "FP32-vector SpMV on FP64 values");
   }
 }
+
+template <typename XT>
+bcmg_status sliced_cluster(const SlicedView &S, const XT *d, const XT *f, XT *u, int k,
+                           bool zero_start, XT *res, cudaStream_t s) {
+  if (S.cl_size <= 0 || k < 1)
+    return set_error(BCMG_ERR_INTERNAL, "no cluster plan for this level");
+  ClusterArgs<XT> a{};
+  a.f = f;
+  a.d = d;
+  a.u = u;
+  a.res = res;
+  a.k = k;
+  a.zero_start = zero_start ? 1 : 0;
+  return cluster_dispatch<XT>(S, a, s, false);
+}
+template bcmg_status sliced_cluster<double>(const SlicedView &, const double *, const double *,
+                                            double *, int, bool, double *, cudaStream_t);
+template bcmg_status sliced_cluster<float>(const SlicedView &, const float *, const float *,
+                                           float *, int, bool, float *, cudaStream_t);
 
 bcmg_status wait_selftest(unsigned long long limit_ns, cudaStream_t s) {
   DevBuf<int4> src;

@@ -79,6 +79,10 @@ struct SlicedView {
   int32_t batch = 0;        // mean slice width (chooses the slot batch size)
   int xtype = kValF64;      // vector type the copy serves (kValF64 or kValF32)
   unsigned long long wait_ns = kDefaultWaitNs;  // bound on each pipeline wait
+  // Small levels (sliced_cluster): the thread-block cluster size that holds
+  // the whole copy in shared memory (0: the copy does not fit), slices per
+  // CTA and the slot capacity of one CTA's shared memory.
+  int32_t cl_size = 0, cl_spc = 0, cl_slots = 0;
 };
 
 struct SlicedMat {
@@ -92,6 +96,7 @@ struct SlicedMat {
   bool narrowed = false;     // values stored narrower than xtype (all exact)
   bool has_columns = false;  // scol allocated (some slice is a column slice)
   unsigned long long wait_ns = kDefaultWaitNs;  // copied into every view
+  int32_t cl_size = 0, cl_spc = 0, cl_slots = 0;  // see SlicedView
   void release(cudaStream_t s);
   size_t bytes() const;  // device bytes held
   SlicedView view() const;
@@ -118,6 +123,15 @@ bcmg_status sliced_spmv_t(const SlicedView &S, const XT *x, XT *y, cudaStream_t 
 bcmg_status sliced_fcg_spmv_dots(const SlicedView &S, const double *v, double *w,
                                  const double *r, const double *q, double *partials,
                                  cudaStream_t s);
+// k sweeps u <- ((-(A u) + f) ./ d) + u (zero_start: the first is f ./ d),
+// then res = f - A u when res is given, in one launch of one thread-block
+// cluster that holds the whole copy in shared memory (S.cl_size > 0): the
+// iterate lives in distributed shared memory and passes are separated by
+// cluster barriers.  Bit-identical to relax_t and residual_t.
+template <typename XT>
+bcmg_status sliced_cluster(const SlicedView &S, const XT *d, const XT *f, XT *u, int k,
+                           bool zero_start, XT *res, cudaStream_t s);
+
 // BCMG_ERR_DEVICE_TIMEOUT (and the flag cleared) if a sliced row pass gave up
 // waiting for its staged copies since the last call; synchronises s.
 bcmg_status sliced_wait_status(cudaStream_t s);
@@ -143,6 +157,10 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
                     bool zero_start, cudaStream_t s);
 template <typename XT>  // res = f - A u
 bcmg_status residual_t(const MatView &A, const XT *f, const XT *u, XT *res, cudaStream_t s);
+// relax_t and then res = f - A u, in one launch on a level with a cluster plan.
+template <typename XT>
+bcmg_status relax_residual_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp,
+                             int k, bool zero_start, XT *res, cudaStream_t s);
 template <typename XT>  // y[I] = sum_{i in I} p_i x_i
 bcmg_status restrict_t(int32_t nc, const int32_t *rptr, const int32_t *ridx, const XT *p,
                        const XT *x, XT *y, cudaStream_t s);

@@ -142,3 +142,33 @@ def test_exact_value_narrowing_is_bit_identical(prec):
     assert out[1][2] == (4 if prec == bc.PREC_MIXED else 8)
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
+@pytest.mark.parametrize("case", ["poisson27_48", "rgg_20000", "fv2d_128"])
+def test_fused_sweeps_equal_single_sweeps(case, prec):
+    """k sweeps in one call (one launch on levels small enough for a
+    thread-block cluster, whose iterate stays in distributed shared memory)
+    give the bits of k calls of one sweep each, on every level."""
+    import ctypes as C
+    import torch
+    from bootcmatchg_b200._lib import check, lib
+    A = {"poisson27_48": lambda: wl.poisson(27, 48, 48, 48),
+         "rgg_20000": lambda: wl.rgg(20000, seed=3),
+         "fv2d_128": lambda: wl.fv2d(128, 128, seed=2)}[case]()
+    dt = torch.float32 if prec == bc.PREC_MIXED else torch.float64
+    ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
+    with bc.Handle(A, c1_params(), ext) as h:
+        for level in range(h.hierarchy_info()["num_levels"]):
+            n = h.level(0, level).n
+            g = torch.Generator(device="cuda").manual_seed(level)
+            f = torch.randn(n, dtype=dt, device="cuda", generator=g)
+            u0 = torch.randn(n, dtype=dt, device="cuda", generator=g)
+            for k in (2, 5, 16):
+                ua, ub = u0.clone(), u0.clone()
+                check(lib.bcmg_level_relax(h.ptr, 0, level, C.c_void_p(f.data_ptr()),
+                                           C.c_void_p(ua.data_ptr()), k), "k sweeps")
+                for _ in range(k):
+                    check(lib.bcmg_level_relax(h.ptr, 0, level, C.c_void_p(f.data_ptr()),
+                                               C.c_void_p(ub.data_ptr()), 1), "one sweep")
+                assert torch.equal(ua, ub), (level, k)
