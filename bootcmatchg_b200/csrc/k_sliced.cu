@@ -335,38 +335,62 @@ __device__ __forceinline__ double gather(const double *x, int32_t i) {
   return v;
 }
 
+// Gathers of a row sum from the iterate in global memory: x[i], or x[r + o]
+// relative to the row set by row() (one 64-bit multiply-add per gather).
+template <typename XT>
+struct GlobalGather {
+  const XT *x;
+  const XT *xr;
+  __device__ void row(int32_t r) { xr = x + r; }
+  __device__ XT operator()(int32_t i) const { return gather(x, i); }
+  __device__ XT rel(int32_t o) const { return gather(xr, o); }
+};
+
+// One batch of KB slots of a slice row sum (see row_sum); Full: every slot
+// of the batch is below the slice width, so no slot is tested.
+template <typename VT, typename XT, int KB, bool Full, typename G>
+__device__ __forceinline__ void row_batch(XT (&t)[4], const VT *v, const int32_t *cidx,
+                                          const int32_t *off, int k, int W, int32_t r,
+                                          int32_t hi, bool interior, const G &g) {
+  const int lane = threadIdx.x & 31;
+  XT xv[KB];
+  if (cidx) {
+#pragma unroll
+    for (int q = 0; q < KB; ++q) xv[q] = g(min(max(cidx[(k + q) * 32], 0), hi));
+  } else if (interior) {
+    const int32_t offl = __ldg(off + k + lane);
+#pragma unroll
+    for (int q = 0; q < KB; ++q) xv[q] = g.rel(__shfl_sync(0xffffffffu, offl, q));
+  } else {
+    const int32_t offl = __ldg(off + k + lane);
+#pragma unroll
+    for (int q = 0; q < KB; ++q)
+      xv[q] = g(min(max(r + __shfl_sync(0xffffffffu, offl, q), 0), hi));
+  }
+#pragma unroll
+  for (int q = 0; q < KB; ++q)
+    if (Full || k + q < W)
+      t[q & 3] = fma(static_cast<XT>(widen(v[(k + q) * 32])), xv[q], t[q & 3]);
+}
+
 // Row sum t = sum_k val[k] * x[col_k] of one slice row, slots in batches of
 // KB.  v: the slice's values at this lane (shared or global memory); cidx: the
 // slice's explicit columns at this lane (column slices), else off: the
-// slice's offsets (offset slices).  Loads past slot W-1 stay inside the
-// padding and their products are dropped.  The four partial sums by slot
-// index mod 4 fix the summation order.
-template <typename VT, typename XT, int KB>
-__device__ __forceinline__ XT slice_row_sum(const VT *v, const int32_t *cidx,
-                                            const int32_t *off, int W, int32_t r, int32_t hi,
-                                            bool interior, const XT *__restrict__ x) {
-  const int lane = threadIdx.x & 31;
+// slice's offsets (offset slices; interior: every r + o lies in [0, n), as
+// every entry of the offset array does for an interior slice, so no clamp).
+// Gathers past slot W-1 read inside the padding and their products are
+// dropped.  The four partial sums by slot index within the batch mod 4 fix
+// the summation order, which therefore depends on KB; the gather functor g
+// (g(i), g.rel(o) = x[r + o]) decides where x lives.
+template <typename VT, typename XT, int KB, typename G>
+__device__ __forceinline__ XT row_sum(const VT *v, const int32_t *cidx, const int32_t *off,
+                                      int W, int32_t r, int32_t hi, bool interior,
+                                      const G &g) {
   XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
-  for (int k = 0; k < W; k += KB) {
-    XT xv[KB];
-    if (cidx) {
-#pragma unroll
-      for (int q = 0; q < KB; ++q) xv[q] = gather(x, min(max(cidx[(k + q) * 32], 0), hi));
-    } else if (KB <= 8 && interior) {  // narrow stencils are issue-bound
-      const int32_t offl = __ldg(off + k + lane);
-#pragma unroll
-      for (int q = 0; q < KB; ++q) xv[q] = gather(x, r + __shfl_sync(0xffffffffu, offl, q));
-    } else {
-      const int32_t offl = __ldg(off + k + lane);
-#pragma unroll
-      for (int q = 0; q < KB; ++q)
-        xv[q] = gather(x, min(max(r + __shfl_sync(0xffffffffu, offl, q), 0), hi));
-    }
-#pragma unroll
-    for (int q = 0; q < KB; ++q)
-      if (k + q < W)
-        t[q & 3] = fma(static_cast<XT>(widen(v[(k + q) * 32])), xv[q], t[q & 3]);
-  }
+  int k = 0;
+  for (; k + KB <= W; k += KB)
+    row_batch<VT, XT, KB, true>(t, v, cidx, off, k, W, r, hi, interior, g);
+  if (k < W) row_batch<VT, XT, KB, false>(t, v, cidx, off, k, W, r, hi, interior, g);
   return (t[0] + t[1]) + (t[2] + t[3]);
 }
 
@@ -497,14 +521,16 @@ struct __align__(16) StageCtl {
 
 // Resident CTAs per SM the register budget is sized for: FP64 vectors three
 // (24 consumer warps, with at most 14 gathers per batch), FP32 vectors four
-// (more would spill).
-template <typename XT>
+// (more would spill), FP32 batches of 27 or more three (four spilled and ran
+// 7% slower on a 27-point level).
+constexpr int kWideMinBlocks = 3;
+template <typename XT, int KB>
 constexpr int pipe_min_blocks() {
-  return sizeof(XT) == 8 ? 3 : 4;
+  return sizeof(XT) == 8 ? 3 : (KB >= 27 ? kWideMinBlocks : 4);
 }
 
 template <typename VT, typename XT, typename Epi, int KB>
-__global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
+__global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT, KB>())
     k_sl_pipe(SlicedView S, const VT *__restrict__ val, const XT *__restrict__ x, Epi epi,
               int cap_slots, int cols_staged) {
   pdl_wait();
@@ -606,6 +632,8 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
     const int32_t s = c * kPipeWarps + wid;
     if (s < S.nslices) {
       const int32_t r = s * 32 + lane;
+      GlobalGather<XT> g{x, x};
+      g.row(r);
       const int4 m = cl.staged ? reinterpret_cast<const int4 *>(base + L.meta)[wid]
                                : __ldg(S.meta + s);
       XT rv[NVS];
@@ -629,11 +657,11 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT>())
             m.z ? nullptr
                 : (cols_staged ? reinterpret_cast<const int32_t *>(base + L.cols) + rel
                                : S.scol + static_cast<int64_t>(m.x) * 32 + lane);
-        T = slice_row_sum<VT, XT, KB>(v, ci, S.soff + m.w, m.y, r, hi, m.z == 2, x);
+        T = row_sum<VT, XT, KB>(v, ci, S.soff + m.w, m.y, r, hi, m.z == 2, g);
       } else {
         const int64_t at = static_cast<int64_t>(m.x) * 32 + lane;
-        T = slice_row_sum<VT, XT, KB>(val + at, m.z ? nullptr : S.scol + at, S.soff + m.w, m.y,
-                                      r, hi, m.z == 2, x);
+        T = row_sum<VT, XT, KB>(val + at, m.z ? nullptr : S.scol + at, S.soff + m.w, m.y, r,
+                                hi, m.z == 2, g);
       }
       if (r < S.n) epi.apply(r, T, rv);
     }
@@ -720,35 +748,21 @@ struct ClusterArgs {
   int zero_start;
 };
 
-// slice_row_sum with the gathers served by the cluster's shared memory.
-template <typename VT, typename XT, int KB, typename Gather>
-__device__ __forceinline__ XT cluster_row_sum(const VT *v, const int32_t *cidx,
-                                              const int32_t *off, int W, int32_t r, int32_t hi,
-                                              bool interior, const Gather &g) {
-  const int lane = threadIdx.x & 31;
-  XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
-  for (int k = 0; k < W; k += KB) {
-    XT xv[KB];
-    if (cidx) {
-#pragma unroll
-      for (int q = 0; q < KB; ++q) xv[q] = g(min(max(cidx[(k + q) * 32], 0), hi));
-    } else if (KB <= 8 && interior) {
-      const int32_t offl = __ldg(off + k + lane);
-#pragma unroll
-      for (int q = 0; q < KB; ++q) xv[q] = g(r + __shfl_sync(0xffffffffu, offl, q));
-    } else {
-      const int32_t offl = __ldg(off + k + lane);
-#pragma unroll
-      for (int q = 0; q < KB; ++q)
-        xv[q] = g(min(max(r + __shfl_sync(0xffffffffu, offl, q), 0), hi));
-    }
-#pragma unroll
-    for (int q = 0; q < KB; ++q)
-      if (k + q < W)
-        t[q & 3] = fma(static_cast<XT>(widen(v[(k + q) * 32])), xv[q], t[q & 3]);
+// Gathers from the iterate held across the cluster's shared memory: row j
+// lives in CTA j >> shift at position j & mask.
+template <typename XT>
+struct ClusterGather {
+  XT *xc;
+  int shift;
+  int32_t mask, r;
+  __device__ void row(int32_t rr) { r = rr; }
+  __device__ XT operator()(int32_t j) const {
+    cg::cluster_group cl = cg::this_cluster();
+    const XT *base = cl.map_shared_rank(xc, static_cast<int>(j >> shift));
+    return base[j & mask];
   }
-  return (t[0] + t[1]) + (t[2] + t[3]);
-}
+  __device__ XT rel(int32_t o) const { return (*this)(r + o); }
+};
 
 template <typename VT, typename XT, int KB>
 __global__ void __launch_bounds__(kClusterThreads)
@@ -805,17 +819,14 @@ __global__ void __launch_bounds__(kClusterThreads)
     const bool resid = p == sweeps;
     XT *xc = cur ? xb1 : xb0;
     XT *xn = cur ? xb0 : xb1;
-    auto gath = [&](int32_t j) -> XT {
-      const int owner = j >> rshift;
-      const XT *base = cl.map_shared_rank(xc, owner);
-      return base[j & (rows_cta - 1)];
-    };
+    ClusterGather<XT> gath{xc, rshift, rows_cta - 1, 0};
     for (int32_t ls = wid; ls < s1 - s0; ls += kClusterWarps) {
       const int4 m = sm[ls];
       const int32_t r = (s0 + ls) * 32 + lane;
       const int64_t rel = static_cast<int64_t>(m.x - p0) * 32 + lane;
-      const XT T = cluster_row_sum<VT, XT, KB>(sv + rel, m.z ? nullptr : sc + rel,
-                                               S.soff + m.w, m.y, r, hi, m.z == 2, gath);
+      gath.row(r);
+      const XT T = row_sum<VT, XT, KB>(sv + rel, m.z ? nullptr : sc + rel, S.soff + m.w, m.y, r,
+                                       hi, m.z == 2, gath);
       if (r < S.n) {
         const int32_t rl = r - r0;
         if (resid)
@@ -894,8 +905,9 @@ bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaSt
       launch_pdl(kern, cfg.grid, kPipeThreads, cfg.smem, st, S, static_cast<const VT *>(S.val), \
              x, epi, S.cap_slots, S.cols_staged);                                           \
   } while (0)
-  // Gathers per batch matched to the mean slice width: 5-point (2-D) and
-  // 7-point (3-D) stencils issue no padding gathers.  FP64 vectors take at
+  // Gathers per batch matched to the mean slice width: 5-point (2-D), 7- and
+  // 27-point (3-D) stencils issue no padding gathers and test no slot
+  // (FP32 vectors).  FP64 vectors take at
   // most 14 gathers per batch (two batches cover a 27-point row), which keeps
   // three CTAs per SM in the register file.
   if constexpr (sizeof(XT) == 8) {
@@ -908,6 +920,7 @@ bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaSt
     else if (S.batch <= 7) BCMG_PIPE_KB(7);
     else if (S.batch <= 8) BCMG_PIPE_KB(8);
     else if (S.batch <= 16) BCMG_PIPE_KB(16);
+    else if (S.batch <= 27) BCMG_PIPE_KB(27);
     else BCMG_PIPE_KB(28);
   }
 #undef BCMG_PIPE_KB
@@ -967,6 +980,7 @@ bcmg_status cluster_launch(const SlicedView &S, const ClusterArgs<XT> &a, cudaSt
     if (S.batch <= 7) return cluster_launch_kb<VT, XT, 7>(S, a, st, warm_only);
     if (S.batch <= 8) return cluster_launch_kb<VT, XT, 8>(S, a, st, warm_only);
     if (S.batch <= 16) return cluster_launch_kb<VT, XT, 16>(S, a, st, warm_only);
+    if (S.batch <= 27) return cluster_launch_kb<VT, XT, 27>(S, a, st, warm_only);
     return cluster_launch_kb<VT, XT, 28>(S, a, st, warm_only);
   }
 }
@@ -1121,10 +1135,10 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
          kind.get(), offrange.get());
   BCMG_TRY(exclusive_scan(width.get(), out->sptr, ns, out->sptr + ns, tmp.get(), s));
   BCMG_CUDA(cudaMemsetAsync(stats.get(), 0, 2 * sizeof(int32_t), s));
-  // Only copies that serve FP64 vectors are narrowed: FP64 -> BF16 cuts the
-  // value stream 4x on a DRAM-bound kernel, while an FP32-vector sweep with
-  // BF16 values stops being DRAM-bound (issue-bound at about the same time).
-  const bool try_narrow = narrow && vtype == kValF64 && A.nnz > 0;
+  // FP64 -> BF16 cuts the value stream 4x, FP32 -> BF16 2x; a copy serving
+  // FP32 vectors narrows to BF16 or FP16 only, and copies already stored in
+  // 16 bits (rounded on purpose) stay as they are.
+  const bool try_narrow = narrow && (vtype == kValF64 || vtype == kValF32) && A.nnz > 0;
   {
     const int32_t all = 7;
     BCMG_CUDA(cudaMemcpyAsync(stats.get() + 2, &all, sizeof(int32_t), cudaMemcpyHostToDevice, s));
@@ -1150,7 +1164,7 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
     const int exact = h_stats[2];
     if (exact & 2) vtype = kValBF16;
     else if (exact & 4) vtype = kValF16;
-    else if (exact & 1) vtype = kValF32;
+    else if ((exact & 1) && vtype == kValF64) vtype = kValF32;
   }
   out->vtype = vtype;
   out->narrowed = out->vtype != (out->xtype == kValF64 ? kValF64 : kValF32);

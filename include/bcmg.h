@@ -103,11 +103,11 @@ typedef struct bcmg_ext {
   int    autotune;        /* batched solves: time the row-kernel shapes of every
                              level once per batch width (default 1); 0 uses a
                              fixed rule.  Results are identical either way.   */
-  int    narrow_values;   /* store the values of the solve-phase copies that
-                             serve FP64 vectors (FP64 cycle, FCG SpMV) in
-                             BF16, FP16 or FP32 when every value converts
-                             exactly (default 1); the kernels widen them, so
-                             results are bit-identical with 0.               */
+  int    narrow_values;   /* store the values of the FP64 and FP32
+                             solve-phase copies (cycle, FCG SpMV) in BF16,
+                             FP16 or (FP64 copies) FP32 when every value
+                             converts exactly (default 1); the kernels widen
+                             them, so results are bit-identical with 0.      */
   int64_t match_step_limit; /* bound on the steps (proposals and displacements)
                              of each suitor-matching thread; 0 (default): 8 nnz
                              + 1024 of the level.  A thread that runs out makes

@@ -116,11 +116,10 @@ def test_sliced_and_csr_solves_agree():
 
 @pytest.mark.parametrize("prec", [bc.PREC_FP64, bc.PREC_MIXED])
 def test_exact_value_narrowing_is_bit_identical(prec):
-    """Solve-phase copies serving FP64 vectors (the FP64 cycle, and the FCG
-    SpMV in both modes) store a level's values in BF16 when every value
-    converts exactly (the 27-point stencil's 26 and -1); the kernels widen
-    them, so the solution matches the unnarrowed run bit for bit.  The mixed
-    cycle's FP32 copy is not narrowed."""
+    """Solve-phase copies (the FP64 or FP32 cycle, and the FCG SpMV in both
+    modes) store a level's values in BF16 when every value converts exactly
+    (the 27-point stencil's 26 and -1); the kernels widen them, so the
+    solution matches the unnarrowed run bit for bit."""
     import ctypes as C
     from bootcmatchg_b200._lib import check, lib
     A = wl.poisson(27, 32, 32, 32)
@@ -138,7 +137,7 @@ def test_exact_value_narrowing_is_bit_identical(prec):
                                         C.byref(nsl), C.byref(vb)), "level_format")
         assert info.converged
         out.append((x, info.iters, vb.value))
-    assert out[0][2] == (4 if prec == bc.PREC_MIXED else 2)
+    assert out[0][2] == 2
     assert out[1][2] == (4 if prec == bc.PREC_MIXED else 8)
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
