@@ -48,7 +48,7 @@ namespace {
 constexpr int kWarpsPerBlock = 8;    // build kernels: one warp per slice
 constexpr int kMaxOffsetSlots = 64;  // wider unions fall back to column slices
 constexpr int kPipeWarps = 8;        // consumer warps per CTA = slices per chunk
-constexpr int kPipeStages = 2;
+constexpr int kPipeStages = 2;  // more stages took L1 from the gathers and ran slower
 constexpr int kPipeThreads = (kPipeWarps + 1) * 32;
 constexpr int kSlotPad = 32;                       // >= the largest slot batch
 constexpr size_t kMaxStageBytes = 108 * 1024;      // two stages fit in 227 KB
@@ -231,7 +231,8 @@ __global__ void k_slice_heads(int32_t nslices, const int32_t *__restrict__ flag,
 // meta.z: 0 column slice, 1 offset slice, 2 interior offset slice — every
 // row r of the slice is below n and r + o stays in [0, n) for every offset o
 // in offrange, which bounds every entry of soff (offsets of offset slices,
-// zeros elsewhere), so its gathers need no clamping.
+// zeros elsewhere), so its gathers need no clamping; 3 (k_slice_stencil) an
+// interior slice whose offsets are the copy's stencil.
 __global__ void k_slice_meta(int32_t n, int32_t nslices, const int32_t *__restrict__ sptr,
                              const int32_t *__restrict__ width,
                              const int32_t *__restrict__ kind,
@@ -246,6 +247,33 @@ __global__ void k_slice_meta(int32_t n, int32_t nslices, const int32_t *__restri
   const bool interior =
       kind[s] == 1 && r1 < n && r0 + offrange[0] >= 0 && r1 + offrange[1] < n;
   meta[s] = make_int4(sptr[s], width[s], interior ? 2 : kind[s], sptr[h]);
+}
+
+// The first interior slice exactly w slots wide (none: *first stays nslices).
+__global__ void k_stencil_pick(int32_t nslices, const int4 *__restrict__ meta, int32_t w,
+                               int32_t *first) {
+  const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  bool hit = false;
+  if (s < nslices) {
+    const int4 m = meta[s];
+    hit = m.z == 2 && m.y == w;
+  }
+  const unsigned lo = __reduce_min_sync(0xffffffffu, hit ? static_cast<unsigned>(s) : ~0u);
+  if ((threadIdx.x & 31) == 0 && lo != ~0u) atomicMin(first, static_cast<int32_t>(lo));
+}
+
+// Marks interior slices whose offset list is the stencil soff[base .. base +
+// w) (the list of one interior slice of width w) as kind 3.
+__global__ void k_slice_stencil(int32_t nslices, const int32_t *__restrict__ soff,
+                                int32_t base, int32_t w, int4 *meta) {
+  const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslices) return;
+  int4 m = meta[s];
+  if (m.z != 2 || m.y != w) return;
+  for (int32_t i = 0; i < w; ++i)
+    if (soff[m.w + i] != soff[base + i]) return;
+  m.z = 3;
+  meta[s] = m;
 }
 
 // ---- pipeline primitives (mbarrier + bulk async copy) ---------------------
@@ -265,13 +293,16 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t *b, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
+// One try_wait: the thread may sleep until the phase completes or about
+// kSuspendHintNs pass (a waiting warp issues no instructions meanwhile).
+constexpr uint32_t kSuspendHintNs = 1000000;
 __device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; "
       "selp.u32 %0, 1, 0, p; }"
       : "=r"(ok)
-      : "r"(smem_addr(b)), "r"(parity)
+      : "r"(smem_addr(b)), "r"(parity), "r"(kSuspendHintNs)
       : "memory");
   return ok != 0;
 }
@@ -344,6 +375,9 @@ struct GlobalGather {
   __device__ void row(int32_t r) { xr = x + r; }
   __device__ XT operator()(int32_t i) const { return gather(x, i); }
   __device__ XT rel(int32_t o) const { return gather(xr, o); }
+  // x[r + o] for an offset held in a kernel parameter: plain C, so the
+  // offset stays a constant-bank operand of the address arithmetic.
+  __device__ XT rel_param(int32_t o) const { return __ldg(xr + o); }
 };
 
 // One batch of KB slots of a slice row sum (see row_sum); Full: every slot
@@ -391,6 +425,42 @@ __device__ __forceinline__ XT row_sum(const VT *v, const int32_t *cidx, const in
   for (; k + KB <= W; k += KB)
     row_batch<VT, XT, KB, true>(t, v, cidx, off, k, W, r, hi, interior, g);
   if (k < W) row_batch<VT, XT, KB, false>(t, v, cidx, off, k, W, r, hi, interior, g);
+  return (t[0] + t[1]) + (t[2] + t[3]);
+}
+
+// row_sum of a stencil slice (meta.z == 3, width W = S.sten_w <= 2 KB): the
+// offsets are kernel parameters, so no offset is loaded or shuffled; the
+// batches and the summation order are row_sum's.  Offsets past W are zero,
+// so the padding gathers stay in the row.
+template <typename VT, typename XT, int KB, typename G>
+__device__ __forceinline__ XT stencil_row_sum(const VT *v, const SlicedView &S, const G &g) {
+  const int W = S.sten_w;
+  XT t[4] = {XT(0), XT(0), XT(0), XT(0)};
+  {
+    XT xv[KB];
+#pragma unroll
+    for (int q = 0; q < KB; ++q) xv[q] = g.rel_param(S.sten_off[q]);
+    if (W >= KB) {
+#pragma unroll
+      for (int q = 0; q < KB; ++q)
+        t[q & 3] = fma(static_cast<XT>(widen(v[q * 32])), xv[q], t[q & 3]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < KB; ++q)
+        if (q < W) t[q & 3] = fma(static_cast<XT>(widen(v[q * 32])), xv[q], t[q & 3]);
+    }
+  }
+  if constexpr (KB < kStencilMax) {
+    constexpr int K2 = kStencilMax - KB < KB ? kStencilMax - KB : KB;
+    if (W > KB) {
+      XT xv[K2];
+#pragma unroll
+      for (int q = 0; q < K2; ++q) xv[q] = g.rel_param(S.sten_off[KB + q]);
+#pragma unroll
+      for (int q = 0; q < K2; ++q)
+        if (KB + q < W) t[q & 3] = fma(static_cast<XT>(widen(v[(KB + q) * 32])), xv[q], t[q & 3]);
+    }
+  }
   return (t[0] + t[1]) + (t[2] + t[3]);
 }
 
@@ -657,11 +727,13 @@ __global__ void __launch_bounds__(kPipeThreads, pipe_min_blocks<XT, KB>())
             m.z ? nullptr
                 : (cols_staged ? reinterpret_cast<const int32_t *>(base + L.cols) + rel
                                : S.scol + static_cast<int64_t>(m.x) * 32 + lane);
-        T = row_sum<VT, XT, KB>(v, ci, S.soff + m.w, m.y, r, hi, m.z == 2, g);
+        T = m.z == 3 ? stencil_row_sum<VT, XT, KB>(v, S, g)
+                     : row_sum<VT, XT, KB>(v, ci, S.soff + m.w, m.y, r, hi, m.z == 2, g);
       } else {
         const int64_t at = static_cast<int64_t>(m.x) * 32 + lane;
-        T = row_sum<VT, XT, KB>(val + at, m.z ? nullptr : S.scol + at, S.soff + m.w, m.y, r,
-                                hi, m.z == 2, g);
+        T = m.z == 3 ? stencil_row_sum<VT, XT, KB>(val + at, S, g)
+                     : row_sum<VT, XT, KB>(val + at, m.z ? nullptr : S.scol + at, S.soff + m.w,
+                                           m.y, r, hi, m.z == 2, g);
       }
       if (r < S.n) epi.apply(r, T, rv);
     }
@@ -762,6 +834,7 @@ struct ClusterGather {
     return base[j & mask];
   }
   __device__ XT rel(int32_t o) const { return (*this)(r + o); }
+  __device__ XT rel_param(int32_t o) const { return (*this)(r + o); }
 };
 
 template <typename VT, typename XT, int KB>
@@ -825,8 +898,9 @@ __global__ void __launch_bounds__(kClusterThreads)
       const int32_t r = (s0 + ls) * 32 + lane;
       const int64_t rel = static_cast<int64_t>(m.x - p0) * 32 + lane;
       gath.row(r);
-      const XT T = row_sum<VT, XT, KB>(sv + rel, m.z ? nullptr : sc + rel, S.soff + m.w, m.y, r,
-                                       hi, m.z == 2, gath);
+      const XT T = m.z == 3 ? stencil_row_sum<VT, XT, KB>(sv + rel, S, gath)
+                            : row_sum<VT, XT, KB>(sv + rel, m.z ? nullptr : sc + rel,
+                                                  S.soff + m.w, m.y, r, hi, m.z == 2, gath);
       if (r < S.n) {
         const int32_t rl = r - r0;
         if (resid)
@@ -886,6 +960,21 @@ bcmg_status pipe_cfg(K kernel, size_t stage_bytes, int32_t nchunks, PipeCfg *out
   return BCMG_OK;
 }
 
+// Gathers per batch (KB) of a copy with mean slice width `batch`, matched to
+// it so that 5-point (2-D), 7- and 27-point (3-D) stencils issue no padding
+// gathers and test no slot (27: FP32 vectors).  FP64 vectors take at most 14
+// gathers per batch (two batches cover a 27-point row), which keeps three
+// CTAs per SM in the register file.  The summation order depends on KB, so
+// every kernel reading a copy uses this rule.
+inline int slot_batch(int32_t batch, bool f64) {
+  if (batch <= 5) return 5;
+  if (batch <= 7) return 7;
+  if (batch <= 8) return 8;
+  if (f64) return 14;
+  if (batch <= 16) return 16;
+  return batch <= 27 ? 27 : 28;
+}
+
 inline int value_bytes(int vtype) {
   return vtype == kValF64 ? 8 : (vtype == kValF32 ? 4 : 2);
 }
@@ -905,23 +994,14 @@ bcmg_status pipe_launch(const SlicedView &S, const XT *x, const Epi &epi, cudaSt
       launch_pdl(kern, cfg.grid, kPipeThreads, cfg.smem, st, S, static_cast<const VT *>(S.val), \
              x, epi, S.cap_slots, S.cols_staged);                                           \
   } while (0)
-  // Gathers per batch matched to the mean slice width: 5-point (2-D), 7- and
-  // 27-point (3-D) stencils issue no padding gathers and test no slot
-  // (FP32 vectors).  FP64 vectors take at
-  // most 14 gathers per batch (two batches cover a 27-point row), which keeps
-  // three CTAs per SM in the register file.
-  if constexpr (sizeof(XT) == 8) {
-    if (S.batch <= 5) BCMG_PIPE_KB(5);
-    else if (S.batch <= 7) BCMG_PIPE_KB(7);
-    else if (S.batch <= 8) BCMG_PIPE_KB(8);
-    else BCMG_PIPE_KB(14);
-  } else {
-    if (S.batch <= 5) BCMG_PIPE_KB(5);
-    else if (S.batch <= 7) BCMG_PIPE_KB(7);
-    else if (S.batch <= 8) BCMG_PIPE_KB(8);
-    else if (S.batch <= 16) BCMG_PIPE_KB(16);
-    else if (S.batch <= 27) BCMG_PIPE_KB(27);
-    else BCMG_PIPE_KB(28);
+  switch (slot_batch(S.batch, sizeof(XT) == 8)) {
+    case 5: BCMG_PIPE_KB(5); break;
+    case 7: BCMG_PIPE_KB(7); break;
+    case 8: BCMG_PIPE_KB(8); break;
+    case 14: if constexpr (sizeof(XT) == 8) BCMG_PIPE_KB(14); break;
+    case 16: if constexpr (sizeof(XT) == 4) BCMG_PIPE_KB(16); break;
+    case 27: if constexpr (sizeof(XT) == 4) BCMG_PIPE_KB(27); break;
+    default: if constexpr (sizeof(XT) == 4) BCMG_PIPE_KB(28); break;
   }
 #undef BCMG_PIPE_KB
   if (!warm_only) BCMG_LAUNCH_CHECK();
@@ -970,18 +1050,20 @@ bcmg_status cluster_launch_kb(const SlicedView &S, const ClusterArgs<XT> &a, cud
 template <typename VT, typename XT>
 bcmg_status cluster_launch(const SlicedView &S, const ClusterArgs<XT> &a, cudaStream_t st,
                            bool warm_only = false) {
+  switch (slot_batch(S.batch, sizeof(XT) == 8)) {
+    case 5: return cluster_launch_kb<VT, XT, 5>(S, a, st, warm_only);
+    case 7: return cluster_launch_kb<VT, XT, 7>(S, a, st, warm_only);
+    case 8: return cluster_launch_kb<VT, XT, 8>(S, a, st, warm_only);
+    default: break;
+  }
   if constexpr (sizeof(XT) == 8) {
-    if (S.batch <= 5) return cluster_launch_kb<VT, XT, 5>(S, a, st, warm_only);
-    if (S.batch <= 7) return cluster_launch_kb<VT, XT, 7>(S, a, st, warm_only);
-    if (S.batch <= 8) return cluster_launch_kb<VT, XT, 8>(S, a, st, warm_only);
     return cluster_launch_kb<VT, XT, 14>(S, a, st, warm_only);
   } else {
-    if (S.batch <= 5) return cluster_launch_kb<VT, XT, 5>(S, a, st, warm_only);
-    if (S.batch <= 7) return cluster_launch_kb<VT, XT, 7>(S, a, st, warm_only);
-    if (S.batch <= 8) return cluster_launch_kb<VT, XT, 8>(S, a, st, warm_only);
-    if (S.batch <= 16) return cluster_launch_kb<VT, XT, 16>(S, a, st, warm_only);
-    if (S.batch <= 27) return cluster_launch_kb<VT, XT, 27>(S, a, st, warm_only);
-    return cluster_launch_kb<VT, XT, 28>(S, a, st, warm_only);
+    switch (slot_batch(S.batch, false)) {
+      case 16: return cluster_launch_kb<VT, XT, 16>(S, a, st, warm_only);
+      case 27: return cluster_launch_kb<VT, XT, 27>(S, a, st, warm_only);
+      default: return cluster_launch_kb<VT, XT, 28>(S, a, st, warm_only);
+    }
   }
 }
 
@@ -1086,6 +1168,7 @@ void SlicedMat::release(cudaStream_t s) {
   dev_free(vp, s);
   val = nullptr;
   cl_size = cl_spc = cl_slots = 0;
+  sten_w = 0;
   nslices = 0;
   has_columns = false;
 }
@@ -1108,6 +1191,8 @@ SlicedView SlicedMat::view() const {
   v.cl_size = cl_size;
   v.cl_spc = cl_spc;
   v.cl_slots = cl_slots;
+  v.sten_w = sten_w;
+  for (int i = 0; i < kStencilMax; ++i) v.sten_off[i] = sten_off[i];
   return v;
 }
 
@@ -1224,6 +1309,34 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
     launch(k_slice_meta, ceil_div(ns, 256), 256, 0, s, n, ns, out->sptr, width.get(),
            kind.get(), flag.get(), rid.get(), head.get(), offrange.get(), out->meta);
     BCMG_LAUNCH_CHECK();
+  }
+  // Stencil: the offsets of the first interior slice as wide as the mean
+  // slice width (at most two slot batches and kStencilMax) become kernel
+  // parameters for every slice that has the same list (kind 3).
+  out->sten_w = 0;
+  std::fill(out->sten_off, out->sten_off + kStencilMax, 0);
+  if (const int kb = out->batch;
+      kb <= kStencilMax && kb <= 2 * slot_batch(out->batch, out->xtype == kValF64)) {
+    BCMG_CUDA(cudaMemcpyAsync(stats.get(), &ns, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    launch(k_stencil_pick, ceil_div(ns, 256), 256, 0, s, ns, out->meta, kb, stats.get());
+    BCMG_LAUNCH_CHECK();
+    int32_t first = ns;
+    BCMG_CUDA(cudaMemcpyAsync(&first, stats.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    BCMG_CUDA(cudaStreamSynchronize(s));
+    int4 hm = make_int4(0, 0, 0, 0);
+    if (first < ns) {
+      BCMG_CUDA(cudaMemcpyAsync(&hm, out->meta + first, sizeof(int4), cudaMemcpyDeviceToHost,
+                                s));
+      BCMG_CUDA(cudaStreamSynchronize(s));
+    }
+    if (first < ns && hm.z == 2 && hm.y == kb) {
+      BCMG_CUDA(cudaMemcpyAsync(out->sten_off, out->soff + hm.w, sizeof(int32_t) * kb,
+                                cudaMemcpyDeviceToHost, s));
+      launch(k_slice_stencil, ceil_div(ns, 256), 256, 0, s, ns, out->soff, hm.w, kb, out->meta);
+      BCMG_LAUNCH_CHECK();
+      BCMG_CUDA(cudaStreamSynchronize(s));
+      out->sten_w = kb;
+    }
   }
   // Stage capacity: the largest chunk, capped so two stages fit in shared
   // memory (larger chunks are read from global memory by the consumers).

@@ -67,6 +67,8 @@ enum ValType { kValF64 = 0, kValF32 = 1, kValBF16 = 2, kValF16 = 3 };
 // (bcmg_ext.max_device_seconds overrides it per handle).
 constexpr unsigned long long kDefaultWaitNs = 2000000000ull;
 
+constexpr int kStencilMax = 32;  // the widest slot batch of the sliced kernels
+
 struct SlicedView {
   int32_t n = 0, nslices = 0;
   const int32_t *sptr = nullptr;  // first slot of each slice (nslices + 1)
@@ -83,6 +85,11 @@ struct SlicedView {
   // the whole copy in shared memory (0: the copy does not fit), slices per
   // CTA and the slot capacity of one CTA's shared memory.
   int32_t cl_size = 0, cl_spc = 0, cl_slots = 0;
+  // Stencil slices (meta.z == 3): interior offset slices whose offsets are
+  // exactly sten_off[0 .. sten_w), sten_w being the slot batch of the copy;
+  // the kernels take those offsets from their parameters.
+  int32_t sten_w = 0;
+  int32_t sten_off[kStencilMax] = {};
 };
 
 struct SlicedMat {
@@ -97,6 +104,7 @@ struct SlicedMat {
   bool has_columns = false;  // scol allocated (some slice is a column slice)
   unsigned long long wait_ns = kDefaultWaitNs;  // copied into every view
   int32_t cl_size = 0, cl_spc = 0, cl_slots = 0;  // see SlicedView
+  int32_t sten_w = 0, sten_off[kStencilMax] = {};  // see SlicedView
   void release(cudaStream_t s);
   size_t bytes() const;  // device bytes held
   SlicedView view() const;
@@ -104,9 +112,9 @@ struct SlicedMat {
 
 // Builds the sliced copy of a CSR matrix with values converted to vtype
 // (kValF64: a copy for FP64 vectors; otherwise for FP32 vectors).  narrow
-// (FP64-vector copies): store the values in BF16 / FP16 / FP32 instead when
-// every value converts exactly (the kernels widen them, so results are
-// bit-identical).
+// (FP64 and FP32 copies): store the values in BF16 / FP16 (or FP32 for an
+// FP64 copy) instead when every value converts exactly (the kernels widen
+// them, so results are bit-identical).
 bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s,
                          bool narrow = false);
 template <typename XT>  // u_out = ((-(A u) + f) ./ d) + u
