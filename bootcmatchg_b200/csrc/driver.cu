@@ -534,6 +534,22 @@ bcmg_status kcycle_inner_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int c);
 // GAMG_cycle (src/SOLVER/GAMG_cycle.cu:25-140); l is 1-based as there.
 // zero[l-1] says the current iterate of level l-1 is identically zero and
 // has not been materialised: the first sweep then reduces to f ./ d.
+// The first relaxation a cycle runs on level l (1-based) of hierarchy k: its
+// sweep count (*sweeps) and diagonal (pre-smoothing, or the coarse solver
+// on the last level).
+template <typename XT>
+const XT *first_relax(const bcmg_handle *h, int k, int l, int *sweeps) {
+  const DevHierarchy &H = h->H[k];
+  const bcmg_params &p = h->prm;
+  const DevLevel &lv = H.lv[l - 1];
+  if (l == static_cast<int>(H.lv.size())) {
+    *sweeps = p.relaxnumber_coarse;
+    return p.coarse_solver == 0 ? Lv<XT>::D(lv) : Lv<XT>::M(lv);
+  }
+  *sweeps = p.prerelax_sweeps;
+  return p.relax_type == 0 ? Lv<XT>::D(lv) : Lv<XT>::M(lv);
+}
+
 template <typename XT>
 bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<char> &zero) {
   DevHierarchy &H = h->H[k];
@@ -545,19 +561,29 @@ bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<
   if (l == L) {
     const XT *d = p.coarse_solver == 0 ? Lv<XT>::D(lv) : Lv<XT>::M(lv);
     BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.relaxnumber_coarse,
-                         zero[l - 1] != 0, s));
+                         zero[l - 1], s));
     zero[l - 1] = 0;
     return BCMG_OK;
   }
   const XT *d = p.relax_type == 0 ? Lv<XT>::D(lv) : Lv<XT>::M(lv);
   BCMG_TRY(relax_residual_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1],
-                                p.prerelax_sweeps, zero[l - 1] != 0, B.res[l - 1], s));
+                                p.prerelax_sweeps, zero[l - 1], B.res[l - 1], s));
   zero[l - 1] = 0;
+  // The coarse level starts from zero: its first sweep (f ./ d) is fused
+  // into the restriction where its relaxation can take it.
+  int kc = 0;
+  const XT *dc = first_relax<XT>(h, k, l + 1, &kc);
+  const bool fuse = !lv.Prow && p.cycle_type != 3 &&
+                    first_sweep_fusable(Lv<XT>::mat(H.lv[l]), kc);
   if (lv.Prow)
     BCMG_TRY(spmv_t<XT>(Lv<XT>::R(lv), B.res[l - 1], B.rhs[l], s));
+  else if (fuse)
+    BCMG_TRY(restrict_first_sweep_t<XT>(lv.nc, lv.rptr, lv.ridx, Lv<XT>::p(lv), B.res[l - 1],
+                                        B.rhs[l], dc, first_sweep_dst(B.x[l], B.xt[l], kc),
+                                        s));
   else
     BCMG_TRY(restrict_t<XT>(lv.nc, lv.rptr, lv.ridx, Lv<XT>::p(lv), B.res[l - 1], B.rhs[l], s));
-  zero[l] = 1;
+  zero[l] = fuse ? kStartFirstDone : kStartZero;
   if (p.cycle_type == 3) {
     // K-cycle (GAMG_cycle.cu:88-100): one cycle on the coarsest level, two
     // inner flexible-CG steps on any other.
@@ -579,8 +605,8 @@ bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<
   } else {
     BCMG_TRY(prolong_t<XT>(lv.n, lv.agg, Lv<XT>::p(lv), B.x[l], B.x[l - 1], s));
   }
-  BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.postrelax_sweeps, false,
-                       s));
+  BCMG_TRY(relax_t<XT>(A, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1], p.postrelax_sweeps,
+                       kStartLive, s, l == 1 ? B.widen_out : nullptr));
   return BCMG_OK;
 }
 
@@ -653,11 +679,11 @@ bcmg_status kcycle_inner_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int c) {
 
 template <typename XT>
 bcmg_status run_cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, const XT *rhs, XT *x,
-                        bool x_zero) {
+                        int start) {
   B.rhs[0] = const_cast<XT *>(rhs);
   B.x[0] = x;
   std::vector<char> zero(B.rhs.size(), 0);
-  zero[0] = x_zero ? 1 : 0;
+  zero[0] = static_cast<char>(start);
   bcmg_status st = cycle_t<XT>(h, B, k, 1, zero);
   B.rhs[0] = nullptr;
   B.x[0] = nullptr;
@@ -703,10 +729,27 @@ bcmg_status precond_apply(bcmg_handle *h, const double *rhs, double *x, bool x_z
   const int32_t n = h->A0.n;
   cudaStream_t s = h->stream;
   CycleBufs<float> &B = h->c32;
-  BCMG_TRY(convert_d2f(n, rhs, B.in0, s));
-  if (!x_zero) BCMG_TRY(convert_d2f(n, x, B.out0, s));
-  BCMG_TRY(precond_apply_t<float>(h, B, B.in0, B.out0, x_zero));
-  BCMG_TRY(convert_f2d(n, B.out0, x, s));
+  // One V-cycle of one hierarchy: the rounding of r is fused with the first
+  // sweep from zero, and the last sweep writes z in FP64 directly.
+  const bool single = h->prm.solver_type == 0 && h->H.size() == 1 && h->prm.cycle_type != 3;
+  const MatView A0 = single ? Lv<float>::mat(h->H[0].lv[0]) : MatView();
+  int k0 = 0;
+  const float *d0 = single ? first_relax<float>(h, 0, 1, &k0) : nullptr;
+  const bool fuse_first = single && x_zero && first_sweep_fusable(A0, k0);
+  const bool fuse_last = single && h->H[0].lv.size() > 1 && widen_fusable(A0, h->prm.postrelax_sweeps);
+  if (fuse_first) {
+    BCMG_TRY(convert_first_sweep(n, rhs, d0, B.in0, first_sweep_dst(B.out0, B.xt[0], k0), s));
+  } else {
+    BCMG_TRY(convert_d2f(n, rhs, B.in0, s));
+    if (!x_zero) BCMG_TRY(convert_d2f(n, x, B.out0, s));
+  }
+  B.widen_out = fuse_last ? x : nullptr;
+  const bcmg_status st =
+      fuse_first ? run_cycle_t<float>(h, B, 0, B.in0, B.out0, kStartFirstDone)
+                 : precond_apply_t<float>(h, B, B.in0, B.out0, x_zero);
+  B.widen_out = nullptr;
+  BCMG_TRY(st);
+  if (!fuse_last) BCMG_TRY(convert_f2d(n, B.out0, x, s));
   return BCMG_OK;
 }
 
@@ -790,7 +833,13 @@ bcmg_status prepare_solve_formats(bcmg_handle *h) {
   cudaStream_t s = h->stream;
   DevLevel &a = h->A0;
   if (!a.own64.nslices) BCMG_TRY(build_sliced(h, a.view(), kValF64, &a.own64, s));
-  if (h->mixed && !a.ownlo.nslices) BCMG_TRY(build_sliced(h, a.view(), kValF32, &a.ownlo, s));
+  if (h->mixed && !a.ownlo.nslices) {
+    // Values narrowed to 16 bits are the same bytes for FP32 vectors: share.
+    if (a.own64.nslices && a.own64.narrowed && a.own64.vtype != kValF32)
+      BCMG_TRY(sliced_alias(a.own64, kValF32, &a.ownlo, s));
+    else
+      BCMG_TRY(build_sliced(h, a.view(), kValF32, &a.ownlo, s));
+  }
   for (auto &H : h->H) {
     for (size_t l = 0; l < H.lv.size(); ++l) {
       DevLevel &lv = H.lv[l];

@@ -71,6 +71,9 @@ struct CycleBufs {
   std::vector<XT *> rhs, x, xt, res;
   std::vector<int32_t> n;
   XT *xk = nullptr, *xadd = nullptr, *in0 = nullptr, *out0 = nullptr;
+  // When set, the last post-smoothing sweep of level 0 writes its result
+  // widened into this FP64 vector instead of x[0] (mixed cycle).
+  double *widen_out = nullptr;
   // K-cycle (cycle_type 3) inner iterations, per coarse level: residual w,
   // directions d0/d1, their products v/v1, the correction kx; kdots holds
   // one device dot product.

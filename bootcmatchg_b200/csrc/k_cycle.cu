@@ -98,6 +98,39 @@ __global__ void k_restrict_t(int32_t nc, const int32_t *__restrict__ rptr,
   y[I] = s;
 }
 
+// k_restrict_t fused with the coarse level's first sweep from zero.
+template <typename XT>
+__global__ void k_restrict_first_t(int32_t nc, const int32_t *__restrict__ rptr,
+                                   const int32_t *__restrict__ ridx, const XT *__restrict__ p,
+                                   const XT *__restrict__ x, XT *__restrict__ y,
+                                   const XT *__restrict__ dc, XT *__restrict__ u1) {
+  pdl_wait();
+  pdl_trigger();
+  const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nc) return;
+  XT s = XT(0);
+  for (int32_t k = rptr[I]; k < rptr[I + 1]; ++k) {
+    const int32_t i = ridx[k];
+    s = fma(p[i], x[i], s);
+  }
+  y[I] = s;
+  u1[I] = s / dc[I];
+}
+
+// FP64 -> FP32 conversion fused with the first sweep from zero.
+__global__ void k_convert_first(int64_t n, const double *__restrict__ in,
+                                const float *__restrict__ d, float *__restrict__ out,
+                                float *__restrict__ u1) {
+  pdl_wait();
+  pdl_trigger();
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float v = static_cast<float>(in[i]);
+    out[i] = v;
+    u1[i] = v / d[i];
+  }
+}
+
 template <typename XT>
 __global__ void k_prolong_t(int32_t n, const int32_t *__restrict__ agg,
                             const XT *__restrict__ p, const XT *__restrict__ xc,
@@ -273,15 +306,19 @@ void residual_pass<float>(int G, int blocks, cudaStream_t s, const MatView &A, c
 
 template <typename XT>
 bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp, int k,
-                    bool zero_start, cudaStream_t s) {
+                    int start, cudaStream_t s, double *widen_out) {
   const int32_t n = A.n;
   if (n <= 0) return BCMG_OK;
   BCMG_TRY(check_types<XT>(A));
+  if (start == kStartFirstDone && !first_sweep_fusable(A, k))
+    return set_error(BCMG_ERR_INTERNAL, "first sweep fused where it cannot be");
+  if (widen_out && (!std::is_same<XT, float>::value || !widen_fusable(A, k)))
+    return set_error(BCMG_ERR_INTERNAL, "widened sweep where it cannot be");
   // A small level held by one thread-block cluster: all sweeps in one launch.
   if (A.has_sl && A.sl.cl_size > 0 && k >= 2)
-    return sliced_cluster<XT>(A.sl, d, f, u, k, zero_start, nullptr, s);
+    return sliced_cluster<XT>(A.sl, d, f, u, k, start != kStartLive, nullptr, s);
   if (k <= 0) {
-    if (zero_start) BCMG_TRY(fill_t<XT>(u, n, XT(0), s));
+    if (start != kStartLive) BCMG_TRY(fill_t<XT>(u, n, XT(0), s));
     return BCMG_OK;
   }
   const int G = group_for(A.nnz, n);
@@ -289,9 +326,10 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
   // Arrange the ping-pong so the final iterate lands in u.
   XT *cur;
   int left = k;
-  if (zero_start) {
-    cur = (k % 2 == 1) ? u : u_tmp;
-    launch_pdl(k_relax_zero_t<XT>, ceil_div(n, kThreads), kThreads, 0, s, n, d, f, cur);
+  if (start != kStartLive) {
+    cur = first_sweep_dst(u, u_tmp, k);
+    if (start == kStartZero)
+      launch_pdl(k_relax_zero_t<XT>, ceil_div(n, kThreads), kThreads, 0, s, n, d, f, cur);
     --left;
   } else if (k % 2 == 1) {
     BCMG_CUDA(cudaMemcpyAsync(u_tmp, u, sizeof(XT) * n, cudaMemcpyDeviceToDevice, s));
@@ -301,6 +339,10 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
   }
   for (; left > 0; --left) {
     XT *dst = (cur == u) ? u_tmp : u;
+    if constexpr (std::is_same<XT, float>::value) {
+      if (widen_out && left == 1)  // the last sweep, widened (widen_fusable: sliced)
+        return sliced_relax_sweep_widen(A.sl, d, f, cur, widen_out, s);
+    }
     if (A.has_sl)
       BCMG_TRY(sliced_relax_sweep<XT>(A.sl, d, f, cur, dst, s));
     else
@@ -308,17 +350,22 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
     cur = dst;
   }
   BCMG_LAUNCH_CHECK();
+  if constexpr (std::is_same<XT, float>::value) {
+    if (widen_out) return convert_f2d(n, u, widen_out, s);  // no sweep after the first
+  }
   return BCMG_OK;
 }
 
 template <typename XT>
 bcmg_status relax_residual_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp,
-                             int k, bool zero_start, XT *res, cudaStream_t s) {
+                             int k, int start, XT *res, cudaStream_t s) {
   if (A.n > 0 && A.has_sl && A.sl.cl_size > 0 && k >= 1) {
     BCMG_TRY(check_types<XT>(A));
-    return sliced_cluster<XT>(A.sl, d, f, u, k, zero_start, res, s);
+    if (start == kStartFirstDone)
+      return set_error(BCMG_ERR_INTERNAL, "first sweep fused where it cannot be");
+    return sliced_cluster<XT>(A.sl, d, f, u, k, start != kStartLive, res, s);
   }
-  BCMG_TRY(relax_t<XT>(A, d, f, u, u_tmp, k, zero_start, s));
+  BCMG_TRY(relax_t<XT>(A, d, f, u, u_tmp, k, start, s));
   return residual_t<XT>(A, f, u, res, s);
 }
 
@@ -379,6 +426,25 @@ template <typename XT>
 bcmg_status copy_t(XT *dst, const XT *src, int64_t n, cudaStream_t s) {
   if (n <= 0 || dst == src) return BCMG_OK;
   BCMG_CUDA(cudaMemcpyAsync(dst, src, sizeof(XT) * n, cudaMemcpyDeviceToDevice, s));
+  return BCMG_OK;
+}
+
+template <typename XT>
+bcmg_status restrict_first_sweep_t(int32_t nc, const int32_t *rptr, const int32_t *ridx,
+                                   const XT *p, const XT *x, XT *y, const XT *dc, XT *u1,
+                                   cudaStream_t s) {
+  if (nc <= 0) return BCMG_OK;
+  launch_pdl(k_restrict_first_t<XT>, ceil_div(nc, kThreads), kThreads, 0, s, nc, rptr, ridx,
+             p, x, y, dc, u1);
+  BCMG_LAUNCH_CHECK();
+  return BCMG_OK;
+}
+
+bcmg_status convert_first_sweep(int64_t n, const double *in, const float *d, float *out,
+                                float *u1, cudaStream_t s) {
+  if (n <= 0) return BCMG_OK;
+  launch_pdl(k_convert_first, stream_grid(n), kThreads, 0, s, n, in, d, out, u1);
+  BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
@@ -455,9 +521,12 @@ bcmg_status dot_t(int64_t n, const XT *a, const XT *b, double *out, double *part
 
 #define BCMG_INSTANTIATE(XT)                                                               \
   template bcmg_status relax_t<XT>(const MatView &, const XT *, const XT *, XT *, XT *, int, \
-                                   bool, cudaStream_t);                                    \
+                                   int, cudaStream_t, double *);                           \
   template bcmg_status relax_residual_t<XT>(const MatView &, const XT *, const XT *, XT *,  \
-                                            XT *, int, bool, XT *, cudaStream_t);          \
+                                            XT *, int, int, XT *, cudaStream_t);           \
+  template bcmg_status restrict_first_sweep_t<XT>(int32_t, const int32_t *, const int32_t *, \
+                                                  const XT *, const XT *, XT *, const XT *, \
+                                                  XT *, cudaStream_t);                     \
   template bcmg_status residual_t<XT>(const MatView &, const XT *, const XT *, XT *,       \
                                       cudaStream_t);                                       \
   template bcmg_status restrict_t<XT>(int32_t, const int32_t *, const int32_t *, const XT *, \

@@ -479,6 +479,20 @@ struct EpiRelax {  // out = ((-T + f) / d) + u
   __device__ void finish(int, int) {}
 };
 
+// EpiRelax on FP32 vectors whose result is written widened to FP64 (the last
+// sweep of the mixed cycle, which hands its result to FP64 vectors).
+struct EpiRelaxWiden {  // out = double(((-T + f) / d) + u)
+  static constexpr int NV = 3;
+  __device__ bool active() const { return true; }
+  const float *f, *d, *u;
+  double *out;
+  __device__ const float *row_vec(int i) const { return i == 0 ? f : (i == 1 ? d : u); }
+  __device__ void apply(int32_t r, float T, const float *rv) {
+    out[r] = static_cast<double>(((-T + rv[0]) / rv[1]) + rv[2]);
+  }
+  __device__ void finish(int, int) {}
+};
+
 template <typename XT>
 struct EpiResidual {  // out = f - T
   static constexpr int NV = 1;
@@ -1094,6 +1108,13 @@ bcmg_status relax_as(const SlicedView &S, const XT *d, const XT *f, const XT *u,
   return pipe_launch<VT, XT>(S, u, e, st, warm_only);
 }
 
+template <typename VT>
+bcmg_status relax_widen_as(const SlicedView &S, const float *d, const float *f, const float *u,
+                           double *out, cudaStream_t st, bool warm_only = false) {
+  EpiRelaxWiden e{f, d, u, out};
+  return pipe_launch<VT, float>(S, u, e, st, warm_only);
+}
+
 template <typename VT, typename XT>
 bcmg_status residual_as(const SlicedView &S, const XT *f, const XT *u, XT *res,
                         cudaStream_t st, bool warm_only = false) {
@@ -1119,6 +1140,7 @@ bcmg_status warm_f64_vectors(const SlicedView &S) {
 template <typename VT>
 bcmg_status warm_f32_vectors(const SlicedView &S) {
   BCMG_TRY((relax_as<VT, float>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
+  BCMG_TRY((relax_widen_as<VT>(S, nullptr, nullptr, nullptr, nullptr, 0, true)));
   BCMG_TRY((residual_as<VT, float>(S, nullptr, nullptr, nullptr, 0, true)));
   EpiSpmvT<float> e{nullptr};
   BCMG_TRY((pipe_launch<VT, float>(S, static_cast<const float *>(nullptr), e, 0, true)));
@@ -1149,10 +1171,45 @@ bcmg_status warm_kernels(const SlicedView &S) {
   }
 }
 
+// Small levels: the thread-block cluster that holds the whole copy, if one
+// does (cl_size 0 otherwise).
+bcmg_status plan_cluster(SlicedMat *out, cudaStream_t s) {
+  const int32_t ns = out->nslices;
+  out->cl_size = out->cl_spc = out->cl_slots = 0;
+  if (ns <= kClusterMax * 64) {
+    std::vector<int32_t> h_sptr(static_cast<size_t>(ns) + 1);
+    BCMG_CUDA(cudaMemcpyAsync(h_sptr.data(), out->sptr, sizeof(int32_t) * (ns + 1),
+                              cudaMemcpyDeviceToHost, s));
+    BCMG_CUDA(cudaStreamSynchronize(s));
+    int32_t spc = 1;  // a power of two with at most kClusterMax CTAs
+    while (static_cast<int64_t>(spc) * kClusterMax < ns) spc <<= 1;
+    const int32_t csize = ceil_div(ns, spc);
+    int32_t cap = 0, warp_slots = 0;
+    for (int32_t q = 0; q < csize; ++q) {
+      const int32_t s0 = q * spc, s1 = std::min(s0 + spc, ns);
+      cap = std::max(cap, h_sptr[s1] - h_sptr[s0]);
+      for (int32_t w = 0; w < kClusterWarps; ++w) {
+        int32_t t = 0;
+        for (int32_t i = s0 + w; i < s1; i += kClusterWarps) t += h_sptr[i + 1] - h_sptr[i];
+        warp_slots = std::max(warp_slots, t);
+      }
+    }
+    cap += kSlotPad;
+    const ClusterLayout CL(cap, static_cast<int>(value_bytes(out->vtype)), out->has_columns, spc,
+                           out->xtype == kValF64 ? 8 : 4);
+    if (CL.bytes <= kClusterSmem && warp_slots <= kClusterWarpSlots) {
+      out->cl_size = csize;
+      out->cl_spc = spc;
+      out->cl_slots = cap;
+    }
+  }
+  return BCMG_OK;
+}
+
 }  // namespace
 
 size_t SlicedMat::bytes() const {
-  if (!nslices) return 0;
+  if (!nslices || borrowed) return 0;
   const size_t vb = value_bytes(vtype);
   const size_t sl = (static_cast<size_t>(slots) + kSlotPad) * 32;
   return vb * sl + (has_columns ? 4 * sl : 0) + 4 * (static_cast<size_t>(slots) + kSlotPad) +
@@ -1160,6 +1217,12 @@ size_t SlicedMat::bytes() const {
 }
 
 void SlicedMat::release(cudaStream_t s) {
+  if (borrowed) {  // another copy owns the arrays
+    sptr = scol = soff = nullptr;
+    meta = nullptr;
+    val = nullptr;
+    borrowed = false;
+  }
   dev_free(sptr, s);
   dev_free(meta, s);
   dev_free(scol, s);
@@ -1345,35 +1408,19 @@ bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream
   const int32_t cap_max =
       static_cast<int32_t>((kMaxStageBytes - fixed) / per_slot) - kSlotPad;
   out->cap_slots = std::max<int32_t>(1, std::min<int32_t>(h_stats[0], cap_max));
-  // Small levels: the cluster that holds the whole copy, if one does.
-  out->cl_size = out->cl_spc = out->cl_slots = 0;
-  if (ns <= kClusterMax * 64) {
-    std::vector<int32_t> h_sptr(static_cast<size_t>(ns) + 1);
-    BCMG_CUDA(cudaMemcpyAsync(h_sptr.data(), out->sptr, sizeof(int32_t) * (ns + 1),
-                              cudaMemcpyDeviceToHost, s));
-    BCMG_CUDA(cudaStreamSynchronize(s));
-    int32_t spc = 1;  // a power of two with at most kClusterMax CTAs
-    while (static_cast<int64_t>(spc) * kClusterMax < ns) spc <<= 1;
-    const int32_t csize = ceil_div(ns, spc);
-    int32_t cap = 0, warp_slots = 0;
-    for (int32_t q = 0; q < csize; ++q) {
-      const int32_t s0 = q * spc, s1 = std::min(s0 + spc, ns);
-      cap = std::max(cap, h_sptr[s1] - h_sptr[s0]);
-      for (int32_t w = 0; w < kClusterWarps; ++w) {
-        int32_t t = 0;
-        for (int32_t i = s0 + w; i < s1; i += kClusterWarps) t += h_sptr[i + 1] - h_sptr[i];
-        warp_slots = std::max(warp_slots, t);
-      }
-    }
-    cap += kSlotPad;
-    const ClusterLayout CL(cap, static_cast<int>(vb), out->has_columns, spc,
-                           out->xtype == kValF64 ? 8 : 4);
-    if (CL.bytes <= kClusterSmem && warp_slots <= kClusterWarpSlots) {
-      out->cl_size = csize;
-      out->cl_spc = spc;
-      out->cl_slots = cap;
-    }
-  }
+  BCMG_TRY(plan_cluster(out, s));
+  BCMG_TRY(warm_kernels(out->view()));
+  return BCMG_OK;
+}
+
+bcmg_status sliced_alias(const SlicedMat &src, int xtype, SlicedMat *out, cudaStream_t s) {
+  out->release(s);
+  if (src.borrowed || !src.narrowed || value_bytes(src.vtype) != 2)
+    return set_error(BCMG_ERR_INTERNAL, "sliced copy cannot be shared");
+  *out = src;  // same arrays: sptr, meta (stencil marks included), offsets, values
+  out->borrowed = true;
+  out->xtype = xtype;
+  BCMG_TRY(plan_cluster(out, s));  // the iterate's width enters the layout
   BCMG_TRY(warm_kernels(out->view()));
   return BCMG_OK;
 }
@@ -1400,6 +1447,15 @@ bcmg_status sliced_relax_sweep(const SlicedView &S, const XT *d, const XT *f, co
   if (S.vtype == kValF32) return relax_as<float, float>(S, df, ff, uf, of, s);
   if (S.vtype == kValBF16) return relax_as<__nv_bfloat16, float>(S, df, ff, uf, of, s);
   if (S.vtype == kValF16) return relax_as<__half, float>(S, df, ff, uf, of, s);
+  return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
+}
+
+bcmg_status sliced_relax_sweep_widen(const SlicedView &S, const float *d, const float *f,
+                                     const float *u, double *out, cudaStream_t s) {
+  if (S.xtype != kValF32) return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
+  if (S.vtype == kValF32) return relax_widen_as<float>(S, d, f, u, out, s);
+  if (S.vtype == kValBF16) return relax_widen_as<__nv_bfloat16>(S, d, f, u, out, s);
+  if (S.vtype == kValF16) return relax_widen_as<__half>(S, d, f, u, out, s);
   return set_error(BCMG_ERR_INTERNAL, "sliced type mismatch");
 }
 

@@ -105,6 +105,7 @@ struct SlicedMat {
   unsigned long long wait_ns = kDefaultWaitNs;  // copied into every view
   int32_t cl_size = 0, cl_spc = 0, cl_slots = 0;  // see SlicedView
   int32_t sten_w = 0, sten_off[kStencilMax] = {};  // see SlicedView
+  bool borrowed = false;  // the arrays belong to another copy (sliced_alias)
   void release(cudaStream_t s);
   size_t bytes() const;  // device bytes held
   SlicedView view() const;
@@ -117,12 +118,19 @@ struct SlicedMat {
 // them, so results are bit-identical).
 bcmg_status sliced_build(const CsrView &A, int vtype, SlicedMat *out, cudaStream_t s,
                          bool narrow = false);
+// A copy serving xtype vectors that shares the arrays of src, a copy whose
+// values are stored in 16 bits (narrowed): the same bytes serve FP64 and FP32
+// vectors.  src must outlive it.
+bcmg_status sliced_alias(const SlicedMat &src, int xtype, SlicedMat *out, cudaStream_t s);
 template <typename XT>  // u_out = ((-(A u) + f) ./ d) + u
 bcmg_status sliced_relax_sweep(const SlicedView &S, const XT *d, const XT *f, const XT *u,
                                XT *u_out, cudaStream_t s);
 template <typename XT>  // res = f - A u
 bcmg_status sliced_residual(const SlicedView &S, const XT *f, const XT *u, XT *res,
                             cudaStream_t s);
+// sliced_relax_sweep on FP32 vectors with the result widened into FP64 out.
+bcmg_status sliced_relax_sweep_widen(const SlicedView &S, const float *d, const float *f,
+                                     const float *u, double *out, cudaStream_t s);
 // y = A x on a sliced FP64 copy.
 bcmg_status sliced_spmv(const SlicedView &S, const double *x, double *y, cudaStream_t s);
 template <typename XT>  // y = A x on the copy serving XT vectors
@@ -157,21 +165,49 @@ struct MatView {
   SlicedView sl;
 };
 
+// How a relaxation starts: from the iterate in u, from u = 0 (the first
+// sweep is f ./ d), or with that first sweep already written by the caller
+// into first_sweep_dst(u, u_tmp, k) (fused into the kernel that made f).
+enum RelaxStart { kStartLive = 0, kStartZero = 1, kStartFirstDone = 2 };
+template <typename XT>
+inline XT *first_sweep_dst(XT *u, XT *u_tmp, int k) {
+  return (k % 2 == 1) ? u : u_tmp;
+}
+// Whether a relaxation of k sweeps on A can take kStartFirstDone (levels run
+// by one thread-block cluster compute f ./ d themselves).
+inline bool first_sweep_fusable(const MatView &A, int k) {
+  return k >= 1 && !(A.has_sl && A.sl.cl_size > 0);
+}
+
 // k sweeps of u <- ((-(A u) + f) ./ d) + u, result in u; u_tmp is the
-// ping-pong buffer.  zero_start: u is taken as 0 (first sweep is f ./ d).
-// XT = double needs FP64 values; XT = float takes FP32 / BF16 / FP16 values.
+// ping-pong buffer; start: a RelaxStart.  XT = double needs FP64 values;
+// XT = float takes FP32 / BF16 / FP16 values.  widen_out (XT = float, sliced
+// copies without a cluster plan): the last sweep writes its result widened
+// into widen_out instead of u.
 template <typename XT>
 bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp, int k,
-                    bool zero_start, cudaStream_t s);
+                    int start, cudaStream_t s, double *widen_out = nullptr);
+// Whether relax_t can take widen_out for A and k.
+inline bool widen_fusable(const MatView &A, int k) {
+  return k >= 1 && A.has_sl && A.sl.cl_size == 0 && A.sl.xtype == kValF32;
+}
 template <typename XT>  // res = f - A u
 bcmg_status residual_t(const MatView &A, const XT *f, const XT *u, XT *res, cudaStream_t s);
 // relax_t and then res = f - A u, in one launch on a level with a cluster plan.
 template <typename XT>
 bcmg_status relax_residual_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp,
-                             int k, bool zero_start, XT *res, cudaStream_t s);
+                             int k, int start, XT *res, cudaStream_t s);
 template <typename XT>  // y[I] = sum_{i in I} p_i x_i
 bcmg_status restrict_t(int32_t nc, const int32_t *rptr, const int32_t *ridx, const XT *p,
                        const XT *x, XT *y, cudaStream_t s);
+// restrict_t and the first sweep from zero of the coarse level: u1 = y ./ dc.
+template <typename XT>
+bcmg_status restrict_first_sweep_t(int32_t nc, const int32_t *rptr, const int32_t *ridx,
+                                   const XT *p, const XT *x, XT *y, const XT *dc, XT *u1,
+                                   cudaStream_t s);
+// out = float(in) and the first sweep from zero u1 = out ./ d.
+bcmg_status convert_first_sweep(int64_t n, const double *in, const float *d, float *out,
+                                float *u1, cudaStream_t s);
 template <typename XT>  // xf[i] += p_i xc[agg_i]
 bcmg_status prolong_t(int32_t n, const int32_t *agg, const XT *p, const XT *xc, XT *xf,
                       cudaStream_t s);
