@@ -531,7 +531,10 @@ def run_ours(args):
     csr_equiv = 12 * A.nnz + 4 * (A.n + 1) + 36 * A.n
     achieved = sweep_bytes / sweep_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = committed_traffic("k_sl_pipe", f"{args.workload}:{args.precision}")
+    # keyed by the copy's value width: a capture of another storage format
+    # (FP32 values, BF16 values) does not describe this launch
+    traffic = committed_traffic("k_sl_pipe",
+                                f"{args.workload}:{args.precision}:{vbytes.value}B")
 
     cpu, err = None, {}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
