@@ -1224,7 +1224,10 @@ bcmg_status capture_while_loop(cudaStream_t stream,
 // Binary, little-endian: the magic "BCMGHRC1", the 14 settings, the input
 // matrix, then per hierarchy its level data (CSR of levels >= 1, D, M, w, and
 // for every level but the last the aggregates and prolongator values; R's
-// member lists are rebuilt from the aggregates on load).  Each array is an
+// member lists are rebuilt from the aggregates on load).  With smoothed
+// aggregation (aggrtype 1) every level but the last also holds its smoothed
+// prolongator P (nnz, then CSR row pointers, columns, values); R = P^T is
+// rebuilt on load by the transpose setup uses, so it is the same bits.  Each array is an
 // int64 count followed by its raw elements, in the manner of the reference's
 // Vector::dump / Vector::load (src/matrix/vector.cu:468-505).
 constexpr char kHrcMagic[8] = {'B', 'C', 'M', 'G', 'H', 'R', 'C', '1'};
@@ -1303,6 +1306,13 @@ bcmg_status save_hierarchies(const bcmg_handle *h, FILE *f) {
       if (lv.nc > 0) {
         BCMG_TRY(put_array(f, lv.agg, lv.n, s));
         BCMG_TRY(put_array(f, lv.p, lv.n, s));
+        if (h->prm.aggrtype == 1) {
+          if (!lv.Prow) return set_error(BCMG_ERR_INTERNAL, "level %d has no smoothed P", l);
+          BCMG_TRY(put_scalars(f, &lv.Pnnz, sizeof(lv.Pnnz)));
+          BCMG_TRY(put_array(f, lv.Prow, static_cast<int64_t>(lv.n) + 1, s));
+          BCMG_TRY(put_array(f, lv.Pcol, lv.Pnnz, s));
+          BCMG_TRY(put_array(f, lv.Pval, lv.Pnnz, s));
+        }
       }
     }
   }
@@ -1376,6 +1386,22 @@ bcmg_status load_hierarchies(bcmg_handle *h, FILE *f) {
         BCMG_TRY(dev_alloc(&lv.rptr, lv.nc + 1, s));
         BCMG_TRY(dev_alloc(&lv.ridx, lv.n, s));
         BCMG_TRY(transpose_agg(lv.n, lv.agg, lv.nc, lv.rptr, lv.ridx, s));
+        if (h->prm.aggrtype == 1) {
+          int32_t pnnz = -1;
+          BCMG_TRY(get_scalars(f, &pnnz, sizeof(pnnz)));
+          if (pnnz < 0 || static_cast<int64_t>(pnnz) > static_cast<int64_t>(lv.n) * lv.nc)
+            return set_error(BCMG_ERR_IO, "hierarchy file: P of level %d has %d entries", l,
+                             pnnz);
+          lv.Pnnz = pnnz;
+          BCMG_TRY(get_array(f, &lv.Prow, static_cast<int64_t>(lv.n) + 1, s));
+          BCMG_TRY(get_array(f, &lv.Pcol, pnnz, s));
+          BCMG_TRY(get_array(f, &lv.Pval, pnnz, s));
+          BCMG_TRY(csr_validate_rect(lv.pview(), lv.nc, s));
+          BCMG_TRY(dev_alloc(&lv.Rrow, static_cast<int64_t>(lv.nc) + 1, s));
+          BCMG_TRY(dev_alloc(&lv.Rcol, pnnz, s));
+          BCMG_TRY(dev_alloc(&lv.Rval, pnnz, s));
+          BCMG_TRY(csr_transpose(lv.pview(), lv.nc, lv.Rrow, lv.Rcol, lv.Rval, s));
+        }
       }
     }
     BCMG_TRY(size_buffers_t<double>(h, h->c64));
@@ -1557,8 +1583,6 @@ bcmg_status bcmg_get_params(const bcmg_handle *h, bcmg_params *p) {
 bcmg_status bcmg_save(const bcmg_handle *h, const char *path) {
   clear_error();
   if (!h || !path) return set_error(BCMG_ERR_PARAM, "null argument");
-  if (h->prm.aggrtype == 1)
-    return set_error(BCMG_ERR_UNSUPPORTED, "hierarchy files hold unsmoothed aggregation only");
   BCMG_CUDA(cudaSetDevice(h->device));
   File f(fopen(path, "wb"));
   if (!f) return set_error(BCMG_ERR_IO, "cannot open %s for writing", path);
@@ -1580,7 +1604,7 @@ bcmg_status bcmg_load(const char *path, const bcmg_ext *ext, bcmg_handle **out) 
     return set_error(BCMG_ERR_IO, "%s is not a hierarchy file", path);
   if (fread(&prm, sizeof(prm), 1, f.get()) != 1)
     return set_error(BCMG_ERR_IO, "hierarchy file truncated");
-  if (prm.aggrtype != 0)
+  if (prm.aggrtype != 0 && prm.aggrtype != 1)
     return set_error(BCMG_ERR_IO, "%s: hierarchy file with aggrtype %d", path, prm.aggrtype);
   const auto t0 = Clock::now();
   bcmg_handle *h = nullptr;

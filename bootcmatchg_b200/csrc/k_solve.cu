@@ -247,9 +247,10 @@ inline int grid_for(int64_t work) {
 // Structural check of a device CSR matrix, one thread per row: row bounds,
 // columns in range and strictly increasing, finite values, a diagonal entry.
 // The smallest offending row wins: err = (row << 8) | code.
-__global__ void k_csr_validate(int32_t n, int32_t nnz, const int32_t *__restrict__ row,
+__global__ void k_csr_validate(int32_t n, int32_t m, int32_t nnz,
+                               const int32_t *__restrict__ row,
                                const int32_t *__restrict__ col,
-                               const double *__restrict__ val,
+                               const double *__restrict__ val, int need_diag,
                                unsigned long long *err) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -262,13 +263,13 @@ __global__ void k_csr_validate(int32_t n, int32_t nnz, const int32_t *__restrict
     int32_t prev = -1;
     for (int32_t j = b; j < e && !code; ++j) {
       const int32_t c = col[j];
-      if (c < 0 || c >= n) code = kCsrBadColumn;
+      if (c < 0 || c >= m) code = kCsrBadColumn;
       else if (c <= prev) code = kCsrUnsorted;
       else if (!isfinite(val[j])) code = kCsrNonFinite;
       diag = diag || c == i;
       prev = c;
     }
-    if (!code && !diag) code = kCsrNoDiagonal;
+    if (!code && need_diag && !diag) code = kCsrNoDiagonal;
   }
   if (code) atomicMin(err, (static_cast<unsigned long long>(i) << 8) | code);
 }
@@ -359,13 +360,14 @@ bcmg_status fcg_replace(const CsrView &A, const SlicedView *S, const double *b, 
   return BCMG_OK;
 }
 
-bcmg_status csr_validate(const CsrView &A, cudaStream_t s) {
-  if (A.n <= 0) return set_error(BCMG_ERR_INVALID_MATRIX, "matrix must have n > 0");
+namespace {
+bcmg_status csr_check(const CsrView &A, int32_t m, bool need_diag, cudaStream_t s) {
+  if (A.n <= 0 || m <= 0) return set_error(BCMG_ERR_INVALID_MATRIX, "matrix must have n > 0");
   DevBuf<unsigned long long> err;
   BCMG_TRY(err.alloc(1, s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0xff, sizeof(unsigned long long), s));
-  launch(k_csr_validate, ceil_div(A.n, kThreads), kThreads, 0, s, A.n, A.nnz, A.row, A.col,
-         A.val, err.get());
+  launch(k_csr_validate, ceil_div(A.n, kThreads), kThreads, 0, s, A.n, m, A.nnz, A.row, A.col,
+         A.val, need_diag ? 1 : 0, err.get());
   BCMG_LAUNCH_CHECK();
   unsigned long long h = 0;
   BCMG_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -386,6 +388,15 @@ bcmg_status csr_validate(const CsrView &A, cudaStream_t s) {
       return set_error(BCMG_ERR_INVALID_MATRIX,
                        "row %lld has no diagonal entry (the AH builder needs one)", r);
   }
+}
+}  // namespace
+
+bcmg_status csr_validate(const CsrView &A, cudaStream_t s) {
+  return csr_check(A, A.n, true, s);
+}
+
+bcmg_status csr_validate_rect(const CsrView &A, int32_t m, cudaStream_t s) {
+  return csr_check(A, m, false, s);
 }
 
 }  // namespace bcmg

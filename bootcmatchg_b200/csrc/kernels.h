@@ -265,6 +265,9 @@ inline bcmg_status scale(int64_t n, double a, double *x, cudaStream_t s) {
 // and returns BCMG_ERR_INVALID_MATRIX naming the first offending row.
 enum CsrFault { kCsrBadRow = 1, kCsrBadColumn, kCsrUnsorted, kCsrNonFinite, kCsrNoDiagonal };
 bcmg_status csr_validate(const CsrView &A, cudaStream_t s);
+// The same checks for an n x m matrix with no diagonal required (a
+// prolongator read from a hierarchy file).
+bcmg_status csr_validate_rect(const CsrView &A, int32_t m, cudaStream_t s);
 
 // y = alpha A x + beta y (FP64)
 bcmg_status spmv(const CsrView &A, double alpha, const double *x, double beta,

@@ -65,9 +65,9 @@ typedef struct bcmg_params {
   double conv_ratio;         /* rho: desired composite convergence rate       */
   int    matchtype;          /* always 3 (AMG.cu:497)                         */
   int    aggrsweeps;         /* pairwise aggregation sweeps per level         */
-  int    aggrtype;           /* 0 unsmoothed (1 smoothed: unsupported)        */
+  int    aggrtype;           /* 0 unsmoothed, 1 smoothed (P = S P_tent)       */
   int    max_levels;         /* max levels per hierarchy                      */
-  int    cycle_type;         /* 0 V, 1 H, 2 W                                 */
+  int    cycle_type;         /* 0 V, 1 H, 2 W, 3 K-cycle                      */
   int    coarse_solver;      /* 0 Jacobi, 4 l1-Jacobi                         */
   int    relax_type;         /* 0 Jacobi, 4 l1-Jacobi                         */
   int    prerelax_sweeps;
@@ -247,7 +247,8 @@ bcmg_status bcmg_destroy(bcmg_handle *h);
 
 /* ---- hierarchy files -------------------------------------------------------
  * Save a set-up handle's hierarchies (settings, input matrix, every level's
- * CSR, D, M, w, aggregates and prolongator values) to a binary file, and
+ * CSR, D, M, w, aggregates and prolongator values, and with smoothed
+ * aggregation every level's smoothed prolongator P) to a binary file, and
  * build a handle from such a file without running setup again.  The
  * reference only dumps single vectors (Vector::dump / Vector::load,
  * src/matrix/vector.cu:468-505) and rebuilds every hierarchy per solve();
