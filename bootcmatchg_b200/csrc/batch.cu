@@ -57,6 +57,9 @@ struct BtLv<double> {
   static const double *D(const DevLevel &l) { return l.D; }
   static const double *M(const DevLevel &l) { return l.M; }
   static const double *p(const DevLevel &l) { return l.p; }
+  // smoothed aggregation: P and R = P^T as CSR
+  static MatView P(const DevLevel &l) { return mat_f64(l.pview()); }
+  static MatView R(const DevLevel &l) { return mat_f64(l.rview()); }
 };
 template <>
 struct BtLv<float> {
@@ -73,6 +76,8 @@ struct BtLv<float> {
   static const float *D(const DevLevel &l) { return l.D32; }
   static const float *M(const DevLevel &l) { return l.M32; }
   static const float *p(const DevLevel &l) { return l.p32; }
+  static MatView P(const DevLevel &l) { return mat_f32(l.pview(), l.Pval32); }
+  static MatView R(const DevLevel &l) { return mat_f32(l.rview(), l.Rval32); }
 };
 
 template <typename XT>
@@ -308,14 +313,22 @@ bcmg_status bt_cycle(bcmg_handle *h, BatchState &S, CycleBufs<XT> &B, int k, int
                         zero[l - 1] != 0, s));
   zero[l - 1] = 0;
   BCMG_TRY(bt_residual<XT>(A, W, cfg, B.rhs[l - 1], B.x[l - 1], B.res[l - 1], s));
-  BCMG_TRY(bt_restrict<XT>(lv.nc, lv.rptr, lv.ridx, BtLv<XT>::p(lv), B.res[l - 1], B.rhs[l], W,
-                           s));
+  if (lv.Prow)  // smoothed aggregation: rhs_c = R res
+    BCMG_TRY(bt_spmm<XT>(BtLv<XT>::R(lv), W, cfg, B.res[l - 1], B.rhs[l], s));
+  else
+    BCMG_TRY(bt_restrict<XT>(lv.nc, lv.rptr, lv.ridx, BtLv<XT>::p(lv), B.res[l - 1], B.rhs[l],
+                             W, s));
   zero[l] = 1;
   for (int i = 1; i <= h->grid_sweeps[l - 1]; ++i) {
     BCMG_TRY(bt_cycle<XT>(h, S, B, k, l + 1, zero));
     if (l == L - 1) break;
   }
-  BCMG_TRY(bt_prolong<XT>(lv.n, lv.agg, BtLv<XT>::p(lv), B.x[l], B.x[l - 1], W, s));
+  if (lv.Prow) {  // x += P x_c
+    BCMG_TRY(bt_spmm<XT>(BtLv<XT>::P(lv), W, cfg, B.x[l], B.xt[l - 1], s));
+    BCMG_TRY(axpy_t<XT>(static_cast<int64_t>(lv.n) * W, XT(1), B.xt[l - 1], B.x[l - 1], s));
+  } else {
+    BCMG_TRY(bt_prolong<XT>(lv.n, lv.agg, BtLv<XT>::p(lv), B.x[l], B.x[l - 1], W, s));
+  }
   BCMG_TRY(bt_relax<XT>(A, W, cfg, d, B.rhs[l - 1], B.x[l - 1], B.xt[l - 1],
                         p.postrelax_sweeps, false, s));
   return BCMG_OK;
@@ -503,9 +516,8 @@ bcmg_status bcmg_solve_batch(bcmg_handle *h, int32_t nrhs, const double *B, int6
                              double *X, int64_t ldx, int on_device, bcmg_solve_info *infos) {
   clear_error();
   if (!h || !B || !X || nrhs <= 0) return set_error(BCMG_ERR_PARAM, "bad arguments");
-  if (h->prm.cycle_type == 3 || h->prm.aggrtype == 1)
-    return set_error(BCMG_ERR_UNSUPPORTED,
-                     "batched solves run neither the K-cycle nor smoothed aggregation");
+  if (h->prm.cycle_type == 3)
+    return set_error(BCMG_ERR_UNSUPPORTED, "batched solves do not run the K-cycle");
   const int32_t n = h->A0.n;
   if (ldb < n || ldx < n)
     return set_error(BCMG_ERR_PARAM, "leading dimensions must be >= n (%d)", n);
@@ -568,9 +580,8 @@ bcmg_status bcmg_precond_apply_batch(bcmg_handle *h, int32_t nrhs, const double 
                                      int64_t ldr, double *d_Z, int64_t ldz) {
   clear_error();
   if (!h || !d_R || !d_Z || nrhs <= 0) return set_error(BCMG_ERR_PARAM, "bad arguments");
-  if (h->prm.cycle_type == 3 || h->prm.aggrtype == 1)
-    return set_error(BCMG_ERR_UNSUPPORTED,
-                     "batched solves run neither the K-cycle nor smoothed aggregation");
+  if (h->prm.cycle_type == 3)
+    return set_error(BCMG_ERR_UNSUPPORTED, "batched solves do not run the K-cycle");
   const int32_t n = h->A0.n;
   if (ldr < n || ldz < n)
     return set_error(BCMG_ERR_PARAM, "leading dimensions must be >= n (%d)", n);

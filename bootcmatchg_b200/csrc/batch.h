@@ -37,6 +37,8 @@ bcmg_status bt_relax(const MatView &A, int W, BtCfg cfg, const XT *d, const XT *
 template <typename XT>  // res = f - A u on W columns
 bcmg_status bt_residual(const MatView &A, int W, BtCfg cfg, const XT *f, const XT *u, XT *res,
                         cudaStream_t s);
+template <typename XT>  // y = A x on W columns (A: n rows; x indexed by A's columns)
+bcmg_status bt_spmm(const MatView &A, int W, BtCfg cfg, const XT *x, XT *y, cudaStream_t s);
 template <typename XT>  // y[I, :] = sum_{i in I} p_i x[i, :]
 bcmg_status bt_restrict(int32_t nc, const int32_t *rptr, const int32_t *ridx, const XT *p,
                         const XT *x, XT *y, int W, cudaStream_t s);

@@ -102,9 +102,10 @@ __device__ __forceinline__ void bt_row_sum(const int32_t *__restrict__ col,
   }
 }
 
-enum { kModeRelax = 0, kModeResid = 1 };
+enum { kModeRelax = 0, kModeResid = 1, kModeSpmv = 2 };
 
-// kModeRelax: out = ((-(A u) + f) ./ d) + u;  kModeResid: out = f - A u.
+// kModeRelax: out = ((-(A u) + f) ./ d) + u;  kModeResid: out = f - A u;
+// kModeSpmv: out = A u (A may be rectangular: n rows, columns indexing u).
 template <int V, int MODE, typename VT, typename XT>
 __global__ void __launch_bounds__(256)
     k_bt_rowop(int32_t n, int W, int lgL, const int32_t *__restrict__ row,
@@ -125,7 +126,8 @@ __global__ void __launch_bounds__(256)
   }
   // The row's own f, u and d do not depend on the row sum: load them first.
   const int64_t o = static_cast<int64_t>(i) * W + static_cast<int64_t>(g) * V;
-  const Cols<XT, V> fv = ldc<XT, V>(f + o);
+  Cols<XT, V> fv;
+  if (MODE != kModeSpmv) fv = ldc<XT, V>(f + o);
   Cols<XT, V> uv;
   XT di = XT(1);
   if (MODE == kModeRelax) {
@@ -147,9 +149,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int v = 0; v < V; ++v) res.v[v] = ((-acc[v] + fv.v[v]) / di) + uv.v[v];
     }
-  } else {
+  } else if (MODE == kModeResid) {
 #pragma unroll
     for (int v = 0; v < V; ++v) res.v[v] = fv.v[v] - acc[v];
+  } else {
+#pragma unroll
+    for (int v = 0; v < V; ++v) res.v[v] = acc[v];
   }
   stc<XT, V>(out + o, res);
 }
@@ -661,6 +666,12 @@ bcmg_status bt_residual(const MatView &A, int W, BtCfg cfg, const XT *f, const X
 }
 
 template <typename XT>
+bcmg_status bt_spmm(const MatView &A, int W, BtCfg cfg, const XT *x, XT *y, cudaStream_t s) {
+  if (A.n <= 0) return BCMG_OK;
+  return launch_rowop<kModeSpmv, XT>(A, W, cfg, nullptr, nullptr, x, y, s);
+}
+
+template <typename XT>
 bcmg_status bt_restrict(int32_t nc, const int32_t *rptr, const int32_t *ridx, const XT *p,
                         const XT *x, XT *y, int W, cudaStream_t s) {
   if (nc <= 0) return BCMG_OK;
@@ -796,6 +807,7 @@ bcmg_status bt_col_norms(int32_t n, int W, const double *a, double *partials, do
                                     XT *, int, bool, cudaStream_t);                            \
   template bcmg_status bt_residual<XT>(const MatView &, int, BtCfg, const XT *, const XT *,    \
                                        XT *, cudaStream_t);                                    \
+  template bcmg_status bt_spmm<XT>(const MatView &, int, BtCfg, const XT *, XT *, cudaStream_t); \
   template bcmg_status bt_restrict<XT>(int32_t, const int32_t *, const int32_t *, const XT *,  \
                                        const XT *, XT *, int, cudaStream_t);                   \
   template bcmg_status bt_prolong<XT>(int32_t, const int32_t *, const XT *, const XT *, XT *,  \
