@@ -1032,6 +1032,9 @@ def run_case(args):
     solve_mixed  one complete mixed-precision solve of 27-point Poisson
                  GRID^3 (--grid, default 128), FCG loop driven from the host
                  (every kernel is a plain launch a profiler can see)
+    solve_rgg    one complete solve of the 2,000,000-node random geometric
+                 graph Laplacian (the rgg_2m workload) in --precision, FCG
+                 loop driven from the host
     batch_solve  one 32-column batched solve of 7-point Poisson 96^3 (mixed),
                  FCG loop driven from the host
     setup        one FP64 setup of 27-point Poisson GRID^3 (--grid, default
@@ -1078,6 +1081,15 @@ def run_case(args):
             x, info = h.solve(b)
         print(f"iters {info.iters} converged {info.converged} setup {info.setup_ms:.1f} ms "
               f"solve {info.solve_ms:.1f} ms")
+    elif case == "solve_rgg":
+        A = wl.rgg(2_000_000, seed=4)
+        b = wl.vector(1, 1, A.n)
+        prec = bc.PREC_MIXED if args.precision == "mixed" else bc.PREC_FP64
+        ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0, use_graphs=0)
+        with bc.Handle(A, p, ext) as h:
+            x, info = h.solve(b)
+        print(f"{args.precision}: iters {info.iters} converged {info.converged} "
+              f"setup {info.setup_ms:.1f} ms solve {info.solve_ms:.1f} ms")
     elif case == "batch_solve":
         A = wl.poisson(7, 96, 96, 96)
         B = np.asfortranarray(wl.vector(1, 3, A.n * 32).reshape(A.n, 32, order="F"))
@@ -1111,7 +1123,7 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", choices=["sweep_fp32", "sweep_fp64", "sweep_fv2d", "batch_fp32",
-                                       "solve_mixed", "batch_solve", "setup"],
+                                       "solve_mixed", "solve_rgg", "batch_solve", "setup"],
                     help="run one small profiling case instead of the benchmark")
     ap.add_argument("--sweeps", type=int, default=3, help="--case: sweeps per launch")
     ap.add_argument("--grid", type=int, default=None, help="--case setup/solve_mixed: side")
