@@ -85,6 +85,24 @@ namespace {
 constexpr int kFtcoarseInc = 100;     // FTCOARSE_INC, matchingAggregation.cu:12
 constexpr double kCoarseRatio = 1.2;  // COARSERATIO_THRSLD, matchingAggregation.cu:13
 constexpr int kBootSolverIt = 15;     // solver_it, AMG.cu:407
+// Relative reduction at which the K-cycle stops after its first inner step
+// (RTOL, src/SOLVER/GAMG_cycle.cu:5).
+constexpr double kKcycleRtol = 0.25;
+// Device scalars of one level's K-cycle inner steps (CycleBufs::kscal).
+constexpr int kKcStride = 16;
+enum KcScal {
+  kKcWW = 0,    // ||w||^2 before the first step (delta0 = its root)
+  kKcDelta,     // w . d0
+  kKcTau,       // d0 . v
+  kKcWW2,       // ||w||^2 after the first step
+  kKcTau1,      // d1 . v
+  kKcTau2,      // d1 . v1
+  kKcTau3,      // d1 . w
+  kKcA0,        // coefficient of d0 in the correction
+  kKcA1,        // coefficient of d1
+  kKcNegAlpha,  // -alpha, for w -= alpha v
+  kKcSecond     // 1: the second inner step ran
+};
 
 using Clock = std::chrono::steady_clock;
 double ms_since(Clock::time_point t0) {
@@ -442,6 +460,11 @@ bcmg_status size_buffers_t(bcmg_handle *h, CycleBufs<XT> &B) {
       B.kn[l] = B.n[l];
     }
     if (!B.kdots) BCMG_TRY(dev_alloc(&B.kdots, 1, s));
+    if (B.kscal_levels < L) {
+      dev_free(B.kscal, s);
+      BCMG_TRY(dev_alloc(&B.kscal, static_cast<int64_t>(L) * kKcStride, s));
+      B.kscal_levels = L;
+    }
   }
   const int32_t n = h->A0.n;
   if (!B.xk) {
@@ -470,6 +493,8 @@ void free_buffers_t(CycleBufs<XT> &B, cudaStream_t s) {
   for (auto *v : {&B.kw, &B.kd0, &B.kd1, &B.kv, &B.kv1, &B.kx})
     for (auto &p : *v) dev_free(p, s);
   dev_free(B.kdots, s);
+  dev_free(B.kscal, s);
+  B.kscal_levels = 0;
 }
 
 // The level data a cycle of vector type XT reads.
@@ -610,18 +635,175 @@ bcmg_status cycle_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int l, std::vector<
   return BCMG_OK;
 }
 
-// Relative reduction at which the K-cycle stops after its first inner step
-// (RTOL, src/SOLVER/GAMG_cycle.cu:5).
-constexpr double kKcycleRtol = 0.25;
+// The K-cycle's inner steps with their scalars on the device, for the
+// captured FCG loop: the same operations in the same order as the host-driven
+// kcycle_inner_t below (so the same bits), the branch on ||w|| an IF node of
+// the graph.  A non-positive curvature sets the FCG loop's indefinite flag,
+// which ends the loop; the correction is then zero.
+__global__ void k_kc_first(double *ks, double *scal) {
+  const double delta_old = ks[kKcDelta], tau = ks[kKcTau];
+  double alpha = 0.0;
+  if (!(delta_old > 0.0) || !(tau > 0.0))
+    scal[kIndef] = 1.0;
+  else
+    alpha = delta_old / tau;
+  ks[kKcA0] = alpha;
+  ks[kKcNegAlpha] = -alpha;
+  ks[kKcA1] = 0.0;
+}
+
+__global__ void k_kc_branch(double *ks, cudaGraphConditionalHandle cond) {
+  const double delta0 = sqrt(ks[kKcWW]), l2 = sqrt(ks[kKcWW2]);
+  const bool second = !(l2 <= kKcycleRtol * delta0);
+  ks[kKcSecond] = second ? 1.0 : 0.0;
+  cudaGraphSetConditional(cond, second ? 1u : 0u);
+}
+
+__global__ void k_kc_second(double *ks) {
+  const double tau = ks[kKcTau], tau1 = ks[kKcTau1], tau2 = ks[kKcTau2], tau3 = ks[kKcTau3];
+  const double tau4 = tau2 - (tau1 * tau1) / tau;
+  ks[kKcA0] = ks[kKcA0] - (tau1 * tau3) / (tau * tau4);
+  ks[kKcA1] = tau3 / tau4;
+}
+
+// y += coef x with the coefficient read on the device (axpy_t's arithmetic).
+template <typename XT>
+__global__ void k_kc_axpy(int64_t n, const double *coef, const XT *__restrict__ x,
+                          XT *__restrict__ y) {
+  const XT a = static_cast<XT>(*coef);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = fma(a, x[i], y[i]);
+}
+
+// xk = a0 d0 (+ a1 d1 after a second step): the host path's zero fill and
+// one or two axpys, element by element in the same order.
+template <typename XT>
+__global__ void k_kc_combine(int64_t n, const double *ks, const XT *__restrict__ d0,
+                             const XT *__restrict__ d1, XT *__restrict__ xk) {
+  const XT a0 = static_cast<XT>(ks[kKcA0]), a1 = static_cast<XT>(ks[kKcA1]);
+  const bool second = ks[kKcSecond] != 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    XT v = fma(a0, d0[i], XT(0));
+    if (second) v = fma(a1, d1[i], v);
+    xk[i] = v;
+  }
+}
+
+inline int kc_grid(int64_t n) {
+  const int64_t b = (n + 255) / 256;
+  return static_cast<int>(b < 1 ? 1 : (b > 4 * kNumSM ? 4 * kNumSM : b));
+}
+
+// Adds an IF node at the current point of the capture on h->stream, whose
+// condition k_kc_branch sets from ks, and captures body() into it on the
+// level's own stream (h->stream points there meanwhile).
+bcmg_status capture_kc_if(bcmg_handle *h, int c, double *ks,
+                          const std::function<bcmg_status()> &body) {
+  cudaStream_t s = h->stream;
+  if (c < 0 || c >= static_cast<int>(h->kc_streams.size()))
+    return set_error(BCMG_ERR_INTERNAL, "no capture stream for K-cycle level %d", c);
+  cudaStream_t s2 = h->kc_streams[c];
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  BCMG_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive || !g)
+    return set_error(BCMG_ERR_INTERNAL, "K-cycle IF node outside a capture");
+  cudaGraphConditionalHandle cond;
+  BCMG_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 0, 0));
+  launch(k_kc_branch, 1, 1, 0, s, ks, cond);
+  BCMG_LAUNCH_CHECK();
+  BCMG_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  alignas(cudaGraphNodeParams) unsigned char np_storage[sizeof(cudaGraphNodeParams)];
+  std::memset(np_storage, 0, sizeof(np_storage));
+  cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_storage);
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = cond;
+  np.conditional.type = cudaGraphCondTypeIf;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  BCMG_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+  cudaGraph_t bg = np.conditional.phGraph_out[0];
+  BCMG_CUDA(cudaStreamBeginCaptureToGraph(s2, bg, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+  h->stream = s2;
+  const bcmg_status st = body();
+  h->stream = s;
+  const cudaError_t e = cudaStreamEndCapture(s2, &bg);
+  BCMG_TRY(st);
+  if (e != cudaSuccess)
+    return set_error(BCMG_ERR_CUDA, "K-cycle IF body capture: %s", cudaGetErrorString(e));
+  BCMG_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return BCMG_OK;
+}
+
+template <typename XT>
+bcmg_status kcycle_inner_graph(bcmg_handle *h, CycleBufs<XT> &B, int k, int c) {
+  const DevLevel &lv = h->H[k].lv[c];
+  const MatView A = Lv<XT>::mat(lv);
+  const int32_t n = lv.n;
+  XT *w = B.kw[c], *d0 = B.kd0[c], *d1 = B.kd1[c], *v = B.kv[c], *v1 = B.kv1[c];
+  XT *xk = B.kx[c];
+  if (!w || !B.kscal || static_cast<size_t>(c) >= B.kscal_levels)
+    return set_error(BCMG_ERR_INTERNAL, "K-cycle buffers missing");
+  double *ks = B.kscal + static_cast<size_t>(c) * kKcStride;
+  // h->stream is read at every call: inside the IF body it is the body's
+  // capture stream.
+  auto dot = [&](const XT *a, const XT *b, int slot) -> bcmg_status {
+    return dot_t<XT>(n, a, b, ks + slot, h->partials, h->stream);
+  };
+  auto precond_k = [&](const XT *r, XT *d) -> bcmg_status {
+    BCMG_TRY(copy_t<XT>(B.rhs[c], r, n, h->stream));
+    std::vector<char> zero(B.rhs.size(), 0);
+    zero[c] = 1;
+    BCMG_TRY(cycle_t<XT>(h, B, k, c + 1, zero));
+    return copy_t<XT>(d, B.x[c], n, h->stream);
+  };
+  BCMG_TRY(copy_t<XT>(w, B.rhs[c], n, h->stream));
+  BCMG_TRY(dot(w, w, kKcWW));
+  BCMG_TRY(precond_k(w, d0));
+  BCMG_TRY(dot(w, d0, kKcDelta));
+  BCMG_TRY(spmv_t<XT>(A, d0, v, h->stream));
+  BCMG_TRY(dot(d0, v, kKcTau));
+  launch(k_kc_first, 1, 1, 0, h->stream, ks, h->scal);
+  launch(k_kc_axpy<XT>, kc_grid(n), 256, 0, h->stream, static_cast<int64_t>(n),
+         static_cast<const double *>(ks + kKcNegAlpha), static_cast<const XT *>(v), w);
+  BCMG_LAUNCH_CHECK();
+  BCMG_TRY(dot(w, w, kKcWW2));
+  BCMG_TRY(capture_kc_if(h, c, ks, [&]() -> bcmg_status {
+    BCMG_TRY(precond_k(w, d1));
+    BCMG_TRY(spmv_t<XT>(A, d1, v1, h->stream));
+    BCMG_TRY(dot(d1, v, kKcTau1));
+    BCMG_TRY(dot(d1, v1, kKcTau2));
+    BCMG_TRY(dot(d1, w, kKcTau3));
+    launch(k_kc_second, 1, 1, 0, h->stream, ks);
+    BCMG_LAUNCH_CHECK();
+    return BCMG_OK;
+  }));
+  launch(k_kc_combine<XT>, kc_grid(n), 256, 0, h->stream, static_cast<int64_t>(n),
+         static_cast<const double *>(ks), static_cast<const XT *>(d0),
+         static_cast<const XT *>(d1), xk);
+  BCMG_LAUNCH_CHECK();
+  return copy_t<XT>(B.x[c], xk, n, h->stream);
+}
 
 // inneritkcycle (src/SOLVER/FCG.cu:633-723): two flexible-CG steps on coarse
 // level c (0-based) preconditioned by the cycle from that level on fresh
 // zero iterates (preconditionApplyK, FCG.cu:590-628); the correction lands
-// in x[c], the right-hand side is rhs[c].  The inner scalars are read on the
-// host (the reference's branch on ||w|| decides whether a second cycle runs),
-// so solves with this cycle are not captured in a graph.
+// in x[c], the right-hand side is rhs[c].  Outside a capture the inner
+// scalars are read on the host (the reference's branch on ||w|| decides
+// whether a second cycle runs); while the FCG loop is captured,
+// kcycle_inner_graph keeps them on the device.
 template <typename XT>
 bcmg_status kcycle_inner_t(bcmg_handle *h, CycleBufs<XT> &B, int k, int c) {
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    BCMG_CUDA(cudaStreamIsCapturing(h->stream, &cs));
+    if (cs == cudaStreamCaptureStatusActive) return kcycle_inner_graph<XT>(h, B, k, c);
+  }
   const DevLevel &lv = h->H[k].lv[c];
   const MatView A = Lv<XT>::mat(lv);
   const int32_t n = lv.n;
@@ -902,6 +1084,7 @@ void destroy_handle(bcmg_handle *h) {
   cudaSetDevice(h->device);
   cudaStream_t s = h->stream;
   if (h->fcg_exec) cudaGraphExecDestroy(h->fcg_exec);
+  for (cudaStream_t ks : h->kc_streams) cudaStreamDestroy(ks);
   destroy_batch(h);
   for (auto &H : h->H) H.release(s);
   h->A0.own_A = true;
@@ -1023,6 +1206,17 @@ bcmg_status fcg_iteration(bcmg_handle *h, cudaGraphConditionalHandle cond, bool 
 // iteration until the device-side condition (k_fcg_continue) turns false,
 // so a whole solve needs no host round trip per iteration.
 bcmg_status build_fcg_graph(bcmg_handle *h) {
+  if (h->prm.cycle_type == 3) {
+    // the K-cycle's IF bodies are captured on streams of their own, one per
+    // level (created here: no stream is created during a capture)
+    size_t L = 0;
+    for (auto &H : h->H) L = std::max(L, H.lv.size());
+    while (h->kc_streams.size() < L) {
+      cudaStream_t ks = nullptr;
+      BCMG_CUDA(cudaStreamCreateWithFlags(&ks, cudaStreamNonBlocking));
+      h->kc_streams.push_back(ks);
+    }
+  }
   return capture_while_loop(
       h->stream, [h](cudaGraphConditionalHandle cond) { return fcg_iteration(h, cond, true); },
       &h->fcg_exec);
@@ -1074,8 +1268,7 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
   BCMG_TRY(fcg_scalars(h->partials, h->scal, true, s));
   BCMG_TRY(fcg_update(n, true, v, d, w, q, x, r, h->partials, h->scal, s));
   double *hs = h->host_scal;
-  const bool graphs = h->ext.use_graphs && h->ext.verbose < 2 && h->stream != nullptr &&
-                      h->prm.cycle_type != 3;  // the K-cycle reads its scalars on the host
+  const bool graphs = h->ext.use_graphs && h->ext.verbose < 2 && h->stream != nullptr;
   g_clock.tick("first_step");
   if (graphs && !h->fcg_exec && build_fcg_graph(h) != BCMG_OK) {
     clear_error();

@@ -80,6 +80,10 @@ struct CycleBufs {
   std::vector<XT *> kw, kd0, kd1, kv, kv1, kx;
   std::vector<int32_t> kn;  // allocated length of the K-cycle vectors
   double *kdots = nullptr;
+  // Device scalars of the K-cycle's inner steps, kKcStride per level, for
+  // the captured FCG loop (the host-driven loop reads them through kdots).
+  double *kscal = nullptr;
+  size_t kscal_levels = 0;
 };
 
 // Multi-right-hand-side solve state (batch.cu), created by the first batched
@@ -121,6 +125,9 @@ struct bcmg_handle {
   double *partials = nullptr, *scal = nullptr;
   double host_scal[bcmg::kNumScal] = {};  // host mirror of scal
   cudaGraphExec_t fcg_exec = nullptr;   // captured FCG loop (WHILE node)
+  // One stream per level to capture the bodies of the K-cycle's IF nodes
+  // on (created before the capture, destroyed with the handle).
+  std::vector<cudaStream_t> kc_streams;
   bcmg::BatchState *batch = nullptr;    // multi-right-hand-side solves
   double setup_ms = 0.0;
 };

@@ -289,8 +289,13 @@ def test_cli_matches_reference_format(tmp_path):
 def test_kcycle_matches_oracle(prec):
     """cycle_type 3 (K-cycle, GAMG_cycle.cu:88-100 + inneritkcycle,
     FCG.cu:633-723) on the GPU against the oracle's: same hierarchy, the
-    solution within 1e-6 and the outer iteration count within one.  Batched
-    solves refuse the K-cycle."""
+    solution within 1e-6 and the outer iteration count within one.  The FCG
+    loop with the K-cycle runs as a captured graph (inner scalars on the
+    device, the second inner step an IF node): a repeated solve launches a
+    fraction of the host-driven loop's kernels and gives the host-driven
+    solution (same iterations, within 1e-10).  Batched solves refuse the
+    K-cycle."""
+    from bootcmatchg_b200._lib import lib
     A = wl.poisson(27, 20, 20, 20)
     p = c1_params()
     p.cycle_type = 3
@@ -298,8 +303,20 @@ def test_kcycle_matches_oracle(prec):
     ext = bc.Extensions(precision=prec, replace_every=10 if prec else 0)
     with bc.Handle(A, p, ext) as h:
         x, info = h.solve(b)
+        n0 = lib.bcmg_kernel_launches()
+        x2, info2 = h.solve(b)
+        graph_launches = lib.bcmg_kernel_launches() - n0
         with pytest.raises(bc.BcmgError, match="UNSUPPORTED"):
             h.solve_batch(np.asfortranarray(np.stack([b, b], axis=1)))
+    ext_host = bc.Extensions(precision=prec, replace_every=10 if prec else 0, use_graphs=0)
+    with bc.Handle(A, p, ext_host) as hh:
+        n0 = lib.bcmg_kernel_launches()
+        xh, ih = hh.solve(b)
+        host_launches = lib.bcmg_kernel_launches() - n0
+    assert info2.iters == info.iters and np.array_equal(x2, x)
+    assert ih.iters == info.iters, (ih.iters, info.iters)
+    assert np.linalg.norm(xh - x) / np.linalg.norm(xh) < 1e-10
+    assert graph_launches * 3 < host_launches, (graph_launches, host_launches)
     o = orc.OracleHandle(A, p)
     xo, oi, st = o.solve(b)
     assert st == 0 and oi["converged"] and info.converged
