@@ -1,11 +1,17 @@
 // BootCMatchG's own matching + aggregation sweep, compiled from the
 // unmodified sources of the reference tree (the unity header below pulls them
 // in; the Makefile adds the separately compiled files and compat.h/compat.cu
-// for the cuSPARSE routines CUDA 11 removed), behind one C entry:
+// for the cuSPARSE routines CUDA 11 removed), behind C entries:
 //   ref_pair_aggregate  one matching + aggregation sweep with the reference's
 //                       kernels (matchingPairAggregation, src/AMG/
 //                       matchingAggregation.cu:181-208, and the W of
-//                       Matching::makeAH/toMaximumProductMatrix).
+//                       Matching::makeAH/toMaximumProductMatrix);
+//   ref_read_mm / ref_write_mm / ref_free
+//                       the reference's Matrix-Market reader
+//                       (readMatrixFromFile with m_type 0 into host memory,
+//                       src/matrix/matrixIO.cu:4-192) and writer
+//                       (CSRMatrixPrintMM, matrixIO.cu:290-333): host code
+//                       only, so the CPU tests call them.
 // TEST INFRASTRUCTURE ONLY: it generated the golden fixture that pins the
 // oracle; nothing in the product links it.  The reference's Galerkin product
 // (nsparse) and its stock solve() are deliberately not exported: on a B200 the
@@ -69,6 +75,35 @@ int ref_pair_aggregate(int n, int nnz, const int *row, const int *col, const dou
   matchingAggregationContext::freeContext();
   drop_host_wrapper(Ah);
   return static_cast<int>(cudaDeviceSynchronize());
+}
+
+// The arrays returned are the reader's own (calloc'ed); release them with
+// ref_free.  The file must exist (the reference's reader exits otherwise).
+int ref_read_mm(const char *path, int *n, int *m, int *nnz, int **row, int **col,
+                double **val) {
+  CSR *A = readMatrixFromFile(path, 0, false);
+  if (!A) return 1;
+  *n = A->n;
+  *m = A->m;
+  *nnz = A->nnz;
+  *row = A->row;
+  *col = A->col;
+  *val = A->val;
+  drop_host_wrapper(A);
+  return 0;
+}
+
+void ref_free(void *p) { std::free(p); }
+
+int ref_write_mm(int n, int m, int nnz, const int *row, const int *col, const double *val,
+                 const char *path) {
+  CSR *A = CSRm::init(n, m, nnz, false, false, false);
+  A->row = const_cast<int *>(row);
+  A->col = const_cast<int *>(col);
+  A->val = const_cast<double *>(val);
+  CSRMatrixPrintMM(A, path);
+  drop_host_wrapper(A);
+  return 0;
 }
 
 }  // extern "C"
