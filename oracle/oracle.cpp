@@ -913,6 +913,18 @@ int fcg(orc_handle &h, const double *b, double *x, int itnlim, bcmg_solve_info *
 
 extern "C" {
 
+// BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311).
+int32_t orc_max_coarse_size(int32_t n) {
+  return static_cast<int32_t>(40 * std::pow(static_cast<double>(n), 1. / 3.));
+}
+
+int orc_grid_sweeps(int cycle_type, int max_levels, int32_t *out) {
+  const IVec g = grid_sweeps(cycle_type, max_levels);
+  const int k = std::max(0, max_levels - 1);
+  for (int i = 0; i < k; ++i) out[i] = g[i];
+  return k;
+}
+
 void orc_set_threads(int nthreads) {
   g_threads = nthreads;
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -926,9 +938,7 @@ int orc_setup(const bcmg_csr *A, const bcmg_params *p, orc_handle **out) {
   auto h = std::make_unique<orc_handle>();
   h->prm = *p;
   h->A0 = std::make_shared<Csr>(from_bcmg(A));
-  // BuildData::setMaxCoarseSize (src/AMG/AMG.cu:309-311).
-  h->maxcoarsesize =
-      static_cast<int32_t>(40 * std::pow(static_cast<double>(A->n), 1. / 3.));
+  h->maxcoarsesize = orc_max_coarse_size(A->n);
   h->grid_sweeps = grid_sweeps(p->cycle_type, p->max_levels);
   bootstrap(*h);
   *out = h.release();
@@ -941,8 +951,7 @@ int orc_setup_from_w(const bcmg_csr *A, const bcmg_params *p, const double *w,
   auto h = std::make_unique<orc_handle>();
   h->prm = *p;
   h->A0 = std::make_shared<Csr>(from_bcmg(A));
-  h->maxcoarsesize =
-      static_cast<int32_t>(40 * std::pow(static_cast<double>(A->n), 1. / 3.));
+  h->maxcoarsesize = orc_max_coarse_size(A->n);
   h->grid_sweeps = grid_sweeps(p->cycle_type, p->max_levels);
   Vec wv(w, w + A->n);
   h->H.push_back(adaptive_coarsening(*h, wv));

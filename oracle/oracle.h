@@ -4,12 +4,18 @@
  * TEST INFRASTRUCTURE ONLY.  The oracle is the parity checker and the timed
  * CPU baseline; nothing in the product library links, loads or calls it.
  *
- * Parity status: the reference ships no tests, golden vectors or sample
- * matrices, and cannot be built here (its solve path calls cuSPARSE legacy
- * routines removed from CUDA 11+), so this restatement is pinned only by the
- * reference's own invariants (a valid symmetric matching, every vertex in one
- * aggregate, P^T P = I on good aggregates, A_c = P^T A P) and by hand-checked
- * known answers in the tests: parity unpinned.
+ * Parity status: partially pinned.  The reference ships no tests, golden
+ * vectors or sample matrices, and its solve path does not build unmodified
+ * with CUDA 12 (legacy cuSPARSE routines).  oracle/ref/ compiles its sources
+ * with a compatibility shim into oracle/_ref/libref.so, which pins this
+ * restatement where the reference's own code could run: one matching +
+ * aggregation sweep recorded on a B200 (tests/golden/, checked by
+ * tests/test_ref_fixtures.py), and its host code run on the CPU
+ * (tests/test_ref_io.py: the Matrix-Market reader and writer, the settings
+ * file, the coarsest-size rule and the grid-sweep table).  The rest is
+ * pinned by the reference's own invariants (a valid symmetric matching,
+ * every vertex in one aggregate, P^T P = I on good aggregates,
+ * A_c = P^T A P) and by hand-checked known answers in the tests.
  *
  * Every function follows the reference file:line cited beside it.  Where
  * the reference is nondeterministic (atomicAdd aggregate numbering, FP64
@@ -34,6 +40,12 @@ extern "C" {
 typedef struct orc_handle orc_handle;
 
 void orc_set_threads(int nthreads);
+
+/* maxcoarsesize = (int)(40 n^(1/3)) (BuildData::setMaxCoarseSize) and the
+ * grid-sweep table of the first max_levels - 1 levels
+ * (ApplyData::setGridSweeps); returns the number of entries written. */
+int32_t orc_max_coarse_size(int32_t n);
+int orc_grid_sweeps(int cycle_type, int max_levels, int32_t *out);
 int orc_get_threads(void);
 
 int orc_setup(const bcmg_csr *A, const bcmg_params *p, orc_handle **out);

@@ -63,6 +63,8 @@ _SIG = {
     "orc_spgemm": (C.c_int, [i32, i32, vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, i32p, vp, vp]),
     "orc_spmv": (C.c_int, [i32, vp, vp, vp, C.c_double, vp, C.c_double, vp]),
     "orc_greedy_match": (C.c_int, [i32, vp, vp, vp, vp]),
+    "orc_max_coarse_size": (i32, [i32]),
+    "orc_grid_sweeps": (C.c_int, [C.c_int, C.c_int, vp]),
 }
 
 

@@ -11,7 +11,14 @@
 //                       (readMatrixFromFile with m_type 0 into host memory,
 //                       src/matrix/matrixIO.cu:4-192) and writer
 //                       (CSRMatrixPrintMM, matrixIO.cu:290-333): host code
-//                       only, so the CPU tests call them.
+//                       only, so the CPU tests call them;
+//   ref_params_from_file / ref_max_coarse_size / ref_grid_sweeps
+//                       the settings-file reader (AMG::Params::initFromFile,
+//                       src/AMG/AMG.cu:480-526; it exits on an invalid value,
+//                       so only valid files are given to it), the coarsest
+//                       size rule (BuildData::setMaxCoarseSize, :309-311) and
+//                       the grid-sweep table (ApplyData::setGridSweeps,
+//                       :371-394): host code as well.
 // TEST INFRASTRUCTURE ONLY: it generated the golden fixture that pins the
 // oracle; nothing in the product links it.  The reference's Galerkin product
 // (nsparse) and its stock solve() are deliberately not exported: on a B200 the
@@ -94,6 +101,30 @@ int ref_read_mm(const char *path, int *n, int *m, int *nnz, int **row, int **col
 }
 
 void ref_free(void *p) { std::free(p); }
+
+int ref_params_from_file(const char *path, params *out) {
+  *out = AMG::Params::initFromFile(path);
+  return static_cast<int>(sizeof(params));
+}
+
+int ref_max_coarse_size(int n) {
+  CSR A;
+  A.n = n;
+  buildData bd;
+  bd.A = &A;
+  AMG::BuildData::setMaxCoarseSize(&bd);
+  return bd.maxcoarsesize;
+}
+
+int ref_grid_sweeps(int cycle_type, int max_level, int *out) {
+  applyData ad;
+  ad.cycle_type = cycle_type;
+  AMG::ApplyData::setGridSweeps(&ad, max_level);
+  const int k = max_level - 1;
+  for (int i = 0; i < k; ++i) out[i] = ad.num_grid_sweeps[i];
+  std::free(ad.num_grid_sweeps);
+  return k;
+}
 
 int ref_write_mm(int n, int m, int nnz, const int *row, const int *col, const double *val,
                  const char *path) {

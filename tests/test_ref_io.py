@@ -1,4 +1,4 @@
-"""Pins the Matrix-Market reader and writer to BootCMatchG's own host code.
+"""Pins host-side parts of the path to BootCMatchG's own host code.
 
 oracle/ref/Makefile compiles the reference's unmodified src/matrix/matrixIO.cu
 into oracle/_ref/libref.so; its reader (readMatrixFromFile with m_type 0 into
@@ -9,7 +9,12 @@ next to bcmg_read_matrix and bcmg_write_matrix_mm on the same files:
     (column, value) pairs bit for bit; the reference keeps each row in file
     order while bcmg_read_matrix sorts it, so rows are compared sorted;
     symmetric files are expanded the same way;
-  - the writer produces the same bytes.
+  - the writer produces the same bytes;
+  - bcmg_params_from_file reads a settings file into the same 15 fields as
+    AMG::Params::initFromFile (src/AMG/AMG.cu:480-526);
+  - the oracle's coarsest-size rule and grid-sweep table equal
+    BuildData::setMaxCoarseSize and ApplyData::setGridSweeps
+    (src/AMG/AMG.cu:309-311, 371-394).
 The library is built where the reference tree is present (this build
 container); elsewhere the tests skip.
 """
@@ -37,6 +42,9 @@ def ref():
     lib.ref_write_mm.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip, C.POINTER(C.c_double),
                                  C.c_char_p]
     lib.ref_free.argtypes = [C.c_void_p]
+    lib.ref_params_from_file.argtypes = [C.c_char_p, C.c_void_p]
+    lib.ref_max_coarse_size.argtypes = [C.c_int]
+    lib.ref_grid_sweeps.argtypes = [C.c_int, C.c_int, C.c_void_p]
     return lib
 
 
@@ -133,3 +141,57 @@ def test_writer_matches_reference_bytes(ref, tmp_path):
     bc.write_matrix_mm(str(ours), A)
     ref_write(ref, A, theirs)
     assert ours.read_bytes() == theirs.read_bytes()
+
+
+SETTINGS = [
+    # the reference's base file, values with its comments
+    ["0 % solver_type", "1 % max_hrc", "0.8 % rho", "2 % aggr_sweeps", "0 % aggr_type",
+     "39 % max_levels", "0 % cycle_type", "4 % coarsest_solver_type", "4 % relax_type",
+     "20 % coarserelax_sweeps", "1 % prerelax_sweeps", "1 % postrelax_sweeps",
+     "200000 % itnlim", "1.e-6 % rtol"],
+    # the settings of the benchmarks' 7-point Poisson case, no comments
+    ["0", "1", "0.8", "2", "0", "20", "0", "4", "4", "16", "4", "4", "1000", "1e-8"],
+    # bootstrap composites, smoothed aggregation, W-cycle, Jacobi
+    ["2", "3", "0.5", "1", "1", "10", "2", "0", "0", "7", "2", "3", "50",
+     "2.5e-10   % tight"],
+    ["1", "2", "0.25", "3", "0", "5", "1", "4", "0", "1", "0", "2", "7", "0.125"],
+]
+
+
+@pytest.mark.parametrize("case", range(len(SETTINGS)))
+def test_settings_file_matches_reference(ref, tmp_path, case):
+    from bootcmatchg_b200._lib import Params as CParams
+    from bootcmatchg_b200._lib import check, lib
+    path = tmp_path / "settings"
+    path.write_text("\n".join(SETTINGS[case]) + "\n")
+    ours, theirs = CParams(), CParams()
+    check(lib.bcmg_params_from_file(str(path).encode(), C.byref(ours)), "params_from_file")
+    assert ref.ref_params_from_file(str(path).encode(), C.byref(theirs)) == C.sizeof(CParams)
+    # field by field (the padding bytes of the reference's struct, returned
+    # by value, are not defined); doubles bit for bit
+    import struct
+    for name, ctype in CParams._fields_:
+        a, b = getattr(ours, name), getattr(theirs, name)
+        if ctype is C.c_double:
+            a, b = struct.pack("<d", a), struct.pack("<d", b)
+        assert a == b, (name, a, b)
+
+
+def test_coarsest_size_rule_matches_reference(ref):
+    from oracle import oracle as orc
+    sizes = [1, 2, 7, 8, 26, 27, 63, 64, 125, 1000, 1728, 4096, 32768, 884736, 1000000,
+             2097152, 4194304, 2000000, 2 ** 31 - 1]
+    for n in sizes:
+        assert orc.olib.orc_max_coarse_size(n) == ref.ref_max_coarse_size(n), n
+
+
+def test_grid_sweeps_match_reference(ref):
+    from oracle import oracle as orc
+    for cycle_type in (0, 1, 2):
+        for max_levels in range(1, 41):
+            a = np.zeros(64, np.int32)
+            b = np.zeros(64, np.int32)
+            ka = orc.olib.orc_grid_sweeps(cycle_type, max_levels, C.c_void_p(a.ctypes.data))
+            kb = ref.ref_grid_sweeps(cycle_type, max_levels, C.c_void_p(b.ctypes.data))
+            assert ka == kb == max_levels - 1
+            assert np.array_equal(a[:ka], b[:kb]), (cycle_type, max_levels)
