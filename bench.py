@@ -151,13 +151,26 @@ class ClockSampler:
         self.proc = None
 
     def start(self):
+        """Starts sampling every 100 ms and returns once the first sample is
+        written (up to 5 s), so that a timed region of a few hundred
+        milliseconds is covered from its start."""
         try:
             self.f = open(self.out_path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            try:
+                with open(self.out_path) as f:
+                    if any(line.count(",") >= 8 for line in f):
+                        break
+            except OSError:
+                pass
+            time.sleep(0.02)
 
     def stop(self, gpu_index=0):
         if not self.proc:
