@@ -68,6 +68,18 @@ __device__ __forceinline__ void pdl_trigger() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// The dependency a launch_pdl kernel relaxes is on the kernel before it: a
+// stream copy or memset just before it is not ordered by its pdl_wait().  A
+// test that ran five sweeps after a device-to-device copy of the iterate
+// read rows the copy had not yet written.  So copies between solve-phase
+// kernels are kernels themselves (copy_t), and an upload that a launch_pdl
+// kernel follows is closed by pdl_fence: an empty kernel launched normally,
+// which starts only after everything before it on the stream has finished.
+namespace {
+__global__ void k_pdl_fence() {}
+}  // namespace
+inline void pdl_fence(cudaStream_t s) { k_pdl_fence<<<1, 1, 0, s>>>(); }
+
 template <typename... KArgs, typename... Args>
 inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
                        cudaStream_t s, Args &&...args) {

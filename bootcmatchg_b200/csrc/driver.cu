@@ -1261,6 +1261,7 @@ bcmg_status fcg(bcmg_handle *h, bcmg_solve_info *info) {
   init[kDelta0] = delta0;
   init[kBnorm] = bnorm;
   BCMG_CUDA(cudaMemcpyAsync(h->scal, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  pdl_fence(s);
   // First step (FCG.cu:464-495): v = B r; w = A v; x += theta v; r -= theta w;
   // d = v; q = w.
   BCMG_TRY(precond_apply(h, r, v, true, h->mixed));
@@ -1684,6 +1685,7 @@ bcmg_status bcmg_solve(bcmg_handle *h, const double *b, double *x, int on_device
   const cudaMemcpyKind in = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   BCMG_CUDA(cudaMemcpyAsync(h->b, b, sizeof(double) * n, in, h->stream));
   BCMG_CUDA(cudaMemcpyAsync(h->xs, x, sizeof(double) * n, in, h->stream));
+  pdl_fence(h->stream);  // the FCG's first kernels are programmatic launches
   bcmg_status st = fcg(h, info);
   const cudaMemcpyKind outk = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   BCMG_CUDA(cudaMemcpyAsync(x, h->xs, sizeof(double) * n, outk, h->stream));

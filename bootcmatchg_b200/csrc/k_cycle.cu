@@ -159,6 +159,16 @@ __global__ void k_axpy_t(int64_t n, XT a, const XT *__restrict__ x, XT *__restri
     y[i] = fma(a, x[i], y[i]);
 }
 
+// dst = src, a kernel in the programmatic-launch chain (see pdl_fence).
+template <typename XT>
+__global__ void k_copy_t(int64_t n, const XT *__restrict__ src, XT *__restrict__ dst) {
+  pdl_wait();
+  pdl_trigger();
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    dst[i] = src[i];
+}
+
 template <typename XT>
 __global__ void k_scale_t(int64_t n, XT a, XT *x) {
   pdl_wait();
@@ -332,7 +342,7 @@ bcmg_status relax_t(const MatView &A, const XT *d, const XT *f, XT *u, XT *u_tmp
       launch_pdl(k_relax_zero_t<XT>, ceil_div(n, kThreads), kThreads, 0, s, n, d, f, cur);
     --left;
   } else if (k % 2 == 1) {
-    BCMG_CUDA(cudaMemcpyAsync(u_tmp, u, sizeof(XT) * n, cudaMemcpyDeviceToDevice, s));
+    BCMG_TRY(copy_t<XT>(u_tmp, u, n, s));  // a kernel: ordered before the first sweep
     cur = u_tmp;
   } else {
     cur = u;
@@ -425,7 +435,8 @@ bcmg_status scale_t(int64_t n, XT a, XT *x, cudaStream_t s) {
 template <typename XT>
 bcmg_status copy_t(XT *dst, const XT *src, int64_t n, cudaStream_t s) {
   if (n <= 0 || dst == src) return BCMG_OK;
-  BCMG_CUDA(cudaMemcpyAsync(dst, src, sizeof(XT) * n, cudaMemcpyDeviceToDevice, s));
+  launch_pdl(k_copy_t<XT>, stream_grid(n), kThreads, 0, s, n, src, dst);
+  BCMG_LAUNCH_CHECK();
   return BCMG_OK;
 }
 
