@@ -9,9 +9,14 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <initializer_list>
 #include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
 
 #include <nvtx3/nvToolsExt.h>
 
@@ -38,6 +43,187 @@ bcmg_status build_sliced(bcmg_handle *h, const CsrView &A, int vtype, SlicedMat 
                          cudaStream_t s) {
   out->wait_ns = wait_ns_of(h);
   return sliced_build(A, vtype, out, s, h->ext.narrow_values != 0);
+}
+
+// The copy a queued build fills: level `lvl` of hierarchy `hrc` (own64, or
+// ownlo when `lo`), or the input matrix's FP64 copy when hrc < 0.  Kept as
+// indices because the hierarchies' level vectors grow while builds run.
+struct SliceTarget {
+  int hrc = -1, lvl = 0;
+  bool lo = false;
+};
+
+// Solve-phase copies of the coarse matrices of unsmoothed aggregation are
+// built by a helper thread on a stream of its own, each once its level is
+// complete, while the handle's stream goes on coarsening.  A coarse copy's
+// build is mostly host round trips (it reads its slice statistics back
+// before it sizes its arrays), which the helper takes off the setup's
+// critical path; its kernels are small.  (The input matrix's copy is not
+// built here: its bandwidth-bound passes took the SMs from the matching
+// kernels running beside them, which fill every warp slot, about as much
+// time as they saved.)  Each build waits for an event recorded on the
+// handle's stream when it was queued (its matrix is complete there).  A
+// copy becomes part of the hierarchy only at drain(), which waits for every
+// queued build and installs the results; drains come before the bootstrap's
+// inner iterations and before the solve formats are finished, so every
+// kernel that reads a copy sees the state that building them in line gives
+// (same copies, same results).  The destructor drains too: on an error path
+// the finished copies go to the handle (freed with it) and partial ones are
+// released.
+class SideBuilder {
+ public:
+  explicit SideBuilder(bcmg_handle *h) : h_(h) {}
+  SideBuilder(const SideBuilder &) = delete;
+  SideBuilder &operator=(const SideBuilder &) = delete;
+  ~SideBuilder() {
+    drain(false);
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) worker_.join();
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  bcmg_status enqueue(const CsrView &A, int vtype, SliceTarget t) {
+    if (!stream_) {
+      BCMG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+      try {
+        worker_ = std::thread([this] { run(); });
+      } catch (...) {
+        cudaStreamDestroy(stream_);
+        stream_ = nullptr;
+        return set_error(BCMG_ERR_INTERNAL, "cannot start the copy-building thread");
+      }
+    }
+    Item it;
+    it.A = A;
+    it.vtype = vtype;
+    it.t = t;
+    it.wait_ns = wait_ns_of(h_);
+    it.narrow = h_->ext.narrow_values != 0;
+    BCMG_CUDA(cudaEventCreateWithFlags(&it.ready, cudaEventDisableTiming));
+    const cudaError_t e = cudaEventRecord(it.ready, h_->stream);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(it.ready);
+      return set_error(BCMG_ERR_CUDA, "cudaEventRecord: %s", cudaGetErrorString(e));
+    }
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      items_.push_back(it);
+    }
+    cv_.notify_all();
+    return BCMG_OK;
+  }
+
+  // Waits for every queued build and installs the copies; returns the first
+  // failure of a build (its message becomes the last error when `report`).
+  bcmg_status drain(bool report = true) {
+    std::deque<Item> done;
+    {
+      std::unique_lock<std::mutex> lk(m_);
+      idle_.wait(lk, [this] { return next_ == items_.size(); });
+      done.swap(items_);
+      next_ = 0;
+    }
+    bcmg_status first = BCMG_OK;
+    std::string msg;
+    for (Item &it : done) {
+      SlicedMat *dst = target(it.t);
+      if (it.st == BCMG_OK && dst && !dst->nslices) {
+        *dst = it.out;
+      } else {
+        it.out.release(h_->stream);
+        if (it.st != BCMG_OK && first == BCMG_OK) {
+          first = it.st;
+          msg = it.err;
+        }
+      }
+    }
+    // Level 0 of every hierarchy reads the input matrix's copy.
+    if (h_->A0.own64.nslices)
+      for (auto &H : h_->H)
+        if (!H.lv.empty()) H.lv[0].s64 = &h_->A0.own64;
+    if (first != BCMG_OK && report) return set_error(first, "%s", msg.c_str());
+    return first;
+  }
+
+ private:
+  struct Item {
+    CsrView A;
+    int vtype = kValF64;
+    SliceTarget t;
+    unsigned long long wait_ns = kDefaultWaitNs;
+    bool narrow = false;
+    cudaEvent_t ready = nullptr;
+    SlicedMat out;
+    bcmg_status st = BCMG_OK;
+    std::string err;
+  };
+
+  SlicedMat *target(const SliceTarget &t) {
+    if (t.hrc < 0) return &h_->A0.own64;
+    if (static_cast<size_t>(t.hrc) >= h_->H.size()) return nullptr;
+    auto &lv = h_->H[t.hrc].lv;
+    if (static_cast<size_t>(t.lvl) >= lv.size()) return nullptr;
+    return t.lo ? &lv[t.lvl].ownlo : &lv[t.lvl].own64;
+  }
+
+  bcmg_status build(Item &it) {
+    BCMG_CUDA(cudaStreamWaitEvent(stream_, it.ready, 0));
+    it.out.wait_ns = it.wait_ns;
+    BCMG_TRY(sliced_build(it.A, it.vtype, &it.out, stream_, it.narrow));
+    BCMG_CUDA(cudaStreamSynchronize(stream_));
+    return BCMG_OK;
+  }
+
+  void run() {
+    cudaSetDevice(h_->device);
+    std::unique_lock<std::mutex> lk(m_);
+    for (;;) {
+      cv_.wait(lk, [this] { return stop_ || next_ < items_.size(); });
+      if (next_ >= items_.size()) return;  // stop_ with nothing queued
+      Item &it = items_[next_];            // deque: stable under push_back
+      lk.unlock();
+      it.st = build(it);
+      if (it.st != BCMG_OK) it.err = bcmg_last_error();
+      cudaEventDestroy(it.ready);
+      it.ready = nullptr;
+      lk.lock();
+      ++next_;
+      idle_.notify_all();
+    }
+  }
+
+  bcmg_handle *h_;
+  cudaStream_t stream_ = nullptr;
+  std::thread worker_;
+  std::mutex m_;
+  std::condition_variable cv_, idle_;
+  std::deque<Item> items_;
+  size_t next_ = 0;  // items_[next_] is the next build (all before it done)
+  bool stop_ = false;
+};
+
+// Rows of the input matrix from which a setup builds its solve copies on the
+// helper thread (below this the copies are built in line: too little work to
+// pay for the thread).
+constexpr int32_t kSideBuildMinRows = 1 << 17;
+
+// The sliced copy of A in *out (the copy named by t), built now on the
+// handle's stream or queued on the setup's helper.
+bcmg_status sliced_copy(bcmg_handle *h, const CsrView &A, int vtype, SlicedMat *out,
+                        SliceTarget t) {
+  if (h->side) return h->side->enqueue(A, vtype, t);
+  return build_sliced(h, A, vtype, out, h->stream);
+}
+
+// Storage of the coarse levels' values in the mixed cycle (ext.coarse_storage).
+int coarse_value_type(const bcmg_handle *h) {
+  return h->ext.coarse_storage == BCMG_STORE_BF16   ? kValBF16
+         : h->ext.coarse_storage == BCMG_STORE_FP16 ? kValF16
+                                                    : kValF32;
 }
 
 // NVTX range for the lifetime of a scope (profilers filter on these names).
@@ -391,10 +577,17 @@ bcmg_status adaptive_coarsening(bcmg_handle *h, const double *w_in, DevHierarchy
       BCMG_TRY(dev_alloc(&coarse.M, coarse.n, s));
       BCMG_TRY(level_prep(coarse.view(), coarse.D, coarse.M, s));
       // FP64 sliced copy now if an FP64 cycle will read this level (the FP64
-      // solve, or the bootstrap's inner iterations).
-      // (Smoothed aggregation replaces the coarse matrices: built afterwards.)
+      // solve, or the bootstrap's inner iterations); with the setup's helper
+      // also the mixed cycle's copy, which is otherwise built after the
+      // bootstrap.  (Smoothed aggregation replaces the coarse matrices: built
+      // afterwards.)
+      const SliceTarget t{static_cast<int>(&H - h->H.data()), static_cast<int>(H.lv.size()) - 1,
+                          false};
       if (h->prm.aggrtype == 0 && wants_coarse_f64(h))
-        BCMG_TRY(build_sliced(h, coarse.view(), kValF64, &coarse.own64, s));
+        BCMG_TRY(sliced_copy(h, coarse.view(), kValF64, &coarse.own64, t));
+      if (h->side && h->prm.aggrtype == 0 && h->ext.precision == BCMG_PREC_MIXED)
+        BCMG_TRY(h->side->enqueue(coarse.view(), coarse_value_type(h),
+                                  SliceTarget{t.hrc, t.lvl, true}));
       const double size_coarse = coarse.n;
       const double coarse_ratio = fine_n / size_coarse;
       avcoarseratio += coarse_ratio;
@@ -970,9 +1163,7 @@ bcmg_status prepare_mixed(bcmg_handle *h) {
     a.vtype_lo = kValF32;
     BCMG_TRY(convert_values(a.nnz, a.val, a.val_lo, kValF32, s));
   }
-  const int coarse_type = h->ext.coarse_storage == BCMG_STORE_BF16   ? kValBF16
-                          : h->ext.coarse_storage == BCMG_STORE_FP16 ? kValF16
-                                                                     : kValF32;
+  const int coarse_type = coarse_value_type(h);
   for (auto &H : h->H) {
     for (size_t l = 0; l < H.lv.size(); ++l) {
       DevLevel &lv = H.lv[l];
@@ -1071,6 +1262,8 @@ bcmg_status bootstrap(bcmg_handle *h) {
     st = size_buffers_t<double>(h, h->c64);
     if (st != BCMG_OK) break;
     if (num_hrc > 1) {
+      if (h->side) st = h->side->drain();  // the inner iterations read the copies
+      if (st != BCMG_OK) break;
       st = inner_iterations(h, w);
       if (st != BCMG_OK) break;
     }
@@ -1125,6 +1318,12 @@ bcmg_status finish_setup(bcmg_handle *h) {
   return sliced_wait_status(h->stream);
 }
 
+// Clears h->side when the setup that owns the helper returns.
+struct SideScope {
+  bcmg_handle *h;
+  ~SideScope() { h->side = nullptr; }
+};
+
 bcmg_status setup_common(bcmg_handle *h) {
   NvtxRange range("bcmg_setup");
   const auto t0 = Clock::now();
@@ -1132,10 +1331,23 @@ bcmg_status setup_common(bcmg_handle *h) {
   g_clock.start(h->ext.verbose >= 1, h->stream);
   set_cycle_tables(h);
   BCMG_TRY(alloc_work(h));
+  // The input matrix's copy is built in line: it is bandwidth-bound work
+  // that would take the SMs from the first matching sweep, and the A-norm
+  // of the smooth vector reads it.
   if (h->ext.sliced) BCMG_TRY(build_sliced(h, h->A0.view(), kValF64, &h->A0.own64, h->stream));
+  // Declared before the scope guard, so h->side is cleared before the
+  // helper's destructor drains it.
+  std::unique_ptr<SideBuilder> side;
+  SideScope scope{h};
+  if (h->ext.sliced && h->A0.n >= kSideBuildMinRows) {
+    side = std::make_unique<SideBuilder>(h);
+    h->side = side.get();
+  }
   g_clock.tick("alloc");
   BCMG_TRY(bootstrap(h));
   g_clock.tick("other");
+  if (side) BCMG_TRY(side->drain());
+  g_clock.tick("side_copies");
   BCMG_TRY(finish_setup(h));
   h->setup_ms = ms_since(t0);
   g_clock.report("setup");

@@ -92,6 +92,9 @@ struct BatchState;
 void destroy_batch(bcmg_handle *h);
 size_t batch_bytes(const bcmg_handle *h);  // device bytes of the batch state
 
+// Builds sliced copies on a helper thread during a setup (driver.cu).
+class SideBuilder;
+
 // Device bytes held by a handle (hierarchies, solve copies, work vectors).
 size_t handle_bytes(const bcmg_handle *h);
 template <typename XT>
@@ -129,5 +132,8 @@ struct bcmg_handle {
   // on (created before the capture, destroyed with the handle).
   std::vector<cudaStream_t> kc_streams;
   bcmg::BatchState *batch = nullptr;    // multi-right-hand-side solves
+  // During a setup of a large matrix: the helper that builds solve-phase
+  // copies on a stream of its own (null otherwise; owned by the setup).
+  bcmg::SideBuilder *side = nullptr;
   double setup_ms = 0.0;
 };

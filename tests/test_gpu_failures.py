@@ -117,6 +117,48 @@ def test_every_allocation_failure_is_reported_without_leaks():
     assert alloc_stats()[0] == live0
 
 
+@pytest.mark.parametrize("max_hrc", [1, 2])
+def test_copies_built_beside_the_setup_fail_cleanly_and_repeat_bits(max_hrc):
+    """7-point Poisson 52^3 (140,608 rows) is large enough for a setup to
+    build its solve-phase copies on a helper thread and stream while it
+    coarsens (inputs of 131,072 rows and more).  Repeated setups + solves
+    give the same bits; failing each allocation of a setup + solve in turn,
+    whichever thread makes it, returns BCMG_ERR_ALLOC and leaks nothing.
+    With max_hrc 2 (conv_ratio 0.01, so the second hierarchy is built) the
+    copies are installed before the bootstrap's inner iterations."""
+    A = wl.poisson(7, 52, 52, 52)
+    b = wl.vector(1, 4, A.n)
+    p = c1_params()
+    p.max_hrc, p.conv_ratio = max_hrc, 0.01
+    ext = bc.Extensions(precision=bc.PREC_MIXED, replace_every=10)
+    live0, made0 = alloc_stats()
+    with bc.Handle(A, p, ext) as h:
+        x_ref, i_ref = h.solve(b)
+        assert h.num_hierarchies()[0] == max_hrc
+    live1, made1 = alloc_stats()
+    assert live1 == live0 and i_ref.converged
+    for _ in range(3):
+        with bc.Handle(A, p, ext) as h:
+            x, info = h.solve(b)
+        assert info.iters == i_ref.iters and np.array_equal(x, x_ref)
+    total = made1 - made0
+    assert total > 10
+    try:
+        for k in range(total):
+            lib.bcmg_debug_fail_alloc(k)
+            with pytest.raises(bc.BcmgError) as e:
+                with bc.Handle(A, p, ext) as h:
+                    h.solve(b)
+            assert e.value.status == ERR_ALLOC and "injected" in str(e.value), (k, str(e.value))
+            assert alloc_stats()[0] == live0, f"allocation {k}: device memory leaked"
+    finally:
+        lib.bcmg_debug_fail_alloc(-1)
+    with bc.Handle(A, p, ext) as h:
+        x, info = h.solve(b)
+    assert info.iters == i_ref.iters and np.array_equal(x, x_ref)
+    assert alloc_stats()[0] == live0
+
+
 def test_batched_state_allocation_failure_leaves_handle_usable():
     A = wl.poisson(7, 16, 16, 16)
     B = np.asfortranarray(wl.vector(1, 3, A.n * 4).reshape(A.n, 4, order="F"))
