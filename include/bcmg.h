@@ -188,7 +188,10 @@ void        bcmg_ext_default(bcmg_ext *e);
  * (solve() lines src/SOLVER/solver.cu:37-62: BootBuildData::initByParams,
  * ApplyData::setGridSweeps, Bootstrap::bootstrap).  The handle owns all
  * device memory.  bcmg_setup_device: same, the CSR already resident in device
- * memory (the library copies it). */
+ * memory (the library copies it).  For inputs of 131,072 rows and more the
+ * setup starts one helper thread and one stream of its own, which build the
+ * coarse levels' solve copies while the setup goes on coarsening; both end
+ * before the call returns. */
 bcmg_status bcmg_setup(const bcmg_csr *A, const bcmg_params *p,
                        const bcmg_ext *ext, bcmg_handle **out);
 bcmg_status bcmg_setup_device(int32_t n, int32_t nnz, const int32_t *d_row,
