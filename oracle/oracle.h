@@ -9,8 +9,9 @@
  * with CUDA 12 (legacy cuSPARSE routines).  oracle/ref/ compiles its sources
  * with a compatibility shim into oracle/_ref/libref.so, which pins this
  * restatement where the reference's own code could run: one matching +
- * aggregation sweep recorded on a B200 (tests/golden/, checked by
- * tests/test_ref_fixtures.py), and its host code run on the CPU
+ * aggregation sweep recorded on a B200 and the reference's sequential suitor
+ * matcher on three more inputs with tie-free weights (tests/golden/, checked
+ * by tests/test_ref_fixtures.py), and its host code run on the CPU
  * (tests/test_ref_io.py: the Matrix-Market reader and writer, the settings
  * file, the coarsest-size rule and the grid-sweep table).  The rest is
  * pinned by the reference's own invariants (a valid symmetric matching,

@@ -12,6 +12,10 @@
 //                       src/matrix/matrixIO.cu:4-192) and writer
 //                       (CSRMatrixPrintMM, matrixIO.cu:290-333): host code
 //                       only, so the CPU tests call them;
+//   ref_cpu_suitor      the reference's sequential suitor matching
+//                       (approx_match_cpu_suitor, src/AMG/suitor.cu:455-526):
+//                       a host loop (it takes and returns device arrays, so
+//                       it runs where a GPU is, but launches no kernel);
 //   ref_params_from_file / ref_max_coarse_size / ref_grid_sweeps
 //                       the settings-file reader (AMG::Params::initFromFile,
 //                       src/AMG/AMG.cu:480-526; it exits on an invalid value,
@@ -81,6 +85,22 @@ int ref_pair_aggregate(int n, int nnz, const int *row, const int *col, const dou
   CSRm::free(A);
   matchingAggregationContext::freeContext();
   drop_host_wrapper(Ah);
+  return static_cast<int>(cudaDeviceSynchronize());
+}
+
+// suitor[v] = the vertex whose offer v holds (-1: none) for the weight
+// matrix W (n x n CSR, no diagonal); the reference compares weights with an
+// absolute tolerance (MY_GT, suitor.cu:458-459), so only inputs whose
+// weights within a row are further apart than that give the exact rule.
+int ref_cpu_suitor(int n, int nnz, const int *row, const int *col, const double *W,
+                   int *suitor) {
+  CSR *Wh = wrap_host(n, nnz, row, col, W);
+  CSR *Wd = CSRm::copyToDevice(Wh);
+  vector<int> *s = approx_match_cpu_suitor<double>(Wd);
+  cudaMemcpy(suitor, s->val, sizeof(int) * n, cudaMemcpyDeviceToHost);
+  Vector::free(s);
+  CSRm::free(Wd);
+  drop_host_wrapper(Wh);
   return static_cast<int>(cudaDeviceSynchronize());
 }
 

@@ -19,7 +19,16 @@ tests/golden/make_ref_fixtures.py).  On the same inputs the oracle must give:
     the oracle's Galerkin values are checked against scipy's P^T A P of the
     same P instead.
 
-Only pair_poisson7_12 exists: on the next input (27-point Poisson 8^3) the
+The suitor_*.npz fixtures pin the matching rule on more inputs (a random
+geometric graph Laplacian, a 2-D anisotropic FV matrix, a 7-point grid, each
+with a random smooth vector): the reference's sequential suitor matcher
+(approx_match_cpu_suitor, src/AMG/suitor.cu:455-526, a host loop) run on the
+oracle's weights.  That matcher compares with an absolute tolerance, so the
+inputs were kept only where the weights within each row are more than ten
+times that tolerance apart; on them its result is the exact rule's, and the
+oracle's matching must equal it.
+
+Only pair_poisson7_12 exercises the reference's kernels: on the next input (27-point Poisson 8^3) the
 reference's matching-and-aggregation call did not finish within 900 s on a
 B200, and its
 stock solve() stopped with an illegal memory access (src/matrix/CSR.cu:140),
@@ -32,6 +41,7 @@ import numpy as np
 import pytest
 
 import bootcmatchg_b200 as bc
+import workloads as wl
 from oracle import oracle as orc
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -55,8 +65,12 @@ def canonical(agg):
     return rank[agg]
 
 
+SUITOR = sorted(glob.glob(os.path.join(GOLDEN, "suitor_*.npz")))
+
+
 def test_fixtures_present():
     assert len(PAIR) >= 1
+    assert len(SUITOR) >= 3
 
 
 @pytest.mark.parametrize("path", PAIR, ids=[os.path.basename(p)[5:-4] for p in PAIR])
@@ -86,3 +100,42 @@ def test_oracle_matches_reference_kernels(path):
     ref = (P.T @ A.to_scipy() @ P).toarray()
     ours = sp.csr_matrix((cval, ccol, crow), shape=(nc, nc)).toarray()
     assert np.abs(ours - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+
+def _fixture_cases():
+    """The generator's case table (tests/golden/make_ref_fixtures.py)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "make_ref_fixtures", os.path.join(GOLDEN, "make_ref_fixtures.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    return mk
+
+
+@pytest.mark.parametrize("path", SUITOR, ids=[os.path.basename(p)[7:-4] for p in SUITOR])
+def test_oracle_matching_equals_reference_suitor(path):
+    """suitor[v] of the reference = the vertex whose offer v holds.  The
+    input is rebuilt from the seeded generators (checked against the
+    fixture's checksum) and W from the oracle; every held offer is mutual
+    (the matching), and the pairs are the oracle's: its greedy rule on W and
+    its suitor restatement on (A, w)."""
+    mk = _fixture_cases()
+    f = np.load(path)
+    name = os.path.basename(path)[:-4]
+    make, wseed = {c[0]: (c[1], c[2]) for c in mk.SUITOR_CASES}[name]
+    A = make()
+    assert A.nnz == int(f["nnz"]) and float(A.val.sum()) == float(f["val_sum"])
+    assert wseed == int(f["wseed"])
+    w = np.abs(wl.vector(1, wseed, A.n)) + 0.1
+    o = orc.pair_aggregate(A, w)
+    wrow, _, wval = mk.off_diagonal(A, o["W"])
+    assert mk.min_row_gap(wrow, wval) > mk.MIN_ROW_GAP  # no tie the tolerance could blur
+    n = A.n
+    s = f["suitor"]
+    assert s.shape == (n,) and s.min() >= -1 and s.max() < n
+    held = s >= 0
+    assert np.array_equal(s[s[held]], np.arange(n)[held]), "an offer is not mutual"
+    ref_match = np.where(held, s, -1)
+    assert np.array_equal(orc.greedy_match(A, o["W"]), ref_match), "greedy differs"
+    assert np.array_equal(o["match"], ref_match), "oracle matching differs from the reference"
