@@ -341,8 +341,11 @@ __device__ __forceinline__ void sort_row_regs(int32_t i, int32_t b, int T, doubl
 // kSortRowsPerWarp consecutive rows, in registers: when both rows have at
 // most 32 entries their weights (and the gathers behind them) are computed
 // before either is ordered, so the two rows' dependent loads overlap (the
-// pass is latency-bound); rows longer than kSortRegMax are queued for
-// k_sort_prefs_long.
+// pass is latency-bound).  Longer rows are queued: up to kSortRegMax entries
+// for k_sort_prefs_mid (2 or 4 entries per lane), beyond that for
+// k_sort_prefs_long.  Keeping the multi-register sorts out of this kernel
+// keeps its register count, and so the warps it has in flight, at what the
+// rows of at most 32 entries need.
 constexpr int kSortRowsPerWarp = 2;
 
 __device__ __forceinline__ void sort_one_row(int32_t i, const int32_t *__restrict__ row,
@@ -351,20 +354,43 @@ __device__ __forceinline__ void sort_one_row(int32_t i, const int32_t *__restric
                                              const double *__restrict__ w,
                                              const double *__restrict__ C, double den,
                                              double *W_out, double *sW, int32_t *scol,
-                                             int32_t *inv, int32_t *ucnt, int32_t *long_rows,
+                                             int32_t *inv, int32_t *ucnt, int32_t *mid_rows,
+                                             int32_t *n_mid, int32_t *long_rows,
                                              int32_t *n_long, int lane) {
   const int32_t b = row[i], T = row[i + 1] - b;
   if (T > kSortRegMax) {
     if (lane == 0) long_rows[atomicAdd(n_long, 1)] = i;
     return;
   }
-  const double ci = C[i], wi = w[i];
-  if (T <= 32)
-    sort_row_regs<1>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
-  else if (T <= 64)
-    sort_row_regs<2>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
-  else
-    sort_row_regs<4>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+  if (T > 32) {
+    if (lane == 0) mid_rows[atomicAdd(n_mid, 1)] = i;
+    return;
+  }
+  sort_row_regs<1>(i, b, T, C[i], w[i], col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+}
+
+// The queued rows of 33..kSortRegMax entries, one warp per row (warps take
+// queue entries q, q + all warps, ...).
+__global__ void __launch_bounds__(kSortWarps * 32)
+    k_sort_prefs_mid(const int32_t *__restrict__ mid_rows, const int32_t *__restrict__ n_mid,
+                     const int32_t *__restrict__ row, const int32_t *__restrict__ col,
+                     const double *__restrict__ val, const double *__restrict__ w,
+                     const double *__restrict__ C,
+                     const unsigned long long *__restrict__ min_bits, double *W_out,
+                     double *sW, int32_t *scol, int32_t *inv, int32_t *ucnt) {
+  const int lane = threadIdx.x & 31;
+  const int32_t nq = *n_mid;
+  const int32_t warps = static_cast<int32_t>(gridDim.x) * kSortWarps;
+  const double den = 0.999 * __longlong_as_double(static_cast<long long>(*min_bits));
+  for (int32_t q = blockIdx.x * kSortWarps + (threadIdx.x >> 5); q < nq; q += warps) {
+    const int32_t i = mid_rows[q];
+    const int32_t b = row[i], T = row[i + 1] - b;
+    const double ci = C[i], wi = w[i];
+    if (T <= 64)
+      sort_row_regs<2>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+    else
+      sort_row_regs<4>(i, b, T, ci, wi, col, val, w, C, den, W_out, sW, scol, inv, ucnt, lane);
+  }
 }
 
 __global__ void __launch_bounds__(kSortWarps * 32)
@@ -372,8 +398,8 @@ __global__ void __launch_bounds__(kSortWarps * 32)
                  const double *__restrict__ val, const double *__restrict__ w,
                  const double *__restrict__ C,
                  const unsigned long long *__restrict__ min_bits, double *W_out, double *sW,
-                 int32_t *scol, int32_t *inv, int32_t *ucnt, int32_t *long_rows,
-                 int32_t *n_long) {
+                 int32_t *scol, int32_t *inv, int32_t *ucnt, int32_t *mid_rows,
+                 int32_t *n_mid, int32_t *long_rows, int32_t *n_long) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int32_t i0 = (blockIdx.x * kSortWarps + wid) * kSortRowsPerWarp;
   if (i0 >= n) return;
@@ -392,11 +418,11 @@ __global__ void __launch_bounds__(kSortWarps * 32)
     order_row<1>(i1, e0, T1, w1, t1, col, sW, scol, inv, ucnt, lane);
     return;
   }
-  sort_one_row(i0, row, col, val, w, C, den, W_out, sW, scol, inv, ucnt, long_rows, n_long,
-               lane);
+  sort_one_row(i0, row, col, val, w, C, den, W_out, sW, scol, inv, ucnt, mid_rows, n_mid,
+               long_rows, n_long, lane);
   if (i1 < n)
-    sort_one_row(i1, row, col, val, w, C, den, W_out, sW, scol, inv, ucnt, long_rows, n_long,
-                 lane);
+    sort_one_row(i1, row, col, val, w, C, den, W_out, sW, scol, inv, ucnt, mid_rows, n_mid,
+                 long_rows, n_long, lane);
 }
 
 // Same for the queued long rows, one block per row in shared memory: each
@@ -1900,7 +1926,7 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   phase_tick("weights");
   // Preference-sorted rows, then the suitor proposals.
   DevBuf<double> sW;
-  DevBuf<int32_t> scol, inv, ucnt, next, long_rows, n_long;
+  DevBuf<int32_t> scol, inv, ucnt, next, long_rows, mid_rows, n_queued;
   DevBuf<unsigned long long> E;
   DevBuf<int> nonsym;
   BCMG_TRY(sW.alloc(A.nnz, s));
@@ -1910,22 +1936,29 @@ bcmg_status pair_aggregate(const CsrView &A, const double *w, int32_t *agg, doub
   BCMG_TRY(ucnt.alloc(n, s));
   BCMG_TRY(next.alloc(n, s));
   BCMG_TRY(long_rows.alloc(n, s));
-  BCMG_TRY(n_long.alloc(1, s));
+  BCMG_TRY(mid_rows.alloc(n, s));
+  BCMG_TRY(n_queued.alloc(2, s));  // [0] rows queued for the long sort, [1] for the mid sort
   BCMG_TRY(nonsym.alloc(1, s));
-  BCMG_CUDA(cudaMemsetAsync(n_long.get(), 0, sizeof(int32_t), s));
+  int32_t *n_long = n_queued.get(), *n_mid = n_queued.get() + 1;
+  BCMG_CUDA(cudaMemsetAsync(n_queued.get(), 0, 2 * sizeof(int32_t), s));
   BCMG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
   BCMG_CUDA(cudaMemsetAsync(nonsym.get(), 0, sizeof(int), s));
   launch(k_sort_prefs, ceil_div(n, kSortWarps * kSortRowsPerWarp), kSortWarps * 32, 0, s, n,
          A.row, A.col, A.val,
          w, C.get(), minb.get(), W_out, sW.get(), scol.get(), inv.get(), ucnt.get(),
-         long_rows.get(), n_long.get());
+         mid_rows.get(), n_mid, long_rows.get(), n_long);
+  // Rows of 33..kSortRegMax entries: a grid of a few warps per SM walks the
+  // queue (its length stays on the device).
+  launch(k_sort_prefs_mid, std::min(ceil_div(n, kSortWarps), 4 * kNumSM), kSortWarps * 32, 0,
+         s, mid_rows.get(), n_mid, A.row, A.col, A.val, w, C.get(), minb.get(), W_out,
+         sW.get(), scol.get(), inv.get(), ucnt.get());
   {
     const size_t smem = (sizeof(double) + sizeof(int32_t)) * kSortCapLong;
     BCMG_CUDA(cudaFuncSetAttribute(k_sort_prefs_long,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(smem)));
     launch(k_sort_prefs_long, std::min(n, kNumSM), 256, smem, s, long_rows.get(),
-           n_long.get(), A.row, A.col, A.val, w, C.get(), minb.get(), W_out, sW.get(),
+           n_long, A.row, A.col, A.val, w, C.get(), minb.get(), W_out, sW.get(),
            scol.get(), inv.get(), ucnt.get(), err.get());
     BCMG_LAUNCH_CHECK();
   }
