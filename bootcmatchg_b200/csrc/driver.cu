@@ -173,8 +173,13 @@ class SideBuilder {
   bcmg_status build(Item &it) {
     BCMG_CUDA(cudaStreamWaitEvent(stream_, it.ready, 0));
     it.out.wait_ns = it.wait_ns;
-    BCMG_TRY(sliced_build(it.A, it.vtype, &it.out, stream_, it.narrow));
-    BCMG_CUDA(cudaStreamSynchronize(stream_));
+    const bcmg_status st = sliced_build(it.A, it.vtype, &it.out, stream_, it.narrow);
+    // Also after a failure: drain() releases a partial copy on the handle's
+    // stream, so nothing queued here may still be writing it.
+    const cudaError_t e = cudaStreamSynchronize(stream_);
+    if (st != BCMG_OK) return st;
+    if (e != cudaSuccess)
+      return set_error(BCMG_ERR_CUDA, "%s", cudaGetErrorString(e));
     return BCMG_OK;
   }
 
