@@ -5,6 +5,8 @@ against the reference's own correctness invariants (src/utility/eval.cu:
 131-212, src/AMG/suitor.cu:395-425), independent scipy computations and
 hand-checked known answers.
 """
+import math
+
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -470,3 +472,127 @@ def test_load_rejects_missing_and_foreign_files(tmp_path):
     f.write_bytes(b"NOTAHRCFILE" + bytes(64))
     with pytest.raises(bc.BcmgError, match="IO"):
         bc.Handle.load(f)
+
+
+# ---------------------------------------------------------------------------
+# The matching weights, the matching and the pairwise aggregation restated a
+# second time, in plain Python on small graphs, as the reference states them:
+#   C_i = a_ii w_i^2 (first diagonal entry)          _makeC, matching.cu:141-162
+#   AH_ij = 1 - (2 a_ij) w_i w_j / (C_i + C_j), or DBL_EPSILON when
+#           C_i + C_j <= DBL_EPSILON                   _makeAH_warp, matching.cu:200-238
+#   W_ij = log(|AH_ij| / (0.999 min |AH|))            _make_w / find_Max_Min,
+#                                                     matching.cu:387-431
+#   matching: greedy on (W, max id, min id), usable W > 0 (suitor.cu:134,
+#           118-214 with the ties broken by id)
+#   aggregates: _aggregate_symmetric, matchingAggregation.cu:92-137, numbered
+#           by ascending master (smallest) vertex.
+EPS = np.finfo(np.float64).eps
+
+
+def py_weights(A, w):
+    n = A.n
+    C = [0.0] * n
+    for i in range(n):
+        for j in range(A.row[i], A.row[i + 1]):
+            if A.col[j] == i:
+                C[i] = float(A.val[j]) * (float(w[i]) * float(w[i]))
+                break
+    ah = {}
+    for i in range(n):
+        for j in range(A.row[i], A.row[i + 1]):
+            c = int(A.col[j])
+            if c == i:
+                continue
+            norm = C[i] + C[c]
+            if norm > EPS:
+                ah[j] = 1.0 - ((2.0 * float(A.val[j])) * (float(w[i]) * float(w[c]))) / norm
+            else:
+                ah[j] = EPS
+    W = np.zeros(A.nnz)
+    if ah:
+        den = np.float64(0.999) * np.float64(min(abs(v) for v in ah.values()))
+        for j, v in ah.items():
+            with np.errstate(divide="ignore", invalid="ignore"):
+                q = float(np.float64(abs(v)) / den)  # inf or NaN when min |AH| = 0
+            # math.log is the C library's log, as in the oracle (NumPy's own
+            # vectorised log can differ in the last bit)
+            W[j] = math.log(q) if q > 0.0 else (-math.inf if q == 0.0 else math.nan)
+    return W
+
+
+def py_greedy(A, W):
+    edges = []
+    for i in range(A.n):
+        for j in range(A.row[i], A.row[i + 1]):
+            c = int(A.col[j])
+            if c > i and W[j] > 0.0:  # NaN is not > 0
+                edges.append((float(W[j]), c, i))
+    edges.sort(reverse=True)
+    m = [-1] * A.n
+    for _, hi, lo in edges:
+        if m[hi] < 0 and m[lo] < 0:
+            m[hi], m[lo] = lo, hi
+    return np.array(m, np.int32)
+
+
+def py_aggregate(m, w):
+    n = len(m)
+    master = {}  # vertex -> (master vertex, p)
+    for v in range(n):
+        u = int(m[v])
+        if u >= 0:
+            norm = np.sqrt(np.float64(w[v]) * w[v] + np.float64(w[u]) * w[u])
+            if norm > EPS:
+                master[v] = (min(u, v), np.float64(w[v]) / norm)
+                continue
+        av = abs(np.float64(w[v]))
+        master[v] = (v, np.float64(w[v]) / av if av > EPS else 0.0)
+    heads = sorted({mv for mv, _ in master.values()})
+    num = {h: k for k, h in enumerate(heads)}
+    agg = np.array([num[master[v][0]] for v in range(n)], np.int32)
+    p = np.array([master[v][1] for v in range(n)])
+    return agg, p, len(heads)
+
+
+def small_graph(rng):
+    n = int(rng.integers(2, 17))
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j in range(i + 1, n):
+            if rng.random() < 0.35:
+                a = float(rng.choice([-1.0, -1.0, -2.0, -0.5, 1.0]))
+                rows += [i, j]
+                cols += [j, i]
+                vals += [a, a]
+    off = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+    rs = np.asarray(abs(off).sum(axis=1)).ravel()
+    diag = rs + rng.choice([0.0, 1.0, 0.5], size=n)
+    diag[diag == 0.0] = 1.0
+    A = bc.CsrMatrix.from_scipy((off + sp.diags(diag)).tocsr())
+    kind = int(rng.integers(0, 4))
+    if kind == 0:
+        w = np.ones(n)
+    elif kind == 1:
+        w = rng.standard_normal(n)
+    elif kind == 2:  # zeros and tiny entries: bad singles and bad pairs
+        w = rng.choice([0.0, 1e-17, 1.0, -2.0], size=n)
+    else:
+        w = rng.choice([1.0, 2.0], size=n)  # many equal weights
+    return A, w
+
+
+def test_matching_and_aggregates_restated_in_python_on_small_graphs():
+    rng = np.random.default_rng(2026)
+    for case in range(400):
+        A, w = small_graph(rng)
+        r = orc.pair_aggregate(A, w)
+        W = py_weights(A, w)
+        assert np.array_equal(np.isnan(W), np.isnan(r["W"])), case
+        ok = ~np.isnan(W)
+        assert np.array_equal(W[ok], r["W"][ok]), f"case {case}: weights differ"
+        m = py_greedy(A, W)
+        assert np.array_equal(r["match"], m), f"case {case}: matching differs"
+        agg, p, nc = py_aggregate(m, w)
+        assert r["nc"] == nc, case
+        assert np.array_equal(r["agg"], agg), f"case {case}: aggregates differ"
+        assert np.array_equal(r["p"], p), f"case {case}: prolongator values differ"
