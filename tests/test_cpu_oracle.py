@@ -596,3 +596,43 @@ def test_matching_and_aggregates_restated_in_python_on_small_graphs():
         assert r["nc"] == nc, case
         assert np.array_equal(r["agg"], agg), f"case {case}: aggregates differ"
         assert np.array_equal(r["p"], p), f"case {case}: prolongator values differ"
+
+
+def py_galerkin(A, agg, p, nc):
+    """A_c = P^T A P with P one entry per row (column agg[i], value p[i]):
+    for coarse row I, every term (p_i p_j) a_ij of a member i of I, summed
+    per coarse column J in ascending (min(i, j), max(i, j), i) order from
+    the first term -- the canonical order the oracle and the GPU use in
+    place of nsparse's FP64 shared-memory atomics
+    (kernel_spgemm_hash_d.cu:1035-1075)."""
+    rows = []
+    for I in range(nc):
+        terms = []
+        for i in range(A.n):
+            if agg[i] != I:
+                continue
+            for e in range(A.row[i], A.row[i + 1]):
+                j = int(A.col[e])
+                terms.append((int(agg[j]), min(i, j), max(i, j), i,
+                              (float(p[i]) * float(p[j])) * float(A.val[e])))
+        terms.sort(key=lambda t: t[:4])
+        row = {}
+        for J, _, _, _, t in terms:
+            row[J] = t if J not in row else row[J] + t
+        rows.append(sorted(row.items()))
+    crow = np.zeros(nc + 1, np.int32)
+    crow[1:] = np.cumsum([len(r) for r in rows])
+    ccol = np.array([J for r in rows for J, _ in r], np.int32)
+    cval = np.array([v for r in rows for _, v in r])
+    return crow, ccol, cval
+
+
+def test_galerkin_restated_in_python_on_small_graphs():
+    rng = np.random.default_rng(7)
+    for case in range(300):
+        A, w = small_graph(rng)
+        r = orc.pair_aggregate(A, w)
+        crow, ccol, cval = orc.galerkin(A, r["agg"], r["p"], r["nc"])
+        prow, pcol, pval = py_galerkin(A, r["agg"], r["p"], r["nc"])
+        assert np.array_equal(crow, prow) and np.array_equal(ccol, pcol), case
+        assert np.array_equal(cval, pval), f"case {case}: Galerkin values differ"
