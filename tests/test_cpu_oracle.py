@@ -636,3 +636,121 @@ def test_galerkin_restated_in_python_on_small_graphs():
         prow, pcol, pval = py_galerkin(A, r["agg"], r["p"], r["nc"])
         assert np.array_equal(crow, prow) and np.array_equal(ccol, pcol), case
         assert np.array_equal(cval, pval), f"case {case}: Galerkin values differ"
+
+
+# ---------------------------------------------------------------------------
+# One preconditioner application restated in plain Python on a small
+# two-hierarchy, four-level problem (the least on which the H- and W-cycles
+# differ), from the oracle's own levels:
+#   sweep    u <- ((-(A u)_i + f_i) / d_i) + u_i      _jacobi_it, relaxation.cu:176-209
+#   cycle    pre-sweeps, Res = Rhs - A X, Rhs_c = R Res (members ascending),
+#            X_c = 0, grid_sweeps[l] coarse cycles (one on the last coarse
+#            level), X += P X_c, post-sweeps; coarsest: relaxnumber_coarse
+#            sweeps                                    GAMG_cycle.cu:25-140
+#   table    V all 1; H 2 on even levels; W 2 but on the last
+#                                                      ApplyData::setGridSweeps, AMG.cu:371-394
+#   composite multiplicative / symmetrized / additive preconditionApply, FCG.cu:112-187
+def py_sweeps(lv, d, f, u, k):
+    row, col, val = lv["row"], lv["col"], lv["val"]
+    n = lv["n"]
+    for _ in range(k):
+        new = [0.0] * n
+        for i in range(n):
+            t = 0.0
+            for j in range(row[i], row[i + 1]):
+                t += val[j] * u[col[j]]
+            new[i] = ((-t + f[i]) / d[i]) + u[i]
+        u[:] = new
+
+
+def py_cycle(levels, prm, gs, rhs, x, l):
+    L = len(levels)
+    lv = levels[l - 1]
+    if l == L:
+        d = lv["D"] if prm.coarse_solver == 0 else lv["M"]
+        py_sweeps(lv, d, rhs[l - 1], x[l - 1], prm.relaxnumber_coarse)
+        return
+    d = lv["D"] if prm.relax_type == 0 else lv["M"]
+    py_sweeps(lv, d, rhs[l - 1], x[l - 1], prm.prerelax_sweeps)
+    row, col, val = lv["row"], lv["col"], lv["val"]
+    res = [0.0] * lv["n"]
+    for i in range(lv["n"]):
+        t = 0.0
+        for j in range(row[i], row[i + 1]):
+            t += val[j] * x[l - 1][col[j]]
+        res[i] = rhs[l - 1][i] - t
+    nc, agg, p = lv["n_coarse"], lv["agg"], lv["p"]
+    members = [[] for _ in range(nc)]
+    for i in range(lv["n"]):
+        members[agg[i]].append(i)
+    rhs[l] = [0.0] * nc
+    for I in range(nc):
+        s = None
+        for i in members[I]:
+            t = p[i] * res[i]
+            s = t if s is None else s + t
+        rhs[l][I] = 0.0 if s is None else s
+    x[l] = [0.0] * nc
+    for _ in range(gs[l - 1]):
+        py_cycle(levels, prm, gs, rhs, x, l + 1)
+        if l == L - 1:
+            break
+    for i in range(lv["n"]):
+        x[l - 1][i] = x[l - 1][i] + p[i] * x[l][agg[i]]
+    py_sweeps(lv, d, rhs[l - 1], x[l - 1], prm.postrelax_sweeps)
+
+
+def py_precond(hier, prm, r, z):
+    ml = max(0, prm.max_levels - 1)
+    gs = [1] * max(ml, 1)
+    for i in range(ml):
+        if (prm.cycle_type == 1 and i % 2 == 0) or (prm.cycle_type == 2 and i < ml - 1):
+            gs[i] = 2
+
+    def run(levels, xin):
+        L = len(levels)
+        rhs, x = [None] * L, [None] * L
+        rhs[0], x[0] = list(r), list(xin)
+        py_cycle(levels, prm, gs, rhs, x, 1)
+        return x[0]
+
+    x = list(z)
+    if prm.solver_type in (0, 1):
+        order = list(range(len(hier)))
+        if prm.solver_type == 1:
+            order += order[::-1]
+        for k in order:
+            x = run(hier[k], x)
+        return x
+    xadd = [0.0] * len(x)
+    for levels in hier:
+        xk = run(levels, x)
+        xadd = [a + b for a, b in zip(xadd, xk)]
+    alpha = 1.0 / float(len(hier))
+    return [a * alpha for a in xadd]
+
+
+@pytest.mark.parametrize("solver_type", [0, 1, 2])
+@pytest.mark.parametrize("cycle_type", [0, 1, 2])
+def test_precond_apply_restated_in_python(solver_type, cycle_type):
+    A = wl.poisson(7, 16, 16, 16)
+    p = c1_params()
+    p.aggrsweeps, p.max_hrc, p.conv_ratio = 1, 2, 0.01
+    p.solver_type, p.cycle_type = solver_type, cycle_type
+    h = orc.OracleHandle(A, p)
+    nh = h.num_hierarchies()[0]
+    hier = []
+    for k in range(nh):
+        L = h.hierarchy_info(k)["num_levels"]
+        levels = []
+        for l in range(L):
+            lv = h.level(k, l)
+            levels.append({key: (v.tolist() if isinstance(v, np.ndarray) else v)
+                           for key, v in lv.items()})
+        hier.append(levels)
+    assert nh == 2 and min(len(lv) for lv in hier) >= 4
+    r = wl.vector(1, 31, A.n)
+    z0 = wl.vector(2, 32, A.n)
+    ours = h.precond_apply(r, z0)
+    ref = np.array(py_precond(hier, p, r.tolist(), z0.tolist()))
+    assert np.array_equal(ours, ref), np.abs(ours - ref).max()
