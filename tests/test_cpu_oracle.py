@@ -754,3 +754,92 @@ def test_precond_apply_restated_in_python(solver_type, cycle_type):
     ours = h.precond_apply(r, z0)
     ref = np.array(py_precond(hier, p, r.tolist(), z0.tolist()))
     assert np.array_equal(ours, ref), np.abs(ours - ref).max()
+
+
+# ---------------------------------------------------------------------------
+# Flexible CG restated in plain Python (flexibileConjugateGradients_v3,
+# src/SOLVER/FCG.cu:433-585): the first step (:464-495), then per iteration
+# z = B r from a zero iterate, three dots (_triple_innerproduct, :6-63),
+# theta = gamma / delta, delta = beta - gamma^2 / delta, theta2 = alpha /
+# delta, the merged updates (_double_merged_axpy, :88-98), the stop test on
+# the recursive residual and num_iter = iter + 1 (:569).  The oracle runs on
+# one thread so its dot products sum in index order, as here; the
+# preconditioner is the oracle's (restated above).
+def py_dot(a, b):
+    s = 0.0
+    for u, v in zip(a, b):
+        s += u * v
+    return s
+
+
+def py_spmv(A, x):
+    out = [0.0] * A.n
+    for i in range(A.n):
+        t = 0.0
+        for j in range(A.row[i], A.row[i + 1]):
+            t += float(A.val[j]) * x[int(A.col[j])]
+        out[i] = t
+    return out
+
+
+def py_fcg(A, h, b, rtol, itnlim):
+    n = A.n
+    B = lambda r: h.precond_apply(np.array(r), np.zeros(n)).tolist()  # noqa: E731
+    x = [0.0] * n
+    w = py_spmv(A, x)
+    r = [bi - wi for bi, wi in zip(b, w)]
+    delta0 = math.sqrt(py_dot(r, r))
+    v = B(r)
+    w = py_spmv(A, v)
+    alpha, beta = py_dot(r, v), py_dot(w, v)
+    delta = beta
+    theta = alpha / delta
+    x = [xi + theta * vi for xi, vi in zip(x, v)]
+    r = [ri - theta * wi for ri, wi in zip(r, w)]
+    l2 = math.sqrt(py_dot(r, r))
+    d, q = list(v), list(w)
+    it = 0
+    while True:
+        if it % 2 == 0:
+            zp, azp = d, q
+        else:
+            zp, azp = v, w
+        z = B(r)
+        az = py_spmv(A, z)
+        alpha, beta, gamma = py_dot(r, z), py_dot(az, z), py_dot(azp, z)
+        theta = gamma / delta
+        delta = beta - (gamma * gamma) / delta
+        theta2 = alpha / delta
+        for i in range(n):
+            zi = -theta * zp[i] + z[i]
+            z[i] = zi
+            x[i] = theta2 * zi + x[i]
+            ai = -theta * azp[i] + az[i]
+            az[i] = ai
+            r[i] = -theta2 * ai + r[i]
+        if it % 2 == 0:
+            v, w = z, az
+        else:
+            d, q = z, az
+        l2 = math.sqrt(py_dot(r, r))
+        it += 1
+        if not (l2 > rtol * delta0 and it < itnlim):
+            break
+    return np.array(x), it + 1, l2
+
+
+def test_fcg_restated_in_python():
+    A = wl.poisson(7, 10, 10, 10)
+    p = c1_params()
+    b = wl.vector(1, 41, A.n)
+    threads = orc.get_threads()
+    orc.set_threads(1)
+    try:
+        h = orc.OracleHandle(A, p)
+        x, info, st = h.solve(b)
+        xp, iters, l2 = py_fcg(A, h, b.tolist(), p.rtol, p.itnlim)
+    finally:
+        orc.set_threads(threads)
+    assert st == 0 and info["converged"]
+    assert info["iters"] == iters and info["residual"] == l2
+    assert np.array_equal(x, xp)
