@@ -843,3 +843,47 @@ def test_fcg_restated_in_python():
     assert st == 0 and info["converged"]
     assert info["iters"] == iters and info["residual"] == l2
     assert np.array_equal(x, xp)
+
+
+# ---------------------------------------------------------------------------
+# The bootstrap's inner iterations restated in plain Python
+# (Bootstrap::innerIterations, src/BOOT/bootstrap.cu:5-44, 15 iterations by
+# BootBuildData::initDefault, AMG.cu:407): x = 1, rhs = 0, x <- B(0, x)
+# fifteen times with the composite of the hierarchies built so far, the
+# ratio of successive A-norms (CSRm::vectorANorm, CSR.cu:360-368), and the
+# next hierarchy's smooth vector w = x / ||x||_A.  With max_hrc 3 the third
+# hierarchy is built from the w of the two-hierarchy composite, and the
+# final estimated ratio comes from the three-hierarchy composite.
+def py_inner_iterations(A, h):
+    n = A.n
+    anorm = lambda x: math.sqrt(py_dot(py_spmv(A, x), x))  # noqa: E731
+    x = [1.0] * n
+    normold = anorm(x)
+    conv = 1.0
+    for _ in range(15):
+        x = h.precond_apply(np.zeros(n), np.array(x)).tolist()
+        normnew = anorm(x)
+        conv = normnew / normold
+        normold = normnew
+    alpha = 1.0 / normnew
+    return conv, np.array([xi * alpha for xi in x])
+
+
+@pytest.mark.parametrize("solver_type", [0, 1, 2])
+def test_bootstrap_inner_iterations_restated_in_python(solver_type):
+    A = wl.poisson(7, 12, 12, 12)
+    threads = orc.get_threads()
+    orc.set_threads(1)
+    try:
+        hs = {}
+        for max_hrc in (2, 3):
+            p = c1_params()
+            p.max_hrc, p.conv_ratio, p.solver_type = max_hrc, 0.01, solver_type
+            hs[max_hrc] = orc.OracleHandle(A, p)
+        conv2, w2 = py_inner_iterations(A, hs[2])
+        conv3, _ = py_inner_iterations(A, hs[3])
+    finally:
+        orc.set_threads(threads)
+    assert hs[2].num_hierarchies() == (2, conv2)
+    assert hs[3].num_hierarchies() == (3, conv3)
+    assert np.array_equal(hs[3].level(2, 0)["w"], w2), "third hierarchy's smooth vector"
