@@ -16,7 +16,11 @@
  * file, the coarsest-size rule and the grid-sweep table).  The rest is
  * pinned by the reference's own invariants (a valid symmetric matching,
  * every vertex in one aggregate, P^T P = I on good aggregates,
- * A_c = P^T A P) and by hand-checked known answers in the tests.
+ * A_c = P^T A P), by hand-checked known answers, and by a second
+ * restatement in plain Python on small cases (weights, matching,
+ * aggregates, Galerkin, the cycle and composites, the bootstrap's inner
+ * iterations, flexible CG) that this code must equal bit for bit
+ * (tests/test_cpu_oracle.py).
  *
  * Every function follows the reference file:line cited beside it.  Where
  * the reference is nondeterministic (atomicAdd aggregate numbering, FP64
