@@ -650,6 +650,8 @@ def test_galerkin_restated_in_python_on_small_graphs():
 #   table    V all 1; H 2 on even levels; W 2 but on the last
 #                                                      ApplyData::setGridSweeps, AMG.cu:371-394
 #   composite multiplicative / symmetrized / additive preconditionApply, FCG.cu:112-187
+#   K-cycle  two inner flexible-CG steps per coarse level but the last
+#            (both of its branches are taken in the test case)
 def py_sweeps(lv, d, f, u, k):
     row, col, val = lv["row"], lv["col"], lv["val"]
     n = lv["n"]
@@ -691,13 +693,60 @@ def py_cycle(levels, prm, gs, rhs, x, l):
             s = t if s is None else s + t
         rhs[l][I] = 0.0 if s is None else s
     x[l] = [0.0] * nc
-    for _ in range(gs[l - 1]):
-        py_cycle(levels, prm, gs, rhs, x, l + 1)
+    if prm.cycle_type == 3:
         if l == L - 1:
-            break
+            py_cycle(levels, prm, gs, rhs, x, l + 1)
+        else:
+            py_kcycle_inner(levels, prm, gs, rhs, x, l)
+    else:
+        for _ in range(gs[l - 1]):
+            py_cycle(levels, prm, gs, rhs, x, l + 1)
+            if l == L - 1:
+                break
     for i in range(lv["n"]):
         x[l - 1][i] = x[l - 1][i] + p[i] * x[l][agg[i]]
     py_sweeps(lv, d, rhs[l - 1], x[l - 1], prm.postrelax_sweeps)
+
+
+def py_kcycle_inner(levels, prm, gs, rhs, x, c):
+    """Two flexible-CG steps on coarse level c (0-based) preconditioned by
+    the cycle from that level on a zero iterate (inneritkcycle and
+    preconditionApplyK, FCG.cu:590-723; stop after the first step when the
+    residual fell below 0.25 of its start, GAMG_cycle.cu:5)."""
+    lv = levels[c]
+    n = lv["n"]
+
+    def B(r):
+        rhs[c], x[c] = list(r), [0.0] * n
+        py_cycle(levels, prm, gs, rhs, x, c + 1)
+        return list(x[c])
+
+    def axpy(a, u, y):
+        return [a * ui + yi for ui, yi in zip(u, y)]
+
+    A = bc.CsrMatrix(n, np.array(lv["row"], np.int32), np.array(lv["col"], np.int32),
+                     np.array(lv["val"]))
+    w = list(rhs[c])
+    delta0 = math.sqrt(py_dot(w, w))
+    d0 = B(w)
+    delta_old = py_dot(w, d0)
+    v = py_spmv(A, d0)
+    tau = py_dot(d0, v)
+    assert delta_old > 0.0 and tau > 0.0
+    alpha = delta_old / tau
+    w = axpy(-alpha, v, w)
+    xk = [0.0] * n
+    if math.sqrt(py_dot(w, w)) <= 0.25 * delta0:
+        xk = axpy(alpha, d0, xk)
+    else:
+        d1 = B(w)
+        v1 = py_spmv(A, d1)
+        tau1, tau2, tau3 = py_dot(d1, v), py_dot(d1, v1), py_dot(d1, w)
+        tau4 = tau2 - (tau1 * tau1) / tau
+        alpha = alpha - (tau1 * tau3) / (tau * tau4)
+        xk = axpy(alpha, d0, xk)
+        xk = axpy(tau3 / tau4, d1, xk)
+    x[c] = xk
 
 
 def py_precond(hier, prm, r, z):
@@ -731,27 +780,31 @@ def py_precond(hier, prm, r, z):
 
 
 @pytest.mark.parametrize("solver_type", [0, 1, 2])
-@pytest.mark.parametrize("cycle_type", [0, 1, 2])
+@pytest.mark.parametrize("cycle_type", [0, 1, 2, 3])
 def test_precond_apply_restated_in_python(solver_type, cycle_type):
     A = wl.poisson(7, 16, 16, 16)
     p = c1_params()
     p.aggrsweeps, p.max_hrc, p.conv_ratio = 1, 2, 0.01
     p.solver_type, p.cycle_type = solver_type, cycle_type
-    h = orc.OracleHandle(A, p)
+    r = wl.vector(1, 31, A.n)
+    z0 = wl.vector(2, 32, A.n)
+    threads = orc.get_threads()
+    orc.set_threads(1)  # the K-cycle's dot products then sum in index order
+    try:
+        h = orc.OracleHandle(A, p)
+        ours = h.precond_apply(r, z0)
+    finally:
+        orc.set_threads(threads)
     nh = h.num_hierarchies()[0]
     hier = []
     for k in range(nh):
-        L = h.hierarchy_info(k)["num_levels"]
         levels = []
-        for l in range(L):
+        for l in range(h.hierarchy_info(k)["num_levels"]):
             lv = h.level(k, l)
             levels.append({key: (v.tolist() if isinstance(v, np.ndarray) else v)
                            for key, v in lv.items()})
         hier.append(levels)
     assert nh == 2 and min(len(lv) for lv in hier) >= 4
-    r = wl.vector(1, 31, A.n)
-    z0 = wl.vector(2, 32, A.n)
-    ours = h.precond_apply(r, z0)
     ref = np.array(py_precond(hier, p, r.tolist(), z0.tolist()))
     assert np.array_equal(ours, ref), np.abs(ours - ref).max()
 
