@@ -940,3 +940,84 @@ def test_bootstrap_inner_iterations_restated_in_python(solver_type):
     assert hs[2].num_hierarchies() == (2, conv2)
     assert hs[3].num_hierarchies() == (3, conv3)
     assert np.array_equal(hs[3].level(2, 0)["w"], w2), "third hierarchy's smooth vector"
+
+
+# ---------------------------------------------------------------------------
+# The suitor matching on asymmetric weights and unsymFix, restated in plain
+# Python.  Proposer x offers to the neighbour y of largest (W_xy, y) whose
+# held offer it beats under (W, proposer id); y keeps the better offer and
+# the displaced proposer searches again (kernel_for_matching / set_suitor,
+# suitor.cu:49-214).  A vertex's proposals do not depend on the offer it
+# holds, so proposers and receivers form a bipartite problem with strict
+# preferences: deferred acceptance ends in the same state in any proposal
+# order, which is why the restatement takes the proposers in a random order.
+# unsymFix (unsymMatching.cu:3-71): mutual suitors are matched; then each v
+# whose suitor u < v is unmatched claims u, resolved as if all claims ran in
+# lockstep (v gets u iff u is still free and no claimer targets v).
+def py_suitor(A, W, order):
+    n = A.n
+    s, ow = [-1] * n, [0.0] * n
+
+    def beats(wv, x, y):
+        return s[y] < 0 or wv > ow[y] or (wv == ow[y] and x > s[y])
+
+    for v in order:
+        cur = v
+        while True:
+            by, bw = -1, 0.0
+            for e in range(A.row[cur], A.row[cur + 1]):
+                y, we = int(A.col[e]), float(W[e])
+                if y == cur or not (we > 0.0) or not beats(we, cur, y):
+                    continue
+                if by < 0 or we > bw or (we == bw and y > by):
+                    by, bw = y, we
+            if by < 0:
+                break
+            prev = s[by]
+            s[by], ow[by] = cur, bw
+            if prev < 0:
+                break
+            cur = prev
+    return np.array(s, np.int32)
+
+
+def py_unsym_fix(s):
+    n = len(s)
+    m = [-1] * n
+    for v in range(n):
+        u = s[v]
+        if u >= 0 and s[u] == v:
+            m[v] = u
+    claimers = [v for v in range(n) if 0 <= s[v] < v and m[v] == -1]
+    targeted = {int(s[v]) for v in claimers}
+    m2 = list(m)
+    for v in claimers:
+        u = int(s[v])
+        if m[u] == -1 and v not in targeted:
+            m2[v], m2[u] = u, v
+    return np.array(m2, np.int32)
+
+
+def test_asymmetric_matching_restated_in_python_on_small_graphs():
+    rng = np.random.default_rng(11)
+    fixed = 0
+    for case in range(300):
+        n = int(rng.integers(2, 17))
+        S = sp.random(n, n, density=0.35, random_state=np.random.RandomState(case), format="csr")
+        S.data = -rng.choice([1.0, 2.0, 0.5, 3.0], size=S.nnz)  # asymmetric values
+        S.setdiag(0.0)
+        S.eliminate_zeros()
+        diag = np.asarray(abs(S).sum(axis=1)).ravel() + 1.0
+        A = bc.CsrMatrix.from_scipy((S + sp.diags(diag)).tocsr())
+        w = rng.standard_normal(n) if case % 2 else np.ones(n)
+        r = orc.pair_aggregate(A, w)
+        W = py_weights(A, w)
+        order = rng.permutation(n).tolist()
+        s = py_suitor(A, W, order)
+        assert np.array_equal(r["suitor"], s), f"case {case}: suitor array differs"
+        m = py_unsym_fix(s)
+        assert np.array_equal(r["match"], m), f"case {case}: unsymFix differs"
+        fixed += int((m >= 0).sum() > 2 * sum(1 for v in range(n) if s[v] >= 0 and s[s[v]] == v))
+        agg, p, nc = py_aggregate(m, w)
+        assert np.array_equal(r["agg"], agg) and np.array_equal(r["p"], p), case
+    assert fixed > 0  # pass 2 of unsymFix matched someone in some case
