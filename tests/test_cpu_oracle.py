@@ -1021,3 +1021,83 @@ def test_asymmetric_matching_restated_in_python_on_small_graphs():
         agg, p, nc = py_aggregate(m, w)
         assert np.array_equal(r["agg"], agg) and np.array_equal(r["p"], p), case
     assert fixed > 0  # pass 2 of unsymFix matched someone in some case
+
+
+# ---------------------------------------------------------------------------
+# Smoothed aggregation restated in plain Python (matchingAggregation.cu:
+# 353-390: matrixVectorScaling, infinityNorm, applyOmega, CSRCSR_product x3,
+# CSRm::T), with the products in the canonical order the oracle and the GPU
+# use in place of cuSPARSE's unspecified one: row i's terms x_ik y_kj in X's
+# row order, then Y's; stably sorted by column; each column summed from its
+# first term.
+def py_spgemm(X, Y):
+    """X, Y: (row, col, val) lists; returns C the same way."""
+    xr, xc, xv = X
+    yr, yc, yv = Y
+    crow, ccol, cval = [0], [], []
+    for i in range(len(xr) - 1):
+        t = []
+        for a in range(xr[i], xr[i + 1]):
+            k, x = xc[a], xv[a]
+            for b in range(yr[k], yr[k + 1]):
+                t.append((yc[b], x * yv[b]))
+        t.sort(key=lambda e: e[0])  # stable
+        q = 0
+        while q < len(t):
+            s, e = t[q][1], q + 1
+            while e < len(t) and t[e][0] == t[q][0]:
+                s = s + t[e][1]
+                e += 1
+            ccol.append(t[q][0])
+            cval.append(s)
+            q = e
+        crow.append(len(ccol))
+    return crow, ccol, cval
+
+
+def py_transpose(M, m):
+    """CSR transpose, rows of the result in increasing row order of M."""
+    r, c, v = M
+    rows = [[] for _ in range(m)]
+    for i in range(len(r) - 1):
+        for e in range(r[i], r[i + 1]):
+            rows[c[e]].append((i, v[e]))
+    tr, tc, tv = [0], [], []
+    for lst in rows:
+        tc += [i for i, _ in lst]
+        tv += [x for _, x in lst]
+        tr.append(len(tc))
+    return tr, tc, tv
+
+
+def test_smoothed_aggregation_restated_in_python():
+    A = wl.poisson(7, 16, 16, 16)
+    p = c1_params()
+    p.aggrtype = 1
+    h = orc.OracleHandle(A, p)
+    L = h.hierarchy_info(0)["num_levels"]
+    assert L >= 3
+    for j in range(L - 1):
+        f, c = h.level(0, j), h.level(0, j + 1)
+        n, nc = f["n"], f["n_coarse"]
+        row, col, val = f["row"].tolist(), f["col"].tolist(), f["val"].tolist()
+        D = f["D"].tolist()
+        sval, inf = [], 0.0
+        for i in range(n):
+            rs = 0.0
+            for e in range(row[i], row[i + 1]):
+                sval.append(val[e] / D[i])
+                rs = rs + abs(sval[-1])
+            inf = max(inf, rs)
+        omega = 4.0 / (3.0 * inf)
+        for i in range(n):
+            for e in range(row[i], row[i + 1]):
+                sval[e] = -omega * sval[e]
+                if col[e] == i:
+                    sval[e] = sval[e] + 1.0
+        Pt = (list(range(n + 1)), f["agg"].tolist(), f["p"].tolist())
+        P = py_spgemm((row, col, sval), Pt)
+        R = py_transpose(P, nc)
+        Ac = py_spgemm(py_spgemm(R, (row, col, val)), P)
+        assert c["row"].tolist() == Ac[0] and c["col"].tolist() == Ac[1], j
+        assert c["val"].tolist() == Ac[2], f"level {j + 1}: smoothed coarse values differ"
