@@ -1101,3 +1101,118 @@ def test_smoothed_aggregation_restated_in_python():
         Ac = py_spgemm(py_spgemm(R, (row, col, val)), P)
         assert c["row"].tolist() == Ac[0] and c["col"].tolist() == Ac[1], j
         assert c["val"].tolist() == Ac[2], f"level {j + 1}: smoothed coarse values differ"
+
+
+# ---------------------------------------------------------------------------
+# Level control restated in plain Python (matchingAggregation and
+# adaptiveCoarsening, matchingAggregation.cu:211-295, 298-423): aggrsweeps
+# pairwise sweeps per level, each on the previous sweep's Galerkin matrix
+# and restricted smooth vector (w_c = R w, members in ascending order),
+# composed into one prolongator (P = P P_i, one entry per row); ftcoarse
+# becomes 100 once a sweep coarsens by at most 1.2 and stays so; a level's
+# sweeps stop, and so does the hierarchy, once the coarse size is at most
+# ftcoarse * maxcoarsesize (= (int)(40 n^(1/3)), AMG.cu:309-311); at most
+# max_levels levels.  Built from the restatements above.
+def py_coarsen(A, w, prm):
+    n0 = A.n
+    maxcoarse = int(40 * n0 ** (1.0 / 3.0))
+    levels = [{"A": A, "w": list(w)}]
+    ftcoarse = 1
+    if not math.sqrt(py_dot(py_spmv(A, list(w)), list(w))) > EPS:
+        return levels
+    cur_w = list(w)
+    level = 1
+    while level < prm.max_levels:
+        fine = levels[-1]
+        cur, wi_ = fine["A"], cur_w
+        agg_c, p_c = None, None
+        for sweep in range(prm.aggrsweeps):
+            W = py_weights(cur, wi_)
+            m = py_unsym_fix(py_suitor(cur, W, list(range(cur.n))))
+            ag, pv, nci = py_aggregate(m, wi_)
+            crow, ccol, cval = py_galerkin(cur, ag, pv, nci)
+            members = [[] for _ in range(nci)]
+            for i in range(cur.n):
+                members[ag[i]].append(i)
+            wi = []
+            for I in range(nci):
+                s = None
+                for i in members[I]:
+                    t = pv[i] * wi_[i]
+                    s = t if s is None else s + t
+                wi.append(s)
+            ratio = cur.n / nci
+            if sweep == 0:
+                agg_c, p_c = list(ag), list(pv)
+            else:
+                p_c = [p_c[i] * pv[agg_c[i]] for i in range(len(agg_c))]
+                agg_c = [int(ag[agg_c[i]]) for i in range(len(agg_c))]
+            cur = bc.CsrMatrix(nci, crow, ccol, cval)
+            wi_ = wi
+            if ratio <= 1.2:
+                ftcoarse = 100
+            if nci <= ftcoarse * maxcoarse:
+                break
+        fine["agg"], fine["p"], fine["nc"] = agg_c, p_c, cur.n
+        levels.append({"A": cur, "w": wi_})
+        cur_w = wi_
+        level += 1
+        if cur.n <= ftcoarse * maxcoarse:
+            break
+    return levels
+
+
+def py_galerkin_fast(A, agg, p, nc):
+    members = [[] for _ in range(nc)]
+    for i in range(A.n):
+        members[agg[i]].append(i)
+    crow, ccol, cval = [0], [], []
+    for I in range(nc):
+        terms = []
+        for i in members[I]:
+            for e in range(A.row[i], A.row[i + 1]):
+                j = int(A.col[e])
+                terms.append((int(agg[j]), min(i, j), max(i, j), i,
+                              (float(p[i]) * float(p[j])) * float(A.val[e])))
+        terms.sort(key=lambda t: t[:4])
+        row = {}
+        for J, _, _, _, t in terms:
+            row[J] = t if J not in row else row[J] + t
+        for J, v in sorted(row.items()):
+            ccol.append(J)
+            cval.append(v)
+        crow.append(len(ccol))
+    return (np.array(crow, np.int32), np.array(ccol, np.int32), np.array(cval))
+
+
+def weakly_coupled(n=3000, path=200):
+    """A path over the first `path` vertices, the rest uncoupled: a sweep
+    coarsens by at most 1.2, so ftcoarse becomes 100 and coarsening stops."""
+    off = sp.coo_matrix(([-1.0] * (path - 1), (list(range(path - 1)), list(range(1, path)))),
+                        shape=(n, n))
+    S = (off + off.T).tocsr()
+    diag = np.asarray(abs(S).sum(axis=1)).ravel() + 1.0
+    return bc.CsrMatrix.from_scipy((S + sp.diags(diag)).tocsr())
+
+
+@pytest.mark.parametrize("case,min_levels", [("rgg", 3), ("poisson7", 3), ("weak", 2)])
+def test_level_control_restated_in_python(case, min_levels, monkeypatch):
+    monkeypatch.setitem(globals(), "py_galerkin", py_galerkin_fast)
+    A = {"rgg": lambda: wl.rgg(3000, 5), "poisson7": lambda: wl.poisson(7, 16, 16, 16),
+         "weak": weakly_coupled}[case]()
+    p = c1_params()
+    h = orc.OracleHandle(A, p)
+    levels = py_coarsen(A, np.ones(A.n), p)
+    L = h.hierarchy_info(0)["num_levels"]
+    assert L == len(levels) and L >= min_levels
+    for l in range(L):
+        o = h.level(0, l)
+        A_l = levels[l]["A"]
+        assert o["n"] == A_l.n, l
+        assert np.array_equal(o["row"], A_l.row) and np.array_equal(o["col"], A_l.col), l
+        assert np.array_equal(o["val"], np.asarray(A_l.val)), f"level {l}: values differ"
+        assert np.array_equal(o["w"], np.array(levels[l]["w"])), f"level {l}: w differs"
+        if l + 1 < L:
+            assert o["n_coarse"] == levels[l]["nc"], l
+            assert np.array_equal(o["agg"], np.array(levels[l]["agg"])), l
+            assert np.array_equal(o["p"], np.array(levels[l]["p"])), l
