@@ -244,8 +244,11 @@ bcmg_status bcmg_batch_config(bcmg_handle *h, int32_t nrhs, int hrc, int level,
                               double *tune_ms);
 
 /* Device memory the handle holds, in bytes (hierarchies, their solve-phase
- * copies, cycle and Krylov work vectors, batch state). */
+ * copies, cycle and Krylov work vectors, batch state); no counterpart in the
+ * reference. */
 bcmg_status bcmg_device_bytes(const bcmg_handle *h, uint64_t *bytes);
+/* Frees everything the handle owns (the frees at the end of solve():
+ * CSRm::free, AMG::Hierarchy / Boot frees, src/SOLVER/solver.cu:120-126). */
 bcmg_status bcmg_destroy(bcmg_handle *h);
 
 /* ---- hierarchy files -------------------------------------------------------
@@ -311,14 +314,24 @@ bcmg_status bcmg_server_wait(bcmg_server *s, uint64_t ticket, double timeout_s,
 bcmg_status bcmg_server_stats_get(bcmg_server *s, bcmg_server_stats *out);
 /* Finishes every queued request, then frees the cache and the streams. */
 bcmg_status bcmg_server_destroy(bcmg_server *s);
-/* Binds the handle to a CUDA stream (cudaStream_t passed as void*). */
+/* Binds the handle to a CUDA stream (cudaStream_t passed as void*); no
+ * counterpart in the reference, which runs on the default stream with
+ * global handles (src/utility/handles.cu). */
 bcmg_status bcmg_set_stream(bcmg_handle *h, void *stream);
 /* z = B r for the composite preconditioner (preconditionApply,
  * src/SOLVER/FCG.cu:112-187) with z's initial content as initial guess.
  * Device pointers, n entries each. */
 bcmg_status bcmg_precond_apply(bcmg_handle *h, const double *d_r, double *d_z);
 
-/* ---- hierarchy introspection (parity tests, #META output) -------------- */
+/* ---- hierarchy introspection (parity tests, #META output) --------------
+ * What the reference prints rather than returns: the number of hierarchies
+ * and the estimated ratio (#META agg;hierarchy_levels_num and
+ * agg;final_estimated_ratio, src/SOLVER/solver.cu:106-107), per hierarchy
+ * the level count, operator complexities and average coarsening ratio
+ * (AMG::Hierarchy::finalize_cmplx / finalize_wcmplx / printInfo,
+ * src/AMG/AMG.cu:221-251, called at src/AMG/matchingAggregation.cu:404-414),
+ * and one level's data (hrrch->A_array / P_array and the relaxPrepare
+ * vectors). */
 bcmg_status bcmg_hierarchy_count(const bcmg_handle *h, int *num_hrc,
                                  double *estimated_ratio);
 bcmg_status bcmg_hierarchy_info(const bcmg_handle *h, int hrc, int *num_levels,
@@ -335,12 +348,14 @@ bcmg_status bcmg_level_copy(const bcmg_handle *h, int hrc, int level,
                             double *M, int32_t *agg, double *p, double *w);
 
 /* k smoother sweeps of one level exactly as the solve-phase cycle runs them
- * (relax_type's diagonal, the level's solve format and precision).  f and u
+ * (relax, src/AMG/relaxation.cu:357-377, with relax_type's diagonal, in the
+ * level's solve format and precision).  f and u
  * are device vectors of the level's size: FP64 for BCMG_PREC_FP64 handles,
  * FP32 for BCMG_PREC_MIXED handles.  Used to time the dominant kernel. */
 bcmg_status bcmg_level_relax(bcmg_handle *h, int hrc, int level, const void *d_f,
                              void *d_u, int k);
-/* Storage of one level's solve-phase copy: value slots (32 values each),
+/* Storage of one level's solve-phase copy (no counterpart in the reference,
+ * which solves from CSR): value slots (32 values each),
  * slots of slices with explicit columns (the rest share column offsets and
  * store no indices), slices, bytes per value (0: the level is solved from
  * CSR). */
