@@ -9,11 +9,17 @@
 // row's columns are sorted and duplicates summed (the reference keeps file
 // order although _makeAH_warp assumes sorted rows with a diagonal).
 #include <algorithm>
+#include <cctype>
 #include <cerrno>
+#include <charconv>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <numeric>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "host_util.h"
@@ -21,6 +27,28 @@
 namespace bcmg {
 
 static thread_local std::string g_last_error;
+
+// Threads for reading or writing `bytes` of matrix text: one per 4 MB, at
+// most the hardware's threads and 16.
+static int io_threads(size_t bytes) {
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  return static_cast<int>(std::min<size_t>({bytes / (size_t{4} << 20) + 1, hw, 16}));
+}
+
+// Runs f(t) for t = 0 .. T-1, t = 0 on the calling thread (a thread that
+// cannot be started runs its share on the caller too).
+template <typename F>
+static void run_threads(int T, const F &f) {
+  std::vector<std::thread> pool;
+  int started = 1;
+  try {
+    for (; started < T; ++started) pool.emplace_back(f, started);
+  } catch (...) {
+  }
+  for (int t = started; t < T; ++t) f(t);
+  f(0);
+  for (auto &th : pool) th.join();
+}
 
 bcmg_status set_error(bcmg_status code, const char *fmt, ...) {
   char buf[1024];
@@ -52,43 +80,60 @@ static bcmg_status coo_to_csr(int32_t n, int32_t m, std::vector<int32_t> &ci,
   for (size_t k = 0; k < nz; ++k) cnt[ci[k] + 1]++;
   for (int32_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
   std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-  std::vector<int32_t> col(nz);
-  std::vector<double> val(nz);
+  // Scatter into rows (file order within a row), then per row: a row whose
+  // columns already increase strictly is kept as it is; otherwise it is
+  // sorted by column (stable: duplicates keep file order) and duplicates are
+  // summed, in place.  Rows in parallel.
+  std::unique_ptr<int32_t[]> col(new int32_t[nz > 0 ? nz : 1]);
+  std::unique_ptr<double[]> val(new double[nz > 0 ? nz : 1]);
   for (size_t k = 0; k < nz; ++k) {
     int64_t p = pos[ci[k]]++;
     col[p] = cj[k];
     val[p] = cv[k];
   }
-  // Sort each row by column (stable: duplicates keep file order) and merge.
-  std::vector<int32_t> outrow(static_cast<size_t>(n) + 1, 0);
-  std::vector<int32_t> perm;
-  int64_t w = 0;
-  std::vector<int32_t> ocol(nz);
-  std::vector<double> oval(nz);
-  for (int32_t i = 0; i < n; ++i) {
-    int64_t b = cnt[i], e = cnt[i + 1];
-    perm.resize(e - b);
-    std::iota(perm.begin(), perm.end(), 0);
-    std::stable_sort(perm.begin(), perm.end(), [&](int32_t x, int32_t y) {
-      return col[b + x] < col[b + y];
-    });
-    int32_t last = -1;
-    for (int32_t t : perm) {
-      int32_t c = col[b + t];
-      if (c == last) {
-        oval[w - 1] += val[b + t];
-      } else {
-        ocol[w] = c;
-        oval[w] = val[b + t];
-        ++w;
-        last = c;
+  const int T = io_threads(nz * 16);
+  std::vector<int64_t> unique(static_cast<size_t>(n), 0);
+  run_threads(T, [&](int t) {
+    const int32_t i0 = static_cast<int32_t>(static_cast<int64_t>(n) * t / T);
+    const int32_t i1 = static_cast<int32_t>(static_cast<int64_t>(n) * (t + 1) / T);
+    std::vector<int32_t> perm, tcol;
+    std::vector<double> tval;
+    for (int32_t i = i0; i < i1; ++i) {
+      const int64_t b = cnt[i], e = cnt[i + 1];
+      bool increasing = true;
+      for (int64_t k = b + 1; k < e && increasing; ++k) increasing = col[k - 1] < col[k];
+      if (increasing) {
+        unique[i] = e - b;
+        continue;
       }
+      perm.resize(e - b);
+      std::iota(perm.begin(), perm.end(), 0);
+      std::stable_sort(perm.begin(), perm.end(), [&](int32_t x, int32_t y) {
+        return col[b + x] < col[b + y];
+      });
+      tcol.clear();
+      tval.clear();
+      for (int32_t q : perm) {
+        const int32_t c = col[b + q];
+        if (!tcol.empty() && tcol.back() == c) {
+          tval.back() += val[b + q];
+        } else {
+          tcol.push_back(c);
+          tval.push_back(val[b + q]);
+        }
+      }
+      std::copy(tcol.begin(), tcol.end(), col.get() + b);
+      std::copy(tval.begin(), tval.end(), val.get() + b);
+      unique[i] = static_cast<int64_t>(tcol.size());
     }
-    outrow[i + 1] = static_cast<int32_t>(w);
+  });
+  int64_t w = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    w += unique[i];
+    if (w > INT32_MAX)
+      return set_error(BCMG_ERR_INVALID_MATRIX, "nnz %lld exceeds int32",
+                       static_cast<long long>(w));
   }
-  if (w > INT32_MAX)
-    return set_error(BCMG_ERR_INVALID_MATRIX, "nnz %lld exceeds int32",
-                     static_cast<long long>(w));
   out->n = n;
   out->m = m;
   out->nnz = static_cast<int32_t>(w);
@@ -104,15 +149,158 @@ static bcmg_status coo_to_csr(int32_t n, int32_t m, std::vector<int32_t> &ci,
     out->val = nullptr;
     return set_error(BCMG_ERR_ALLOC, "host allocation of CSR failed");
   }
-  std::memcpy(out->row, outrow.data(), sizeof(int32_t) * (n + 1));
-  std::memcpy(out->col, ocol.data(), sizeof(int32_t) * w);
-  std::memcpy(out->val, oval.data(), sizeof(double) * w);
+  out->row[0] = 0;
+  for (int32_t i = 0; i < n; ++i) out->row[i + 1] = out->row[i] + static_cast<int32_t>(unique[i]);
+  run_threads(T, [&](int t) {
+    const int32_t i0 = static_cast<int32_t>(static_cast<int64_t>(n) * t / T);
+    const int32_t i1 = static_cast<int32_t>(static_cast<int64_t>(n) * (t + 1) / T);
+    for (int32_t i = i0; i < i1; ++i) {
+      std::copy(col.get() + cnt[i], col.get() + cnt[i] + unique[i], out->col + out->row[i]);
+      std::copy(val.get() + cnt[i], val.get() + cnt[i] + unique[i], out->val + out->row[i]);
+    }
+  });
   return BCMG_OK;
 }
 
 static void lower(char *s) {
   for (; *s; ++s)
     if (*s >= 'A' && *s <= 'Z') *s = static_cast<char>(*s - 'A' + 'a');
+}
+
+static inline bool mm_space(char c) {
+  return c == ' ' || c == '\t' || c == '\r' || c == '\n' || c == '\v' || c == '\f';
+}
+
+// One integer as %lld reads it: leading white space, an optional sign, at
+// least one digit (saturating on overflow); nullptr if there is none.
+static const char *scan_ll(const char *p, const char *e, long long *out) {
+  while (p < e && mm_space(*p)) ++p;
+  bool neg = false;
+  if (p < e && (*p == '+' || *p == '-')) neg = *p++ == '-';
+  if (p >= e || *p < '0' || *p > '9') return nullptr;
+  unsigned long long v = 0;
+  for (; p < e && *p >= '0' && *p <= '9'; ++p)
+    v = v > (ULLONG_MAX - 9) / 10 ? ULLONG_MAX : v * 10 + static_cast<unsigned>(*p - '0');
+  v = std::min(v, static_cast<unsigned long long>(LLONG_MAX));
+  *out = neg ? -static_cast<long long>(v) : static_cast<long long>(v);
+  return p;
+}
+
+// One number as %lf reads it (strtod's syntax): std::from_chars for the
+// usual forms, strtod where from_chars stops short of what strtod would
+// take (a hexadecimal float, a value out of range).  The text is
+// NUL-terminated, so strtod stays inside it.
+static const char *scan_double(const char *p, const char *e, double *out) {
+  while (p < e && mm_space(*p)) ++p;
+  if (p >= e) return nullptr;
+  const char *q = p;
+  if (*q == '+') {  // from_chars takes no plus sign
+    ++q;
+    if (q < e && (*q == '+' || *q == '-')) return nullptr;
+  }
+  double v = 0.0;
+  const auto r = std::from_chars(q, e, v);
+  const bool more = r.ptr < e && (std::isalnum(static_cast<unsigned char>(*r.ptr)) || *r.ptr == '.');
+  if (r.ec == std::errc() && !more) {
+    *out = v;
+    return r.ptr;
+  }
+  char *end = nullptr;
+  const double s = std::strtod(p, &end);
+  if (end == p) return nullptr;
+  *out = s;
+  return end;
+}
+
+// The first nz lines of `text` as Matrix-Market records "i j [v]" (1-based;
+// v = 1 for a pattern matrix), in file order, with the mirrored entry of an
+// off-diagonal record right after it for symmetric storage.  The text is cut
+// into line-aligned chunks parsed by threads.  *bad = the first malformed
+// record (-1: none); *lines = the lines the text has (fewer than nz: records
+// are missing).
+static void parse_records(const std::string &text, long long nz, bool pattern, bool symmetric,
+                          std::vector<int32_t> &ci, std::vector<int32_t> &cj,
+                          std::vector<double> &cv, long long *bad, long long *lines) {
+  const char *base = text.c_str();
+  const size_t size = text.size();
+  const int T = io_threads(size);
+  std::vector<size_t> cut(T + 1, size);
+  cut[0] = 0;
+  for (int t = 1; t < T; ++t) {
+    size_t c = std::max(cut[t - 1], size * static_cast<size_t>(t) / T);
+    while (c > 0 && c < size && base[c - 1] != '\n') ++c;
+    cut[t] = c;
+  }
+  // Lines per chunk (every chunk but the last ends just after a newline).
+  std::vector<long long> count(T, 0), first(T + 1, 0), tbad(T, -1);
+  run_threads(T, [&](int t) {
+    const char *p = base + cut[t], *e = base + cut[t + 1];
+    long long c = std::count(p, e, '\n');
+    if (e > p && e[-1] != '\n') ++c;
+    count[t] = c;
+  });
+  for (int t = 0; t < T; ++t) first[t + 1] = first[t] + count[t];
+  *lines = first[T];
+  // Every chunk writes its entries from `per` slots per record before it
+  // (one record gives at most `per` entries); a symmetric file's entries
+  // are compacted afterwards, chunk by chunk in file order.
+  const size_t per = symmetric ? 2 : 1;
+  const size_t records = static_cast<size_t>(std::min(first[T], nz));
+  ci.resize(records * per);
+  cj.resize(records * per);
+  cv.resize(records * per);
+  std::vector<size_t> made(T, 0);
+  run_threads(T, [&](int t) {
+    long long g = first[t];
+    if (g >= nz) return;
+    const long long mine = std::min(count[t], nz - g);
+    size_t w = static_cast<size_t>(g) * per;
+    const size_t w0 = w;
+    const char *p = base + cut[t], *end = base + cut[t + 1];
+    for (long long k = 0; k < mine; ++k, ++g) {
+      const char *nl = static_cast<const char *>(std::memchr(p, '\n', end - p));
+      const char *le = nl ? nl : end;
+      long long i = 0, j = 0;
+      double v = 1.0;
+      const char *q = scan_ll(p, le, &i);
+      if (q) q = scan_ll(q, le, &j);
+      if (q && !pattern) q = scan_double(q, le, &v);
+      if (!q) {
+        tbad[t] = g;
+        return;
+      }
+      ci[w] = static_cast<int32_t>(i - 1);
+      cj[w] = static_cast<int32_t>(j - 1);
+      cv[w++] = v;
+      if (symmetric && i != j) {
+        ci[w] = static_cast<int32_t>(j - 1);
+        cj[w] = static_cast<int32_t>(i - 1);
+        cv[w++] = v;
+      }
+      p = nl ? nl + 1 : end;
+    }
+    made[t] = w - w0;
+  });
+  *bad = -1;
+  for (int t = 0; t < T; ++t)
+    if (tbad[t] >= 0) {
+      *bad = tbad[t];  // chunks are in file order: the first one found is the first
+      return;
+    }
+  if (per == 1) return;  // one entry per record: already in place
+  size_t at = 0;
+  for (int t = 0; t < T && first[t] < nz; ++t) {
+    const size_t from = static_cast<size_t>(first[t]) * per;
+    if (at != from) {
+      std::memmove(ci.data() + at, ci.data() + from, made[t] * sizeof(int32_t));
+      std::memmove(cj.data() + at, cj.data() + from, made[t] * sizeof(int32_t));
+      std::memmove(cv.data() + at, cv.data() + from, made[t] * sizeof(double));
+    }
+    at += made[t];
+  }
+  ci.resize(at);
+  cj.resize(at);
+  cv.resize(at);
 }
 
 // Matrix Market coordinate reader (readMTXDouble, matrixIO.cu:33-192):
@@ -165,37 +353,31 @@ static bcmg_status read_mm(const char *path, bcmg_csr *out) {
     fclose(fp);
     return set_error(BCMG_ERR_IO, "'%s': bad size line", path);
   }
+  // The records: the rest of the file in one read, one record per line.
+  std::string body;
+  {
+    const long here = ftell(fp);
+    if (here >= 0 && fseek(fp, 0, SEEK_END) == 0) {
+      const long end = ftell(fp);
+      if (end > here) body.reserve(static_cast<size_t>(end - here));
+      fseek(fp, here, SEEK_SET);
+    }
+    char chunk[1 << 16];
+    size_t got_bytes;
+    while ((got_bytes = fread(chunk, 1, sizeof(chunk), fp)) > 0) body.append(chunk, got_bytes);
+    const bool failed = ferror(fp) != 0;
+    fclose(fp);
+    if (failed) return set_error(BCMG_ERR_IO, "'%s': read error", path);
+  }
   std::vector<int32_t> ci, cj;
   std::vector<double> cv;
-  size_t reserve = static_cast<size_t>(symmetric ? 2 * nz : nz);
-  ci.reserve(reserve);
-  cj.reserve(reserve);
-  cv.reserve(reserve);
-  for (long long k = 0; k < nz; ++k) {
-    if (!fgets(line, sizeof(line), fp)) {
-      fclose(fp);
-      return set_error(BCMG_ERR_IO, "'%s': error reading record %lld of %lld", path,
-                       k, nz);
-    }
-    long long i = 0, j = 0;
-    double v = 1.0;
-    int need = pattern ? 2 : 3;
-    int r = pattern ? sscanf(line, "%lld %lld", &i, &j)
-                    : sscanf(line, "%lld %lld %lf", &i, &j, &v);
-    if (r != need) {
-      fclose(fp);
-      return set_error(BCMG_ERR_IO, "'%s': malformed record %lld", path, k);
-    }
-    ci.push_back(static_cast<int32_t>(i - 1));
-    cj.push_back(static_cast<int32_t>(j - 1));
-    cv.push_back(v);
-    if (symmetric && i != j) {
-      ci.push_back(static_cast<int32_t>(j - 1));
-      cj.push_back(static_cast<int32_t>(i - 1));
-      cv.push_back(v);
-    }
-  }
-  fclose(fp);
+  long long bad = -1, lines = 0;
+  parse_records(body, nz, pattern, symmetric, ci, cj, cv, &bad, &lines);
+  std::string().swap(body);
+  if (bad >= 0) return set_error(BCMG_ERR_IO, "'%s': malformed record %lld", path, bad);
+  if (lines < nz)
+    return set_error(BCMG_ERR_IO, "'%s': error reading record %lld of %lld", path, lines,
+                     nz);
   return coo_to_csr(static_cast<int32_t>(nr), static_cast<int32_t>(nc), ci, cj, cv,
                     out);
 }
@@ -309,10 +491,28 @@ bcmg_status bcmg_write_matrix_mm(const char *path, const bcmg_csr *A) {
   if (!fp) return set_error(BCMG_ERR_IO, "cannot write '%s'", path);
   fprintf(fp, "%%%%MatrixMarket matrix coordinate real general\n");
   fprintf(fp, "%d  %d %d \n", A->n, A->m, A->nnz);
-  for (int32_t i = 0; i < A->n; ++i)
-    for (int32_t j = A->row[i]; j < A->row[i + 1]; ++j)
-      fprintf(fp, "%d   %d  %.18e\n", i + 1, A->col[j] + 1, A->val[j]);
-  fclose(fp);
+  // Rows formatted in parallel (ranges of rows, each into its own text),
+  // written in order: the same bytes as one fprintf per entry.
+  const int T = io_threads(static_cast<size_t>(std::max(A->nnz, 0)) * 48);
+  std::vector<std::string> text(T);
+  run_threads(T, [&](int t) {
+    const int32_t i0 = static_cast<int32_t>(static_cast<int64_t>(A->n) * t / T);
+    const int32_t i1 = static_cast<int32_t>(static_cast<int64_t>(A->n) * (t + 1) / T);
+    std::string &s = text[t];
+    s.reserve(static_cast<size_t>(A->row[i1] - A->row[i0]) * 48);
+    char rec[96];
+    for (int32_t i = i0; i < i1; ++i)
+      for (int32_t j = A->row[i]; j < A->row[i + 1]; ++j) {
+        const int len =
+            snprintf(rec, sizeof(rec), "%d   %d  %.18e\n", i + 1, A->col[j] + 1, A->val[j]);
+        s.append(rec, static_cast<size_t>(std::min<int>(len, sizeof(rec) - 1)));
+      }
+  });
+  bool ok = true;
+  for (const std::string &s : text)
+    ok = ok && fwrite(s.data(), 1, s.size(), fp) == s.size();
+  ok = (fclose(fp) == 0) && ok;
+  if (!ok) return set_error(BCMG_ERR_IO, "error writing '%s'", path);
   return BCMG_OK;
 }
 
