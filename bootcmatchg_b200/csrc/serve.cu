@@ -84,21 +84,67 @@ size_t estimate_batch(int32_t n, int m) {
   return static_cast<size_t>(n) * W * (8 * 8 + 4 * 8);
 }
 
-uint64_t hash_csr(const bcmg_csr &A) {
-  uint64_t h = 1469598103934665603ull;
-  auto mix = [&h](const void *p, size_t bytes) {
+// The matrix key of a key-0 submission: a 64-bit hash of n, nnz and the three
+// arrays, computed in the submitting thread.  Words of 8 bytes go four at a
+// time into four independent lanes (the round of xxHash64: add the word
+// times an odd constant, rotate, multiply), the tail bytes of each array
+// into one last word; the lanes and the byte count are folded with the
+// splitmix64 finalizer.  The lanes' multiplies do not wait on each other,
+// so this runs at memory speed, where a byte-at-a-time hash would take most
+// of a second for a 700 MB matrix.
+uint64_t rotl64(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+
+uint64_t fold64(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+
+struct KeyHash {
+  static constexpr uint64_t kMul = 0x9e3779b185ebca87ull, kRound = 0xc2b2ae3d27d4eb4full;
+  uint64_t lane[4] = {0x243f6a8885a308d3ull, 0x13198a2e03707344ull, 0xa4093822299f31d0ull,
+                      0x082efa98ec4e6c89ull};
+  uint64_t bytes = 0;
+  void round(int l, uint64_t w) { lane[l] = rotl64(lane[l] + w * kMul, 31) * kRound; }
+  void add(const void *p, size_t n) {
     const unsigned char *c = static_cast<const unsigned char *>(p);
-    for (size_t i = 0; i < bytes; ++i) {
-      h ^= c[i];
-      h *= 1099511628211ull;
+    size_t i = 0;
+    uint64_t w[4];
+    for (; i + 32 <= n; i += 32) {
+      std::memcpy(w, c + i, 32);
+      round(0, w[0]);
+      round(1, w[1]);
+      round(2, w[2]);
+      round(3, w[3]);
     }
-  };
-  mix(&A.n, sizeof(A.n));
-  mix(&A.nnz, sizeof(A.nnz));
-  mix(A.row, sizeof(int32_t) * (static_cast<size_t>(A.n) + 1));
-  mix(A.col, sizeof(int32_t) * static_cast<size_t>(A.nnz));
-  mix(A.val, sizeof(double) * static_cast<size_t>(A.nnz));
-  return h == 0 ? 1 : h;
+    for (; i + 8 <= n; i += 8) {
+      std::memcpy(w, c + i, 8);
+      round(0, w[0]);
+    }
+    if (i < n) {
+      w[0] = 0;
+      std::memcpy(w, c + i, n - i);
+      round(1, w[0]);
+    }
+    bytes += n;
+  }
+  uint64_t finish() const {
+    uint64_t h = fold64(bytes);
+    for (uint64_t l : lane) h = fold64(h ^ l);
+    return h == 0 ? 1 : h;
+  }
+};
+
+uint64_t hash_csr(const bcmg_csr &A) {
+  KeyHash k;
+  k.add(&A.n, sizeof(A.n));
+  k.add(&A.nnz, sizeof(A.nnz));
+  k.add(A.row, sizeof(int32_t) * (static_cast<size_t>(A.n) + 1));
+  k.add(A.col, sizeof(int32_t) * static_cast<size_t>(A.nnz));
+  k.add(A.val, sizeof(double) * static_cast<size_t>(A.nnz));
+  return k.finish();
 }
 
 }  // namespace
