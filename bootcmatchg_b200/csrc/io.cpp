@@ -387,36 +387,53 @@ static bcmg_status read_mm(const char *path, bcmg_csr *out) {
 static bcmg_status read_coo_list(const char *path, bcmg_csr *out) {
   FILE *fp = fopen(path, "r");
   if (!fp) return set_error(BCMG_ERR_IO, "cannot open matrix file '%s'", path);
-  long long n = 0, nz = 0;
-  if (fscanf(fp, "%lld %lld", &n, &nz) != 2 || n <= 0 || nz < 0 || n > INT32_MAX) {
+  std::string text;
+  {
+    if (fseek(fp, 0, SEEK_END) == 0) {
+      const long end = ftell(fp);
+      if (end > 0) text.reserve(static_cast<size_t>(end));
+      fseek(fp, 0, SEEK_SET);
+    }
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = fread(chunk, 1, sizeof(chunk), fp)) > 0) text.append(chunk, got);
+    const bool failed = ferror(fp) != 0;
     fclose(fp);
+    if (failed) return set_error(BCMG_ERR_IO, "'%s': read error", path);
+  }
+  // Numbers read one after the other, each from where the previous one
+  // stopped, as fscanf("%lld") / fscanf("%lf") on the stream read them.
+  const char *p = text.c_str(), *e = p + text.size();
+  long long n = 0, nz = 0;
+  p = scan_ll(p, e, &n);
+  if (p) p = scan_ll(p, e, &nz);
+  if (!p || n <= 0 || nz < 0 || n > INT32_MAX)
     return set_error(BCMG_ERR_IO, "'%s': bad COO header", path);
-  }
-  std::vector<int32_t> ci(nz), cj(nz);
-  std::vector<double> cv(nz);
+  // A number takes at least two bytes, so no list is longer than this.
+  const size_t cap = std::min(static_cast<size_t>(nz), text.size() / 2 + 1);
+  std::vector<int32_t> ci, cj;
+  std::vector<double> cv;
+  ci.reserve(cap);
+  cj.reserve(cap);
+  cv.reserve(cap);
   for (long long k = 0; k < nz; ++k) {
-    long long t;
-    if (fscanf(fp, "%lld", &t) != 1) {
-      fclose(fp);
-      return set_error(BCMG_ERR_IO, "'%s': short row list", path);
-    }
-    ci[k] = static_cast<int32_t>(t - 1);
+    long long t = 0;
+    if (!(p = scan_ll(p, e, &t))) return set_error(BCMG_ERR_IO, "'%s': short row list", path);
+    ci.push_back(static_cast<int32_t>(t - 1));
   }
   for (long long k = 0; k < nz; ++k) {
-    long long t;
-    if (fscanf(fp, "%lld", &t) != 1) {
-      fclose(fp);
+    long long t = 0;
+    if (!(p = scan_ll(p, e, &t)))
       return set_error(BCMG_ERR_IO, "'%s': short column list", path);
-    }
-    cj[k] = static_cast<int32_t>(t - 1);
+    cj.push_back(static_cast<int32_t>(t - 1));
   }
   for (long long k = 0; k < nz; ++k) {
-    if (fscanf(fp, "%lf", &cv[k]) != 1) {
-      fclose(fp);
+    double v = 0.0;
+    if (!(p = scan_double(p, e, &v)))
       return set_error(BCMG_ERR_IO, "'%s': short value list", path);
-    }
+    cv.push_back(v);
   }
-  fclose(fp);
+  std::string().swap(text);
   return coo_to_csr(static_cast<int32_t>(n), static_cast<int32_t>(n), ci, cj, cv,
                     out);
 }

@@ -144,3 +144,32 @@ def test_written_file_reads_back_exactly(tmp_path):
     B = bc.read_matrix_from_file(str(p))
     assert np.array_equal(B.row, row) and np.array_equal(B.col, col)
     assert np.array_equal(B.val, val)
+
+
+# The plain COO list (readMTX2Double, matrixIO.cu:194-289): "n nnz", then nnz
+# row indices, nnz column indices and nnz values, 1-based, separated by any
+# white space; each number is read from where the previous one stopped.
+def test_coo_list_syntax_and_errors(tmp_path):
+    def coo(text):
+        p = tmp_path / "a.coo"
+        p.write_text(text)
+        return bc.read_matrix_from_file(str(p), m_type=1)
+
+    A = coo("3 4\n1\t2 3 3\r\n1 1 3 1\n+2.5 -1e-1 0x1p2 7 trailing text\n")
+    check(A, 3, [(1, 1, 2.5), (2, 1, -0.1), (3, 3, 4.0), (3, 1, 7.0)])
+    for text, what in [("2 3\n1 2\n", "short row list"), ("2 2\n1 2\n1\n", "short column list"),
+                       ("2 2\n1 2\n1 2\n3.0 x\n", "short value list"),
+                       ("2 1000000000000\n1 2\n", "short row list"), ("0 1\n", "bad COO header"),
+                       ("2\n", "bad COO header")]:
+        with pytest.raises(bc.BcmgError, match=what):
+            coo(text)
+
+
+def test_coo_list_large(tmp_path):
+    n, count = 5000, 200_000
+    recs = random_records(n, count, 21)
+    text = f"{n} {count}\n" + " ".join(str(i) for i, _, _ in recs) + "\n" + \
+        " ".join(str(j) for _, j, _ in recs) + "\n" + " ".join(repr(v) for _, _, v in recs) + "\n"
+    p = tmp_path / "b.coo"
+    p.write_text(text)
+    check(bc.read_matrix_from_file(str(p), m_type=1), n, recs)
